@@ -1,0 +1,314 @@
+"""FDV step throughput on B200: mixed precision vs FP64 at equal residual.
+
+Workload (default): the 2D supersonic flat plate, 200x100 quad4 (20,000 elements,
+81,204 DOF), Mach 3, Re 1e4, each step = CFL + element formation (+ApplyBC) +
+restarted GMRES(30) to a 1e-8 true relative residual + update.  One "step" of the
+metric is one such FDV step.  Both forms run: FP64 and mixed (FP32 element matrices
+and products inside FP64 iterative refinement); ``value`` is the mixed form's
+steps/s, the FP64 figure is reported beside it.
+
+Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events on the
+solver's stream; between timed steps L2 is flushed by writing a 512 MiB buffer
+(the plate's matrices fit in L2).  Under torchrun every rank runs its own replica
+(the path is not partitioned: "replicas only"), the time is the max over ranks.
+
+``--impl reference`` times the reference's own CPU path (oracle/_ref/cfdv_ref, the
+CFDV sources built unmodified) on the same case on the host, one core.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FDV steps/s & EBE matvec GB/s: mixed vs FP64 on 1 B200 at equal residual"
+WORKLOADS = {
+    "plate": dict(desc="2D supersonic flat plate 200x100 quad4, M=3, Re=1e4, GMRES(30) to 1e-8",
+                  make=lambda mg: mg.plate(200, 100), m=30, cfl=1.0),
+    "lid": dict(desc="2D lid-driven cavity 32x32 quad4, M=0.1, Re=100, GMRES(20) to 1e-8",
+                make=lambda mg: mg.lid(32), m=20, cfl=0.5),
+    "ramp": dict(desc="3D compression ramp 128x64x32 hex8, M=2.5, Re=1e5, GMRES(50) to 1e-8",
+                 make=lambda mg: mg.ramp(128, 64, 32), m=50, cfl=0.25),
+}
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_cpu(case, steps, warmup):
+    """Time the reference build on the host: (seconds per step list, sample description)."""
+    from oracle import oracle as O
+    from cfdv_b200 import meshgen as mg
+    with tempfile.TemporaryDirectory() as d:
+        mg.write_case(case, d)
+        rec = O.run_reference(d, os.path.join(d, "ref.rec"), steps=warmup + steps)
+    times = [float(rec[f"steptime@{k}"][0]) for k in range(warmup, warmup + steps)]
+    return times
+
+
+def bench_gpu(args, ws, rank, local):
+    import numpy as np
+    import torch
+    from cfdv_b200 import gpu as G, meshgen as mg
+
+    torch.cuda.set_device(local)
+    W = WORKLOADS[args.workload]
+    case = W["make"](mg)
+    m, cfl, rtol = W["m"], W["cfl"], 1e-8
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if ws == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    solver = G.FDVSolver(case)
+    ext = torch.cuda.ExternalStream(solver.stream)
+    sampler = ClockSampler(local)
+    for prec_name, prec in (("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)):
+        solver.load_node_records()
+        for _ in range(args.warmup):
+            solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=prec)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        if prec_name == "mixed":
+            sampler.start()
+        solver.profile(True)
+        step_ms, res, mvs = [], [], []
+        for _ in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.fill_(1.0)  # evict the previous step's matrices from L2
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+            rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=prec)
+            with torch.cuda.stream(ext):
+                e1.record(ext)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            res.append(rep["true_rel_res"])
+            mvs.append(rep["matvecs"])
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        stats = solver.profile_read()
+        solver.profile(False)
+        if prec_name == "mixed":
+            clocks = sampler.stop()
+        total_s = max_over_ranks(sum(step_ms) / 1e3)
+        results[prec_name] = dict(steps_per_s=ws * args.steps / total_s, ms_per_step=1e3 * total_s / args.steps,
+                                  true_rel_res_max=max(res), matvecs_per_step=sum(mvs) / len(mvs), stats=stats,
+                                  state=solver.get_state())
+
+    # end-to-end through the C ABI with host buffers: H2D state, step, D2H state every step
+    n = solver.n_dof
+    host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    out = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    solver.load_node_records()
+    host.numpy()[:] = solver.get_state()
+    for _ in range(2):
+        solver.set_state(host.numpy())
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=G.PREC_MIXED)
+        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(out.numpy()), None, n))
+        host.copy_(out)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+        solver.set_state(host.numpy())
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=G.PREC_MIXED)
+        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(out.numpy()), None, n))
+        with torch.cuda.stream(ext):
+            e1.record(ext)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+        host.copy_(out)
+    e2e_s = max_over_ranks(sum(e2e_ms) / 1e3)
+
+    mixed, fp64 = results["mixed"], results["fp64"]
+    err = float(np.abs(mixed["state"] - fp64["state"]).max() / np.abs(fp64["state"]).max())
+    st = mixed["stats"]
+    achieved = st["bytes"] / (st["total_ms"] / 1e3) / 1e9 if st["total_ms"] > 0 else None
+    peak, peak_kind = peaks()
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"ebe_traffic_{args.workload}.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch_fp32")
+    line = {
+        "metric": METRIC,
+        "value": mixed["steps_per_s"],
+        "unit": "FDV steps/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": mixed["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 matrices/f64 vectors (mixed); f64",
+        "data": "synthetic",
+        "config": {"workload": W["desc"], "elements": case.n_elements, "dof": solver.n_dof,
+                   "gmres": f"restarted GMRES({m}), MGS, to true relative residual {rtol:g}",
+                   "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": fp64["steps_per_s"], "ms_per_step": fp64["ms_per_step"],
+                 "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"]},
+        "mixed": {"true_rel_res_max": mixed["true_rel_res_max"], "matvecs_per_step": mixed["matvecs_per_step"],
+                  "max_field_diff_vs_fp64": err},
+        "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
+        "roofline": {"kernel": "ebe element pass (FP32 matrices)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                     "peak_kind": peak_kind,
+                     "traffic": traffic, "bytes_per_launch": st["bytes"] / max(st["launches"], 1),
+                     "launches": st["launches"], "avg_launch_us": 1e3 * st["total_ms"] / max(st["launches"], 1)},
+        "e2e": {"value": ws * args.steps / e2e_s, "unit": "FDV steps/s", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": int(st["kernel_launches"]),
+        "clocks": clocks,
+    }
+    solver.close()
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            k = 2
+            times = run_reference_cpu(case, k, 0)
+            line["cpu_baseline"] = {"value": k / sum(times), "unit": "FDV steps/s", "cores": 1, "kind": "reference",
+                                    "sample": f"{k} steps of the same case through oracle/_ref/cfdv_ref (reference "
+                                              f"sources, reference GMRES({m}) x1 restart, not equal residual)"}
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def bench_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from cfdv_b200 import meshgen as mg
+    W = WORKLOADS[args.workload]
+    case = W["make"](mg)
+    times = run_reference_cpu(case, args.steps, args.warmup)
+    v = args.steps / sum(times)
+    line = {
+        "metric": METRIC, "impl": "reference", "value": v, "unit": "FDV steps/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": W["desc"], "elements": case.n_elements, "dof": case.n_nodes * case.neqn,
+                   "gmres": f"reference MPI_GMRES({W['m']}), 1 restart (its own stopping rule)"},
+        "cpu_baseline": {"value": v, "unit": "FDV steps/s", "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps of the full case"},
+        "e2e": {"value": v, "unit": "FDV steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cfdv_b200", choices=["cfdv_b200", "reference"])
+    ap.add_argument("--workload", default="plate", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_info()
+    if args.impl == "reference":
+        bench_reference(args, ws, rank)
+    else:
+        bench_gpu(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,528 @@
+// Device-side FDV physics for one Gauss point: gas model, shape functions,
+// Gauss-point flow state, viscous stress, flux Jacobians and fluxes.
+//
+// Formulas follow the CFDV reference (paths relative to its src/):
+//   gas model            FDV/Thermo.h:148-211
+//   shape functions      FiniteElement/TestFunctions2D.h:173-256, TestFunctions3D.h:7-123
+//   Gauss-point state    FDV/FDVGalerkin.h:761-797, FDV/tau.h:105-133
+//   a = dF/dU            FDV/NavierStokes2D.h:59-97,  FDV/NavierStokes3D.h:74-189
+//   b = dG/dU            FDV/NavierStokes2D.h:100-158, FDV/NavierStokes3D.h:193-343
+//   c = dG/dU_,j         FDV/NavierStokes2D.h:163-222, FDV/NavierStokes3D.h:347-477
+//   F, G                 FDV/NavierStokes2D.h:11-47,  FDV/NavierStokes3D.h:10-64
+// Jacobian tensors are written to shared memory with a fixed 5-equation stride:
+//   a(i,r,s) -> a[(i*5+r)*5+s],  c(i,j,r,s) -> c[((i*3+j)*5+r)*5+s].
+#pragma once
+#include "cfdv_types.h"
+
+namespace cfdv {
+
+#define JA(t, i, r, s) (t)[((i)*5 + (r)) * 5 + (s)]
+#define JC(t, i, j, r, s) (t)[(((i)*3 + (j)) * 5 + (r)) * 5 + (s)]
+
+CFDV_HD CFDV_INLINE double gas_mu(const GasParams& g, double T) {
+  if (T < 1.0E-12) return 1.0;
+  return ((1 + g.csuth) / (T + g.csuth)) * T * sqrt(T);
+}
+CFDV_HD CFDV_INLINE double gas_k(const GasParams& g, double mu) {
+  return mu / ((g.gamma - 1.0) * (g.cmach * g.cmach) * g.Pr);
+}
+
+// primitive state of a node (NodeUnpack.h:185-205)
+struct NodePrim {
+  double U[5], x[3], v[3];
+  double rho, E, T, p;
+};
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void node_unpack(const GasParams& g, const double* U, const double* x, NodePrim& n) {
+#pragma unroll
+  for (int k = 0; k < NDIM + 2; k++) n.U[k] = U[k];
+#pragma unroll
+  for (int k = 0; k < NDIM; k++) n.x[k] = x[k];
+  n.rho = U[0];
+  double vsqr = 0;
+#pragma unroll
+  for (int i = 0; i < NDIM; i++) {
+    n.v[i] = U[1 + i] / U[0];
+    vsqr += n.v[i] * n.v[i];
+  }
+  n.E = U[NDIM + 1] / U[0];
+  double e = n.E - 0.5 * vsqr;
+  n.T = e / g.Cv;
+  n.p = n.rho * (g.gamma - 1.0) * e;
+}
+
+// shape functions and natural-coordinate derivatives
+template <int NDIM>
+CFDV_HD CFDV_INLINE void shape_fn(const double* z, double* Phi, double (*dPxi)[3]);
+
+template <>
+CFDV_HD CFDV_INLINE void shape_fn<2>(const double* z, double* Phi, double (*dPxi)[3]) {
+  const double a0 = 1 - z[0], b0 = 1 + z[0], a1 = 1 - z[1], b1 = 1 + z[1];
+  Phi[0] = 0.25 * a0 * a1;
+  Phi[1] = 0.25 * b0 * a1;
+  Phi[2] = 0.25 * b0 * b1;
+  Phi[3] = 0.25 * a0 * b1;
+  dPxi[0][0] = -0.25 * a1; dPxi[1][0] = 0.25 * a1; dPxi[2][0] = 0.25 * b1; dPxi[3][0] = -0.25 * b1;
+  dPxi[0][1] = -0.25 * a0; dPxi[1][1] = -0.25 * b0; dPxi[2][1] = 0.25 * b0; dPxi[3][1] = 0.25 * a0;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void shape_fn<3>(const double* z, double* Phi, double (*dPxi)[3]) {
+  const double m[3] = {1 - z[0], 1 - z[1], 1 - z[2]};
+  const double p[3] = {1 + z[0], 1 + z[1], 1 + z[2]};
+  // hex8 corner signs: node N sits at (sx, sy, sz)
+#pragma unroll
+  for (int N = 0; N < 8; N++) {
+    const int sx = ((N & 1) ^ ((N >> 1) & 1)) ? 1 : -1;  // 0:-,1:+,2:+,3:-
+    const int sy = ((N >> 1) & 1) ? 1 : -1;              // 0,1:- 2,3:+
+    const int sz = (N >> 2) ? 1 : -1;
+    const double fx = sx > 0 ? p[0] : m[0], fy = sy > 0 ? p[1] : m[1], fz = sz > 0 ? p[2] : m[2];
+    Phi[N] = 0.125 * fx * fy * fz;
+    dPxi[N][0] = (sx * 0.125) * fy * fz;
+    dPxi[N][1] = (sy * 0.125) * fx * fz;
+    dPxi[N][2] = (sz * 0.125) * fx * fy;
+  }
+}
+
+// isoparametric Jacobian, physical derivatives dPhi, returns det J; jac[i][j] = dx_i/dxi_j
+template <int NDIM>
+CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
+                                             double (*jac)[3]);
+
+template <>
+CFDV_HD CFDV_INLINE double phys_deriv<2>(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
+                                                double (*jac)[3]) {
+  double j00 = 0, j01 = 0, j10 = 0, j11 = 0;
+#pragma unroll
+  for (int N = 0; N < 4; N++) {
+    j00 += dPxi[N][0] * nd[N].x[0];
+    j01 += dPxi[N][1] * nd[N].x[0];
+    j10 += dPxi[N][0] * nd[N].x[1];
+    j11 += dPxi[N][1] * nd[N].x[1];
+  }
+  jac[0][0] = j00; jac[0][1] = j01; jac[1][0] = j10; jac[1][1] = j11;
+  const double J = j00 * j11 - j10 * j01;
+  const double iJ = 1.0 / J;
+#pragma unroll
+  for (int N = 0; N < 4; N++) {
+    dPhi[N][0] = iJ * (dPxi[N][0] * j11 - j10 * dPxi[N][1]);
+    dPhi[N][1] = iJ * (j00 * dPxi[N][1] - dPxi[N][0] * j01);
+  }
+  return J;
+}
+
+template <>
+CFDV_HD CFDV_INLINE double phys_deriv<3>(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
+                                                double (*jac)[3]) {
+  double j[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+#pragma unroll
+  for (int N = 0; N < 8; N++)
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) j[i][k] += dPxi[N][k] * nd[N].x[i];
+  const double J = j[0][0] * j[1][1] * j[2][2] + j[0][1] * j[1][2] * j[2][0] + j[0][2] * j[1][0] * j[2][1] -
+                   j[0][2] * j[1][1] * j[2][0] - j[0][1] * j[1][0] * j[2][2] - j[0][0] * j[1][2] * j[2][1];
+  double inv[3][3];
+  inv[0][0] = j[1][1] * j[2][2] - j[1][2] * j[2][1];
+  inv[0][1] = -(j[1][0] * j[2][2] - j[1][2] * j[2][0]);
+  inv[0][2] = j[1][0] * j[2][1] - j[1][1] * j[2][0];
+  inv[1][0] = -(j[0][1] * j[2][2] - j[0][2] * j[2][1]);
+  inv[1][1] = j[0][0] * j[2][2] - j[0][2] * j[2][0];
+  inv[1][2] = -(j[0][0] * j[2][1] - j[0][1] * j[2][0]);
+  inv[2][0] = j[0][1] * j[1][2] - j[0][2] * j[1][1];
+  inv[2][1] = -(j[0][0] * j[1][2] - j[0][2] * j[1][0]);
+  inv[2][2] = j[0][0] * j[1][1] - j[0][1] * j[1][0];
+  const double iJ = 1.0 / J;
+#pragma unroll
+  for (int N = 0; N < 8; N++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) dPhi[N][i] = iJ * (inv[i][0] * dPxi[N][0]) + iJ * (inv[i][1] * dPxi[N][1]) +
+                                             iJ * (inv[i][2] * dPxi[N][2]);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) jac[i][k] = j[i][k];
+  return J;
+}
+
+// Gauss-point flow state
+struct GpState {
+  double E, T, U[5], dU[5][3], v[3], dV[3][3], dT[3], mu, k, tau[3][3];
+};
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void gp_state(const GasParams& g, int nn, const NodePrim* const* nd, const double* Phi,
+                                         const double (*dPhi)[3], GpState& f) {
+  constexpr int NEQ = NDIM + 2;
+  f.E = 0; f.T = 0;
+#pragma unroll
+  for (int i = 0; i < NEQ; i++) {
+    f.U[i] = 0;
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) f.dU[i][j] = 0;
+  }
+#pragma unroll
+  for (int i = 0; i < NDIM; i++) {
+    f.v[i] = 0; f.dT[i] = 0;
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) { f.dV[i][j] = 0; f.tau[i][j] = 0; }
+  }
+  for (int N = 0; N < nn; N++) {
+    const NodePrim& n = *nd[N];
+    f.E += Phi[N] * n.E;
+    f.T += Phi[N] * n.T;
+#pragma unroll
+    for (int i = 0; i < NEQ; i++) {
+      f.U[i] += Phi[N] * n.U[i];
+#pragma unroll
+      for (int j = 0; j < NDIM; j++) f.dU[i][j] += dPhi[N][j] * n.U[i];
+    }
+#pragma unroll
+    for (int i = 0; i < NDIM; i++) {
+      f.v[i] += Phi[N] * n.v[i];
+      f.dT[i] += dPhi[N][i] * n.T;
+#pragma unroll
+      for (int d = 0; d < NDIM; d++) f.dV[i][d] += dPhi[N][d] * n.v[i];
+    }
+  }
+  f.mu = gas_mu(g, f.T);
+  f.k = gas_k(g, f.mu);
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void viscous_stress(GpState& f) {
+  double vkk = 0;
+#pragma unroll
+  for (int k = 0; k < NDIM; k++) vkk += f.dV[k][k];
+#pragma unroll
+  for (int i = 0; i < NDIM; i++)
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) {
+      double t = f.mu * (f.dV[i][j] + f.dV[j][i]);
+      if (i == j) t -= (2.0 / 3.0) * f.mu * vkk;
+      f.tau[i][j] = t;
+    }
+}
+
+// ---- flux Jacobians ---------------------------------------------------------
+template <int NDIM>
+CFDV_HD void jac_a(const GasParams& th, const GpState& f, double* m);
+template <int NDIM>
+CFDV_HD void jac_b(const GasParams& th, const GpState& f, double* m);
+template <int NDIM>
+CFDV_HD void jac_c(const GasParams& th, const GpState& f, double* m);
+
+template <>
+CFDV_HD CFDV_INLINE void jac_a<2>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 2 * 25; i++) m[i] = 0.0;
+  const double u = f.v[0], v = f.v[1], uu = u * u, uv = u * v, vv = v * v, E = f.E;
+  JA(m, 0, 0, 1) = 1.0;
+  JA(m, 0, 1, 0) = th.gm3d2 * uu + th.gm1d2 * vv;
+  JA(m, 0, 1, 1) = -th.gamm3 * u;
+  JA(m, 0, 1, 2) = -th.gamm1 * v;
+  JA(m, 0, 1, 3) = th.gamm1;
+  JA(m, 0, 2, 0) = -uv;
+  JA(m, 0, 2, 1) = v;
+  JA(m, 0, 2, 2) = u;
+  JA(m, 0, 3, 0) = -th.gamma * E * u + th.gamm1 * u * (uu + vv);
+  JA(m, 0, 3, 1) = th.gamma * E - th.gm1d2 * (3. * uu + vv);
+  JA(m, 0, 3, 2) = -th.gamm1 * uv;
+  JA(m, 0, 3, 3) = th.gamma * u;
+  JA(m, 1, 0, 2) = 1.0;
+  JA(m, 1, 1, 0) = -uv;
+  JA(m, 1, 1, 1) = v;
+  JA(m, 1, 1, 2) = u;
+  JA(m, 1, 2, 0) = th.gm1d2 * uu + th.gm3d2 * vv;
+  JA(m, 1, 2, 1) = -th.gamm1 * u;
+  JA(m, 1, 2, 2) = -th.gamm3 * v;
+  JA(m, 1, 2, 3) = th.gamm1;
+  JA(m, 1, 3, 0) = -th.gamma * E * v + th.gamm1 * v * (uu + vv);
+  JA(m, 1, 3, 1) = -th.gamm1 * uv;
+  JA(m, 1, 3, 2) = th.gamma * E - th.gm1d2 * (uu + 3. * vv);
+  JA(m, 1, 3, 3) = th.gamma * v;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void jac_b<2>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 2 * 25; i++) m[i] = 0.0;
+  const double reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
+  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const double rho = f.U[0], DENOM = 1. / (rho * rho), TERM1 = f.k * DENOM / th.Cv;
+  const double u = f.v[0], v = f.v[1], uu = u * u, vv = v * v;
+  const double drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dedx = f.dU[3][0];
+  const double drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dedy = f.dU[3][1];
+  const double t00 = f.tau[0][0], t01 = f.tau[0][1], t10 = f.tau[1][0], t11 = f.tau[1][1];
+  const double b010 = (DENOM * (mu_R * dldx + lambda * dmdy - 2. * (mu_R * u * drdx + lambda * v * drdy))) * reinv;
+  const double b011 = mu_R * drdx * DENOM * reinv, b012 = lambda * drdy * DENOM * reinv;
+  const double b020 = (mu * DENOM * (dldy + dmdx - 2. * (u * drdy + v * drdx))) * reinv;
+  const double b021 = mu * drdy * DENOM * reinv, b022 = mu * drdx * DENOM * reinv;
+  JA(m, 0, 1, 0) = b010; JA(m, 0, 1, 1) = b011; JA(m, 0, 1, 2) = b012;
+  JA(m, 0, 2, 0) = b020; JA(m, 0, 2, 1) = b021; JA(m, 0, 2, 2) = b022;
+  JA(m, 0, 3, 0) = u * b010 + v * b020 +
+                   ((u * t00 + v * t10) / rho -
+                    TERM1 * (-dedx + (2. * E - 3. * uu - 3. * vv) * drdx + 2. * u * dldx + 2. * v * dmdx)) * reinv;
+  JA(m, 0, 3, 1) = u * b011 + v * b021 + (-t00 / rho - TERM1 * (2. * u * drdx - dldx)) * reinv;
+  JA(m, 0, 3, 2) = u * b012 + v * b022 + (-t10 / rho - TERM1 * (-dmdx + 2. * v * drdx)) * reinv;
+  JA(m, 0, 3, 3) = TERM1 * drdx * reinv;
+  const double b120 = (DENOM * (lambda * (dldx + 4. * v * drdy) + mu_R * (u * drdx + dmdy))) * reinv;
+  const double b121 = lambda * drdx * DENOM * reinv, b122 = mu_R * drdy * DENOM * reinv;
+  JA(m, 1, 1, 0) = b020; JA(m, 1, 1, 1) = b021; JA(m, 1, 1, 2) = b022;
+  JA(m, 1, 2, 0) = b120; JA(m, 1, 2, 1) = b121; JA(m, 1, 2, 2) = b122;
+  JA(m, 1, 3, 0) = u * b020 + v * b120 +
+                   ((u * t01 + v * t11) / rho -
+                    TERM1 * (-dedy + (2. * E - 3. * uu - 3. * vv) * drdy + 2. * u * dldy + 2. * v * dmdy)) * reinv;
+  JA(m, 1, 3, 1) = u * b021 + v * b121 + (-t10 / rho - TERM1 * (-dldy + 2. * u * drdy)) * reinv;
+  JA(m, 1, 3, 2) = u * b022 + v * b122 + (-t11 / rho - TERM1 * (2. * v * drdy - dmdy)) * reinv;
+  JA(m, 1, 3, 3) = TERM1 * drdy * reinv;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void jac_c<2>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 3 * 3 * 25; i++) m[i] = 0.0;
+  const double reinv = 1.0 / th.creyn, mu = f.mu;
+  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const double rho = f.U[0], denom = 1. / (rho * rho), denom2 = denom / rho;
+  const double l = f.U[1], mv = f.U[2], re = f.U[3];
+  const double ll = l * l, lm = l * mv, mm = mv * mv, rv = ll + mm, hkocv = f.k / th.Cv;
+  JC(m, 0, 0, 1, 0) = mu_R * l * denom * reinv;
+  JC(m, 0, 0, 1, 1) = -mu_R / rho * reinv;
+  JC(m, 0, 0, 2, 0) = mu * mv * denom * reinv;
+  JC(m, 0, 0, 2, 2) = -mu / rho * reinv;
+  JC(m, 0, 0, 3, 0) = ((mu_R * ll * denom2 + mu * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+  JC(m, 0, 0, 3, 1) = (-mu_R + hkocv) * l * denom * reinv;
+  JC(m, 0, 0, 3, 2) = (-mu + hkocv) * mv * denom * reinv;
+  JC(m, 0, 0, 3, 3) = -hkocv / rho * reinv;
+  JC(m, 0, 1, 1, 0) = lambda * mv * denom * reinv;
+  JC(m, 0, 1, 1, 2) = -lambda / rho * reinv;
+  JC(m, 0, 1, 2, 0) = mu * l * denom * reinv;
+  JC(m, 0, 1, 2, 1) = -mu / rho * reinv;
+  JC(m, 0, 1, 3, 0) = (lambda + mu) * lm * denom2 * reinv;
+  JC(m, 0, 1, 3, 1) = -mu * mv * denom * reinv;
+  JC(m, 0, 1, 3, 2) = -lambda * l * denom * reinv;
+  JC(m, 1, 0, 1, 0) = mu * mv * denom * reinv;
+  JC(m, 1, 0, 1, 2) = -mu / rho * reinv;
+  JC(m, 1, 0, 2, 0) = lambda * l * denom * reinv;
+  JC(m, 1, 0, 2, 1) = -lambda / rho * reinv;
+  JC(m, 1, 0, 3, 0) = (mu + lambda) * lm * denom2 * reinv;
+  JC(m, 1, 0, 3, 1) = -lambda * mv * denom * reinv;
+  JC(m, 1, 0, 3, 2) = -mu * l * denom * reinv;
+  JC(m, 1, 1, 1, 0) = mu * l * denom * reinv;
+  JC(m, 1, 1, 1, 1) = -mu / rho * reinv;
+  JC(m, 1, 1, 2, 0) = mu_R * mv * denom * reinv;
+  JC(m, 1, 1, 2, 2) = -mu_R / rho * reinv;
+  JC(m, 1, 1, 3, 0) = ((mu * ll * denom2 + mu_R * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+  JC(m, 1, 1, 3, 1) = (-mu + hkocv) * l * denom * reinv;
+  JC(m, 1, 1, 3, 2) = (-mu_R + hkocv) * mv * denom * reinv;
+  JC(m, 1, 1, 3, 3) = -hkocv / rho * reinv;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void jac_a<3>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 3 * 25; i++) m[i] = 0.0;
+  const double gamma = th.gamma, g1 = th.gamm1, g3 = th.gamm3, gm3d2 = th.gm3d2, gm1d2 = th.gm1d2;
+  const double u = f.v[0], v = f.v[1], w = f.v[2];
+  const double uu = u * u, uv = u * v, vv = v * v, ww = w * w, uw = u * w, vw = v * w, E = f.E;
+  const double q2 = uu + vv + ww;
+  JA(m, 0, 0, 1) = 1.0;
+  JA(m, 0, 1, 0) = gm3d2 * uu + gm1d2 * (vv + ww);
+  JA(m, 0, 1, 1) = -g3 * u; JA(m, 0, 1, 2) = -g1 * v; JA(m, 0, 1, 3) = -g1 * w; JA(m, 0, 1, 4) = g1;
+  JA(m, 0, 2, 0) = -uv; JA(m, 0, 2, 1) = v; JA(m, 0, 2, 2) = u;
+  JA(m, 0, 3, 0) = -uw; JA(m, 0, 3, 1) = w; JA(m, 0, 3, 3) = u;
+  JA(m, 0, 4, 0) = -gamma * E * u + g1 * u * q2;
+  JA(m, 0, 4, 1) = gamma * E - gm1d2 * (3. * uu + (vv + ww));
+  JA(m, 0, 4, 2) = -g1 * uv; JA(m, 0, 4, 3) = -g1 * uw; JA(m, 0, 4, 4) = gamma * u;
+  JA(m, 1, 0, 2) = 1.0;
+  JA(m, 1, 1, 0) = -uv; JA(m, 1, 1, 1) = v; JA(m, 1, 1, 2) = u;
+  JA(m, 1, 2, 0) = gm1d2 * (uu + ww) + gm3d2 * vv;
+  JA(m, 1, 2, 1) = -g1 * u; JA(m, 1, 2, 2) = -g3 * v; JA(m, 1, 2, 3) = -g1 * w; JA(m, 1, 2, 4) = g1;
+  JA(m, 1, 3, 0) = -vw; JA(m, 1, 3, 2) = w; JA(m, 1, 3, 3) = v;
+  JA(m, 1, 4, 0) = -gamma * E * v + g1 * v * q2;
+  JA(m, 1, 4, 1) = -g1 * uv;
+  JA(m, 1, 4, 2) = gamma * E - gm1d2 * ((uu + ww) + 3. * vv);
+  JA(m, 1, 4, 3) = -g1 * vw; JA(m, 1, 4, 4) = gamma * v;
+  JA(m, 2, 0, 3) = 1.0;
+  JA(m, 2, 1, 0) = -uw; JA(m, 2, 1, 1) = w; JA(m, 2, 1, 3) = u;
+  JA(m, 2, 2, 0) = -vw; JA(m, 2, 2, 2) = w; JA(m, 2, 2, 3) = v;
+  JA(m, 2, 3, 0) = gm1d2 * (uu + vv) + gm3d2 * ww;
+  JA(m, 2, 3, 1) = -g1 * u; JA(m, 2, 3, 2) = -g1 * v; JA(m, 2, 3, 3) = -g3 * w; JA(m, 2, 3, 4) = g1;
+  JA(m, 2, 4, 0) = -gamma * E * w + g1 * w * q2;
+  JA(m, 2, 4, 1) = -g1 * uw; JA(m, 2, 4, 2) = -g1 * vw;
+  JA(m, 2, 4, 3) = gamma * E - gm1d2 * ((uu + vv) + 3. * ww);
+  JA(m, 2, 4, 4) = gamma * w;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void jac_b<3>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 3 * 25; i++) m[i] = 0.0;
+  const double mu = f.mu, E = f.E;
+  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const double rho = f.U[0], denom = 1. / (rho * rho), TERM1 = f.k * denom / th.Cv;
+  const double u = f.v[0], v = f.v[1], w = f.v[2], uu = u * u, vv = v * v, ww = w * w, q2 = uu + vv + ww;
+  const double drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dndx = f.dU[3][0], dedx = f.dU[4][0];
+  const double drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dndy = f.dU[3][1], dedy = f.dU[4][1];
+  const double drdz = f.dU[0][2], dldz = f.dU[1][2], dmdz = f.dU[2][2], dndz = f.dU[3][2], dedz = f.dU[4][2];
+  const double l = f.U[1], mv = f.U[2], n = f.U[3];
+  const auto& t = f.tau;
+  // built unscaled, then multiplied by 1/Re (NavierStokes3D.h:331-342)
+  const double b010 = (denom * (mu_R * dldx + lambda * (dmdy + dndz) + mu_R * (-2. * u * drdx + v * drdy + w * drdz)));
+  const double b011 = mu_R * drdx * denom, b012 = lambda * drdy * denom, b013 = lambda * drdz * denom;
+  const double b020 = (mu * denom * (dldy + dmdx - 2. * (u * drdy + v * drdx)));
+  const double b021 = mu * drdy * denom, b022 = mu * drdx * denom;
+  const double b030 = (mu * denom * (dldz + dndx - 2. * (u * drdz + w * drdx)));
+  const double b031 = mu * drdz * denom, b033 = mu * drdx * denom;
+  JA(m, 0, 1, 0) = b010; JA(m, 0, 1, 1) = b011; JA(m, 0, 1, 2) = b012; JA(m, 0, 1, 3) = b013;
+  JA(m, 0, 2, 0) = b020; JA(m, 0, 2, 1) = b021; JA(m, 0, 2, 2) = b022;
+  JA(m, 0, 3, 0) = b030; JA(m, 0, 3, 1) = b031; JA(m, 0, 3, 3) = b033;
+  JA(m, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
+                   (denom * (l * t[0][0] + mv * t[0][1] + n * t[0][2]) -
+                    TERM1 * (-dedx + (2. * E - 3. * q2) * drdx + 2. * (u * dldx + v * dmdx + w * dndx)));
+  JA(m, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
+  JA(m, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
+  JA(m, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
+  JA(m, 0, 4, 4) = TERM1 * drdx;
+  const double b120 = (denom * (lambda * (dldx + dndz) + mu_R * (dmdy + u * drdx - 2. * v * drdy + w * drdz)));
+  const double b121 = lambda * drdx * denom, b122 = mu_R * drdy * denom, b123 = lambda * drdz * denom;
+  const double b130 = (mu * denom * (dmdz + dndy - 2. * (v * drdz + w * drdy)));
+  const double b132 = mu * denom * drdz, b133 = mu * denom * drdy;
+  JA(m, 1, 1, 0) = b020; JA(m, 1, 1, 1) = b021; JA(m, 1, 1, 2) = b022;
+  JA(m, 1, 2, 0) = b120; JA(m, 1, 2, 1) = b121; JA(m, 1, 2, 2) = b122; JA(m, 1, 2, 3) = b123;
+  JA(m, 1, 3, 0) = b130; JA(m, 1, 3, 2) = b132; JA(m, 1, 3, 3) = b133;
+  JA(m, 1, 4, 0) = u * b020 + v * b120 + w * b130 +
+                   (denom * (l * t[1][0] + mv * t[1][1] + n * t[1][2]) -
+                    TERM1 * (-dedy + (2. * E - 3. * q2) * drdy + 2. * (u * dldy + v * dmdy + w * dndy)));
+  JA(m, 1, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
+  JA(m, 1, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
+  JA(m, 1, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
+  JA(m, 1, 4, 4) = TERM1 * drdy;
+  const double b230 = (denom * (mu_R * (dndz + u * drdx + v * drdy - 2. * w * drdz) + lambda * (dldx + dmdy)));
+  const double b231 = lambda * drdx * denom, b232 = lambda * drdy * denom, b233 = mu_R * drdz * denom;
+  JA(m, 2, 1, 0) = b030; JA(m, 2, 1, 1) = b031; JA(m, 2, 1, 3) = b033;
+  JA(m, 2, 2, 0) = b130; JA(m, 2, 2, 2) = b132; JA(m, 2, 2, 3) = b133;
+  JA(m, 2, 3, 0) = b230; JA(m, 2, 3, 1) = b231; JA(m, 2, 3, 2) = b232; JA(m, 2, 3, 3) = b233;
+  JA(m, 2, 4, 0) = u * b030 + v * b130 + w * b230 +
+                   (denom * (l * t[2][0] + mv * t[2][1] + n * t[2][2]) -
+                    TERM1 * (-dedz + (2. * E - 3. * q2) * drdz + 2. * (u * dldz + v * dmdz + w * dndz)));
+  JA(m, 2, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
+  JA(m, 2, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
+  JA(m, 2, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
+  JA(m, 2, 4, 4) = TERM1 * drdz;
+  const double reinv = 1.0 / th.creyn;
+  for (int i = 0; i < 75; i++) m[i] *= reinv;
+}
+
+template <>
+CFDV_HD CFDV_INLINE void jac_c<3>(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < 225; i++) m[i] = 0.0;
+  const double mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const double rho = f.U[0], denom = 1. / (rho * rho), irho = 1.0;
+  (void)irho;
+  const double l = f.U[1], mv = f.U[2], n = f.U[3], re = f.U[4];
+  const double ll = l * l, mm = mv * mv, nn = n * n, hkocv = f.k / th.Cv, TERM1 = f.k / th.Cv * denom;
+  const double q = (-re + (ll + mm + nn) / rho);
+  // diagonal (i == j) blocks
+  const double d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
+  JC(m, 0, 0, 1, 0) = mu_R * l * denom; JC(m, 0, 0, 1, 1) = (-mu_R / rho);
+  JC(m, 0, 0, 2, 0) = mu * mv * denom;  JC(m, 0, 0, 2, 2) = (-mu / rho);
+  JC(m, 0, 0, 3, 0) = mu * n * denom;   JC(m, 0, 0, 3, 3) = (-mu / rho);
+  JC(m, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
+  JC(m, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
+  JC(m, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+  JC(m, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+  JC(m, 0, 0, 4, 4) = (-hkocv / rho);
+  const double e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
+  JC(m, 1, 1, 1, 0) = e10; JC(m, 1, 1, 1, 1) = (-mu / rho);
+  JC(m, 1, 1, 2, 0) = e20; JC(m, 1, 1, 2, 2) = (-mu_R / rho);
+  JC(m, 1, 1, 3, 0) = e30; JC(m, 1, 1, 3, 3) = (-mu / rho);
+  JC(m, 1, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
+  JC(m, 1, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+  JC(m, 1, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
+  JC(m, 1, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+  JC(m, 1, 1, 4, 4) = (-hkocv / rho);
+  const double f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
+  JC(m, 2, 2, 1, 0) = f10; JC(m, 2, 2, 1, 1) = (-mu / rho);
+  JC(m, 2, 2, 2, 0) = f20; JC(m, 2, 2, 2, 2) = (-mu / rho);
+  JC(m, 2, 2, 3, 0) = f30; JC(m, 2, 2, 3, 3) = (-mu_R / rho);
+  JC(m, 2, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
+  JC(m, 2, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+  JC(m, 2, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+  JC(m, 2, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
+  JC(m, 2, 2, 4, 4) = (-hkocv / rho);
+  // off-diagonal blocks (i != j)
+  JC(m, 0, 1, 1, 0) = lambda * mv * denom; JC(m, 0, 1, 1, 2) = (-lambda / rho);
+  JC(m, 0, 1, 2, 0) = mu * l * denom;      JC(m, 0, 1, 2, 1) = (-mu / rho);
+  JC(m, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
+  JC(m, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
+  JC(m, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
+  JC(m, 0, 2, 1, 0) = lambda * n * denom;  JC(m, 0, 2, 1, 3) = (-lambda / rho);
+  JC(m, 0, 2, 3, 0) = mu * l * denom;      JC(m, 0, 2, 3, 1) = (-mu / rho);
+  JC(m, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
+  JC(m, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
+  JC(m, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
+  JC(m, 1, 0, 1, 0) = mu * mv * denom;     JC(m, 1, 0, 1, 2) = (-mu / rho);
+  JC(m, 1, 0, 2, 0) = lambda * l * denom;  JC(m, 1, 0, 2, 1) = (-lambda / rho);
+  JC(m, 1, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
+  JC(m, 1, 0, 4, 1) = (mv / rho) * (-lambda / rho);
+  JC(m, 1, 0, 4, 2) = (l / rho) * (-mu / rho);
+  JC(m, 1, 2, 2, 0) = lambda * n * denom;  JC(m, 1, 2, 2, 3) = (-lambda / rho);
+  JC(m, 1, 2, 3, 0) = mu * mv * denom;     JC(m, 1, 2, 3, 2) = (-mu / rho);
+  JC(m, 1, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
+  JC(m, 1, 2, 4, 2) = (n / rho) * (-mu / rho);
+  JC(m, 1, 2, 4, 3) = (mv / rho) * (-lambda / rho);
+  JC(m, 2, 0, 1, 0) = mu * n * denom;      JC(m, 2, 0, 1, 3) = (-mu / rho);
+  JC(m, 2, 0, 3, 0) = lambda * l * denom;  JC(m, 2, 0, 3, 1) = (-lambda / rho);
+  JC(m, 2, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
+  JC(m, 2, 0, 4, 1) = (n / rho) * (-lambda / rho);
+  JC(m, 2, 0, 4, 3) = (l / rho) * (-mu / rho);
+  JC(m, 2, 1, 2, 0) = mu * n * denom;      JC(m, 2, 1, 2, 3) = (-mu / rho);
+  JC(m, 2, 1, 3, 0) = lambda * mv * denom; JC(m, 2, 1, 3, 2) = (-lambda / rho);
+  JC(m, 2, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
+  JC(m, 2, 1, 4, 2) = (n / rho) * (-lambda / rho);
+  JC(m, 2, 1, 4, 3) = (mv / rho) * (-mu / rho);
+  const double reinv = 1.0 / th.creyn;
+  for (int i = 0; i < 225; i++) m[i] *= reinv;
+}
+
+// convective + viscous flux of one node, FG[i*5+r] = F(i,r) + G(i,r).
+// F is the node's own flux; G uses the Gauss-point stress, dT, k with the node velocity.
+// with_F = 0 drops F (the 3D reference evaluates the empty base-class flux).
+template <int NDIM>
+CFDV_HD CFDV_INLINE void node_flux(const GpState& f, const NodePrim& n, double Re, bool with_F, double* FG) {
+  constexpr int NEQ = NDIM + 2;
+  const double reinv = 1.0 / Re;
+#pragma unroll
+  for (int i = 0; i < NDIM; i++) {
+    double Gi[5];
+    Gi[0] = 0.0;
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) Gi[1 + j] = -f.tau[i][j] * reinv;
+    double s = -f.tau[i][0] * n.v[0];
+#pragma unroll
+    for (int j = 1; j < NDIM; j++) s = s - f.tau[i][j] * n.v[j];
+    Gi[NDIM + 1] = (s - f.k * f.dT[i]) * reinv;
+    double Fi[5] = {0, 0, 0, 0, 0};
+    if (with_F) {
+      if (NDIM == 2) {
+        const double rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
+        const double li = (i == 0) ? l : m;
+        Fi[0] = li;
+        Fi[1] = (i == 0) ? p + l * l / rho : (l * m) / rho;
+        Fi[2] = (i == 0) ? (l * m) / rho : p + m * m / rho;
+        Fi[3] = (p + e) * (li / rho);
+      } else {
+        const double rho = n.U[0], p = n.p;
+        const double vel[3] = {n.U[1] / n.U[0], n.U[2] / n.U[0], n.U[3] / n.U[0]};
+        const double E = n.U[4] / n.U[0];
+        Fi[0] = rho * vel[i];
+#pragma unroll
+        for (int j = 0; j < 3; j++) Fi[1 + j] = rho * vel[i] * vel[j] + (i == j ? p : 0.0);
+        Fi[4] = (rho * E + p) * vel[i];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < NEQ; r++) FG[i * 5 + r] = Fi[r] + Gi[r];
+  }
+}
+
+}  // namespace cfdv

@@ -1,0 +1,657 @@
+// FDV element formation as the phases of one thread block ("CTA") per element.
+//
+// Per element the CTA computes what the reference builds in FDVGalerkin::operator()
+// (FDV/FDVGalerkin.h:121-154) followed by ApplyBC (FDV/Function/ApplyBC.h:131-250):
+//   load      node unpack (NodeUnpack.h:185-205), boundary face list
+//   domain    one thread per Gauss point: FDVParam (FDVParam.h:15-111), shape functions,
+//             Gauss-point state, stress, SUPG/discontinuity-capturing test function
+//             (FDVGalerkin.h:225-387), flux Jacobians and the rhs flux terms
+//   hmat      all threads: h_ij = -dt s3 c_ij + dt^2/2 (a_i+b_i)(s2 a_j + s4 b_j)
+//             (FDVGalerkin.h:611-628; for a face m_ij = -h_ij, :698-715)
+//   contract  R(N r, M s) += sum_k B_k(N,M) C_k(r,s) with
+//             B = wJ Phi_N Phi_M (C = I), wJ(Psi_N sum_j dPhi_Mj - dPhi_Ni Phi_M) (C = X_i),
+//             wJ dPhi_Ni dPhi_Mj (C = h_ij); X_i = dt (s1 a_i + s3 b_i) = -g_i = nd_i
+//             (FDVGalerkin.h:405-451)
+//   faces     same three phases per boundary face with 0 != bc < 100
+//             (FDVGalerkin.h:455-533, 643-756; TFNorm2D TestFunctions1D.h:207-216,
+//             TFNorm3D calc_TF_norm3D.h:9-167, eval1dboundary.h, eval2dboundary.h)
+//   write     ApplyBC through the precomputed Dirichlet row mask, then a coalesced
+//             store of R (column-major, FP64 or FP32) and rhs.
+// Every phase is a host/device function of (block state, thread id) so that the
+// same code runs in the CUDA kernel (phases separated by __syncthreads()).
+#pragma once
+#include "fdv_physics.cuh"
+
+namespace cfdv {
+
+template <int NDIM>
+struct FormTraits {
+  static constexpr int NNOD = (NDIM == 2) ? 4 : 8;
+  static constexpr int NEQ = NDIM + 2;
+  static constexpr int KE = NNOD * NEQ;
+  static constexpr int Q = (NDIM == 2) ? 4 : 8;      // domain Gauss points
+  static constexpr int NBN = (NDIM == 2) ? 2 : 4;    // nodes per face
+  static constexpr int QF = (NDIM == 2) ? 2 : 4;     // Gauss points per face
+  static constexpr int NFACE = (NDIM == 2) ? 4 : 6;
+  static constexpr int NP = NNOD * NNOD;             // (N, M) node pairs
+  static constexpr int SPLIT = (NDIM == 2) ? 4 : 2;  // threads per node pair
+  static constexpr int THREADS = NP * SPLIT;         // 64 (2D) / 128 (3D)
+  static constexpr int RS = NEQ * NEQ;
+  static constexpr int RS_PER = (RS + SPLIT - 1) / SPLIT;  // (r,s) entries per thread
+};
+
+// one Gauss point's worth of coefficients
+template <int NDIM>
+struct GpSlot {
+  static constexpr int NNOD = FormTraits<NDIM>::NNOD;
+  double wJ;
+  double Phi[NNOD];
+  double dPhi[NNOD][3];
+  double Psi[NNOD];
+  double en[3];
+  double A[NDIM][25];  // a, then a + b
+  double D[NDIM][25];  // b, then s2 a + s4 b
+  double X[NDIM][25];  // dt (s1 a + s3 b)
+  double H[9][25];     // c, then h (domain) or m (face)
+  double P[NDIM][5];   // rhs coefficient per direction and equation
+};
+
+template <int NDIM>
+struct FormShared {
+  using T = FormTraits<NDIM>;
+  NodePrim nd[T::NNOD];
+  int faces[T::NFACE];
+  int codes[T::NFACE];
+  int nfaces;
+  uint64_t mask;
+  double s[4];  // s1..s4 of the element (written by Gauss-point thread 0)
+  union {
+    GpSlot<NDIM> slot[T::Q];
+    double Rt[T::KE * T::KE];
+  };
+};
+
+template <int NDIM>
+struct FormRegs {
+  double acc[FormTraits<NDIM>::RS_PER];
+  double rhs;
+};
+
+// hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)
+CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
+  if (ndim == 2) return (f + i) & 3;
+  const int tbl[6][4] = {{3, 2, 1, 0}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}, {6, 7, 4, 5}};
+  return tbl[f][i];
+}
+
+// ---------------------------------------------------------------------------
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_load(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid) {
+  using T = FormTraits<NDIM>;
+  if (tid < T::NNOD) {
+    const int n = a.conn[(size_t)e * T::NNOD + tid];
+    node_unpack<NDIM>(a.gas, a.U + (size_t)n * T::NEQ, a.x + (size_t)n * NDIM, sh.nd[tid]);
+  }
+  if (tid == 0) {
+    int nf = 0;
+    for (int f = 0; f < T::NFACE; f++) {
+      const int c = a.bc[(size_t)e * T::NFACE + f];
+      if (c != 0 && c < 100) {  // FDVGalerkin.h:460
+        sh.faces[nf] = f;
+        sh.codes[nf] = c;
+        nf++;
+      }
+    }
+    sh.nfaces = nf;
+    sh.mask = a.rowmask ? a.rowmask[e] : 0ull;
+  }
+}
+
+// FDVParam.h:15-111 on the element's nodes; s = {s1, s2, s3, s4}
+template <int NDIM>
+CFDV_HD CFDV_INLINE void fdv_params(const GasParams& g, const NodePrim* nd, double* s) {
+  using T = FormTraits<NDIM>;
+  double M_min = 0, M_max = 0, Re_min = 0, Re_max = 0;
+  for (int b = 0; b < T::NNOD; b++) {
+    double vv = 0;
+    for (int i = 0; i < NDIM; i++) vv += nd[b].v[i] * nd[b].v[i];
+    const double V = sqrt(vv);
+    double Tn = nd[b].T;
+    if (Tn < 1.0E-12) Tn = 0;
+    const double snd = sqrt(g.gamma * g.cgas * Tn);
+    const double M = (snd < 1.0E-12) ? 0 : V / snd;
+    const double Re = (nd[b].rho * V) / gas_mu(g, Tn);
+    if (b == 0) { M_max = M; M_min = M; Re_max = Re; Re_min = Re; }
+    M_max = fmax(M_max, M); M_min = fmin(M_min, M);
+    Re_max = fmax(Re_max, Re); Re_min = fmin(Re_min, Re);
+  }
+  const double eps = 0.0000001;
+  // the Mach spread stays in FP64: M_max ~ M_min cancels
+  double r = sqrt(M_max * M_max - M_min * M_min) / (M_min + eps);
+  double s1 = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
+  if (r > 0.01) s1 = fmin(r, 1.0);
+  else if (r < 0.01 && M_min >= 10E-10) s1 = 0;
+  else if (M_min < 10E-10) s1 = 1.0;
+  r = sqrt(Re_max * Re_max - Re_min * Re_min) / (Re_min + eps);
+  double s3 = 0.0;
+  if (r > 0.01) s3 = fmin(r, 1.0);
+  else if (r < 0.01 && Re_min >= 10E-10) s3 = 0.0;
+  else if (Re_min <= 10E-10) s3 = 1.0;
+  s[0] = s1;
+  s[1] = 0.5 * (1 + pow(s1, 0.2));
+  s[2] = s3;
+  s[3] = 0.5 * (1 + pow(s3, 0.2));
+}
+
+// a, b, c at the Gauss point -> X, A = a+b, D = s2 a + s4 b (in place), c stays in H
+template <int NDIM>
+CFDV_HD CFDV_INLINE void gp_jacobians(const FormArgs& a, const GpState& f, const double* s, GpSlot<NDIM>& sl) {
+  constexpr int NEQ = NDIM + 2;
+  jac_a<NDIM>(a.gas, f, &sl.A[0][0]);
+  jac_b<NDIM>(a.gas, f, &sl.D[0][0]);
+  jac_c<NDIM>(a.gas, f, &sl.H[0][0]);
+  for (int i = 0; i < NDIM; i++)
+    for (int r = 0; r < NEQ; r++)
+      for (int q = 0; q < NEQ; q++) {
+        const int k = r * 5 + q;
+        const double av = sl.A[i][k], bv = sl.D[i][k];
+        sl.X[i][k] = a.dt * (s[0] * av + s[2] * bv);
+        sl.A[i][k] = av + bv;
+        sl.D[i][k] = s[1] * av + s[3] * bv;
+      }
+}
+
+// Domain Gauss point q (GaussQuad.h:69-112 loop order: q = (i*2 + j)*2 + k)
+template <int NDIM>
+CFDV_HD void phase_domain_gp(const FormArgs& a, FormShared<NDIM>& sh, int q) {
+  using T = FormTraits<NDIM>;
+  constexpr int NNOD = T::NNOD, NEQ = T::NEQ;
+  GpSlot<NDIM>& sl = sh.slot[q];
+  double z[3], w = 1.0;
+  for (int d = 0; d < NDIM; d++) {
+    const int bit = (q >> (NDIM - 1 - d)) & 1;
+    z[d] = a.gz[bit];
+    w *= a.gw[bit];
+  }
+  double s[4];
+  fdv_params<NDIM>(a.gas, sh.nd, s);
+  if (q == 0)
+    for (int i = 0; i < 4; i++) sh.s[i] = s[i];
+  double dPxi[NNOD][3], jac[3][3];
+  shape_fn<NDIM>(z, sl.Phi, dPxi);
+  const double J = phys_deriv<NDIM>(dPxi, sh.nd, sl.dPhi, jac);
+  sl.wJ = w * J;
+  const NodePrim* ndp[NNOD];
+  for (int N = 0; N < NNOD; N++) ndp[N] = &sh.nd[N];
+  GpState f;
+  gp_state<NDIM>(a.gas, NNOD, ndp, sl.Phi, sl.dPhi, f);
+  viscous_stress<NDIM>(f);
+
+  double tau = 0.0;
+  for (int N = 0; N < NNOD; N++) sl.Psi[N] = 0.0;
+  if (NDIM == 2) {  // streamline-upwind numerical diffusion (FDVGalerkin.h:225-332)
+    const double J_xi = jac[0][0] * jac[0][0] + jac[1][0] * jac[1][0];
+    const double J_eta = jac[0][1] * jac[0][1] + jac[1][1] * jac[1][1];
+    const double ixi = 1. / sqrt(J_xi), ieta = 1. / sqrt(J_eta);
+    const double v_xi = f.v[0] * (ixi * jac[0][0]) + f.v[1] * (ixi * jac[1][0]);
+    const double v_eta = f.v[0] * (ieta * jac[0][1]) + f.v[1] * (ieta * jac[1][1]);
+    const double S = f.v[0] * f.v[0] + f.v[1] * f.v[1];
+    // element extents between opposite edge midpoints (eta extent taken bottom - top)
+    const double h_xi = 0.5 * (sh.nd[1].x[0] + sh.nd[2].x[0]) - 0.5 * (sh.nd[0].x[0] + sh.nd[3].x[0]);
+    const double h_eta = 0.5 * (sh.nd[0].x[1] + sh.nd[1].x[1]) - 0.5 * (sh.nd[2].x[1] + sh.nd[3].x[1]);
+    const double R_xi = f.U[0] * v_xi * h_xi / f.mu;
+    const double R_eta = f.U[0] * v_eta * h_eta / f.mu;
+    const double al_xi = (R_xi == 0) ? 0.0 : cosh(R_xi / 2.) / sinh(R_xi / 2.) - 2. / R_xi;
+    const double al_eta = (R_eta == 0) ? 0.0 : cosh(R_eta / 2.) / sinh(R_eta / 2.) - 2. / R_eta;
+    tau = (S == 0) ? 0.0 : 0.25 * (al_xi * h_xi * v_xi + al_eta * h_eta * v_eta) / S;
+    for (int N = 0; N < NNOD; N++) sl.Psi[N] = tau * (f.v[0] * sl.dPhi[N][0] + f.v[1] * sl.dPhi[N][1]);
+    // discontinuity capturing (FDVGalerkin.h:336-387); in 3D tau = 0 makes it vanish
+    double A[2] = {0, 0};
+    for (int k = 0; k < 2; k++)
+      for (int j = 0; j < 2; j++) A[j] += f.dV[j][k] * f.v[k];
+    const double gam = sqrt(f.v[0] * f.v[0] + f.v[1] * f.v[1]) * sqrt(A[0] * A[0] + A[1] * A[1]);
+    double tau_b = 0.0;
+    if (gam != 0) {
+      tau_b = tau * f.v[0] * A[0] / gam + tau * f.v[1] * A[1] / gam;
+      if ((tau_b - tau) < 0) tau_b = tau;
+    }
+    for (int N = 0; N < NNOD; N++) sl.Psi[N] += tau_b * (f.v[0] * sl.dPhi[N][0] + f.v[1] * sl.dPhi[N][1]);
+  }
+
+  gp_jacobians<NDIM>(a, f, s, sl);
+
+  // rhs coefficient: P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s)
+  // with Fbar = sum_b Phi_b FG_b, divF(s) = sum_j sum_b dPhi_bj FG_b(j,s)  (FDVGalerkin.h:549-609, 410-427)
+  double Fbar[NDIM][5], divF[5];
+  for (int i = 0; i < NDIM; i++)
+    for (int r = 0; r < 5; r++) Fbar[i][r] = 0.0;
+  for (int r = 0; r < 5; r++) divF[r] = 0.0;
+  const bool withF = (NDIM == 2) || a.physical_3d_flux;
+  for (int b = 0; b < NNOD; b++) {
+    double FG[15];
+    node_flux<NDIM>(f, sh.nd[b], a.gas.creyn, withF, FG);
+    for (int i = 0; i < NDIM; i++)
+      for (int r = 0; r < NEQ; r++) {
+        Fbar[i][r] += sl.Phi[b] * FG[i * 5 + r];
+        divF[r] += sl.dPhi[b][i] * FG[i * 5 + r];
+      }
+  }
+  for (int i = 0; i < NDIM; i++)
+    for (int r = 0; r < NEQ; r++) {
+      double t = 0.0;
+      for (int q2 = 0; q2 < NEQ; q2++) t += sl.A[i][r * 5 + q2] * divF[q2];
+      sl.P[i][r] = a.dt * Fbar[i][r] - a.dtsq_2 * t;
+    }
+}
+
+// h (sign = +1, domain) or m (sign = -1, face) over nslots slots, all threads
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_hmat(const FormArgs& a, FormShared<NDIM>& sh, int nslots, double sign, int tid) {
+  const double s3_dt = a.dt * sh.s[2];
+  constexpr int NEQ = NDIM + 2;
+  constexpr int PER = NDIM * NDIM * NEQ * NEQ;
+  for (int it = tid; it < nslots * PER; it += FormTraits<NDIM>::THREADS) {
+    const int q = it / PER;
+    int rem = it % PER;
+    const int ij = rem / (NEQ * NEQ);
+    rem %= NEQ * NEQ;
+    const int r = rem / NEQ, s = rem % NEQ;
+    const int i = ij / NDIM, j = ij % NDIM;
+    GpSlot<NDIM>& sl = sh.slot[q];
+    double t = 0.0;
+    for (int k = 0; k < NEQ; k++) t += sl.A[i][r * 5 + k] * sl.D[j][k * 5 + s];
+    const double c = sl.H[i * 3 + j][r * 5 + s];
+    sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
+  }
+}
+
+// thread -> (node pair, (r,s) range)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void thread_pair(int tid, int& N, int& M, int& rs0, int& nrs) {
+  using T = FormTraits<NDIM>;
+  const int pair = tid % T::NP, split = tid / T::NP;
+  N = pair / T::NNOD;
+  M = pair % T::NNOD;
+  rs0 = split * T::RS_PER;
+  nrs = T::RS - rs0;
+  if (nrs > T::RS_PER) nrs = T::RS_PER;
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_contract_domain(FormShared<NDIM>& sh, int tid, FormRegs<NDIM>& rg) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ;
+  int N, M, rs0, nrs;
+  thread_pair<NDIM>(tid, N, M, rs0, nrs);
+  for (int k = 0; k < T::RS_PER; k++) rg.acc[k] = 0.0;
+  for (int q = 0; q < T::Q; q++) {
+    const GpSlot<NDIM>& sl = sh.slot[q];
+    const double wJ = sl.wJ;
+    const double B0 = wJ * sl.Phi[N] * sl.Phi[M];
+    double sdM = 0.0;
+    for (int j = 0; j < NDIM; j++) sdM += sl.dPhi[M][j];
+    double Cx[NDIM], Bh[NDIM][NDIM];
+    for (int i = 0; i < NDIM; i++) {
+      Cx[i] = wJ * (sl.Psi[N] * sdM - sl.dPhi[N][i] * sl.Phi[M]);
+      for (int j = 0; j < NDIM; j++) Bh[i][j] = wJ * sl.dPhi[N][i] * sl.dPhi[M][j];
+    }
+    for (int k = 0; k < T::RS_PER; k++) {
+      if (k >= nrs) break;
+      const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
+      double t = (r == s) ? B0 : 0.0;
+      for (int i = 0; i < NDIM; i++) {
+        t += Cx[i] * sl.X[i][idx];
+        for (int j = 0; j < NDIM; j++) t += Bh[i][j] * sl.H[i * 3 + j][idx];
+      }
+      rg.acc[k] += t;
+    }
+  }
+  // rhs(N r) = sum_q wJ sum_i dPhi_Ni P_q(i, r)
+  rg.rhs = 0.0;
+  if (tid < T::KE) {
+    const int Nn = tid / NEQ, r = tid % NEQ;
+    for (int q = 0; q < T::Q; q++) {
+      const GpSlot<NDIM>& sl = sh.slot[q];
+      double t = 0.0;
+      for (int i = 0; i < NDIM; i++) t += sl.dPhi[Nn][i] * sl.P[i][r];
+      rg.rhs += sl.wJ * t;
+    }
+  }
+}
+
+// 3D boundary-state edits (eval2dboundary.h:14-371); tau enters as zero
+CFDV_HD CFDV_INLINE void edit_face_state_3d(int code, GpState& f, const double* en, int adiabatic) {
+  switch (code) {
+    case 2:
+    case 12:
+      for (int i = 0; i < 3; i++) f.dV[i][2] = 0;
+      f.dT[2] = 0;
+      break;
+    case 22:
+      for (int i = 0; i < 3; i++) f.dV[i][1] = 0;
+      f.dT[1] = 0;
+      viscous_stress<3>(f);
+      f.tau[0][1] = 0.0; f.tau[1][1] = 0.0; f.tau[2][1] = 0.0; f.tau[1][0] = 0.0; f.tau[1][2] = 0.0;
+      break;
+    case 1:
+    case 51:
+      if (adiabatic) f.dT[2] = 0.0;
+      viscous_stress<3>(f);
+      break;
+    case 21:
+    case 31:
+      if (adiabatic) f.dT[1] = 0.0;
+      viscous_stress<3>(f);
+      break;
+    case 11:
+      if (adiabatic) f.dT[0] = 0.0;
+      viscous_stress<3>(f);
+      break;
+    case -1:
+      break;
+    case 6:
+      f.dT[0] = 0.0;
+      viscous_stress<3>(f);
+      for (int i = 0; i < 3; i++) f.tau[i][0] = 0;
+      break;
+    case 7:  // falls through into 77/32 in the reference (eval2dboundary.h:113-145)
+      f.dT[2] = 0.0;
+      f.dT[1] = 0.0;
+      viscous_stress<3>(f);
+      for (int i = 0; i < 3; i++) { f.tau[i][2] = 0; f.tau[i][1] = 0; }
+      break;
+    case 77:
+    case 32:
+      f.dT[1] = 0.0;
+      viscous_stress<3>(f);
+      for (int i = 0; i < 3; i++) f.tau[i][1] = 0;
+      break;
+    case 4: {
+      f.v[0] = 0; f.v[1] = 0; f.v[2] = 0;
+      const double* n = en;  // the weighted normal, not a unit vector
+      const double dud = f.dV[0][0] * n[0] + f.dV[0][1] * n[1] + f.dV[0][2] * n[2];
+      const double dvd = f.dV[1][0] * n[0] + f.dV[1][1] * n[1] + f.dV[1][2] * n[2];
+      const double dtd = f.dT[0] * n[0] + f.dT[1] * n[1] + f.dT[2] * n[2];
+      for (int j = 0; j < 3; j++) { f.dV[0][j] -= dud * n[j]; f.dV[1][j] -= dvd * n[j]; f.dT[j] -= dtd * n[j]; }
+      double dUd[3];
+      for (int i = 0; i < 3; i++) dUd[i] = f.dU[i][0] * n[0] + f.dU[i][1] * n[1] + f.dU[i][2] * n[2];
+      for (int i = 0; i < 3; i++)  // only the first three equations (loop bound dU.jmax() = 3)
+        for (int j = 0; j < 3; j++) f.dU[i][j] -= dUd[i] * n[j];
+    } break;
+    case 8:
+      viscous_stress<3>(f);
+      break;
+    case -12:
+      f.dV[0][2] = 0.0; f.dV[1][2] = 0.0; f.dV[2][2] = 0.0;
+      f.dT[2] = 0.0;
+      f.v[2] = 0.0;
+      break;
+    default:
+      break;
+  }
+}
+
+// 2D boundary-state edits (eval1dboundary.h:9-251)
+CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim* n0, const NodePrim* n1,
+                                            const double* en) {
+  const double len = sqrt(en[0] * en[0] + en[1] * en[1]);
+  const double n[2] = {en[0] / len, en[1] / len};
+  switch (code) {
+    case 2:
+    case 12: {
+      double d = f.v[0] * n[0] + f.v[1] * n[1];
+      f.v[0] -= d * n[0];
+      d = f.v[0] * n[0] + f.v[1] * n[1];  // re-evaluated after the first component
+      f.v[1] -= d * n[1];
+      d = f.dT[0] * n[0] + f.dT[1] * n[1];
+      f.dT[0] -= d * n[0];
+      d = f.dT[0] * n[0] + f.dT[1] * n[1];
+      f.dT[1] -= d * n[1];
+    } break;
+    case 1:
+    case 51: {
+      double d = f.dT[0] * n[0] + f.dT[1] * n[1];
+      f.dT[0] -= d * n[0];
+      d = f.dT[0] * n[0] + f.dT[1] * n[1];
+      f.dT[1] -= d * n[1];
+    } break;
+    case -1:
+      f.dV[0][0] = 0.0; f.dV[1][0] = 0.0; f.dV[0][1] = 0.0; f.dV[1][1] = 0.0;
+      f.dT[0] = 0.0;
+      break;
+    case 6:
+      f.dV[0][0] = 0.0; f.dV[1][0] = 0.0; f.dV[0][1] = 0.0; f.dV[1][1] = 0.0;
+      f.dT[0] = 0.0;
+      for (int i = 0; i < 4; i++) f.dU[i][0] = 0.0;
+      break;
+    case -2:
+    case 7:
+      f.dV[0][1] = 0.0; f.dV[1][1] = 0.0;
+      f.dT[1] = 0.0;
+      for (int i = 0; i < 4; i++) f.dU[i][1] = 0.0;
+      break;
+    case 4:
+    case 8: {
+      double nn[2];
+      if (code == 4) {
+        f.v[0] = 0; f.v[1] = 0;
+        nn[0] = en[0]; nn[1] = en[1];
+      } else {  // fixed 10 degree ramp direction scaled by the edge height
+        const double alpha = 10 * (3.14159 / 180.0);
+        const double dl = fabs(n1->x[1] - n0->x[1]);
+        nn[0] = cos(alpha) * dl;
+        nn[1] = sin(alpha) * dl;
+      }
+      const double dud = f.dV[0][0] * nn[0] + f.dV[0][1] * nn[1];
+      const double dvd = f.dV[1][0] * nn[0] + f.dV[1][1] * nn[1];
+      const double dtd = f.dT[0] * nn[0] + f.dT[1] * nn[1];
+      f.dV[0][0] -= dud * nn[0]; f.dV[0][1] -= dud * nn[1];
+      f.dV[1][0] -= dvd * nn[0]; f.dV[1][1] -= dvd * nn[1];
+      f.dT[0] -= dtd * nn[0]; f.dT[1] -= dtd * nn[1];
+      double dUd[4];
+      for (int i = 0; i < 4; i++) dUd[i] = f.dU[i][0] * nn[0] + f.dU[i][1] * nn[1];
+      for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 2; j++) f.dU[i][j] -= dUd[i] * nn[j];
+    } break;
+    case -12:
+      f.dV[0][1] = 0.0; f.dV[1][1] = 0.0;
+      f.dT[1] = 0.0;
+      f.v[1] = 0.0;
+      for (int i = 0; i < 4; i++) f.dU[i][1] = 0.0;
+      break;
+    case 11:
+    case 21:
+      f.v[0] = 0; f.v[1] = 0;
+      f.dV[0][0] = 0.0; f.dV[1][0] = 0.0;
+      f.dT[1] = 0.0;
+      for (int i = 0; i < 4; i++) f.dU[i][1] = 0.0;
+      break;
+    default:
+      break;
+  }
+  viscous_stress<2>(f);
+  if (code == 2 || code == 12 || code == 7) { f.tau[0][1] = 0.0; f.tau[1][0] = 0.0; }
+  if (code == 6) { f.tau[0][0] = 0.; f.tau[1][0] = 0.; }
+}
+
+// face Gauss point qf of face `lf` (index into sh.faces)
+template <int NDIM>
+CFDV_HD void phase_face_gp(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ, NBN = T::NBN;
+  GpSlot<NDIM>& sl = sh.slot[qf];
+  const int f = sh.faces[lf], code = sh.codes[lf];
+  const NodePrim* nd[NBN];
+  for (int i = 0; i < NBN; i++) nd[i] = &sh.nd[face_node(NDIM, f, i)];
+  const double* s = sh.s;
+  double* phib = sl.Phi;
+  double (*dpidx)[3] = sl.dPhi;
+  double* en = sl.en;
+  for (int i = 0; i < NBN; i++)
+    for (int j = 0; j < 3; j++) dpidx[i][j] = 0.0;
+  en[2] = 0.0;
+  if (NDIM == 2) {  // TestFunctions1D.h:141-216
+    const double z = a.gz[qf], w = a.gw[qf];
+    phib[0] = 0.5 * (1 - z);
+    phib[1] = 0.5 * (1 + z);
+    const double dxds = -0.5 * nd[0]->x[0] + 0.5 * nd[1]->x[0];
+    const double dyds = -0.5 * nd[0]->x[1] + 0.5 * nd[1]->x[1];
+    en[0] = dyds * w;
+    en[1] = -dxds * w;
+    const double delx = nd[1]->x[0] - nd[0]->x[0], dely = nd[1]->x[1] - nd[0]->x[1];
+    if (!(fabs(delx) < 1.0E-12)) { dpidx[0][0] = -1.0 / delx; dpidx[1][0] = 1.0 / delx; }
+    if (!(fabs(dely) < 1.0E-12)) { dpidx[0][1] = -1.0 / dely; dpidx[1][1] = 1.0 / dely; }
+  } else {  // calc_TF_norm3D.h:9-167
+    const double z[2] = {a.gz[qf >> 1], a.gz[qf & 1]};
+    const double w0 = a.gw[qf >> 1], w1 = a.gw[qf & 1];
+    double ph[4], dpxi[4][3];
+    shape_fn<2>(z, ph, dpxi);
+    for (int i = 0; i < 4; i++) phib[i] = ph[i];
+    double L[3], Mu[3];
+    for (int i = 0; i < 3; i++) { L[i] = nd[1]->x[i] - nd[0]->x[i]; Mu[i] = nd[3]->x[i] - nd[0]->x[i]; }
+    for (int j = 0; j < 3; j++) {  // magnitude re-evaluated after each component
+      L[j] /= sqrt(L[0] * L[0] + L[1] * L[1] + L[2] * L[2]);
+      Mu[j] /= sqrt(Mu[0] * Mu[0] + Mu[1] * Mu[1] + Mu[2] * Mu[2]);
+    }
+    double nrm[3], gm[3];
+    nrm[0] = L[1] * Mu[2] - L[2] * Mu[1];
+    nrm[1] = L[2] * Mu[0] - L[0] * Mu[2];
+    nrm[2] = L[0] * Mu[1] - L[1] * Mu[0];
+    gm[0] = nrm[1] * L[2] - nrm[2] * L[1];
+    gm[1] = nrm[2] * L[0] - nrm[0] * L[2];
+    gm[2] = nrm[0] * L[1] - nrm[1] * L[0];
+    double dxd[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int N = 0; N < 4; N++)
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 2; j++) dxd[i][j] += dpxi[N][j] * nd[N]->x[i];
+    double tr[2][2];
+    for (int j = 0; j < 2; j++) {
+      tr[0][j] = L[0] * dxd[0][j] + L[1] * dxd[1][j] + L[2] * dxd[2][j];
+      tr[1][j] = gm[0] * dxd[0][j] + gm[1] * dxd[1][j] + gm[2] * dxd[2][j];
+    }
+    const double det = tr[0][0] * tr[1][1] - tr[1][0] * tr[0][1];
+    const double idet = 1. / det;
+    for (int N = 0; N < 4; N++) {
+      const double p0 = (tr[1][1] * dpxi[N][0] - tr[1][0] * dpxi[N][1]) * idet;
+      const double p1 = (-tr[0][1] * dpxi[N][0] + tr[0][0] * dpxi[N][1]) * idet;
+      for (int i = 0; i < 3; i++) dpidx[N][i] = L[i] * p0 + gm[i] * p1;
+    }
+    for (int i = 0; i < 3; i++) en[i] = nrm[i] * w0 * w1 * det;
+  }
+  GpState fs;
+  gp_state<NDIM>(a.gas, NBN, nd, phib, dpidx, fs);
+  if (NDIM == 2) edit_face_state_2d(code, fs, nd[0], nd[1], en);
+  else edit_face_state_3d(code, fs, en, a.gas.adiabatic);
+  gp_jacobians<NDIM>(a, fs, s, sl);
+  // face rhs: P(i,r) = -dt Fbar(i,r) + dt^2/2 sum_s A_i(r,s) divF(s)   (FDVGalerkin.h:643-680, 720-738)
+  double Fbar[NDIM][5], divF[5];
+  for (int i = 0; i < NDIM; i++)
+    for (int r = 0; r < 5; r++) Fbar[i][r] = 0.0;
+  for (int r = 0; r < 5; r++) divF[r] = 0.0;
+  const bool withF = (NDIM == 2) || a.physical_3d_flux;
+  for (int b = 0; b < NBN; b++) {
+    double FG[15];
+    node_flux<NDIM>(fs, *nd[b], a.gas.creyn, withF, FG);
+    for (int i = 0; i < NDIM; i++)
+      for (int r = 0; r < NEQ; r++) {
+        Fbar[i][r] += phib[b] * FG[i * 5 + r];
+        divF[r] += dpidx[b][i] * FG[i * 5 + r];
+      }
+  }
+  for (int i = 0; i < NDIM; i++)
+    for (int r = 0; r < NEQ; r++) {
+      double t = 0.0;
+      for (int q2 = 0; q2 < NEQ; q2++) t += sl.A[i][r * 5 + q2] * divF[q2];
+      sl.P[i][r] = -a.dt * Fbar[i][r] + a.dtsq_2 * t;
+    }
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE int face_pos(int f, int node) {
+  for (int i = 0; i < FormTraits<NDIM>::NBN; i++)
+    if (face_node(NDIM, f, i) == node) return i;
+  return -1;
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_contract_face(FormShared<NDIM>& sh, int lf, int tid, FormRegs<NDIM>& rg) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ;
+  const int f = sh.faces[lf];
+  int N, M, rs0, nrs;
+  thread_pair<NDIM>(tid, N, M, rs0, nrs);
+  const int fN = face_pos<NDIM>(f, N), fM = face_pos<NDIM>(f, M);
+  if (fN >= 0 && fM >= 0) {
+    for (int q = 0; q < T::QF; q++) {
+      const GpSlot<NDIM>& sl = sh.slot[q];
+      double Cx[NDIM], Bh[NDIM][NDIM];
+      for (int i = 0; i < NDIM; i++) {
+        Cx[i] = sl.en[i] * sl.Phi[fN] * sl.Phi[fM];
+        for (int j = 0; j < NDIM; j++) Bh[i][j] = sl.en[i] * sl.Phi[fN] * sl.dPhi[fM][j];
+      }
+      for (int k = 0; k < T::RS_PER; k++) {
+        if (k >= nrs) break;
+        const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
+        double t = 0.0;
+        for (int i = 0; i < NDIM; i++) {
+          t += Cx[i] * sl.X[i][idx];
+          for (int j = 0; j < NDIM; j++) t += Bh[i][j] * sl.H[i * 3 + j][idx];
+        }
+        rg.acc[k] += t;
+      }
+    }
+  }
+  if (tid < T::KE) {
+    const int Nn = tid / NEQ, r = tid % NEQ;
+    const int fp = face_pos<NDIM>(f, Nn);
+    if (fp >= 0) {
+      for (int q = 0; q < T::QF; q++) {
+        const GpSlot<NDIM>& sl = sh.slot[q];
+        double t = 0.0;
+        for (int i = 0; i < NDIM; i++) t += sl.en[i] * sl.P[i][r];
+        rg.rhs += sl.Phi[fp] * t;
+      }
+    }
+  }
+}
+
+// accumulators -> column-major staging tile (after the slots are no longer read)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_stage(FormShared<NDIM>& sh, int tid, const FormRegs<NDIM>& rg) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ;
+  int N, M, rs0, nrs;
+  thread_pair<NDIM>(tid, N, M, rs0, nrs);
+  for (int k = 0; k < T::RS_PER; k++) {
+    if (k >= nrs) break;
+    const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ;
+    sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r] = rg.acc[k];
+  }
+}
+
+// ApplyBC (rows of Dirichlet DOFs: zero, diagonal 0.5, rhs 0) and the coalesced store
+template <int NDIM>
+CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid,
+                                     const FormRegs<NDIM>& rg, int* bad) {
+  using T = FormTraits<NDIM>;
+  constexpr int KE = T::KE;
+  const uint64_t mk = sh.mask;
+  const size_t base = (size_t)e * KE * KE;
+  for (int k = tid; k < KE * KE; k += T::THREADS) {
+    const int I = k % KE, J = k / KE;
+    double v = sh.Rt[k];
+    if ((mk >> I) & 1ull) v = (I == J) ? 0.5 : 0.0;
+    if (!(v == v) || v - v != 0.0) *bad = 1;
+    if (a.R64) a.R64[base + k] = v;
+    if (a.R32) a.R32[base + k] = (float)v;
+  }
+  if (tid < KE) {
+    double v = ((mk >> tid) & 1ull) ? 0.0 : rg.rhs;
+    if (!(v == v) || v - v != 0.0) *bad = 1;
+    a.rhs[(size_t)e * KE + tid] = v;
+  }
+  if (tid == 0 && a.s_out)
+    for (int i = 0; i < 4; i++) a.s_out[(size_t)e * 4 + i] = sh.s[i];
+}
+
+}  // namespace cfdv

@@ -1,0 +1,214 @@
+// Element-by-element product and Krylov vector kernels of the GMRES solve.
+//
+// The EBE product y = sum_e P_e^T R_e P_e x (MPI_GMRES::sum_Av / sum_Ax,
+// Utility/Solvers/MPI_GMRES.h:442-693) runs as two deterministic passes:
+//   element pass  Y_e = R_e x_e, x_e gathered through the connectivity; R_e streamed
+//                 once, element-major, rows read coalesced (column-major storage)
+//   node pass     y_n = sum over the node's (element, local node) list of Y_e; the list
+//                 is a CSR built once per mesh, so the scatter needs no atomics and no
+//                 colouring, and sums always run in the same order.
+// Krylov dots/norms reduce to a fixed set of block partials; every consumer block
+// re-reduces them in the same order, so all scalars are bitwise reproducible.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace cfdv {
+
+template <int KE, int NEQ, int NNOD, int EPB, typename TR, typename TY, bool TRANS>
+__global__ void __launch_bounds__(KE* EPB) ebe_elem_kernel(const TR* __restrict__ R, const int* __restrict__ conn,
+                                                            const double* __restrict__ x, TY* __restrict__ Y,
+                                                            int E) {
+  __shared__ TR xs[EPB][KE];
+  const int le = threadIdx.x / KE, i = threadIdx.x % KE;
+  const int e = blockIdx.x * EPB + le;
+  if (e < E) xs[le][i] = (TR)x[(size_t)conn[(size_t)e * NNOD + i / NEQ] * NEQ + i % NEQ];
+  __syncthreads();
+  if (e >= E) return;
+  const TR* __restrict__ Re = R + (size_t)e * KE * KE;
+  TR acc = 0;
+  if (!TRANS) {
+#pragma unroll 8
+    for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[le][j];
+  } else {
+#pragma unroll 8
+    for (int j = 0; j < KE; j++) acc += __ldg(Re + i * KE + j) * xs[le][j];
+  }
+  Y[(size_t)e * KE + i] = (TY)acc;
+}
+
+template <int NEQ, int NNOD, typename TY>
+__global__ void __launch_bounds__(kRedThreads) ebe_node_kernel(const int* __restrict__ ptr,
+                                                               const int* __restrict__ idx,
+                                                               const TY* __restrict__ Y, int ndof, int mode,
+                                                               const double* __restrict__ b, double* out,
+                                                               const double* dotv, double* partial) {
+  constexpr int KE = NEQ * NNOD;
+  double part = 0.0;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < ndof; d += gridDim.x * blockDim.x) {
+    const int n = d / NEQ, k = d % NEQ;
+    double s = 0.0;
+    const int p1 = ptr[n + 1];
+    for (int p = ptr[n]; p < p1; p++) {
+      const int v = idx[p];
+      const int e = v / NNOD, l = v % NNOD;
+      s += (double)Y[(size_t)e * KE + l * NEQ + k];
+    }
+    const double val = mode ? b[d] - s : s;
+    out[d] = val;
+    if (dotv) part += val * ((dotv == out) ? val : dotv[d]);
+  }
+  if (partial) {
+    part = block_reduce_sum(part);
+    if (threadIdx.x == 0) partial[blockIdx.x] = part;
+  }
+}
+
+template <int NEQ, int NNOD>
+static cudaError_t ebe_dispatch(const EbeArgs& a, int use_fp32, int transpose, const double* x, double* out,
+                                int mode, const double* b, const double* dot_with, double* partial,
+                                cudaStream_t st, cudaEvent_t* ev) {
+  constexpr int KE = NEQ * NNOD;
+  constexpr int EPB = (KE == 16) ? 16 : 8;
+  const int grid = (a.n_elements + EPB - 1) / EPB;
+  if (ev) cudaEventRecord(ev[0], st);
+  if (grid > 0) {
+    if (use_fp32) {
+      if (transpose) ebe_elem_kernel<KE, NEQ, NNOD, EPB, float, float, true><<<grid, KE * EPB, 0, st>>>(a.R32, a.conn, x, a.Y32, a.n_elements);
+      else ebe_elem_kernel<KE, NEQ, NNOD, EPB, float, float, false><<<grid, KE * EPB, 0, st>>>(a.R32, a.conn, x, a.Y32, a.n_elements);
+    } else {
+      if (transpose) ebe_elem_kernel<KE, NEQ, NNOD, EPB, double, double, true><<<grid, KE * EPB, 0, st>>>(a.R64, a.conn, x, a.Y64, a.n_elements);
+      else ebe_elem_kernel<KE, NEQ, NNOD, EPB, double, double, false><<<grid, KE * EPB, 0, st>>>(a.R64, a.conn, x, a.Y64, a.n_elements);
+    }
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  if (use_fp32)
+    ebe_node_kernel<NEQ, NNOD, float><<<kRedBlocks, kRedThreads, 0, st>>>(a.csr_ptr, a.csr_idx, a.Y32, a.n_dof, mode, b, out, dot_with, partial);
+  else
+    ebe_node_kernel<NEQ, NNOD, double><<<kRedBlocks, kRedThreads, 0, st>>>(a.csr_ptr, a.csr_idx, a.Y64, a.n_dof, mode, b, out, dot_with, partial);
+  if (ev) cudaEventRecord(ev[2], st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ebe(const EbeArgs& a, int use_fp32, int transpose, const double* x, double* out, int mode,
+                       const double* b, const double* dot_with, double* partial, cudaStream_t st, cudaEvent_t* ev) {
+  if (a.ndim == 2) return ebe_dispatch<4, 4>(a, use_fp32, transpose, x, out, mode, b, dot_with, partial, st, ev);
+  return ebe_dispatch<5, 8>(a, use_fp32, transpose, x, out, mode, b, dot_with, partial, st, ev);
+}
+
+cudaError_t launch_compose_rhs(const EbeArgs& a, const double* rhs, double* b, double* partial, cudaStream_t st) {
+  if (a.ndim == 2)
+    ebe_node_kernel<4, 4, double><<<kRedBlocks, kRedThreads, 0, st>>>(a.csr_ptr, a.csr_idx, rhs, a.n_dof, 0, nullptr, b, b, partial);
+  else
+    ebe_node_kernel<5, 8, double><<<kRedBlocks, kRedThreads, 0, st>>>(a.csr_ptr, a.csr_idx, rhs, a.n_dof, 0, nullptr, b, b, partial);
+  return cudaGetLastError();
+}
+
+// ---- Krylov vector kernels ---------------------------------------------------
+__global__ void __launch_bounds__(kRedThreads) dot_kernel(const double* __restrict__ a,
+                                                          const double* __restrict__ b, int n, double* partial) {
+  double part = 0.0;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) part += a[d] * b[d];
+  part = block_reduce_sum(part);
+  if (threadIdx.x == 0) partial[blockIdx.x] = part;
+}
+
+__global__ void __launch_bounds__(kRedThreads) mgs_kernel(double* w, const double* __restrict__ v, int n,
+                                                          const double* __restrict__ pin, double* hout,
+                                                          const double* next, double* pout) {
+  const double h = reduce_partials(pin, kRedBlocks);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *hout = h;
+  double part = 0.0;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+    const double wn = w[d] - h * v[d];
+    w[d] = wn;
+    part += wn * (next ? next[d] : wn);
+  }
+  part = block_reduce_sum(part);
+  if (threadIdx.x == 0) pout[blockIdx.x] = part;
+}
+
+__global__ void __launch_bounds__(kRedThreads) normalize_kernel(const double* w, int n,
+                                                                const double* __restrict__ pin, double* hout,
+                                                                double* vout) {
+  const double nrm = sqrt(reduce_partials(pin, kRedBlocks));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *hout = nrm;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) vout[d] = w[d] / nrm;
+}
+
+__global__ void reduce_kernel(const double* __restrict__ pin, double* out, int do_sqrt) {
+  const double s = reduce_partials(pin, kRedBlocks);
+  if (threadIdx.x == 0) out[0] = do_sqrt ? sqrt(s) : s;
+}
+
+__global__ void __launch_bounds__(kRedThreads) combine_kernel(double* x, const double* __restrict__ V, int n,
+                                                              const double* __restrict__ y, int m) {
+  __shared__ double ys[256];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) ys[i] = y[i];
+  __syncthreads();
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+    double z = 0.0;
+    for (int i = 0; i < m; i++) z += ys[i] * V[(size_t)i * n + d];
+    x[d] += z;
+  }
+}
+
+__global__ void state_update_kernel(double* U, double* U0, const double* __restrict__ du, int n) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+    const double u = U[d];
+    U0[d] = u;
+    U[d] = u + du[d];
+  }
+}
+
+__global__ void __launch_bounds__(kRedThreads) rms_partial_kernel(const double* __restrict__ U,
+                                                                  const double* __restrict__ U0, int n_nodes,
+                                                                  int neqn, double* partial) {
+  double s[10];
+  for (int k = 0; k < 10; k++) s[k] = 0.0;
+  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < n_nodes; nd += gridDim.x * blockDim.x)
+    for (int k = 0; k < neqn; k++) {
+      const double u = U[(size_t)nd * neqn + k], u0 = U0[(size_t)nd * neqn + k];
+      s[k] += u * u;
+      s[5 + k] += u0 * u0;
+    }
+  for (int k = 0; k < 10; k++) {
+    const double t = block_reduce_sum(s[k]);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * 10 + k] = t;
+  }
+}
+
+cudaError_t launch_dot(const double* a, const double* b, int n, double* partial, cudaStream_t st) {
+  dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, b, n, partial);
+  return cudaGetLastError();
+}
+cudaError_t launch_mgs(double* w, const double* v, int n, const double* pin, double* hout, const double* next,
+                       double* pout, cudaStream_t st) {
+  mgs_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, v, n, pin, hout, next, pout);
+  return cudaGetLastError();
+}
+cudaError_t launch_normalize(const double* w, int n, const double* pin, double* hout, double* vout,
+                             cudaStream_t st) {
+  normalize_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(w, n, pin, hout, vout);
+  return cudaGetLastError();
+}
+cudaError_t launch_reduce(const double* pin, double* out, int do_sqrt, cudaStream_t st) {
+  reduce_kernel<<<1, kRedThreads, 0, st>>>(pin, out, do_sqrt);
+  return cudaGetLastError();
+}
+cudaError_t launch_combine(double* x, const double* V, int n, const double* y, int m, cudaStream_t st) {
+  if (m > 256) return cudaErrorInvalidValue;
+  combine_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(x, V, n, y, m);
+  return cudaGetLastError();
+}
+cudaError_t launch_state_update(double* U, double* U0, const double* du, int n, cudaStream_t st) {
+  state_update_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(U, U0, du, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_rms_partial(const double* U, const double* U0, int n_nodes, int neqn, double* partial,
+                               cudaStream_t st) {
+  rms_partial_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(U, U0, n_nodes, neqn, partial);
+  return cudaGetLastError();
+}
+
+}  // namespace cfdv

@@ -1,0 +1,272 @@
+"""ctypes binding of libcfdv_gpu.so (include/cfdv_gpu.h) for Python callers.
+
+``FDVSolver`` mirrors the objects the reference driver owns per case
+(src/main.cpp:104-197): the mesh and node state, the element matrices formed each
+step, and the GMRES solver (``GMRESbase``, Utility/Solvers/GMRESbase.h:8-23).
+There is no CPU implementation behind it: if the CUDA library is missing or no GPU
+is present the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcfdv_gpu.so")
+
+PREC_FP64, PREC_MIXED = 0, 1
+GMRES_REFERENCE, GMRES_CORRECT = 0, 1
+
+STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "bad mesh", 4: "non-finite value",
+          5: "allocation failed", 6: "call out of order", 7: "not converged"}
+
+# every entry point declared in include/cfdv_gpu.h
+EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error", "cfdv_get_stream",
+           "cfdv_set_state", "cfdv_load_node_records", "cfdv_get_state", "cfdv_state_device_ptr", "cfdv_cfl",
+           "cfdv_form", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
+           "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
+           "cfdv_profile_read"]
+
+
+class CfdvError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cfdv error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Mesh(C.Structure):
+    _fields_ = [("ndim", C.c_int), ("n_nodes", C.c_int), ("n_elements", C.c_int),
+                ("x", C.c_void_p), ("conn", C.c_void_p), ("bc", C.c_void_p)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double), ("prandtl", C.c_double),
+                ("tinf", C.c_double), ("twall", C.c_double), ("adiabatic", C.c_int), ("physical_3d_flux", C.c_int)]
+
+
+class _Opts(C.Structure):
+    _fields_ = [("mode", C.c_int), ("m", C.c_int), ("restarts", C.c_int), ("rtol", C.c_double),
+                ("precision", C.c_int), ("true_residual", C.c_int)]
+
+
+class _Report(C.Structure):
+    _fields_ = [("tol", C.c_double), ("bnorm", C.c_double), ("n_est", C.c_int), ("est_capacity", C.c_int),
+                ("est", C.c_void_p), ("gfinal_capacity", C.c_int), ("gfinal", C.c_void_p),
+                ("n_restarts", C.c_int), ("n_matvec", C.c_int), ("true_rel_res", C.c_double)]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("launches", C.c_long), ("total_ms", C.c_double), ("bytes", C.c_double),
+                ("form_launches", C.c_long), ("form_ms", C.c_double), ("kernel_launches", C.c_long)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA library not built: {LIB_PATH} (run __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        P, I, D = C.c_void_p, C.c_int, C.c_double
+        L.cfdv_create.argtypes = [P, P, P]
+        L.cfdv_upload_mesh.argtypes = [P, P]
+        L.cfdv_destroy.argtypes = [P]
+        L.cfdv_destroy.restype = None
+        L.cfdv_last_error.argtypes = [P]
+        L.cfdv_last_error.restype = C.c_char_p
+        L.cfdv_get_stream.argtypes = [P, P]
+        L.cfdv_set_state.argtypes = [P, P, C.c_size_t]
+        L.cfdv_load_node_records.argtypes = [P, P, C.c_size_t]
+        L.cfdv_get_state.argtypes = [P, P, P, C.c_size_t]
+        L.cfdv_state_device_ptr.argtypes = [P, P]
+        L.cfdv_cfl.argtypes = [P, D, P]
+        L.cfdv_form.argtypes = [P, D, I]
+        L.cfdv_gmres.argtypes = [P, P, P]
+        L.cfdv_update.argtypes = [P]
+        L.cfdv_rms.argtypes = [P, P]
+        L.cfdv_step.argtypes = [P, D, P, P, P]
+        L.cfdv_get_fdv_params.argtypes = [P, P]
+        L.cfdv_get_element_matrices.argtypes = [P, P, P]
+        L.cfdv_get_rhs_vector.argtypes = [P, P]
+        L.cfdv_get_du.argtypes = [P, P]
+        L.cfdv_matvec.argtypes = [P, P, P, I, I]
+        L.cfdv_profile.argtypes = [P, I]
+        L.cfdv_profile_read.argtypes = [P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class FDVSolver:
+    """One mesh + state on the current CUDA device."""
+
+    def __init__(self, case, physical_3d_flux: bool = False):
+        self.L = lib()
+        self.case = case
+        self.ndim = case.ndim
+        self.nnod, self.neqn = case.nnod, case.neqn
+        self.Ke = self.nnod * self.neqn
+        self.n_nodes, self.n_elements = case.n_nodes, case.n_elements
+        self.n_dof = self.n_nodes * self.neqn
+        self._x = np.ascontiguousarray(case.nodes[:, : self.ndim], dtype=np.float64)
+        self._conn = np.ascontiguousarray(case.conn, dtype=np.int32)
+        self._bc = np.ascontiguousarray(case.bc, dtype=np.int32)
+        mesh = _Mesh(self.ndim, self.n_nodes, self.n_elements, _p(self._x).value, _p(self._conn).value,
+                     _p(self._bc).value)
+        a = case.aero
+        params = _Params(float(a["gamma"]), float(a["M"]), float(a["Re"]), float(a["Pr"]), float(a["Tinf"]),
+                         float(a["Twall"]), int(float(a["Adiabatic"])), int(bool(physical_3d_flux)))
+        self._ctx = C.c_void_p()
+        rc = self.L.cfdv_create(C.byref(mesh), C.byref(params), C.byref(self._ctx))
+        if rc:
+            msg = self.L.cfdv_last_error(self._ctx).decode() if self._ctx else ""
+            if self._ctx:
+                self.L.cfdv_destroy(self._ctx)
+                self._ctx = C.c_void_p()
+            raise CfdvError(rc, msg)
+
+    def _ck(self, rc):
+        if rc:
+            raise CfdvError(rc, self.L.cfdv_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self.L.cfdv_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state --
+    def load_node_records(self):
+        rec = np.ascontiguousarray(self.case.nodes, dtype=np.float64)
+        self._ck(self.L.cfdv_load_node_records(self._ctx, _p(rec), self.n_nodes))
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._ck(self.L.cfdv_set_state(self._ctx, _p(U), U.size))
+
+    def get_state(self, U0=False):
+        U = np.empty(self.n_dof)
+        if U0:
+            U0a = np.empty(self.n_dof)
+            self._ck(self.L.cfdv_get_state(self._ctx, _p(U), _p(U0a), self.n_dof))
+            return U, U0a
+        self._ck(self.L.cfdv_get_state(self._ctx, _p(U), None, self.n_dof))
+        return U
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._ck(self.L.cfdv_get_stream(self._ctx, C.byref(s)))
+        return s.value or 0
+
+    @property
+    def state_ptr(self) -> int:
+        p = C.c_void_p()
+        self._ck(self.L.cfdv_state_device_ptr(self._ctx, C.byref(p)))
+        return p.value
+
+    # -- the step --
+    def cfl(self, cfl: float) -> float:
+        dt = C.c_double()
+        self._ck(self.L.cfdv_cfl(self._ctx, float(cfl), C.byref(dt)))
+        return dt.value
+
+    def form(self, dt: float, precision: int = PREC_FP64):
+        self._ck(self.L.cfdv_form(self._ctx, float(dt), int(precision)))
+
+    @staticmethod
+    def _opts(mode, m, restarts, rtol, precision, true_residual):
+        return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)))
+
+    def _report(self, m, restarts):
+        est = np.zeros(max(m * max(restarts, 1), 1))
+        fin = np.zeros(max(restarts, 1))
+        rep = _Report(0, 0, 0, est.size, _p(est).value, fin.size, _p(fin).value, 0, 0, -1.0)
+        return rep, est, fin
+
+    @staticmethod
+    def _unpack(rep, est, fin):
+        return {"tol": rep.tol, "bnorm": rep.bnorm, "est": est[: min(rep.n_est, est.size)].copy(),
+                "gfinal": fin[: min(rep.n_restarts, fin.size)].copy(), "restarts": rep.n_restarts,
+                "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
+
+    def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual)
+        rep, est, fin = self._report(m, restarts)
+        self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
+        return self._unpack(rep, est, fin)
+
+    def update(self):
+        self._ck(self.L.cfdv_update(self._ctx))
+
+    def rms(self):
+        r = np.zeros(self.neqn)
+        self._ck(self.L.cfdv_rms(self._ctx, _p(r)))
+        return r
+
+    def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
+             true_residual=False):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual)
+        rep, est, fin = self._report(m, restarts)
+        dt = C.c_double()
+        self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))
+        out = self._unpack(rep, est, fin)
+        out["dt"] = dt.value
+        return out
+
+    # -- inspection --
+    def fdv_params(self):
+        s = np.zeros((self.n_elements, 4))
+        self._ck(self.L.cfdv_get_fdv_params(self._ctx, _p(s)))
+        return s
+
+    def element_matrices(self):
+        R = np.zeros((self.n_elements, self.Ke, self.Ke))
+        rhs = np.zeros((self.n_elements, self.Ke))
+        self._ck(self.L.cfdv_get_element_matrices(self._ctx, _p(R), _p(rhs)))
+        return R, rhs
+
+    def rhs_vector(self):
+        b = np.zeros(self.n_dof)
+        self._ck(self.L.cfdv_get_rhs_vector(self._ctx, _p(b)))
+        return b
+
+    def du(self):
+        d = np.zeros(self.n_dof)
+        self._ck(self.L.cfdv_get_du(self._ctx, _p(d)))
+        return d
+
+    def matvec(self, x, precision=PREC_FP64, transpose=False):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.n_dof)
+        self._ck(self.L.cfdv_matvec(self._ctx, _p(x), _p(y), int(precision), int(bool(transpose))))
+        return y
+
+    def profile(self, enable=True):
+        self._ck(self.L.cfdv_profile(self._ctx, int(bool(enable))))
+
+    def profile_read(self):
+        s = _Stats()
+        self._ck(self.L.cfdv_profile_read(self._ctx, C.byref(s)))
+        return {"launches": s.launches, "total_ms": s.total_ms, "bytes": s.bytes,
+                "form_launches": s.form_launches, "form_ms": s.form_ms,
+                "kernel_launches": s.kernel_launches}

@@ -1,0 +1,164 @@
+/* cfdv_gpu.h -- C ABI of the B200 FDV step library (libcfdv_gpu.so).
+ *
+ * Drop-in boundary for the per-step path of the CFDV driver (src/main.cpp:169-198):
+ *
+ *   reference call (CFDV src/)                           replaced by
+ *   ---------------------------------------------------  ----------------------------------
+ *   LoadBinaryData::read_nodes/read_elements             cfdv_create / cfdv_upload_mesh
+ *     (Utility/IO/ASCIItoBinary/LoadBinary.h:116-246)      + cfdv_load_node_records
+ *   CalcLength (FDV/Function/CalcLength.h:34-66)         inside cfdv_create
+ *   ClearElement + NodeUnpack (main.cpp:169-171)         fused into cfdv_cfl / cfdv_form
+ *   CFL (FDV/Function/MPI_CFL.h:124-134, main.cpp:179)   cfdv_cfl
+ *   FDVGalerkin over elements (main.cpp:185-186,         cfdv_form
+ *     FDV/FDVGalerkin.h:121-154) + ApplyBC (main.cpp:194,
+ *     FDV/Function/ApplyBC.h:131-250)
+ *   GMRESbase::iterate (Utility/Solvers/GMRESbase.h:16,  cfdv_gmres
+ *     MPI_GMRES.h:125-220)
+ *   GMRESbase::update (GMRESbase.h:21, MPI_GMRES.h:224)  cfdv_update
+ *   RMSErr (MPIBinaryConfiguration.h:138-142,            cfdv_rms
+ *     FDV/Function/MPI_RMSError.h:21-75)
+ *   MPI_TecplotOut s1..s4 (Utility/IO/MPI_TecplotOut.h)  cfdv_get_fdv_params + cfdv_get_state
+ *
+ * Conventions: every call returns 0 on success or a cfdv_status code; the message of
+ * the last failure is cfdv_last_error(ctx).  No exception crosses the boundary.  A
+ * context belongs to one host thread and one CUDA device (the current device at
+ * cfdv_create); all work is ordered on the context's stream and the library
+ * synchronises only where a result comes back to the host.  Layouts: U is node-major
+ * [n_nodes][neqn] (the reference's global DOF order neqn*node + eq); element
+ * matrices are column-major per element, R_e(i,j) at R[e*Ke*Ke + j*Ke + i]
+ * (Utility/Tensor.h:89-92), with Ke = nnod*neqn.
+ */
+#ifndef CFDV_GPU_H
+#define CFDV_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cfdv_ctx cfdv_ctx;
+
+typedef enum {
+  CFDV_OK = 0,
+  CFDV_ERR_ARG = 1,        /* bad argument or size */
+  CFDV_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+  CFDV_ERR_MESH = 3,       /* degenerate or inverted element / face */
+  CFDV_ERR_NONFINITE = 4,  /* NaN/Inf in an element matrix, rhs or Krylov scalar */
+  CFDV_ERR_ALLOC = 5,      /* device allocation failed */
+  CFDV_ERR_STATE = 6,      /* call out of order (e.g. cfdv_gmres before cfdv_form) */
+  CFDV_ERR_NOT_CONVERGED = 7
+} cfdv_status;
+
+/* Mesh as the reference loads it (LoadBinary.h:156-246): 0-based node ids, the
+ * element's nnod node ids in reference order, and nface boundary codes per element
+ * (0 = interior face).  2D: nnod 4, nface 4; 3D: nnod 8, nface 6. */
+typedef struct {
+  int ndim;        /* 2 or 3 */
+  int n_nodes;
+  int n_elements;
+  const double* x; /* [n_nodes][ndim] */
+  const int* conn; /* [n_elements][nnod] */
+  const int* bc;   /* [n_elements][nface] */
+} cfdv_mesh;
+
+/* aero + control parameters (MPIBinaryConfiguration.h:29-69, Thermo.h:158-169) */
+typedef struct {
+  double gamma, mach, reynolds, prandtl, tinf, twall;
+  int adiabatic;
+  int physical_3d_flux; /* 0: as the reference (3D convective flux F = 0); 1: F evaluated */
+} cfdv_params;
+
+typedef enum { CFDV_PREC_FP64 = 0, CFDV_PREC_MIXED = 1 } cfdv_precision;
+typedef enum { CFDV_GMRES_REFERENCE = 0, CFDV_GMRES_CORRECT = 1 } cfdv_gmres_mode;
+
+typedef struct {
+  int mode;       /* cfdv_gmres_mode: REFERENCE reproduces MPI_GMRES::iterate (restart count,
+                     tol = ||b||*1e-9 inner break, rotate_and_check, back substitution);
+                     CORRECT is restarted GMRES(m), MGS + Givens, to rtol */
+  int m;          /* Krylov dimension (control "gmresiter") */
+  int restarts;   /* REFERENCE: restart count (control "gmresrestart"); CORRECT: maximum */
+  double rtol;    /* CORRECT: stop when ||b - A du|| / ||b|| < rtol */
+  int precision;  /* cfdv_precision: MIXED = FP32 element matrices and matvec inside
+                     FP64 iterative refinement (CORRECT mode only) */
+  int true_residual; /* 1: report ||b - A du||/||b|| with an extra FP64 product */
+} cfdv_gmres_opts;
+
+typedef struct {
+  double tol;          /* REFERENCE: ||b||*1e-9 ; CORRECT: rtol*||b|| */
+  double bnorm;
+  int n_est;           /* inner-iteration Givens residual estimates written to est */
+  int est_capacity;    /* caller buffer sizes */
+  double* est;
+  int gfinal_capacity;
+  double* gfinal;      /* g(m) after each restart's rotation (MPI_GMRES.h:202-203) */
+  int n_restarts;
+  int n_matvec;        /* EBE products issued */
+  double true_rel_res; /* when requested */
+} cfdv_gmres_report;
+
+/* ---- lifetime --------------------------------------------------------------- */
+/* Create a context on the current CUDA device; uploads the mesh, builds the Dirichlet
+ * row masks of ApplyBC (flags per LoadBinary.h:264-318), the node->element CSR used by
+ * the scatter, and element lengths (CalcLength.h:34-66). */
+int cfdv_create(const cfdv_mesh* mesh, const cfdv_params* params, cfdv_ctx** out);
+/* Replace the mesh (e.g. after host-side refinement); state and matrices are reset. */
+int cfdv_upload_mesh(cfdv_ctx* ctx, const cfdv_mesh* mesh);
+void cfdv_destroy(cfdv_ctx* ctx);
+const char* cfdv_last_error(const cfdv_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for event timing by the caller. */
+int cfdv_get_stream(cfdv_ctx* ctx, void** stream);
+
+/* ---- state ------------------------------------------------------------------ */
+/* Upload conserved U [n_nodes*neqn] from host memory. */
+int cfdv_set_state(cfdv_ctx* ctx, const double* U, size_t n);
+/* Set U from binary node records {x[ndim], rho, v[ndim], T} (LoadBinary.h:156-205). */
+int cfdv_load_node_records(cfdv_ctx* ctx, const double* records, size_t n_nodes);
+/* Read U and U0 (state before the last update); either pointer may be NULL. */
+int cfdv_get_state(cfdv_ctx* ctx, double* U, double* U0, size_t n);
+/* Device pointer of U (resident state; valid until the context is destroyed). */
+int cfdv_state_device_ptr(cfdv_ctx* ctx, double** U);
+
+/* ---- the step --------------------------------------------------------------- */
+/* dt = cfl * min_e min_nodes cleng/(|v| + sqrt(1.4 cgas T)) (MPI_CFL.h:124-171). */
+int cfdv_cfl(cfdv_ctx* ctx, double cfl, double* dt);
+/* Element LHS/RHS at time step dt with ApplyBC; precision MIXED also keeps FP32
+ * copies of the matrices for the FP32 products. */
+int cfdv_form(cfdv_ctx* ctx, double dt, int precision);
+/* Solve for dU from the formed matrices (GMRESbase::iterate). */
+int cfdv_gmres(cfdv_ctx* ctx, const cfdv_gmres_opts* opts, cfdv_gmres_report* report);
+/* U0 = U; U += dU (GMRESbase::update). */
+int cfdv_update(cfdv_ctx* ctx);
+/* Per-field RMS change sqrt(sum U^2 / sum U0^2) - 1 (MPI_RMSError.h:46-52), rms[neqn]. */
+int cfdv_rms(cfdv_ctx* ctx, double* rms);
+/* cfdv_cfl + cfdv_form + cfdv_gmres + cfdv_update in the driver's order (main.cpp:179-197). */
+int cfdv_step(cfdv_ctx* ctx, double cfl, const cfdv_gmres_opts* opts, cfdv_gmres_report* report, double* dt);
+
+/* ---- inspection (tests, output) --------------------------------------------- */
+/* s1..s4 per element [n_elements][4] from the last cfdv_form (Tecplot cell data). */
+int cfdv_get_fdv_params(cfdv_ctx* ctx, double* s);
+/* Element matrices [E][Ke*Ke] (FP64) and rhs [E][Ke] from the last cfdv_form. */
+int cfdv_get_element_matrices(cfdv_ctx* ctx, double* R, double* rhs);
+/* Assembled rhs b [n_nodes*neqn] (MPI_GMRES::compose_rhs, MPI_GMRES.h:369-438). */
+int cfdv_get_rhs_vector(cfdv_ctx* ctx, double* b);
+/* dU of the last solve [n_nodes*neqn]. */
+int cfdv_get_du(cfdv_ctx* ctx, double* du);
+/* y = A x (transpose = 1: A^T x) with the formed matrices, host vectors. */
+int cfdv_matvec(cfdv_ctx* ctx, const double* x, double* y, int precision, int transpose);
+
+/* ---- measurement -------------------------------------------------------------- */
+typedef struct {
+  long launches;      /* element-pass launches of the EBE product while profiling */
+  double total_ms;    /* their summed device time (CUDA events on the context stream) */
+  double bytes;       /* algorithmic bytes of those launches: E*Ke^2*s_R + DOF*8 + E*Ke*s_R each */
+  long form_launches;
+  double form_ms;
+  long kernel_launches; /* every kernel this context launched since cfdv_profile() */
+} cfdv_kernel_stats;
+int cfdv_profile(cfdv_ctx* ctx, int enable);
+int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDV_GPU_H */

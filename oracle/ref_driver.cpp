@@ -162,6 +162,7 @@ int main(int argc, char** argv) {
   double t = 0, dt = 0, t_form = 0, t_gmres = 0;
   std::cout.precision(17);
   for (int iter = 0; iter < nsteps; iter++) {
+    auto t_step0 = std::chrono::steady_clock::now();
     for_each(elements.begin(), elements.end(), ClearElement<Element*>());  // main.cpp:169
     for_each(nodes.begin(), nodes.end(), NodeUnpack<Node*>());             // main.cpp:171
     double cfl_v = cfl;
@@ -237,6 +238,8 @@ int main(int argc, char** argv) {
       rms[k] = (b == 0) ? 1.0 : std::sqrt(a / b) - 1.0;
     }
     rf.putd("rms" + sfx, rms);
+    // wall time of the step's path: CFL, formation, ApplyBC, GMRES, update
+    rf.putd("steptime" + sfx, {std::chrono::duration<double>(t2 - t_step0).count()});
     t += dt;
     if (!quiet) fprintf(stderr, "step %d dt %.6e gfinal %.3e\n", iter, dt, fin.empty() ? -1.0 : fin.back());
   }

@@ -1,0 +1,54 @@
+// Test-only CPU emulation of the element-formation thread block.
+//
+// Runs the host/device phase functions of cfdv_b200/csrc/formation.cuh thread by
+// thread, with each __syncthreads() of the CUDA kernel becoming a phase boundary,
+// so the kernel's index arithmetic and algebra can be checked against the oracle
+// without a GPU.  Used only by tests/test_form_emulated.py; the product library
+// never contains or calls it.
+#include <cstring>
+#include <vector>
+
+#include "../../cfdv_b200/csrc/formation.cuh"
+
+using namespace cfdv;
+
+template <int NDIM>
+static int run(const FormArgs& a) {
+  using T = FormTraits<NDIM>;
+  int bad = 0;
+  std::vector<FormRegs<NDIM>> rg(T::THREADS);
+  FormShared<NDIM>* sh = new FormShared<NDIM>;
+  for (int e = 0; e < a.n_elements; e++) {
+    std::memset(sh, 0xff, sizeof(*sh));  // garbage in shared memory, as on the device
+    for (int t = 0; t < T::THREADS; t++) phase_load<NDIM>(a, *sh, e, t);
+    for (int q = 0; q < T::Q; q++) phase_domain_gp<NDIM>(a, *sh, q);
+    for (int t = 0; t < T::THREADS; t++) phase_hmat<NDIM>(a, *sh, T::Q, 1.0, t);
+    for (int t = 0; t < T::THREADS; t++) phase_contract_domain<NDIM>(*sh, t, rg[t]);
+    for (int lf = 0; lf < sh->nfaces; lf++) {
+      for (int q = 0; q < T::QF; q++) phase_face_gp<NDIM>(a, *sh, lf, q);
+      for (int t = 0; t < T::THREADS; t++) phase_hmat<NDIM>(a, *sh, T::QF, -1.0, t);
+      for (int t = 0; t < T::THREADS; t++) phase_contract_face<NDIM>(*sh, lf, t, rg[t]);
+    }
+    for (int t = 0; t < T::THREADS; t++) phase_stage<NDIM>(*sh, t, rg[t]);
+    for (int t = 0; t < T::THREADS; t++) phase_write<NDIM>(a, *sh, e, t, rg[t], &bad);
+  }
+  delete sh;
+  return bad;
+}
+
+extern "C" int emu_form(int ndim, int n_elements, const double* U, const double* x, const int* conn, const int* bc,
+                        const uint64_t* rowmask, double gamma, double M, double Re, double Pr, double Tinf,
+                        double Tw, int adiabatic, double dt, int physical_3d_flux, double* R64, float* R32,
+                        double* rhs, double* s_out) {
+  FormArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.gas = make_gas(gamma, M, Re, Pr, Tinf, Tw, adiabatic);
+  a.dt = dt;
+  a.dtsq_2 = dt * dt / 2.0;
+  gauss_legendre(2, a.gz, a.gw);
+  a.n_elements = n_elements;
+  a.physical_3d_flux = physical_3d_flux;
+  a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
+  a.R64 = R64; a.R32 = R32; a.rhs = rhs; a.s_out = s_out;
+  return ndim == 2 ? run<2>(a) : run<3>(a);
+}
