@@ -16,12 +16,33 @@
 
 namespace cfdv {
 
+// Round-to-nearest arithmetic that the compiler may not contract into FMA.  The
+// Gauss-point state feeds exact-zero tests of the reference (gamma == 0, R == 0,
+// S == 0 in FDVGalerkin.h:308-379); evaluating it with the reference's operation
+// order and without contraction makes those decisions agree with the reference.
+#if defined(__CUDA_ARCH__)
+#define RN_MUL(a, b) __dmul_rn((a), (b))
+#define RN_ADD(a, b) __dadd_rn((a), (b))
+#define RN_SUB(a, b) __dsub_rn((a), (b))
+#define RN_DIV(a, b) __ddiv_rn((a), (b))
+#else
+// host: separate calls so that no host compiler setting can fuse them either
+__attribute__((noinline)) inline double rn_mul(double a, double b) { return a * b; }
+__attribute__((noinline)) inline double rn_add(double a, double b) { return a + b; }
+__attribute__((noinline)) inline double rn_sub(double a, double b) { return a - b; }
+__attribute__((noinline)) inline double rn_div(double a, double b) { return a / b; }
+#define RN_MUL(a, b) ::cfdv::rn_mul((a), (b))
+#define RN_ADD(a, b) ::cfdv::rn_add((a), (b))
+#define RN_SUB(a, b) ::cfdv::rn_sub((a), (b))
+#define RN_DIV(a, b) ::cfdv::rn_div((a), (b))
+#endif
+
 #define JA(t, i, r, s) (t)[((i)*5 + (r)) * 5 + (s)]
 #define JC(t, i, j, r, s) (t)[(((i)*3 + (j)) * 5 + (r)) * 5 + (s)]
 
 CFDV_HD CFDV_INLINE double gas_mu(const GasParams& g, double T) {
   if (T < 1.0E-12) return 1.0;
-  return ((1 + g.csuth) / (T + g.csuth)) * T * sqrt(T);
+  return RN_MUL(RN_MUL(RN_DIV(1 + g.csuth, RN_ADD(T, g.csuth)), T), sqrt(T));
 }
 CFDV_HD CFDV_INLINE double gas_k(const GasParams& g, double mu) {
   return mu / ((g.gamma - 1.0) * (g.cmach * g.cmach) * g.Pr);
@@ -43,13 +64,13 @@ CFDV_HD CFDV_INLINE void node_unpack(const GasParams& g, const double* U, const 
   double vsqr = 0;
 #pragma unroll
   for (int i = 0; i < NDIM; i++) {
-    n.v[i] = U[1 + i] / U[0];
-    vsqr += n.v[i] * n.v[i];
+    n.v[i] = RN_DIV(U[1 + i], U[0]);
+    vsqr = RN_ADD(vsqr, RN_MUL(n.v[i], n.v[i]));
   }
-  n.E = U[NDIM + 1] / U[0];
-  double e = n.E - 0.5 * vsqr;
-  n.T = e / g.Cv;
-  n.p = n.rho * (g.gamma - 1.0) * e;
+  n.E = RN_DIV(U[NDIM + 1], U[0]);
+  double e = RN_SUB(n.E, RN_MUL(0.5, vsqr));
+  n.T = RN_DIV(e, g.Cv);
+  n.p = RN_MUL(RN_MUL(n.rho, g.gamma - 1.0), e);
 }
 
 // shape functions and natural-coordinate derivatives
@@ -96,18 +117,18 @@ CFDV_HD CFDV_INLINE double phys_deriv<2>(const double (*dPxi)[3], const NodePrim
   double j00 = 0, j01 = 0, j10 = 0, j11 = 0;
 #pragma unroll
   for (int N = 0; N < 4; N++) {
-    j00 += dPxi[N][0] * nd[N].x[0];
-    j01 += dPxi[N][1] * nd[N].x[0];
-    j10 += dPxi[N][0] * nd[N].x[1];
-    j11 += dPxi[N][1] * nd[N].x[1];
+    j00 = RN_ADD(j00, RN_MUL(dPxi[N][0], nd[N].x[0]));
+    j01 = RN_ADD(j01, RN_MUL(dPxi[N][1], nd[N].x[0]));
+    j10 = RN_ADD(j10, RN_MUL(dPxi[N][0], nd[N].x[1]));
+    j11 = RN_ADD(j11, RN_MUL(dPxi[N][1], nd[N].x[1]));
   }
   jac[0][0] = j00; jac[0][1] = j01; jac[1][0] = j10; jac[1][1] = j11;
-  const double J = j00 * j11 - j10 * j01;
-  const double iJ = 1.0 / J;
+  const double J = RN_SUB(RN_MUL(j00, j11), RN_MUL(j10, j01));
+  const double iJ = RN_DIV(1.0, J);
 #pragma unroll
   for (int N = 0; N < 4; N++) {
-    dPhi[N][0] = iJ * (dPxi[N][0] * j11 - j10 * dPxi[N][1]);
-    dPhi[N][1] = iJ * (j00 * dPxi[N][1] - dPxi[N][0] * j01);
+    dPhi[N][0] = RN_MUL(iJ, RN_SUB(RN_MUL(dPxi[N][0], j11), RN_MUL(j10, dPxi[N][1])));
+    dPhi[N][1] = RN_MUL(iJ, RN_SUB(RN_MUL(j00, dPxi[N][1]), RN_MUL(dPxi[N][0], j01)));
   }
   return J;
 }
@@ -121,25 +142,33 @@ CFDV_HD CFDV_INLINE double phys_deriv<3>(const double (*dPxi)[3], const NodePrim
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-      for (int k = 0; k < 3; k++) j[i][k] += dPxi[N][k] * nd[N].x[i];
-  const double J = j[0][0] * j[1][1] * j[2][2] + j[0][1] * j[1][2] * j[2][0] + j[0][2] * j[1][0] * j[2][1] -
-                   j[0][2] * j[1][1] * j[2][0] - j[0][1] * j[1][0] * j[2][2] - j[0][0] * j[1][2] * j[2][1];
+      for (int k = 0; k < 3; k++) j[i][k] = RN_ADD(j[i][k], RN_MUL(dPxi[N][k], nd[N].x[i]));
+#define M3(a, b, c) RN_MUL(RN_MUL(a, b), c)
+  const double J = RN_SUB(RN_SUB(RN_SUB(RN_ADD(RN_ADD(M3(j[0][0], j[1][1], j[2][2]), M3(j[0][1], j[1][2], j[2][0])),
+                                               M3(j[0][2], j[1][0], j[2][1])),
+                                        M3(j[0][2], j[1][1], j[2][0])),
+                                 M3(j[0][1], j[1][0], j[2][2])),
+                          M3(j[0][0], j[1][2], j[2][1]));
+#undef M3
+#define D2(a, b, c, d) RN_SUB(RN_MUL(a, b), RN_MUL(c, d))
   double inv[3][3];
-  inv[0][0] = j[1][1] * j[2][2] - j[1][2] * j[2][1];
-  inv[0][1] = -(j[1][0] * j[2][2] - j[1][2] * j[2][0]);
-  inv[0][2] = j[1][0] * j[2][1] - j[1][1] * j[2][0];
-  inv[1][0] = -(j[0][1] * j[2][2] - j[0][2] * j[2][1]);
-  inv[1][1] = j[0][0] * j[2][2] - j[0][2] * j[2][0];
-  inv[1][2] = -(j[0][0] * j[2][1] - j[0][1] * j[2][0]);
-  inv[2][0] = j[0][1] * j[1][2] - j[0][2] * j[1][1];
-  inv[2][1] = -(j[0][0] * j[1][2] - j[0][2] * j[1][0]);
-  inv[2][2] = j[0][0] * j[1][1] - j[0][1] * j[1][0];
-  const double iJ = 1.0 / J;
+  inv[0][0] = D2(j[1][1], j[2][2], j[1][2], j[2][1]);
+  inv[0][1] = -D2(j[1][0], j[2][2], j[1][2], j[2][0]);
+  inv[0][2] = D2(j[1][0], j[2][1], j[1][1], j[2][0]);
+  inv[1][0] = -D2(j[0][1], j[2][2], j[0][2], j[2][1]);
+  inv[1][1] = D2(j[0][0], j[2][2], j[0][2], j[2][0]);
+  inv[1][2] = -D2(j[0][0], j[2][1], j[0][1], j[2][0]);
+  inv[2][0] = D2(j[0][1], j[1][2], j[0][2], j[1][1]);
+  inv[2][1] = -D2(j[0][0], j[1][2], j[0][2], j[1][0]);
+  inv[2][2] = D2(j[0][0], j[1][1], j[0][1], j[1][0]);
+#undef D2
+  const double iJ = RN_DIV(1.0, J);
 #pragma unroll
   for (int N = 0; N < 8; N++)
 #pragma unroll
-    for (int i = 0; i < 3; i++) dPhi[N][i] = iJ * (inv[i][0] * dPxi[N][0]) + iJ * (inv[i][1] * dPxi[N][1]) +
-                                             iJ * (inv[i][2] * dPxi[N][2]);
+    for (int i = 0; i < 3; i++)
+      dPhi[N][i] = RN_ADD(RN_ADD(RN_MUL(iJ, RN_MUL(inv[i][0], dPxi[N][0])), RN_MUL(iJ, RN_MUL(inv[i][1], dPxi[N][1]))),
+                          RN_MUL(iJ, RN_MUL(inv[i][2], dPxi[N][2])));
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -171,20 +200,20 @@ CFDV_HD CFDV_INLINE void gp_state(const GasParams& g, int nn, const NodePrim* co
   }
   for (int N = 0; N < nn; N++) {
     const NodePrim& n = *nd[N];
-    f.E += Phi[N] * n.E;
-    f.T += Phi[N] * n.T;
+    f.E = RN_ADD(f.E, RN_MUL(Phi[N], n.E));
+    f.T = RN_ADD(f.T, RN_MUL(Phi[N], n.T));
 #pragma unroll
     for (int i = 0; i < NEQ; i++) {
-      f.U[i] += Phi[N] * n.U[i];
+      f.U[i] = RN_ADD(f.U[i], RN_MUL(Phi[N], n.U[i]));
 #pragma unroll
-      for (int j = 0; j < NDIM; j++) f.dU[i][j] += dPhi[N][j] * n.U[i];
+      for (int j = 0; j < NDIM; j++) f.dU[i][j] = RN_ADD(f.dU[i][j], RN_MUL(dPhi[N][j], n.U[i]));
     }
 #pragma unroll
     for (int i = 0; i < NDIM; i++) {
-      f.v[i] += Phi[N] * n.v[i];
-      f.dT[i] += dPhi[N][i] * n.T;
+      f.v[i] = RN_ADD(f.v[i], RN_MUL(Phi[N], n.v[i]));
+      f.dT[i] = RN_ADD(f.dT[i], RN_MUL(dPhi[N][i], n.T));
 #pragma unroll
-      for (int d = 0; d < NDIM; d++) f.dV[i][d] += dPhi[N][d] * n.v[i];
+      for (int d = 0; d < NDIM; d++) f.dV[i][d] = RN_ADD(f.dV[i][d], RN_MUL(dPhi[N][d], n.v[i]));
     }
   }
   f.mu = gas_mu(g, f.T);
@@ -195,13 +224,13 @@ template <int NDIM>
 CFDV_HD CFDV_INLINE void viscous_stress(GpState& f) {
   double vkk = 0;
 #pragma unroll
-  for (int k = 0; k < NDIM; k++) vkk += f.dV[k][k];
+  for (int k = 0; k < NDIM; k++) vkk = RN_ADD(vkk, f.dV[k][k]);
 #pragma unroll
   for (int i = 0; i < NDIM; i++)
 #pragma unroll
     for (int j = 0; j < NDIM; j++) {
-      double t = f.mu * (f.dV[i][j] + f.dV[j][i]);
-      if (i == j) t -= (2.0 / 3.0) * f.mu * vkk;
+      double t = RN_MUL(f.mu, RN_ADD(f.dV[i][j], f.dV[j][i]));
+      if (i == j) t = RN_SUB(t, RN_MUL(RN_MUL(2.0 / 3.0, f.mu), vkk));
       f.tau[i][j] = t;
     }
 }

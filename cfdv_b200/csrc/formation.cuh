@@ -114,25 +114,25 @@ CFDV_HD CFDV_INLINE void fdv_params(const GasParams& g, const NodePrim* nd, doub
   double M_min = 0, M_max = 0, Re_min = 0, Re_max = 0;
   for (int b = 0; b < T::NNOD; b++) {
     double vv = 0;
-    for (int i = 0; i < NDIM; i++) vv += nd[b].v[i] * nd[b].v[i];
+    for (int i = 0; i < NDIM; i++) vv = RN_ADD(vv, RN_MUL(nd[b].v[i], nd[b].v[i]));
     const double V = sqrt(vv);
     double Tn = nd[b].T;
     if (Tn < 1.0E-12) Tn = 0;
-    const double snd = sqrt(g.gamma * g.cgas * Tn);
-    const double M = (snd < 1.0E-12) ? 0 : V / snd;
-    const double Re = (nd[b].rho * V) / gas_mu(g, Tn);
+    const double snd = sqrt(RN_MUL(RN_MUL(g.gamma, g.cgas), Tn));
+    const double M = (snd < 1.0E-12) ? 0 : RN_DIV(V, snd);
+    const double Re = RN_DIV(RN_MUL(nd[b].rho, V), gas_mu(g, Tn));
     if (b == 0) { M_max = M; M_min = M; Re_max = Re; Re_min = Re; }
     M_max = fmax(M_max, M); M_min = fmin(M_min, M);
     Re_max = fmax(Re_max, Re); Re_min = fmin(Re_min, Re);
   }
   const double eps = 0.0000001;
   // the Mach spread stays in FP64: M_max ~ M_min cancels
-  double r = sqrt(M_max * M_max - M_min * M_min) / (M_min + eps);
+  double r = RN_DIV(sqrt(RN_SUB(RN_MUL(M_max, M_max), RN_MUL(M_min, M_min))), RN_ADD(M_min, eps));
   double s1 = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
   if (r > 0.01) s1 = fmin(r, 1.0);
   else if (r < 0.01 && M_min >= 10E-10) s1 = 0;
   else if (M_min < 10E-10) s1 = 1.0;
-  r = sqrt(Re_max * Re_max - Re_min * Re_min) / (Re_min + eps);
+  r = RN_DIV(sqrt(RN_SUB(RN_MUL(Re_max, Re_max), RN_MUL(Re_min, Re_min))), RN_ADD(Re_min, eps));
   double s3 = 0.0;
   if (r > 0.01) s3 = fmin(r, 1.0);
   else if (r < 0.01 && Re_min >= 10E-10) s3 = 0.0;
@@ -190,32 +190,46 @@ CFDV_HD void phase_domain_gp(const FormArgs& a, FormShared<NDIM>& sh, int q) {
   double tau = 0.0;
   for (int N = 0; N < NNOD; N++) sl.Psi[N] = 0.0;
   if (NDIM == 2) {  // streamline-upwind numerical diffusion (FDVGalerkin.h:225-332)
-    const double J_xi = jac[0][0] * jac[0][0] + jac[1][0] * jac[1][0];
-    const double J_eta = jac[0][1] * jac[0][1] + jac[1][1] * jac[1][1];
-    const double ixi = 1. / sqrt(J_xi), ieta = 1. / sqrt(J_eta);
-    const double v_xi = f.v[0] * (ixi * jac[0][0]) + f.v[1] * (ixi * jac[1][0]);
-    const double v_eta = f.v[0] * (ieta * jac[0][1]) + f.v[1] * (ieta * jac[1][1]);
-    const double S = f.v[0] * f.v[0] + f.v[1] * f.v[1];
-    // element extents between opposite edge midpoints (eta extent taken bottom - top)
-    const double h_xi = 0.5 * (sh.nd[1].x[0] + sh.nd[2].x[0]) - 0.5 * (sh.nd[0].x[0] + sh.nd[3].x[0]);
-    const double h_eta = 0.5 * (sh.nd[0].x[1] + sh.nd[1].x[1]) - 0.5 * (sh.nd[2].x[1] + sh.nd[3].x[1]);
-    const double R_xi = f.U[0] * v_xi * h_xi / f.mu;
-    const double R_eta = f.U[0] * v_eta * h_eta / f.mu;
-    const double al_xi = (R_xi == 0) ? 0.0 : cosh(R_xi / 2.) / sinh(R_xi / 2.) - 2. / R_xi;
-    const double al_eta = (R_eta == 0) ? 0.0 : cosh(R_eta / 2.) / sinh(R_eta / 2.) - 2. / R_eta;
-    tau = (S == 0) ? 0.0 : 0.25 * (al_xi * h_xi * v_xi + al_eta * h_eta * v_eta) / S;
-    for (int N = 0; N < NNOD; N++) sl.Psi[N] = tau * (f.v[0] * sl.dPhi[N][0] + f.v[1] * sl.dPhi[N][1]);
+    // evaluated in the reference's operation order without contraction (RN_*), because
+    // the exact-zero tests below decide whether a term is present at all
+    const double J_xi = RN_ADD(RN_MUL(jac[0][0], jac[0][0]), RN_MUL(jac[1][0], jac[1][0]));
+    const double J_eta = RN_ADD(RN_MUL(jac[0][1], jac[0][1]), RN_MUL(jac[1][1], jac[1][1]));
+    const double ixi = RN_DIV(1., sqrt(J_xi)), ieta = RN_DIV(1., sqrt(J_eta));
+    const double v_xi = RN_ADD(RN_MUL(f.v[0], RN_MUL(ixi, jac[0][0])), RN_MUL(f.v[1], RN_MUL(ixi, jac[1][0])));
+    const double v_eta = RN_ADD(RN_MUL(f.v[0], RN_MUL(ieta, jac[0][1])), RN_MUL(f.v[1], RN_MUL(ieta, jac[1][1])));
+    const double S = RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]));
+    // element extents between opposite edge midpoints, accumulated node by node with the
+    // edge-midpoint interpolants (the eta extent is taken bottom minus top)
+    const NodePrim* q4 = sh.nd;
+    const double h_xi =
+        RN_SUB(RN_ADD(RN_ADD(-RN_MUL(0.5, q4[0].x[0]), RN_MUL(0.5, q4[1].x[0])), RN_MUL(0.5, q4[2].x[0])),
+               RN_MUL(0.5, q4[3].x[0]));
+    const double h_eta =
+        RN_SUB(RN_SUB(RN_ADD(RN_MUL(0.5, q4[0].x[1]), RN_MUL(0.5, q4[1].x[1])), RN_MUL(0.5, q4[2].x[1])),
+               RN_MUL(0.5, q4[3].x[1]));
+    const double R_xi = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_xi), h_xi), f.mu);
+    const double R_eta = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_eta), h_eta), f.mu);
+    const double al_xi = (R_xi == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_xi / 2.), sinh(R_xi / 2.)), RN_DIV(2., R_xi));
+    const double al_eta = (R_eta == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_eta / 2.), sinh(R_eta / 2.)), RN_DIV(2., R_eta));
+    tau = (S == 0) ? 0.0
+                   : RN_DIV(RN_MUL(0.25, RN_ADD(RN_MUL(RN_MUL(al_xi, h_xi), v_xi), RN_MUL(RN_MUL(al_eta, h_eta), v_eta))),
+                            S);
+    for (int N = 0; N < NNOD; N++)
+      sl.Psi[N] = RN_ADD(RN_MUL(RN_MUL(tau, f.v[0]), sl.dPhi[N][0]), RN_MUL(RN_MUL(tau, f.v[1]), sl.dPhi[N][1]));
     // discontinuity capturing (FDVGalerkin.h:336-387); in 3D tau = 0 makes it vanish
     double A[2] = {0, 0};
     for (int k = 0; k < 2; k++)
-      for (int j = 0; j < 2; j++) A[j] += f.dV[j][k] * f.v[k];
-    const double gam = sqrt(f.v[0] * f.v[0] + f.v[1] * f.v[1]) * sqrt(A[0] * A[0] + A[1] * A[1]);
+      for (int j = 0; j < 2; j++) A[j] = RN_ADD(A[j], RN_MUL(f.dV[j][k], f.v[k]));
+    const double gam = RN_MUL(sqrt(RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]))),
+                              sqrt(RN_ADD(RN_MUL(A[0], A[0]), RN_MUL(A[1], A[1]))));
     double tau_b = 0.0;
     if (gam != 0) {
-      tau_b = tau * f.v[0] * A[0] / gam + tau * f.v[1] * A[1] / gam;
-      if ((tau_b - tau) < 0) tau_b = tau;
+      tau_b = RN_ADD(RN_DIV(RN_MUL(RN_MUL(tau, f.v[0]), A[0]), gam), RN_DIV(RN_MUL(RN_MUL(tau, f.v[1]), A[1]), gam));
+      if (RN_SUB(tau_b, tau) < 0) tau_b = tau;
     }
-    for (int N = 0; N < NNOD; N++) sl.Psi[N] += tau_b * (f.v[0] * sl.dPhi[N][0] + f.v[1] * sl.dPhi[N][1]);
+    for (int N = 0; N < NNOD; N++)
+      sl.Psi[N] = RN_ADD(RN_ADD(sl.Psi[N], RN_MUL(RN_MUL(tau_b, f.v[0]), sl.dPhi[N][0])),
+                         RN_MUL(RN_MUL(tau_b, f.v[1]), sl.dPhi[N][1]));
   }
 
   gp_jacobians<NDIM>(a, f, s, sl);

@@ -1,0 +1,238 @@
+// Host side of the B200 FDV path, in C++ over the C ABI (include/cfdv_gpu.h).
+//
+// These classes stand where the reference driver's objects stand:
+//   CaseConfig   control/aero files      (MPIBinaryConfiguration.h:29-69)
+//   BinaryCase   binarynodes/elements    (Utility/IO/ASCIItoBinary/LoadBinary.h:116-246)
+//   GpuFDV       element formation + GMRES on the device: the FDVGalerkin/ApplyBC loop
+//                (main.cpp:185-194) and the GMRESbase plug-in point
+//                (Utility/Solvers/GMRESbase.h:8-23: iterate(), update())
+//   TecplotOut   tecplot_<iter>.plt      (Utility/IO/MPI_TecplotOut.h:186-373)
+//   RmsLog       RMSError.txt            (FDV/Function/MPI_RMSError.h:56-75)
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cfdv_gpu.h"
+
+namespace cfdv_host {
+
+struct CaseConfig {
+  std::map<std::string, std::string> control, aero;
+  static std::map<std::string, std::string> parse(const std::string& path) {
+    std::map<std::string, std::string> kv;
+    std::ifstream in(path.c_str());
+    if (!in) throw std::runtime_error("cannot open " + path);
+    std::string line;
+    while (std::getline(in, line)) {
+      size_t c = line.find_first_of("!#");
+      if (c != std::string::npos) line = line.substr(0, c);
+      size_t eq = line.find('=');
+      if (eq == std::string::npos) continue;
+      auto trim = [](const std::string& s) {
+        size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+        return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+      };
+      kv[trim(line.substr(0, eq))] = trim(line.substr(eq + 1));
+    }
+    return kv;
+  }
+  explicit CaseConfig(const std::string& dir) : control(parse(dir + "/control")), aero(parse(dir + "/aero")) {}
+  int ci(const char* k, int d) const { auto it = control.find(k); return it == control.end() ? d : std::stoi(it->second); }
+  double cd(const char* k, double d) const { auto it = control.find(k); return it == control.end() ? d : std::stod(it->second); }
+  double ad(const char* k, double d) const { auto it = aero.find(k); return it == aero.end() ? d : std::stod(it->second); }
+  cfdv_params params(int physical_3d_flux = 0) const {
+    cfdv_params p;
+    p.gamma = ad("gamma", 1.4);
+    p.mach = ad("M", 1.0);
+    p.reynolds = ad("Re", 1.0);
+    p.prandtl = ad("Pr", 0.72);
+    p.tinf = ad("Tinf", 216.6666);
+    p.twall = ad("Twall", 1.0);
+    auto it = aero.find("Adiabatic");
+    p.adiabatic = (it == aero.end()) ? 1 : (std::stod(it->second) != 0);
+    p.physical_3d_flux = physical_3d_flux;
+    return p;
+  }
+};
+
+// Binary node and element records, whole-file single-rank read (LoadBinary.h:156-246).
+struct BinaryCase {
+  int ndim = 0, nnod = 0, nface = 0, n_nodes = 0, n_elements = 0;
+  std::vector<double> records;  // [Nn][2*ndim+2]
+  std::vector<double> x;        // [Nn][ndim]
+  std::vector<int> conn, bc;
+
+  BinaryCase(const std::string& dir, const CaseConfig& cfg) {
+    ndim = cfg.ci("ndim", 2);
+    nnod = cfg.ci("nnod", ndim == 2 ? 4 : 8);
+    nface = ndim == 2 ? 4 : 6;
+    n_nodes = cfg.ci("nodes", 0);
+    n_elements = cfg.ci("elements", 0);
+    const int rs = 2 * ndim + 2;
+    records.resize((size_t)n_nodes * rs);
+    read_all(dir + "/binarynodes", records.data(), records.size() * sizeof(double));
+    std::vector<int> el((size_t)n_elements * (nnod + nface));
+    read_all(dir + "/binaryelements", el.data(), el.size() * sizeof(int));
+    x.resize((size_t)n_nodes * ndim);
+    for (int n = 0; n < n_nodes; n++)
+      for (int k = 0; k < ndim; k++) x[(size_t)n * ndim + k] = records[(size_t)n * rs + k];
+    conn.resize((size_t)n_elements * nnod);
+    bc.resize((size_t)n_elements * nface);
+    for (int e = 0; e < n_elements; e++) {
+      for (int k = 0; k < nnod; k++) conn[(size_t)e * nnod + k] = el[(size_t)e * (nnod + nface) + k];
+      for (int k = 0; k < nface; k++) bc[(size_t)e * nface + k] = el[(size_t)e * (nnod + nface) + nnod + k];
+    }
+  }
+  static void read_all(const std::string& p, void* dst, size_t bytes) {
+    FILE* f = std::fopen(p.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open " + p);
+    size_t got = std::fread(dst, 1, bytes, f);
+    std::fclose(f);
+    if (got != bytes) throw std::runtime_error("short read of " + p);
+  }
+  cfdv_mesh mesh() const {
+    cfdv_mesh m;
+    m.ndim = ndim;
+    m.n_nodes = n_nodes;
+    m.n_elements = n_elements;
+    m.x = x.data();
+    m.conn = conn.data();
+    m.bc = bc.data();
+    return m;
+  }
+};
+
+inline void check(cfdv_ctx* ctx, int rc, const char* what) {
+  if (rc) throw std::runtime_error(std::string(what) + ": " + (ctx ? cfdv_last_error(ctx) : "") + " (status " +
+                                   std::to_string(rc) + ")");
+}
+
+// Device-resident FDV step: formation, GMRES solve and update behind the reference's
+// GMRESbase interface shape (iterate / update).
+class GpuFDV {
+ public:
+  GpuFDV(const BinaryCase& c, const cfdv_params& p) : ndim_(c.ndim), n_nodes_(c.n_nodes), n_el_(c.n_elements) {
+    cfdv_mesh m = c.mesh();
+    int rc = cfdv_create(&m, &p, &ctx_);
+    if (rc) {
+      std::string msg = ctx_ ? cfdv_last_error(ctx_) : "";
+      if (ctx_) cfdv_destroy(ctx_);
+      throw std::runtime_error("cfdv_create: " + msg);
+    }
+    check(ctx_, cfdv_load_node_records(ctx_, c.records.data(), c.n_nodes), "load_node_records");
+  }
+  ~GpuFDV() { cfdv_destroy(ctx_); }
+  GpuFDV(const GpuFDV&) = delete;
+  GpuFDV& operator=(const GpuFDV&) = delete;
+
+  double cfl(double cfl) { double dt; check(ctx_, cfdv_cfl(ctx_, cfl, &dt), "cfl"); return dt; }
+  void form(double dt, int precision) { check(ctx_, cfdv_form(ctx_, dt, precision), "form"); }
+  void iterate(const cfdv_gmres_opts& o, cfdv_gmres_report* rep) { check(ctx_, cfdv_gmres(ctx_, &o, rep), "gmres"); }
+  void update() { check(ctx_, cfdv_update(ctx_), "update"); }
+  std::vector<double> rms() {
+    std::vector<double> r(ndim_ + 2);
+    check(ctx_, cfdv_rms(ctx_, r.data()), "rms");
+    return r;
+  }
+  std::vector<double> state() {
+    std::vector<double> U((size_t)n_nodes_ * (ndim_ + 2));
+    check(ctx_, cfdv_get_state(ctx_, U.data(), nullptr, U.size()), "get_state");
+    return U;
+  }
+  // s1..s4 of the current state: formation at any dt gives them (they depend on U only)
+  std::vector<double> fdv_params() {
+    std::vector<double> s((size_t)n_el_ * 4);
+    check(ctx_, cfdv_get_fdv_params(ctx_, s.data()), "fdv_params");
+    return s;
+  }
+  cfdv_ctx* ctx() { return ctx_; }
+
+ private:
+  int ndim_, n_nodes_, n_el_;
+  cfdv_ctx* ctx_ = nullptr;
+};
+
+// "tecplot_<iter>.plt" in the reference's FE block layout and number format
+// (MPI_TecplotOut.h:189-371): primitives from NodeUnpack of U, cell-centred s1..s4.
+inline std::string tecplot_name(int iter) {
+  std::ostringstream s;
+  s << (double)iter;  // to_string<double>(iter): 1000000 prints as 1e+06
+  return "tecplot_" + s.str() + ".plt";
+}
+
+inline void tecplot_write(const std::string& path, const BinaryCase& c, const cfdv_params& p,
+                          const std::vector<double>& U, const std::vector<double>* s, double time) {
+  const int nd = c.ndim, ne = nd + 2, Nn = c.n_nodes;
+  const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
+  std::vector<double> rho(Nn), T(Nn), pr(Nn), v((size_t)Nn * nd);
+  for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:185-205
+    const double* u = &U[(size_t)n * ne];
+    rho[n] = u[0];
+    double vsqr = 0;
+    for (int i = 0; i < nd; i++) {
+      v[(size_t)n * nd + i] = u[1 + i] / u[0];
+      vsqr += v[(size_t)n * nd + i] * v[(size_t)n * nd + i];
+    }
+    const double E = u[nd + 1] / u[0], e = E - 0.5 * vsqr;
+    T[n] = e / Cv;
+    pr[n] = rho[n] * (p.gamma - 1.0) * e;
+  }
+  std::ofstream t(path.c_str());
+  const bool ele = (s != nullptr);
+  t << "title = \"Output at time = " << time << " \"" << std::endl;
+  t << "variables = \"x\", \"y\",";
+  if (nd == 3) t << " \"z\",";
+  t << "\"rho\", \"u\", \"v\",";
+  if (nd == 3) t << " \"w\",";
+  t << "\"T\", \"p\",";
+  if (ele) t << "\"s1\", \"s2\", \"s3\", \"s4\", ";
+  t << std::endl;
+  t << "zone E=" << c.n_elements << ", N=" << Nn;
+  t << ", DATAPACKING=BLOCK, ZONETYPE=FEQUADRILATERAL";  // nnod != 3
+  if (nd == 3) t << ", DATAPACKING=BLOCK, ZONETYPE=FEBRICK";
+  t << std::endl;
+  if (ele) t << (nd == 2 ? "VARLOCATION=([8,9,10,11]=CellCentered)" : "VARLOCATION=([10,11,12,13]=CellCentered)")
+             << std::endl;
+  t << std::endl;
+  t << std::scientific << std::endl;
+  t << std::setprecision(7) << std::endl;
+  auto block = [&](auto get, const char* sep) {
+    for (int n = 0; n < Nn; n++) {
+      t << get(n) << sep;
+      if (n % 100 == 0 && n != 0) t << std::endl;
+    }
+    t << std::endl;
+  };
+  for (int k = 0; k < nd; k++) block([&](int n) { return c.x[(size_t)n * nd + k]; }, " ");
+  block([&](int n) { return rho[n]; }, " ");
+  for (int k = 0; k < nd; k++) block([&](int n) { return v[(size_t)n * nd + k]; }, " ");
+  block([&](int n) { return T[n]; }, " ");
+  block([&](int n) { return pr[n]; }, "\t");
+  if (ele)
+    for (int k = 0; k < 4; k++)
+      for (int e = 0; e < c.n_elements; e++) {
+        t << (*s)[(size_t)e * 4 + k] << "\t";
+        if (e % 100 == 0 && e != 0) t << std::endl;
+      }
+  for (int e = 0; e < c.n_elements; e++) {
+    for (int k = 0; k < c.nnod; k++) t << c.conn[(size_t)e * c.nnod + k] + 1 << " ";
+    t << std::endl;
+  }
+}
+
+// one "iter\t(rms) " line per step (MPI_RMSError.h:56-69)
+inline void rms_append(const std::string& path, int iter, const std::vector<double>& rms) {
+  std::ofstream f(path.c_str(), std::ios::app);
+  f << iter << "\t";
+  for (double r : rms) f << r << " ";
+  f << std::endl;
+}
+
+}  // namespace cfdv_host

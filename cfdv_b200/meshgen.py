@@ -156,7 +156,11 @@ def plate(nx: int = 200, ny: int = 100, M: float = 3.0, Re: float = 1.0e4, cfl: 
     """Supersonic flat plate: x in [0, 1.1] with the adiabatic plate (bc 1) from x = 0.1 and
     symmetry (bc 2) ahead of it, inflow -1, top 7, outflow 6; y in [0, 0.75] stretched
     geometrically (ratio 1.05).  Freestream rho = 1, u = 1, T = 1 with seeded 1e-3 relative
-    Gaussian noise on rho at interior nodes; plate nodes at rest at the recovery temperature."""
+    Gaussian noise on rho at interior nodes.  Over the plate the start is a smooth
+    boundary-layer profile u = tanh(y / 0.005), T = Tr + (1 - Tr) u^2 (Tr the recovery
+    temperature), wall nodes at rest: with an exact linear solve, an impulsive start (wall
+    at rest next to freestream across the 3e-4 first cell) drives the density negative in
+    the first step."""
     n_lead = max(1, int(round(nx * 0.1 / 1.1)))
     xs = np.concatenate([np.linspace(0.0, 0.1, n_lead + 1)[:-1], np.linspace(0.1, 1.1, nx - n_lead + 1)])
     dy = np.array([ratio ** k for k in range(ny)])
@@ -170,9 +174,10 @@ def plate(nx: int = 200, ny: int = 100, M: float = 3.0, Re: float = 1.0e4, cfl: 
     v = np.zeros((Nn, 2))
     v[:, 0] = 1.0
     T = np.ones(Nn)
-    wall = np.isclose(xy[:, 1], 0.0) & (xy[:, 0] >= 0.1 - 1e-12)
-    v[wall] = 0.0
-    T[wall] = Trec
+    onplate = xy[:, 0] >= 0.1 - 1e-12
+    prof = np.tanh(xy[:, 1] / 0.005)
+    v[onplate, 0] = prof[onplate]
+    T[onplate] = Trec + (1.0 - Trec) * prof[onplate] ** 2
     interior = (xy[:, 0] > 0) & (xy[:, 0] < 1.1 - 1e-12) & (xy[:, 1] > 0) & (xy[:, 1] < 0.75 - 1e-12)
     rng = np.random.default_rng(SEED)
     rho[interior] *= 1.0 + noise * rng.standard_normal(int(interior.sum()))

@@ -13,6 +13,10 @@ from conftest import SMALL_CASES, get_case, golden, rel_err, elem_rel_err
 
 pytestmark = pytest.mark.gpu
 
+# Element matrices: max-norm error per element relative to that element's max entry;
+# rhs vectors: relative to the global max (uniform-state elements carry roundoff-only rhs).
+TOL_R = {name: 1e-12 for name in SMALL_CASES}
+
 
 @pytest.fixture(scope="module")
 def gpu():
@@ -40,8 +44,8 @@ def test_formation_matches_oracle(gpu, oracle_lib, name):
         R, rhs = s.element_matrices()
         sp = s.fdv_params()
     Ro, ro = o.form(U, dt, apply_bc=True)
-    assert elem_rel_err(R, Ro) <= 1e-12
-    assert elem_rel_err(rhs, ro) <= 1e-12
+    assert elem_rel_err(R, Ro) <= TOL_R[name]
+    assert rel_err(rhs, ro) <= TOL_R[name]
     assert rel_err(sp, o.fdvparam(U)) <= 1e-14
 
 
@@ -52,8 +56,8 @@ def test_formation_matches_reference_golden(gpu, name):
         s.form(float(g["dt_dump"][0]))
         R, rhs = s.element_matrices()
     el = g["elements"]
-    assert elem_rel_err(R[el], g["R_bc"]) <= 1e-12
-    assert elem_rel_err(rhs[el], g["rhs_bc"]) <= 1e-12
+    assert elem_rel_err(R[el], g["R_bc"]) <= TOL_R[name]
+    assert rel_err(rhs[el], g["rhs_bc"]) <= TOL_R[name]
 
 
 @pytest.mark.parametrize("name", ["lid8", "ramp4"])
@@ -66,7 +70,7 @@ def test_physical_3d_flux_switch(gpu, oracle_lib, name):
         s.form(dt)
         R, rhs = s.element_matrices()
     Ro, ro = o.form(U, dt, apply_bc=True, physical_3d_flux=True)
-    assert elem_rel_err(R, Ro) <= 1e-12 and elem_rel_err(rhs, ro) <= 1e-12
+    assert elem_rel_err(R, Ro) <= 1e-12 and rel_err(rhs, ro) <= 1e-12
 
 
 @pytest.mark.parametrize("name", SMALL_CASES)
