@@ -105,7 +105,9 @@ def test_reference_gmres_matches_golden_history(gpu, name):
             assert rep["tol"] == pytest.approx(g[f"tol@{k}"][0], rel=1e-12)
             assert len(rep["est"]) == len(g[f"est@{k}"])
             assert rel_err(rep["est"], g[f"est@{k}"]) <= 1e-10
-            assert rel_err(rep["gfinal"], g[f"gfinal@{k}"]) <= 1e-10
+            # g(m) is the converged estimate: compare it on the history's scale (~||r0||)
+            scale = np.abs(g[f"est@{k}"]).max()
+            assert np.abs(rep["gfinal"] - g[f"gfinal@{k}"]).max() <= 1e-10 * scale
             assert rel_err(s.get_state(), g[f"U@{k}"]) <= 1e-10
             assert rel_err(s.rms(), g[f"rms@{k}"]) <= 1e-10
 
