@@ -38,6 +38,8 @@ WORKLOADS = {
                 make=lambda mg: mg.lid(32), m=20, cfl=0.5),
     "ramp": dict(desc="3D compression ramp 128x64x32 hex8, M=2.5, Re=1e5, GMRES(50) to 1e-8",
                  make=lambda mg: mg.ramp(128, 64, 32), m=50, cfl=0.25),
+    "ramp64": dict(desc="3D compression ramp 64x32x32 hex8 (profiling size), M=2.5, Re=1e5, GMRES(50) to 1e-8",
+                   make=lambda mg: mg.ramp(64, 32, 32), m=50, cfl=0.25),
 }
 
 
@@ -152,14 +154,18 @@ def bench_gpu(args, ws, rank, local):
     solver = G.FDVSolver(case)
     ext = torch.cuda.ExternalStream(solver.stream)
     sampler = ClockSampler(local)
-    for prec_name, prec in (("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)):
+    forms = [("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)]
+    if args.only:
+        forms = [f for f in forms if f[0] == args.only]
+    clocks = None
+    for prec_name, prec in forms:
         solver.load_node_records()
         for _ in range(args.warmup):
             solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=prec)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
-        if prec_name == "mixed":
+        if prec_name == forms[-1][0]:
             sampler.start()
         solver.profile(True)
         step_ms, res, mvs = [], [], []
@@ -181,13 +187,21 @@ def bench_gpu(args, ws, rank, local):
         torch.cuda.synchronize()
         stats = solver.profile_read()
         solver.profile(False)
-        if prec_name == "mixed":
+        if prec_name == forms[-1][0]:
             clocks = sampler.stop()
         total_s = max_over_ranks(sum(step_ms) / 1e3)
         results[prec_name] = dict(steps_per_s=ws * args.steps / total_s, ms_per_step=1e3 * total_s / args.steps,
                                   true_rel_res_max=max(res), matvecs_per_step=sum(mvs) / len(mvs), stats=stats,
                                   state=solver.get_state())
 
+    if args.only:  # profiling runs: one form, no end-to-end loop, no JSON line
+        solver.close()
+        if rank == 0:
+            r = results[args.only]
+            print(json.dumps({"form": args.only, "steps_per_s": r["steps_per_s"], "ms_per_step": r["ms_per_step"],
+                              "true_rel_res_max": r["true_rel_res_max"], "matvecs_per_step": r["matvecs_per_step"],
+                              "ebe": {k: v for k, v in r["stats"].items()}}))
+        return
     # end-to-end through the C ABI with host buffers: H2D state, step, D2H state every step
     n = solver.n_dof
     host = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -302,6 +316,7 @@ def main():
     ap.add_argument("--impl", default="cfdv_b200", choices=["cfdv_b200", "reference"])
     ap.add_argument("--workload", default="plate", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", choices=["fp64", "mixed"], help="time one form only (profiling runs)")
     args = ap.parse_args()
     ws, rank, local = dist_info()
     if args.impl == "reference":
