@@ -699,6 +699,26 @@ int cfdv_form(cfdv_ctx* c, double dt, int precision) {
   return read_status(c);
 }
 
+int cfdv_set_element_matrices(cfdv_ctx* c, const double* R, const double* rhs, int precision) {
+  if (!c || !R || !rhs) return CFDV_ERR_ARG;
+  cudaSetDevice(c->dev);
+  const size_t E = c->n_elements, Ke = c->Ke;
+  CK(cudaMemcpyAsync(c->d_R64, R, sizeof(double) * E * Ke * Ke, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_rhs, rhs, sizeof(double) * E * Ke, cudaMemcpyHostToDevice, c->st));
+  if (precision == CFDV_PREC_MIXED) {
+    if (!c->d_R32) {
+      int rc = dalloc(c, &c->d_R32, E * Ke * Ke);
+      if (rc) return rc;
+    }
+    CK(launch_to_float(c->d_R64, c->d_R32, E * Ke * Ke, c->st));
+    c->launches++;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  c->formed = true;
+  c->have32 = (precision == CFDV_PREC_MIXED);
+  return CFDV_OK;
+}
+
 int cfdv_gmres(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
   if (!c || !o) return CFDV_ERR_ARG;
   if (!c->formed) return fail(c, CFDV_ERR_STATE, "gmres before form");

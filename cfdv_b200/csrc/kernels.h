@@ -103,6 +103,8 @@ cudaError_t launch_normalize(const double* w, int n, const double* pin, double* 
 cudaError_t launch_reduce(const double* pin, double* out, int do_sqrt, cudaStream_t st);
 // x += sum_i y_i V_i  (V column-major, ld = n), summed in i order per entry
 cudaError_t launch_combine(double* x, const double* V, int n, const double* y, int m, cudaStream_t st);
+// out[i] = (float) in[i]
+cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t st);
 // U0 = U ; U += du
 cudaError_t launch_state_update(double* U, double* U0, const double* du, int n, cudaStream_t st);
 // per-field sums of U^2 and U0^2 -> partial[blk][2*neqn]

@@ -178,6 +178,16 @@ __global__ void __launch_bounds__(kRedThreads) rms_partial_kernel(const double* 
   }
 }
 
+__global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t st) {
+  to_float_kernel<<<4 * 148, 256, 0, st>>>(in, out, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dot(const double* a, const double* b, int n, double* partial, cudaStream_t st) {
   dot_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(a, b, n, partial);
   return cudaGetLastError();

@@ -25,7 +25,7 @@ STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "bad mesh", 4: "non-fi
 # every entry point declared in include/cfdv_gpu.h
 EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error", "cfdv_get_stream",
            "cfdv_set_state", "cfdv_load_node_records", "cfdv_get_state", "cfdv_state_device_ptr", "cfdv_cfl",
-           "cfdv_form", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
+           "cfdv_form", "cfdv_set_element_matrices", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
            "cfdv_profile_read"]
 
@@ -86,6 +86,7 @@ def lib():
         L.cfdv_state_device_ptr.argtypes = [P, P]
         L.cfdv_cfl.argtypes = [P, D, P]
         L.cfdv_form.argtypes = [P, D, I]
+        L.cfdv_set_element_matrices.argtypes = [P, P, P, I]
         L.cfdv_gmres.argtypes = [P, P, P]
         L.cfdv_update.argtypes = [P]
         L.cfdv_rms.argtypes = [P, P]
@@ -192,6 +193,12 @@ class FDVSolver:
 
     def form(self, dt: float, precision: int = PREC_FP64):
         self._ck(self.L.cfdv_form(self._ctx, float(dt), int(precision)))
+
+    def set_element_matrices(self, R, rhs, precision: int = PREC_FP64):
+        R = np.ascontiguousarray(R, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        assert R.size == self.n_elements * self.Ke * self.Ke and rhs.size == self.n_elements * self.Ke
+        self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
     def _opts(mode, m, restarts, rtol, precision, true_residual):

@@ -125,6 +125,10 @@ int cfdv_cfl(cfdv_ctx* ctx, double cfl, double* dt);
 /* Element LHS/RHS at time step dt with ApplyBC; precision MIXED also keeps FP32
  * copies of the matrices for the FP32 products. */
 int cfdv_form(cfdv_ctx* ctx, double dt, int precision);
+/* Element matrices formed elsewhere (e.g. by the reference's FDVGalerkin on the CPU):
+ * R [E][Ke*Ke] column-major per element, rhs [E][Ke], ApplyBC already applied.  Lets
+ * the GPU solver plug in at GMRESbase alone (GMRESbase.h:8-23). */
+int cfdv_set_element_matrices(cfdv_ctx* ctx, const double* R, const double* rhs, int precision);
 /* Solve for dU from the formed matrices (GMRESbase::iterate). */
 int cfdv_gmres(cfdv_ctx* ctx, const cfdv_gmres_opts* opts, cfdv_gmres_report* report);
 /* U0 = U; U += dU (GMRESbase::update). */
