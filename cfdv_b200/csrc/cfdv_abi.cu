@@ -12,6 +12,7 @@
 
 #include "../../include/cfdv_gpu.h"
 #include "formation.cuh"
+#include "gmres_persistent.h"
 #include "kernels.h"
 
 using namespace cfdv;
@@ -56,6 +57,9 @@ struct cfdv_ctx {
   double* d_rms = nullptr;
   int* d_status = nullptr;
   double* h_pin = nullptr;  // pinned host staging
+  double* d_pers = nullptr;  // persistent-solve scratch
+  size_t pers_cap = 0;
+  int* d_pers_int = nullptr;
   // profiling
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -105,7 +109,8 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_U); dfree(c->d_U0); dfree(c->d_du);
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
-  dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status);
+  dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int);
+  c->pers_cap = 0;
   if (c->h_pin) cudaFreeHost(c->h_pin);
   c->h_pin = nullptr;
   c->m_cap = 0;
@@ -533,6 +538,78 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
   return CFDV_OK;
 }
 
+// The same textbook solve as gmres_correct, run as one persistent cooperative kernel
+// (gmres_persistent.cu): one launch and one read-back per solve.
+int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
+  const int m = o->m;
+  const int fp32 = (o->precision == CFDV_PREC_MIXED);
+  if (fp32 && !c->have32) return fail(c, CFDV_ERR_STATE, "mixed precision needs cfdv_form(..., CFDV_PREC_MIXED)");
+  int rc = ensure_krylov(c, m);
+  if (rc) return rc;
+  const int est_cap = std::max(1, m * std::max(o->restarts, 1));
+  const int gf_cap = std::max(1, o->restarts);
+  // scratch: g, cs, sn, y (m+1 each) | est | gfinal | result(4)
+  const size_t need = 4 * (size_t)(m + 1) + est_cap + gf_cap + 4;
+  if (need > c->pers_cap) {
+    if ((rc = dalloc(c, &c->d_pers, need))) return rc;
+    c->pers_cap = need;
+  }
+  if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, 8))) return rc;
+  CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
+  double bnorm;
+  if ((rc = compose_b(c, &bnorm))) return rc;
+  const double atol = o->rtol * bnorm;
+  if (rep) { rep->tol = atol; rep->bnorm = bnorm; }
+  if (bnorm == 0.0) { if (rep) rep->true_rel_res = 0.0; return CFDV_OK; }
+  CK(cudaMemsetAsync(c->d_pers_int, 0, sizeof(int) * 8, c->st));
+  PersistentArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n_dof = c->n_dof; a.n_elements = c->n_elements; a.m = m; a.max_restarts = o->restarts;
+  a.max_blocks = persistent_max_blocks();
+  a.atol = atol;
+  a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
+  a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;
+  a.b = c->d_b; a.du = c->d_du; a.V = c->d_V; a.W = c->d_W; a.part0 = c->d_pa; a.part1 = c->d_pb;
+  a.H = c->d_H;
+  double* p = c->d_pers;
+  a.g = p; a.cs = p + (m + 1); a.sn = p + 2 * (m + 1); a.y = p + 3 * (m + 1);
+  a.est = p + 4 * (m + 1); a.est_capacity = est_cap;
+  a.gfinal = a.est + est_cap; a.gfinal_capacity = gf_cap;
+  a.result = a.gfinal + gf_cap;
+  int* pi = c->d_pers_int;
+  a.stop = pi; a.out = pi + 1; a.err = pi + 2;
+  a.bar_count = (unsigned int*)(pi + 3); a.bar_gen = (unsigned int*)(pi + 4);
+  cudaEvent_t* ev = next_events(c);
+  if (ev) cudaEventRecord(ev[0], c->st);
+  CK(launch_gmres_persistent(c->ndim, fp32, a, c->st));
+  if (ev) { cudaEventRecord(ev[1], c->st); cudaEventRecord(ev[2], c->st); }
+  c->launches++;
+  int hi[8];
+  double res[4];
+  CK(cudaMemcpyAsync(hi, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(res, a.result, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (hi[2] & 1) return fail(c, CFDV_ERR_CUDA, "persistent GMRES: grid barrier timed out");
+  if (hi[2] & 2) return fail(c, CFDV_ERR_NONFINITE, "persistent GMRES: non-finite residual");
+  if (rep) {
+    const int nest = (int)res[2];
+    rep->n_est = nest;
+    rep->n_restarts = hi[1];
+    rep->n_matvec += (int)res[3];
+    rep->true_rel_res = res[0] / bnorm;
+    if (rep->est && rep->est_capacity > 0) {
+      const int k = std::min(std::min(nest, rep->est_capacity), est_cap);
+      if (k > 0) CK(cudaMemcpy(rep->est, a.est, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    }
+    if (rep->gfinal && rep->gfinal_capacity > 0) {
+      const int k = std::min(std::min(hi[1], rep->gfinal_capacity), gf_cap);
+      if (k > 0) CK(cudaMemcpy(rep->gfinal, a.gfinal, sizeof(double) * k, cudaMemcpyDeviceToHost));
+    }
+  }
+  c->mv_launches += (long)res[3];
+  return CFDV_OK;
+}
+
 int true_residual(cfdv_ctx* c, cfdv_gmres_report* rep) {
   double beta;
   int rc = matvec(c, 0, c->d_du, c->d_W, 1, c->d_b, c->d_W, c->d_pa, nullptr);
@@ -729,8 +806,10 @@ int cfdv_gmres(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
   if (o->mode == CFDV_GMRES_REFERENCE) {
     if (o->precision != CFDV_PREC_FP64) return fail(c, CFDV_ERR_ARG, "reference GMRES runs in FP64 only");
     rc = gmres_reference(c, o, rep);
-  } else {
+  } else if (o->engine == 1) {
     rc = gmres_correct(c, o, rep);
+  } else {
+    rc = gmres_correct_device(c, o, rep);
   }
   if (rc) return rc;
   if (o->true_residual && rep && o->mode == CFDV_GMRES_REFERENCE) rc = true_residual(c, rep);

@@ -1,0 +1,312 @@
+// Restarted GMRES(m) to a relative tolerance as ONE persistent cooperative kernel.
+//
+// For meshes whose per-product work is a few microseconds (the 2D cases fit in L2),
+// launching one kernel per MGS pass and reading every Hessenberg column back to the
+// host costs more than the arithmetic.  This kernel keeps the whole solve on the
+// device: every restart recomputes r = b - A du with the FP64 matrices, then runs
+// the Arnoldi cycle with MGS (dots reduced from fixed block partials, so every block
+// derives the same scalar), block 0 applies the Givens rotations and tests
+// |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver), back-substitutes
+// the small triangular system and all blocks add V y to du.  Products use the FP64
+// matrices, or the FP32 matrices with FP32 accumulation for the mixed form (the
+// restart residual stays FP64: GMRES-based iterative refinement).
+//
+// Phases are separated by a grid barrier.  Its spin is bounded: a block that waits
+// longer than the limit sets an error flag and every block returns at the next
+// barrier, so a broken launch ends instead of hanging.  The launch is cooperative,
+// which guarantees that all blocks are resident.  Data written by other blocks in the
+// same launch is read through L2 (__ldcg): L1 is not coherent across SMs.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "gmres_persistent.h"
+#include "kernels.h"
+
+namespace cfdv {
+
+namespace {
+
+constexpr long long kSpinLimit = 1ll << 27;  // ~ seconds of polling: far above any barrier
+
+struct Barrier {
+  unsigned int* count;
+  unsigned int* gen;
+  int* err;
+};
+
+// sense-counting barrier over all blocks; returns false if this or another block failed
+__device__ __forceinline__ bool grid_sync(const Barrier& b, unsigned int nblocks) {
+  __syncthreads();
+  __shared__ int ok;
+  if (threadIdx.x == 0) {
+    ok = 1;
+    const unsigned int g = *(volatile unsigned int*)b.gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(b.count, 1u) + 1u;
+    if (arrived == nblocks) {
+      *(volatile unsigned int*)b.count = 0u;
+      __threadfence();
+      atomicAdd(b.gen, 1u);
+    } else {
+      long long spins = 0;
+      while (*(volatile unsigned int*)b.gen == g) {
+        if (++spins > kSpinLimit) {
+          atomicOr(b.err, 1);
+          break;
+        }
+        __nanosleep(20);
+      }
+    }
+    __threadfence();
+    if (*(volatile int*)b.err) ok = 0;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double ws[32];
+  __shared__ double res;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) ws[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = (lane < nw) ? ws[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) res = v;
+  }
+  __syncthreads();
+  return res;
+}
+
+// the same partials summed in the same order by every block
+__device__ __forceinline__ double sum_partials(const double* p, int n) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(p + i);
+  return block_sum(v);
+}
+
+}  // namespace
+
+template <int KE, int NEQ, int NNOD, typename TR>
+__global__ void gmres_persistent_kernel(PersistentArgs a) {
+  const unsigned int nb = gridDim.x;
+  const int tid = threadIdx.x, bid = blockIdx.x;
+  const int nthr = blockDim.x;
+  const int gtid = bid * nthr + tid, gstride = nb * nthr;
+  const int n = a.n_dof;
+  Barrier bar{a.bar_count, a.bar_gen, a.err};
+  constexpr int EPB = 256 / KE;  // elements per block-iteration of the element pass
+  __shared__ TR xs[EPB > 0 ? EPB : 1][KE];
+  __shared__ double xs64[EPB > 0 ? EPB : 1][KE];
+  double* V = a.V;
+  double* W = a.W;
+  double* pa = a.part0;
+  double* pb = a.part1;
+
+  // element pass: Y = R x (FP64 matrices, or FP32 matrices with FP32 accumulation)
+  auto elem_pass64 = [&](const double* x) {
+    const int le = tid / KE, i = tid % KE;
+    for (int e0 = bid * EPB; e0 < a.n_elements; e0 += nb * EPB) {
+      const int e = e0 + le;
+      if (le < EPB && e < a.n_elements)
+        xs64[le][i] = __ldcg(x + (size_t)a.conn[(size_t)e * NNOD + i / NEQ] * NEQ + i % NEQ);
+      __syncthreads();
+      if (le < EPB && e < a.n_elements) {
+        const double* Re = a.R64 + (size_t)e * KE * KE;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs64[le][j];
+        a.Y64[(size_t)e * KE + i] = acc;
+      }
+      __syncthreads();
+    }
+  };
+  auto elem_pass_op = [&](const double* x) {
+    if (sizeof(TR) == 8) {
+      elem_pass64(x);
+      return;
+    }
+    const int le = tid / KE, i = tid % KE;
+    for (int e0 = bid * EPB; e0 < a.n_elements; e0 += nb * EPB) {
+      const int e = e0 + le;
+      if (le < EPB && e < a.n_elements)
+        xs[le][i] = (TR)__ldcg(x + (size_t)a.conn[(size_t)e * NNOD + i / NEQ] * NEQ + i % NEQ);
+      __syncthreads();
+      if (le < EPB && e < a.n_elements) {
+        const TR* Re = (const TR*)a.R32 + (size_t)e * KE * KE;
+        TR acc = 0;
+#pragma unroll 8
+        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[le][j];
+        a.Y32[(size_t)e * KE + i] = (float)acc;
+      }
+      __syncthreads();
+    }
+  };
+  // node pass: out = gather(Y) (mode 0) or b - gather(Y) (mode 1); partial of out . dotv
+  auto node_pass = [&](bool fp32, int mode, double* out, const double* dotv, double* part) {
+    double acc = 0.0;
+    for (int d = gtid; d < n; d += gstride) {
+      const int nd = d / NEQ, k = d % NEQ;
+      double s = 0.0;
+      const int p1 = a.csr_ptr[nd + 1];
+      for (int p = a.csr_ptr[nd]; p < p1; p++) {
+        const int v = a.csr_idx[p];
+        const size_t yi = (size_t)(v / NNOD) * KE + (v % NNOD) * NEQ + k;
+        s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
+      }
+      const double val = mode ? a.b[d] - s : s;
+      out[d] = val;
+      acc += val * (dotv ? __ldcg(dotv + d) : val);
+    }
+    acc = block_sum(acc);
+    if (tid == 0) part[bid] = acc;
+  };
+
+  const int m = a.m;
+  double* H = a.H;  // (m+1) x m column-major, rotated in place by block 0
+  int total_est = 0, mv = 0;
+  bool converged = false;
+  double beta = 0.0;
+  for (int cycle = 0; cycle < a.max_restarts; cycle++) {
+    // r = b - A64 du, beta = ||r||
+    elem_pass64(a.du);
+    if (!grid_sync(bar, nb)) return;
+    {
+      const bool f32 = false;
+      node_pass(f32, 1, W, nullptr, pa);
+    }
+    mv++;
+    if (!grid_sync(bar, nb)) return;
+    beta = sqrt(sum_partials(pa, nb));
+    if (!(beta == beta)) {
+      if (bid == 0 && tid == 0) atomicOr(a.err, 2);
+      return;
+    }
+    if (beta < a.atol) {
+      converged = true;
+      break;
+    }
+    for (int d = gtid; d < n; d += gstride) V[d] = __ldcg(W + d) / beta;
+    if (bid == 0 && tid == 0) {
+      for (int i = 0; i <= m; i++) a.g[i] = 0.0;
+      a.g[0] = beta;
+    }
+    if (!grid_sync(bar, nb)) return;
+    int k = 0;
+    for (int j = 0; j < m; j++) {
+      double* vj = V + (size_t)j * n;
+      elem_pass_op(vj);
+      if (!grid_sync(bar, nb)) return;
+      node_pass(sizeof(TR) == 4, 0, W, V, pa);
+      mv++;
+      if (!grid_sync(bar, nb)) return;
+      double* Hj = H + (size_t)j * (m + 1);
+      for (int i = 0; i <= j; i++) {
+        const double h = sum_partials(pa, nb);
+        if (bid == 0 && tid == 0) Hj[i] = h;
+        const double* vi = V + (size_t)i * n;
+        const double* nx = (i < j) ? V + (size_t)(i + 1) * n : nullptr;
+        double acc = 0.0;
+        for (int d = gtid; d < n; d += gstride) {
+          const double wn = __ldcg(W + d) - h * __ldcg(vi + d);
+          W[d] = wn;
+          acc += wn * (nx ? __ldcg(nx + d) : wn);
+        }
+        acc = block_sum(acc);
+        if (tid == 0) pb[bid] = acc;
+        double* t = pa; pa = pb; pb = t;
+        if (!grid_sync(bar, nb)) return;
+      }
+      const double nrm = sqrt(sum_partials(pa, nb));
+      double* vn = V + (size_t)(j + 1) * n;
+      for (int d = gtid; d < n; d += gstride) vn[d] = __ldcg(W + d) / nrm;
+      if (bid == 0 && tid == 0) {
+        // Givens QR of column j (rotations of earlier columns are stored in cs/sn)
+        Hj[j + 1] = nrm;
+        for (int i = 0; i < j; i++) {
+          const double t0 = a.cs[i] * Hj[i] + a.sn[i] * Hj[i + 1];
+          Hj[i + 1] = -a.sn[i] * Hj[i] + a.cs[i] * Hj[i + 1];
+          Hj[i] = t0;
+        }
+        const double den = hypot(Hj[j], Hj[j + 1]);
+        const double c = den > 0 ? Hj[j] / den : 1.0, s = den > 0 ? Hj[j + 1] / den : 0.0;
+        a.cs[j] = c;
+        a.sn[j] = s;
+        Hj[j] = den;
+        Hj[j + 1] = 0.0;
+        a.g[j + 1] = -s * a.g[j];
+        a.g[j] = c * a.g[j];
+        if (total_est < a.est_capacity) a.est[total_est] = a.g[j + 1];
+        *a.stop = (fabs(a.g[j + 1]) < a.atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
+      }
+      total_est++;
+      k = j + 1;
+      if (!grid_sync(bar, nb)) return;
+      if (*(volatile int*)a.stop) break;
+    }
+    // y from the upper-triangular system, du += V y
+    if (bid == 0 && tid == 0) {
+      for (int i = k - 1; i >= 0; i--) {
+        double s = a.g[i];
+        for (int jj = i + 1; jj < k; jj++) s -= H[(size_t)jj * (m + 1) + i] * a.y[jj];
+        a.y[i] = s / H[(size_t)i * (m + 1) + i];
+      }
+      if (cycle < a.gfinal_capacity) a.gfinal[cycle] = a.g[k];
+    }
+    if (!grid_sync(bar, nb)) return;
+    for (int d = gtid; d < n; d += gstride) {
+      double z = 0.0;
+      for (int i = 0; i < k; i++) z += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + d);
+      a.du[d] += z;
+    }
+    if (!grid_sync(bar, nb)) return;
+    if (bid == 0 && tid == 0) a.out[0] = cycle + 1;
+  }
+  if (!converged) {  // residual after the last cycle
+    elem_pass64(a.du);
+    if (!grid_sync(bar, nb)) return;
+    node_pass(false, 1, W, nullptr, pa);
+    mv++;
+    if (!grid_sync(bar, nb)) return;
+    beta = sqrt(sum_partials(pa, nb));
+  }
+  if (bid == 0 && tid == 0) {
+    a.result[0] = beta;
+    a.result[1] = converged ? 1.0 : 0.0;
+    a.result[2] = (double)total_est;
+    a.result[3] = (double)mv;
+  }
+}
+
+template <int KE, int NEQ, int NNOD, typename TR>
+static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
+  constexpr int THREADS = (256 / KE) * KE;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_persistent_kernel<KE, NEQ, NNOD, TR>,
+                                                                THREADS, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+  int blocks = sms * per_sm;
+  if (blocks > a.max_blocks) blocks = a.max_blocks;
+  PersistentArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR>, dim3(blocks), dim3(THREADS),
+                                     params, 0, st);
+}
+
+cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
+  if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float>(a, st) : launch_one<16, 4, 4, double>(a, st);
+  return fp32 ? launch_one<40, 5, 8, float>(a, st) : launch_one<40, 5, 8, double>(a, st);
+}
+
+int persistent_max_blocks() { return kRedBlocks; }
+
+}  // namespace cfdv

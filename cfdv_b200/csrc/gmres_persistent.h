@@ -1,0 +1,43 @@
+// Arguments of the single-launch restarted GMRES solve (gmres_persistent.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace cfdv {
+
+struct PersistentArgs {
+  int n_dof, n_elements, m, max_restarts, max_blocks;
+  double atol;                 // stop when ||b - A du|| < atol (true residual, FP64 matrices)
+  const int* conn;
+  const int* csr_ptr;
+  const int* csr_idx;
+  const double* R64;
+  const float* R32;
+  double* Y64;
+  float* Y32;
+  const double* b;
+  double* du;                  // solution, starts at zero
+  double* V;                   // (m+1) Krylov vectors
+  double* W;
+  double* part0;               // block partials (>= gridDim.x each)
+  double* part1;
+  double* H;                   // (m+1) x m, column-major
+  double* g;                   // m+1
+  double* cs;                  // m
+  double* sn;                  // m
+  double* y;                   // m
+  double* est;                 // Givens residual estimate per inner step
+  int est_capacity;
+  double* gfinal;              // |g_k| at the end of each cycle
+  int gfinal_capacity;
+  int* stop;
+  int* out;                    // [0] cycles run
+  double* result;              // [0] final ||r||, [1] converged, [2] estimates, [3] products
+  unsigned int* bar_count;     // grid barrier state, zero before launch
+  unsigned int* bar_gen;
+  int* err;                    // bit 0: barrier timeout, bit 1: non-finite residual
+};
+
+cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st);
+int persistent_max_blocks();
+
+}  // namespace cfdv

@@ -48,7 +48,7 @@ class _Params(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("mode", C.c_int), ("m", C.c_int), ("restarts", C.c_int), ("rtol", C.c_double),
-                ("precision", C.c_int), ("true_residual", C.c_int)]
+                ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int)]
 
 
 class _Report(C.Structure):
@@ -201,8 +201,9 @@ class FDVSolver:
         self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
-    def _opts(mode, m, restarts, rtol, precision, true_residual):
-        return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)))
+    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0):
+        return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)),
+                     int(engine))
 
     def _report(self, m, restarts):
         est = np.zeros(max(m * max(restarts, 1), 1))
@@ -216,8 +217,9 @@ class FDVSolver:
                 "gfinal": fin[: min(rep.n_restarts, fin.size)].copy(), "restarts": rep.n_restarts,
                 "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
 
-    def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual)
+    def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False,
+              engine=0):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine)
         rep, est, fin = self._report(m, restarts)
         self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
         return self._unpack(rep, est, fin)
@@ -231,8 +233,8 @@ class FDVSolver:
         return r
 
     def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-             true_residual=False):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual)
+             true_residual=False, engine=0):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))

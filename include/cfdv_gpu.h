@@ -82,6 +82,9 @@ typedef struct {
   int precision;  /* cfdv_precision: MIXED = FP32 element matrices and matvec inside
                      FP64 iterative refinement (CORRECT mode only) */
   int true_residual; /* 1: report ||b - A du||/||b|| with an extra FP64 product */
+  int engine;        /* CORRECT mode: 0 = the whole solve as one persistent cooperative kernel
+                        (no host round trip per Arnoldi step), 1 = host-driven (one kernel per
+                        pass, Hessenberg column read back every step) */
 } cfdv_gmres_opts;
 
 typedef struct {

@@ -19,7 +19,9 @@
 //   u32 name_len, name bytes, u8 type ('d' f64 | 'i' i32), u64 count, payload
 //
 // Usage: cfdv_ref <case_dir> <out_file> [--steps N] [--dump-step K]
-//                 [--gmresiter M] [--restart R] [--quiet]
+//                 [--gmresiter M] [--restart R] [--quiet] [--tecplot]
+// --tecplot writes the reference's tecplot_<iter>.plt (MPI_TecplotOut.h) into the working
+// directory at every iteration divisible by 100, as main.cpp:183 does.
 #include "mpi.h"
 
 #include <algorithm>
@@ -45,6 +47,7 @@
 #include "FDV/Function/FDVParam.h"
 #include "Utility/Solvers/MPI_GMRES.h"
 #include "Utility/IO/ASCIItoBinary/LoadBinary.h"
+#include "Utility/IO/MPI_TecplotOut.h"
 
 namespace {
 
@@ -103,7 +106,7 @@ int main(int argc, char** argv) {
   std::string path = argv[1];
   std::string out = argv[2];
   int nsteps = 1, dump_step = -1, m_override = -1, r_override = -1;
-  bool quiet = false;
+  bool quiet = false, tecplot = false;
   for (int i = 3; i < argc; i++) {
     std::string a = argv[i];
     if (a == "--steps" && i + 1 < argc) nsteps = atoi(argv[++i]);
@@ -111,6 +114,7 @@ int main(int argc, char** argv) {
     else if (a == "--gmresiter" && i + 1 < argc) m_override = atoi(argv[++i]);
     else if (a == "--restart" && i + 1 < argc) r_override = atoi(argv[++i]);
     else if (a == "--quiet") quiet = true;
+    else if (a == "--tecplot") tecplot = true;
   }
 
   auto cm = parse_kv(path + "/control");
@@ -167,6 +171,11 @@ int main(int argc, char** argv) {
     for_each(nodes.begin(), nodes.end(), NodeUnpack<Node*>());             // main.cpp:171
     double cfl_v = cfl;
     CFL<Element*>(elements, cfl_v, dt);  // main.cpp:179
+    if (tecplot && iter % 100 == 0) {  // main.cpp:183, after NodeUnpack and CFL
+      std::cout.rdbuf(sink.rdbuf());
+      MPI_TecplotOut(elements, nodes, iter, ndim, t, true, 0, 0, 1, 0, nnod, neqn);
+      std::cout.rdbuf(saved);
+    }
     auto t0 = std::chrono::steady_clock::now();
     FDVGalerkin<Element*> fdv(nnod, neqn, ndim, nbnod, dt, NS);  // main.cpp:185-186
     for_each(elements.begin(), elements.end(), std::ref(fdv));

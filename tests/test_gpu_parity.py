@@ -153,3 +153,41 @@ def test_correct_gmres_fp64_and_mixed(gpu, oracle_lib, name):
     duo, _ = o.gmres_correct(Ro, ro, 30, 60, 1e-12)
     assert rel_err(du64, duo) <= 1e-6
     assert rel_err(du32, du64) <= 1e-6
+
+
+@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_persistent_engine_matches_host_driven(gpu, name, prec):
+    """The single-launch cooperative solve against the one-kernel-per-pass solve."""
+    case = get_case(name)
+    p = gpu.PREC_MIXED if prec == "mixed" else gpu.PREC_FP64
+    with solver(gpu, case) as s:
+        dt = s.cfl(float(case.control["cfl"]))
+        s.form(dt, precision=gpu.PREC_MIXED)
+        r0 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=0)
+        d0 = s.du()
+        r1 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=1)
+        d1 = s.du()
+    assert r0["true_rel_res"] < 1e-8 and r1["true_rel_res"] < 1e-8
+    assert rel_err(d0, d1) <= 1e-6
+    assert r0["restarts"] == r1["restarts"]
+
+
+@pytest.mark.parametrize("name", ["lid8", "ramp4"])
+def test_solver_plugin_with_host_matrices(gpu, oracle_lib, name):
+    """GMRESbase-only use: matrices formed on the CPU (the oracle stands in for the
+    reference's FDVGalerkin), uploaded, and solved by the reference-mode GPU GMRES."""
+    case = get_case(name)
+    o = oracle_lib.Oracle(case)
+    U = o.init_U()
+    dt = o.cfl(U, float(case.control["cfl"]))
+    R, rhs = o.form(U, dt)
+    m, r = int(case.control["gmresiter"]), int(case.control["gmresrestart"])
+    du_o, rep_o = o.gmres_ref(R, rhs, m, r)
+    with solver(gpu, case) as s:
+        s.set_element_matrices(R, rhs)
+        rep = s.gmres(mode=gpu.GMRES_REFERENCE, m=m, restarts=r)
+        du = s.du()
+    assert len(rep["est"]) == len(rep_o["est"])
+    assert rel_err(rep["est"], rep_o["est"]) <= 1e-10
+    assert rel_err(du, du_o) <= 1e-10
