@@ -20,8 +20,9 @@
 //
 // Usage: cfdv_ref <case_dir> <out_file> [--steps N] [--dump-step K]
 //                 [--gmresiter M] [--restart R] [--quiet] [--tecplot]
-// --tecplot writes the reference's tecplot_<iter>.plt (MPI_TecplotOut.h) into the working
-// directory at every iteration divisible by 100, as main.cpp:183 does.
+// --tecplot writes the reference's outputs into the working directory: tecplot_<iter>.plt
+// (MPI_TecplotOut.h) at every iteration divisible by 100, as main.cpp:183 does, and the
+// RMSError.txt line of every step (MPI_RMSError.h), as main.cpp:198 does.
 #include "mpi.h"
 
 #include <algorithm>
@@ -45,6 +46,7 @@
 #include "FDV/Function/NodeUnpack.h"
 #include "FDV/Function/MPI_CFL.h"
 #include "FDV/Function/FDVParam.h"
+#include "FDV/Function/MPI_RMSError.h"
 #include "Utility/Solvers/MPI_GMRES.h"
 #include "Utility/IO/ASCIItoBinary/LoadBinary.h"
 #include "Utility/IO/MPI_TecplotOut.h"
@@ -247,6 +249,14 @@ int main(int argc, char** argv) {
       rms[k] = (b == 0) ? 1.0 : std::sqrt(a / b) - 1.0;
     }
     rf.putd("rms" + sfx, rms);
+    if (tecplot) {  // the reference's RMSError.txt line (MPIBinaryConfiguration.h:138-142)
+      std::cout.rdbuf(sink.rdbuf());
+      {
+        MPI_RMSError<Node*> rmserr("RMSError.txt", t, iter, neqn);
+        for_each(nodes.begin(), nodes.end(), std::ref(rmserr));
+      }
+      std::cout.rdbuf(saved);
+    }
     // wall time of the step's path: CFL, formation, ApplyBC, GMRES, update
     rf.putd("steptime" + sfx, {std::chrono::duration<double>(t2 - t_step0).count()});
     t += dt;

@@ -1,0 +1,40 @@
+"""The C++ host driver (cfdv_b200/cfdv_gpu, the reference's time loop over the C ABI)
+writes the same output files as the reference: tecplot_0.plt byte for byte, and the
+RMSError.txt lines (iteration, per-field RMS change) to the printed precision."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, get_case
+
+pytestmark = pytest.mark.gpu
+REF = os.path.join(ROOT, "oracle", "_ref", "cfdv_ref")
+DRIVER = os.path.join(ROOT, "cfdv_b200", "cfdv_gpu")
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference build oracle/_ref not present")
+@pytest.mark.parametrize("name,steps", [("lid8", 5), ("plate20", 3), ("ramp4", 2)])
+def test_driver_outputs_match_reference(name, steps):
+    from cfdv_b200 import meshgen as mg
+    case = get_case(name)
+    with tempfile.TemporaryDirectory() as d:
+        cdir = os.path.join(d, "case")
+        mg.write_case(case, cdir)
+        rdir, gdir = os.path.join(d, "ref"), os.path.join(d, "gpu")
+        os.makedirs(rdir)
+        os.makedirs(gdir)
+        subprocess.run([REF, cdir, os.path.join(d, "r.rec"), "--steps", str(steps), "--tecplot", "--quiet"],
+                       cwd=rdir, check=True, stdin=subprocess.DEVNULL)
+        subprocess.run([DRIVER, cdir, "--steps", str(steps), "--out", gdir], check=True, capture_output=True)
+        assert open(os.path.join(gdir, "tecplot_0.plt"), "rb").read() == \
+            open(os.path.join(rdir, "tecplot_0.plt"), "rb").read()
+        ref = [ln.split() for ln in open(os.path.join(rdir, "RMSError.txt"))]
+        got = [ln.split() for ln in open(os.path.join(gdir, "RMSError.txt"))]
+    assert len(ref) == len(got) == steps
+    for a, b in zip(got, ref):
+        assert a[0] == b[0]
+        # 6 significant digits are printed; allow one unit in the last place
+        np.testing.assert_allclose(np.array(a[1:], float), np.array(b[1:], float), rtol=2e-5, atol=1e-12)

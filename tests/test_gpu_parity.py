@@ -173,7 +173,7 @@ def test_persistent_engine_matches_host_driven(gpu, name, prec):
     assert r0["restarts"] == r1["restarts"]
 
 
-@pytest.mark.parametrize("name", ["lid8", "ramp4"])
+@pytest.mark.parametrize("name", ["lid8", "ramp4", "cyl4"])
 def test_solver_plugin_with_host_matrices(gpu, oracle_lib, name):
     """GMRESbase-only use: matrices formed on the CPU (the oracle stands in for the
     reference's FDVGalerkin), uploaded, and solved by the reference-mode GPU GMRES."""
