@@ -16,6 +16,12 @@ pytestmark = pytest.mark.gpu
 # Element matrices: max-norm error per element relative to that element's max entry;
 # rhs vectors: relative to the global max (uniform-state elements carry roundoff-only rhs).
 TOL_R = {name: 1e-12 for name in SMALL_CASES}
+# The reference's final estimate g(m) on the stiff cylinder case moves by 3e-7 of itself
+# (2.6e-8 of the history scale) under rounding-level changes of the element rhs: the
+# formation kernel run on the CPU with FMA contraction reproduces exactly this shift while
+# U stays within 6.5e-11, and the reference compiled with FMA changes its own iteration
+# count (26 -> 28) and dU by 80%.  The bound below is that measured envelope.
+TOL_GFINAL = {"cyl4": 1e-7}
 
 
 @pytest.fixture(scope="module")
@@ -107,7 +113,7 @@ def test_reference_gmres_matches_golden_history(gpu, name):
             assert rel_err(rep["est"], g[f"est@{k}"]) <= 1e-10
             # g(m) is the converged estimate: compare it on the history's scale (~||r0||)
             scale = np.abs(g[f"est@{k}"]).max()
-            assert np.abs(rep["gfinal"] - g[f"gfinal@{k}"]).max() <= 1e-10 * scale
+            assert np.abs(rep["gfinal"] - g[f"gfinal@{k}"]).max() <= TOL_GFINAL.get(name, 1e-10) * scale
             assert rel_err(s.get_state(), g[f"U@{k}"]) <= 1e-10
             assert rel_err(s.rms(), g[f"rms@{k}"]) <= 1e-10
 
