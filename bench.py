@@ -122,15 +122,87 @@ def run_reference_cpu(case, steps, warmup):
     return times
 
 
-def bench_gpu(args, ws, rank, local):
+def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ranks, sampler=None):
+    """Time FP64 and mixed FDV steps of one workload; returns per-form results and the
+    live EBE element-pass roofline (one extra host-driven step with CUDA events)."""
     import numpy as np
     import torch
     from cfdv_b200 import gpu as G, meshgen as mg
 
-    torch.cuda.set_device(local)
-    W = WORKLOADS[args.workload]
+    W = WORKLOADS[name]
     case = W["make"](mg)
     m, cfl, rtol = W["m"], W["cfl"], 1e-8
+    solver = G.FDVSolver(case)
+    ext = torch.cuda.ExternalStream(solver.stream)
+    forms = [("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)]
+    if args.only:
+        forms = [f for f in forms if f[0] == args.only]
+    out = {"case": case, "solver": solver, "ext": ext, "m": m, "cfl": cfl, "rtol": rtol, "desc": W["desc"]}
+    clocks = None
+    for prec_name, prec in forms:
+        solver.load_node_records()
+        for _ in range(warmup):
+            solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        if sampler is not None and prec_name == forms[-1][0]:
+            sampler.start()
+        solver.profile(True)
+        step_ms, res, mvs = [], [], []
+        for _ in range(steps):
+            with torch.cuda.stream(ext):
+                flush.fill_(1.0)  # evict the previous step's matrices from L2
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+            rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec)
+            with torch.cuda.stream(ext):
+                e1.record(ext)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            res.append(rep["true_rel_res"])
+            mvs.append(rep["matvecs"])
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        stats = solver.profile_read()
+        solver.profile(False)
+        if sampler is not None and prec_name == forms[-1][0]:
+            clocks = sampler.stop()
+        total_s = max_over_ranks(sum(step_ms) / 1e3)
+        # live roofline of the EBE element pass: one more step with the host-driven engine,
+        # whose element passes are separate launches bracketed by CUDA events
+        solver.profile(True)
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec, engine=1)
+        ebe = solver.profile_read()
+        solver.profile(False)
+        out[prec_name] = dict(steps_per_s=ws * steps / total_s, ms_per_step=1e3 * total_s / steps,
+                              true_rel_res_max=max(res), matvecs_per_step=sum(mvs) / len(mvs), stats=stats,
+                              ebe=ebe, state=solver.get_state(),
+                              form_ms=stats["form_ms"] / max(stats["form_launches"], 1),
+                              solve_ms=stats["solve_ms"] / max(stats["solves"], 1))
+    out["clocks"] = clocks
+    return out
+
+
+def ebe_roofline(r, peak, peak_kind, label, traffic=None):
+    e = r["ebe"]
+    if e["total_ms"] <= 0 or e["launches"] == 0:
+        return None
+    achieved = e["bytes"] / (e["total_ms"] / 1e3) / 1e9
+    return {"kernel": label, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "bytes_per_launch": e["bytes"] / e["launches"], "launches": e["launches"],
+            "avg_launch_us": 1e3 * e["total_ms"] / e["launches"]}
+
+
+def bench_gpu(args, ws, rank, local):
+    import numpy as np
+    import torch
+    from cfdv_b200 import gpu as G
+
+    torch.cuda.set_device(local)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     if ws > 1:
         import torch.distributed as dist
@@ -150,71 +222,35 @@ def bench_gpu(args, ws, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    results = {}
-    solver = G.FDVSolver(case)
-    ext = torch.cuda.ExternalStream(solver.stream)
+    peak, peak_kind = peaks()
     sampler = ClockSampler(local)
-    forms = [("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)]
-    if args.only:
-        forms = [f for f in forms if f[0] == args.only]
-    clocks = None
-    for prec_name, prec in forms:
-        solver.load_node_records()
-        for _ in range(args.warmup):
-            solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=prec)
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        if prec_name == forms[-1][0]:
-            sampler.start()
-        solver.profile(True)
-        step_ms, res, mvs = [], [], []
-        for _ in range(args.steps):
-            with torch.cuda.stream(ext):
-                flush.fill_(1.0)  # evict the previous step's matrices from L2
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record(ext)
-            rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=prec)
-            with torch.cuda.stream(ext):
-                e1.record(ext)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            res.append(rep["true_rel_res"])
-            mvs.append(rep["matvecs"])
-        torch.cuda.synchronize()
-        barrier()
-        torch.cuda.synchronize()
-        stats = solver.profile_read()
-        solver.profile(False)
-        if prec_name == forms[-1][0]:
-            clocks = sampler.stop()
-        total_s = max_over_ranks(sum(step_ms) / 1e3)
-        results[prec_name] = dict(steps_per_s=ws * args.steps / total_s, ms_per_step=1e3 * total_s / args.steps,
-                                  true_rel_res_max=max(res), matvecs_per_step=sum(mvs) / len(mvs), stats=stats,
-                                  state=solver.get_state())
-
+    head = measure_workload(args, args.workload, args.steps, args.warmup, flush, ws, barrier, max_over_ranks, sampler)
+    solver, case = head["solver"], head["case"]
     if args.only:  # profiling runs: one form, no end-to-end loop, no JSON line
         solver.close()
         if rank == 0:
-            r = results[args.only]
+            r = head[args.only]
             print(json.dumps({"form": args.only, "steps_per_s": r["steps_per_s"], "ms_per_step": r["ms_per_step"],
                               "true_rel_res_max": r["true_rel_res_max"], "matvecs_per_step": r["matvecs_per_step"],
-                              "ebe": {k: v for k, v in r["stats"].items()}}))
+                              "form_ms": r["form_ms"], "solve_ms": r["solve_ms"], "ebe": r["ebe"]}))
         return
+
     # end-to-end through the C ABI with host buffers: H2D state, step, D2H state every step
+    m, cfl, rtol, ext = head["m"], head["cfl"], head["rtol"], head["ext"]
     n = solver.n_dof
     host = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    out = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    outb = torch.empty(n, dtype=torch.float64, pin_memory=True)
     solver.load_node_records()
     host.numpy()[:] = solver.get_state()
+    solver.profile(True)
     for _ in range(2):
         solver.set_state(host.numpy())
-        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=G.PREC_MIXED)
-        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(out.numpy()), None, n))
-        host.copy_(out)
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED)
+        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(outb.numpy()), None, n))
+        host.copy_(outb)
     torch.cuda.synchronize()
     barrier()
+    solver.profile(True)
     e2e_ms = []
     for _ in range(args.steps):
         with torch.cuda.stream(ext):
@@ -223,25 +259,25 @@ def bench_gpu(args, ws, rank, local):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(ext)
         solver.set_state(host.numpy())
-        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=100, rtol=rtol, precision=G.PREC_MIXED)
-        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(out.numpy()), None, n))
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED)
+        solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(outb.numpy()), None, n))
         with torch.cuda.stream(ext):
             e1.record(ext)
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
-        host.copy_(out)
+        host.copy_(outb)
+    launches_per_step = solver.profile_read()["kernel_launches"] / args.steps
+    solver.profile(False)
     e2e_s = max_over_ranks(sum(e2e_ms) / 1e3)
+    solver.close()
 
-    mixed, fp64 = results["mixed"], results["fp64"]
+    mixed, fp64 = head["mixed"], head["fp64"]
     err = float(np.abs(mixed["state"] - fp64["state"]).max() / np.abs(fp64["state"]).max())
-    st = mixed["stats"]
-    achieved = st["bytes"] / (st["total_ms"] / 1e3) / 1e9 if st["total_ms"] > 0 else None
-    peak, peak_kind = peaks()
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", f"ebe_traffic_{args.workload}.json")
+    tfile = os.path.join(ROOT, "profiles", "ebe_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch_fp32")
+            traffic = json.load(f).get(args.workload)
     line = {
         "metric": METRIC,
         "value": mixed["steps_per_s"],
@@ -255,32 +291,55 @@ def bench_gpu(args, ws, rank, local):
         "vs_baseline": None,
         "dtype": "f32 matrices/f64 vectors (mixed); f64",
         "data": "synthetic",
-        "config": {"workload": W["desc"], "elements": case.n_elements, "dof": solver.n_dof,
-                   "gmres": f"restarted GMRES({m}), MGS, to true relative residual {rtol:g}",
+        "config": {"workload": head["desc"], "elements": case.n_elements, "dof": n,
+                   "gmres": f"restarted GMRES({m}), MGS, right node-block Jacobi, to true relative residual {rtol:g}",
                    "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
         "fp64": {"value": fp64["steps_per_s"], "ms_per_step": fp64["ms_per_step"],
-                 "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"]},
+                 "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"],
+                 "form_ms": fp64["form_ms"], "solve_ms": fp64["solve_ms"]},
         "mixed": {"true_rel_res_max": mixed["true_rel_res_max"], "matvecs_per_step": mixed["matvecs_per_step"],
-                  "max_field_diff_vs_fp64": err},
+                  "form_ms": mixed["form_ms"], "solve_ms": mixed["solve_ms"], "max_field_diff_vs_fp64": err},
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
-        "roofline": {"kernel": "ebe element pass (FP32 matrices)", "bound": "hbm", "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                     "peak_kind": peak_kind,
-                     "traffic": traffic, "bytes_per_launch": st["bytes"] / max(st["launches"], 1),
-                     "launches": st["launches"], "avg_launch_us": 1e3 * st["total_ms"] / max(st["launches"], 1)},
+        "roofline": ebe_roofline(mixed, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.workload + ")",
+                                 traffic),
+        "roofline_fp64": ebe_roofline(fp64, peak, peak_kind, "ebe_elem_kernel, FP64 matrices (" + args.workload + ")"),
         "e2e": {"value": ws * args.steps / e2e_s, "unit": "FDV steps/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": int(st["kernel_launches"]),
-        "clocks": clocks,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "clocks": head["clocks"],
     }
-    solver.close()
+    del head
+    if args.secondary and args.secondary != args.workload:
+        sec = measure_workload(args, args.secondary, 3, 3, flush, ws, barrier, max_over_ranks)
+        sec["solver"].close()
+        s_m, s_f = sec["mixed"], sec["fp64"]
+        stile = None
+        if os.path.exists(tfile):
+            with open(tfile) as f:
+                stile = json.load(f).get(args.secondary)
+        line["secondary"] = {
+            "workload": sec["desc"], "elements": sec["case"].n_elements,
+            "dof": sec["case"].n_nodes * sec["case"].neqn, "steps": 3, "warmup": 3,
+            "mixed": {"value": s_m["steps_per_s"], "ms_per_step": s_m["ms_per_step"],
+                      "true_rel_res_max": s_m["true_rel_res_max"], "matvecs_per_step": s_m["matvecs_per_step"],
+                      "form_ms": s_m["form_ms"], "solve_ms": s_m["solve_ms"]},
+            "fp64": {"value": s_f["steps_per_s"], "ms_per_step": s_f["ms_per_step"],
+                     "true_rel_res_max": s_f["true_rel_res_max"], "matvecs_per_step": s_f["matvecs_per_step"],
+                     "form_ms": s_f["form_ms"], "solve_ms": s_f["solve_ms"]},
+            "mixed_over_fp64": s_m["steps_per_s"] / s_f["steps_per_s"],
+            "roofline": ebe_roofline(s_m, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.secondary + ")",
+                                     stile),
+            "roofline_fp64": ebe_roofline(s_f, peak, peak_kind,
+                                          "ebe_elem_kernel, FP64 matrices (" + args.secondary + ")"),
+        }
     if rank == 0:
         if not args.no_cpu_baseline:
             k = 2
-            times = run_reference_cpu(case, k, 0)
+            from cfdv_b200 import meshgen as mg
+            times = run_reference_cpu(WORKLOADS[args.workload]["make"](mg), k, 0)
             line["cpu_baseline"] = {"value": k / sum(times), "unit": "FDV steps/s", "cores": 1, "kind": "reference",
                                     "sample": f"{k} steps of the same case through oracle/_ref/cfdv_ref (reference "
-                                              f"sources, reference GMRES({m}) x1 restart, not equal residual)"}
+                                              f"sources, reference GMRES({m}) x1 restart: not equal residual)"}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
@@ -317,6 +376,7 @@ def main():
     ap.add_argument("--workload", default="plate", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp64", "mixed"], help="time one form only (profiling runs)")
+    ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('' to skip)")
     args = ap.parse_args()
     ws, rank, local = dist_info()
     if args.impl == "reference":

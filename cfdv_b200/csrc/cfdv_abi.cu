@@ -60,11 +60,14 @@ struct cfdv_ctx {
   double* d_pers = nullptr;  // persistent-solve scratch
   size_t pers_cap = 0;
   int* d_pers_int = nullptr;
+  double* d_Dinv = nullptr;  // node-block Jacobi inverse [Nn][neqn][neqn]
+  double* d_Z = nullptr;     // preconditioned Krylov vector
   // profiling
   bool prof = false;
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_form;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve;
   long mv_launches = 0;
   long launches = 0;    // kernels launched since the last cfdv_profile()
   double mv_bytes = 0;  // algorithmic bytes of the timed element passes
@@ -109,7 +112,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_U); dfree(c->d_U0); dfree(c->d_du);
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
-  dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int);
+  dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
   c->pers_cap = 0;
   if (c->h_pin) cudaFreeHost(c->h_pin);
   c->h_pin = nullptr;
@@ -343,12 +346,14 @@ int read_status(cfdv_ctx* c) {
 
 // One Arnoldi step j: V_{j+1} from A V_j by modified Gram-Schmidt (MPI_GMRES.h:164-181).
 // Leaves h(0..j+1, j) in d_H and copies them to hcol.
-int arnoldi_step(cfdv_ctx* c, int fp32, int m, int j, double* hcol, cfdv_gmres_report* rep) {
+int arnoldi_step(cfdv_ctx* c, int fp32, int m, int j, double* hcol, cfdv_gmres_report* rep, bool pc = false) {
   const size_t n = c->n_dof;
   double* V = c->d_V;
   double* pa = c->d_pa;
   double* pb = c->d_pb;
-  int rc = matvec(c, fp32, V + (size_t)j * n, c->d_W, 0, nullptr, V, pa, rep);  // partial <W, v_0>
+  // right preconditioning: the product acts on z_j = Dinv v_j (written with v_j)
+  const double* x = pc ? c->d_Z : V + (size_t)j * n;
+  int rc = matvec(c, fp32, x, c->d_W, 0, nullptr, V, pa, rep);  // partial <W, v_0>
   if (rc) return rc;
   double* H = c->d_H + (size_t)j * (m + 1);
   for (int i = 0; i <= j; i++) {
@@ -359,6 +364,10 @@ int arnoldi_step(cfdv_ctx* c, int fp32, int m, int j, double* hcol, cfdv_gmres_r
   }
   CK(launch_normalize(c->d_W, (int)n, pa, H + j + 1, V + (size_t)(j + 1) * n, c->st));
   c->launches++;
+  if (pc) {
+    CK(launch_block_apply(c->ndim, c->d_Dinv, V + (size_t)(j + 1) * n, c->d_Z, c->n_nodes, c->st));
+    c->launches++;
+  }
   CK(cudaMemcpyAsync(c->h_pin, H, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   for (int i = 0; i < j + 2; i++) hcol[i] = c->h_pin[i];
@@ -368,11 +377,15 @@ int arnoldi_step(cfdv_ctx* c, int fp32, int m, int j, double* hcol, cfdv_gmres_r
 }
 
 // r = b - A x into W with ||r|| (host), v_0 = r / ||r||
-int restart_residual(cfdv_ctx* c, int fp32, const double* x, double* beta, cfdv_gmres_report* rep) {
+int restart_residual(cfdv_ctx* c, int fp32, const double* x, double* beta, cfdv_gmres_report* rep, bool pc = false) {
   int rc = matvec(c, fp32, x, c->d_W, 1, c->d_b, c->d_W, c->d_pa, rep);
   if (rc) return rc;
   CK(launch_normalize(c->d_W, c->n_dof, c->d_pa, c->d_sc + 0, c->d_V, c->st));
   c->launches++;
+  if (pc) {
+    CK(launch_block_apply(c->ndim, c->d_Dinv, c->d_V, c->d_Z, c->n_nodes, c->st));
+    c->launches++;
+  }
   CK(cudaMemcpyAsync(c->h_pin, c->d_sc, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   *beta = c->h_pin[0];
@@ -389,10 +402,11 @@ int compose_b(cfdv_ctx* c, double* bnorm) {
   return CFDV_OK;
 }
 
-int add_combination(cfdv_ctx* c, const std::vector<double>& y, int mm) {
+int add_combination(cfdv_ctx* c, const std::vector<double>& y, int mm, bool pc = false) {
   for (int i = 0; i < mm; i++) c->h_pin[i] = y[i];
   CK(cudaMemcpyAsync(c->d_y, c->h_pin, sizeof(double) * mm, cudaMemcpyHostToDevice, c->st));
-  CK(launch_combine(c->d_du, c->d_V, c->n_dof, c->d_y, mm, c->st));
+  if (pc) CK(launch_combine_precond(c->ndim, c->d_du, c->d_V, c->n_dof, c->d_y, mm, c->d_Dinv, c->n_nodes, c->st));
+  else CK(launch_combine(c->d_du, c->d_V, c->n_dof, c->d_y, mm, c->st));
   c->launches++;
   CK(cudaStreamSynchronize(c->st));  // h_pin is reused by the next read-back
   return CFDV_OK;
@@ -474,6 +488,16 @@ int gmres_reference(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* re
   return CFDV_OK;
 }
 
+// node-block Jacobi inverse from the FP64 element matrices (one pass over them)
+int build_block_jacobi(cfdv_ctx* c) {
+  int rc;
+  if (!c->d_Dinv && (rc = dalloc(c, &c->d_Dinv, (size_t)c->n_nodes * c->neqn * c->neqn))) return rc;
+  if (!c->d_Z && (rc = dalloc(c, &c->d_Z, (size_t)c->n_dof))) return rc;
+  CK(launch_block_jacobi(c->ndim, c->d_csr_ptr, c->d_csr_idx, c->d_R64, c->n_nodes, c->d_Dinv, c->d_status, c->st));
+  c->launches++;
+  return CFDV_OK;
+}
+
 // Restarted GMRES(m) to ||b - A du|| < rtol ||b||: MGS Arnoldi, Givens QR updated per
 // column, upper-triangular back substitution.  With MIXED precision the Krylov cycles
 // use the FP32 matrices while every restart residual is recomputed with the FP64
@@ -490,19 +514,21 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
   const double atol = o->rtol * bnorm;
   if (rep) { rep->tol = atol; rep->bnorm = bnorm; }
   if (bnorm == 0.0) { if (rep) rep->true_rel_res = 0.0; return CFDV_OK; }
+  const bool pc = o->precond != 0;
+  if (pc && (rc = build_block_jacobi(c))) return rc;
   std::vector<double> h((size_t)(m + 1) * m), g(m + 1), y(m), cs(m), sn(m), hcol(m + 2);
   auto H = [&](int i, int j) -> double& { return h[(size_t)j * (m + 1) + i]; };
   double beta = bnorm;
   bool converged = false;
   for (int gloop = 0; gloop < o->restarts; gloop++) {
-    if ((rc = restart_residual(c, 0, c->d_du, &beta, rep))) return rc;  // FP64 residual
+    if ((rc = restart_residual(c, 0, c->d_du, &beta, rep, pc))) return rc;  // FP64 residual
     if (!std::isfinite(beta)) return fail(c, CFDV_ERR_NONFINITE, "non-finite GMRES residual");
     if (beta < atol) { converged = true; break; }
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
     int k = 0;
     for (int j = 0; j < m; j++) {
-      if ((rc = arnoldi_step(c, fp32, m, j, hcol.data(), rep))) return rc;
+      if ((rc = arnoldi_step(c, fp32, m, j, hcol.data(), rep, pc))) return rc;
       for (int i = 0; i < j + 2; i++) H(i, j) = hcol[i];
       for (int i = 0; i < j; i++) {
         const double t = cs[i] * H(i, j) + sn[i] * H(i + 1, j);
@@ -525,7 +551,7 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
       for (int jj = i + 1; jj < k; jj++) s -= H(i, jj) * y[jj];
       y[i] = s / H(i, i);
     }
-    if ((rc = add_combination(c, y, k))) return rc;
+    if ((rc = add_combination(c, y, k, pc))) return rc;
     if (rep && rep->gfinal && gloop < rep->gfinal_capacity) rep->gfinal[gloop] = g[k];
     if (rep) rep->n_restarts = gloop + 1;
   }
@@ -570,6 +596,11 @@ int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_repor
   a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
   a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;
   a.b = c->d_b; a.du = c->d_du; a.V = c->d_V; a.W = c->d_W; a.part0 = c->d_pa; a.part1 = c->d_pb;
+  if (o->precond) {
+    if ((rc = build_block_jacobi(c))) return rc;
+    a.Dinv = c->d_Dinv;
+    a.Z = c->d_Z;
+  }
   a.H = c->d_H;
   double* p = c->d_pers;
   a.g = p; a.cs = p + (m + 1); a.sn = p + 2 * (m + 1); a.y = p + 3 * (m + 1);
@@ -579,10 +610,17 @@ int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_repor
   int* pi = c->d_pers_int;
   a.stop = pi; a.out = pi + 1; a.err = pi + 2;
   a.bar_count = (unsigned int*)(pi + 3); a.bar_gen = (unsigned int*)(pi + 4);
-  cudaEvent_t* ev = next_events(c);
-  if (ev) cudaEventRecord(ev[0], c->st);
+  std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+  if (c->prof) {
+    cudaEventCreate(&ev.first);
+    cudaEventCreate(&ev.second);
+    cudaEventRecord(ev.first, c->st);
+  }
   CK(launch_gmres_persistent(c->ndim, fp32, a, c->st));
-  if (ev) { cudaEventRecord(ev[1], c->st); cudaEventRecord(ev[2], c->st); }
+  if (c->prof) {
+    cudaEventRecord(ev.second, c->st);
+    c->ev_solve.push_back(ev);
+  }
   c->launches++;
   int hi[8];
   double res[4];
@@ -667,6 +705,7 @@ void cfdv_destroy(cfdv_ctx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto e : c->ev_pool) cudaEventDestroy(e);
   for (auto& e : c->ev_form) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  for (auto& e : c->ev_solve) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   free_all(c);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -913,6 +952,8 @@ int cfdv_profile(cfdv_ctx* c, int enable) {
   }
   for (auto& e : c->ev_form) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   c->ev_form.clear();
+  for (auto& e : c->ev_solve) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  c->ev_solve.clear();
   c->ev_used = 0;
   c->mv_launches = 0;
   c->mv_bytes = 0;
@@ -937,6 +978,12 @@ int cfdv_profile_read(cfdv_ctx* c, cfdv_kernel_stats* out) {
     CK(cudaEventElapsedTime(&ms, e.first, e.second));
     out->form_ms += ms;
     out->form_launches++;
+  }
+  for (auto& e : c->ev_solve) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e.first, e.second));
+    out->solve_ms += ms;
+    out->solves++;
   }
   out->bytes = c->mv_bytes;
   out->kernel_launches = c->launches;

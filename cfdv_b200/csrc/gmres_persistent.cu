@@ -91,6 +91,18 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
   return block_sum(v);
 }
 
+// z_d = sum_s Dinv[n][r][s] * (w[n*NEQ + s] / scale), d = n*NEQ + r, with the same
+// division as the stored v so that z = Dinv v exactly
+template <int NEQ>
+__device__ __forceinline__ double precond_at(const double* Dinv, const double* w, int d, double scale) {
+  const int n = d / NEQ, r = d % NEQ;
+  const double* D = Dinv + (size_t)n * NEQ * NEQ + r * NEQ;
+  double t = 0.0;
+#pragma unroll
+  for (int s = 0; s < NEQ; s++) t += D[s] * (__ldcg(w + (size_t)n * NEQ + s) / scale);
+  return t;
+}
+
 }  // namespace
 
 template <int KE, int NEQ, int NNOD, typename TR>
@@ -192,7 +204,10 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
       converged = true;
       break;
     }
-    for (int d = gtid; d < n; d += gstride) V[d] = __ldcg(W + d) / beta;
+    for (int d = gtid; d < n; d += gstride) {
+      V[d] = __ldcg(W + d) / beta;
+      if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, beta);
+    }
     if (bid == 0 && tid == 0) {
       for (int i = 0; i <= m; i++) a.g[i] = 0.0;
       a.g[0] = beta;
@@ -200,8 +215,8 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     if (!grid_sync(bar, nb)) return;
     int k = 0;
     for (int j = 0; j < m; j++) {
-      double* vj = V + (size_t)j * n;
-      elem_pass_op(vj);
+      const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A Dinv v_j
+      elem_pass_op(xj);
       if (!grid_sync(bar, nb)) return;
       node_pass(sizeof(TR) == 4, 0, W, V, pa);
       mv++;
@@ -225,7 +240,10 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
       }
       const double nrm = sqrt(sum_partials(pa, nb));
       double* vn = V + (size_t)(j + 1) * n;
-      for (int d = gtid; d < n; d += gstride) vn[d] = __ldcg(W + d) / nrm;
+      for (int d = gtid; d < n; d += gstride) {
+        vn[d] = __ldcg(W + d) / nrm;
+        if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, nrm);
+      }
       if (bid == 0 && tid == 0) {
         // Givens QR of column j (rotations of earlier columns are stored in cs/sn)
         Hj[j + 1] = nrm;
@@ -261,9 +279,21 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     }
     if (!grid_sync(bar, nb)) return;
     for (int d = gtid; d < n; d += gstride) {
-      double z = 0.0;
-      for (int i = 0; i < k; i++) z += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + d);
-      a.du[d] += z;
+      if (a.Dinv) {  // du += Dinv (V y)
+        const int nd = d / NEQ, r = d % NEQ;
+        double acc = 0.0;
+#pragma unroll
+        for (int s2 = 0; s2 < NEQ; s2++) {
+          double t = 0.0;
+          for (int i = 0; i < k; i++) t += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + (size_t)nd * NEQ + s2);
+          acc += a.Dinv[(size_t)nd * NEQ * NEQ + r * NEQ + s2] * t;
+        }
+        a.du[d] += acc;
+      } else {
+        double z = 0.0;
+        for (int i = 0; i < k; i++) z += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + d);
+        a.du[d] += z;
+      }
     }
     if (!grid_sync(bar, nb)) return;
     if (bid == 0 && tid == 0) a.out[0] = cycle + 1;
@@ -294,7 +324,9 @@ static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
                                                                 THREADS, 0);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidConfiguration;
-  int blocks = sms * per_sm;
+  // few blocks keep the grid barrier short; large systems take two per SM for bandwidth
+  int blocks = sms * (a.n_dof > (1 << 20) ? 2 : 1);
+  if (blocks > sms * per_sm) blocks = sms * per_sm;
   if (blocks > a.max_blocks) blocks = a.max_blocks;
   PersistentArgs args = a;
   void* params[] = {&args};

@@ -18,6 +18,8 @@ struct PersistentArgs {
   double* du;                  // solution, starts at zero
   double* V;                   // (m+1) Krylov vectors
   double* W;
+  const double* Dinv;          // node-block Jacobi inverse (right preconditioning) or null
+  double* Z;                   // preconditioned vector z_j = Dinv v_j
   double* part0;               // block partials (>= gridDim.x each)
   double* part1;
   double* H;                   // (m+1) x m, column-major

@@ -11,6 +11,7 @@ namespace cfdv {
 enum : int {
   STATUS_NONFINITE_MATRIX = 1,  // a non-finite entry in an element matrix or rhs
   STATUS_NONFINITE_VECTOR = 2,  // a non-finite Krylov scalar
+  STATUS_SINGULAR_BLOCK = 4,    // a node block of the preconditioner is singular (identity used)
 };
 
 constexpr int kRedBlocks = 4 * 148;  // fixed partial count: reductions are deterministic
@@ -105,6 +106,14 @@ cudaError_t launch_reduce(const double* pin, double* out, int do_sqrt, cudaStrea
 cudaError_t launch_combine(double* x, const double* V, int n, const double* y, int m, cudaStream_t st);
 // out[i] = (float) in[i]
 cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t st);
+// node-block Jacobi: Dinv_n = (sum of the node's diagonal element blocks)^-1, FP64
+cudaError_t launch_block_jacobi(int ndim, const int* ptr, const int* idx, const double* R, int n_nodes, double* Dinv,
+                                int* status, cudaStream_t st);
+// z = Dinv v
+cudaError_t launch_block_apply(int ndim, const double* Dinv, const double* v, double* z, int n_nodes, cudaStream_t st);
+// du += Dinv (V y)
+cudaError_t launch_combine_precond(int ndim, double* du, const double* V, size_t ld, const double* y, int m,
+                                   const double* Dinv, int n_nodes, cudaStream_t st);
 // U0 = U ; U += du
 cudaError_t launch_state_update(double* U, double* U0, const double* du, int n, cudaStream_t st);
 // per-field sums of U^2 and U0^2 -> partial[blk][2*neqn]

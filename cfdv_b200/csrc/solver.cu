@@ -222,3 +222,127 @@ cudaError_t launch_rms_partial(const double* U, const double* U0, int n_nodes, i
 }
 
 }  // namespace cfdv
+
+// ---- node-block Jacobi preconditioner (textbook mode) -------------------------
+// D_n = sum over the node's (element, local node) list of the element matrix's diagonal
+// neqn x neqn block at that local node; Dinv_n by Gauss-Jordan with partial pivoting in FP64.
+namespace cfdv {
+
+template <int NEQ, int NNOD>
+__global__ void block_jacobi_kernel(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                    const double* __restrict__ R, int n_nodes, double* Dinv, int* status) {
+  constexpr int KE = NEQ * NNOD;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+    double A[NEQ][2 * NEQ];
+#pragma unroll
+    for (int r = 0; r < NEQ; r++)
+#pragma unroll
+      for (int s = 0; s < 2 * NEQ; s++) A[r][s] = (s - NEQ == r) ? 1.0 : 0.0;
+    for (int p = ptr[n]; p < ptr[n + 1]; p++) {
+      const int v = idx[p];
+      const int e = v / NNOD, l = v % NNOD;
+      const double* Re = R + (size_t)e * KE * KE;
+#pragma unroll
+      for (int s = 0; s < NEQ; s++)
+#pragma unroll
+        for (int r = 0; r < NEQ; r++) A[r][s] += Re[(l * NEQ + s) * KE + l * NEQ + r];
+    }
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < NEQ; c++) {
+      int piv = c;
+      double best = fabs(A[c][c]);
+#pragma unroll
+      for (int r = c + 1; r < NEQ; r++)
+        if (fabs(A[r][c]) > best) { best = fabs(A[r][c]); piv = r; }
+      if (!(best > 0.0)) { ok = false; break; }
+      if (piv != c)
+#pragma unroll
+        for (int s = 0; s < 2 * NEQ; s++) { const double t = A[c][s]; A[c][s] = A[piv][s]; A[piv][s] = t; }
+      const double inv = 1.0 / A[c][c];
+#pragma unroll
+      for (int s = 0; s < 2 * NEQ; s++) A[c][s] *= inv;
+#pragma unroll
+      for (int r = 0; r < NEQ; r++) {
+        if (r == c) continue;
+        const double f = A[r][c];
+#pragma unroll
+        for (int s = 0; s < 2 * NEQ; s++) A[r][s] -= f * A[c][s];
+      }
+    }
+    double* D = Dinv + (size_t)n * NEQ * NEQ;
+#pragma unroll
+    for (int r = 0; r < NEQ; r++)
+#pragma unroll
+      for (int s = 0; s < NEQ; s++) D[r * NEQ + s] = ok ? A[r][NEQ + s] : (r == s ? 1.0 : 0.0);
+    if (!ok) atomicOr(status, STATUS_SINGULAR_BLOCK);
+  }
+}
+
+// z = Dinv v node by node (v may be scaled by 1/nrm on the fly: z = Dinv (w / nrm))
+template <int NEQ>
+__global__ void block_apply_kernel(const double* __restrict__ Dinv, const double* __restrict__ v, double* z,
+                                   int n_nodes) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+    double x[NEQ];
+#pragma unroll
+    for (int s = 0; s < NEQ; s++) x[s] = v[(size_t)n * NEQ + s];
+    const double* D = Dinv + (size_t)n * NEQ * NEQ;
+#pragma unroll
+    for (int r = 0; r < NEQ; r++) {
+      double t = 0.0;
+#pragma unroll
+      for (int s = 0; s < NEQ; s++) t += D[r * NEQ + s] * x[s];
+      z[(size_t)n * NEQ + r] = t;
+    }
+  }
+}
+
+// du += Dinv (sum_i y_i V_i) node by node
+template <int NEQ>
+__global__ void combine_precond_kernel(double* du, const double* __restrict__ V, size_t ld, const double* __restrict__ y,
+                                       int m, const double* __restrict__ Dinv, int n_nodes) {
+  __shared__ double ys[256];
+  for (int i = threadIdx.x; i < m; i += blockDim.x) ys[i] = y[i];
+  __syncthreads();
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+    double t[NEQ];
+#pragma unroll
+    for (int s = 0; s < NEQ; s++) {
+      double acc = 0.0;
+      for (int i = 0; i < m; i++) acc += ys[i] * V[(size_t)i * ld + (size_t)n * NEQ + s];
+      t[s] = acc;
+    }
+    const double* D = Dinv + (size_t)n * NEQ * NEQ;
+#pragma unroll
+    for (int r = 0; r < NEQ; r++) {
+      double acc = 0.0;
+#pragma unroll
+      for (int s = 0; s < NEQ; s++) acc += D[r * NEQ + s] * t[s];
+      du[(size_t)n * NEQ + r] += acc;
+    }
+  }
+}
+
+cudaError_t launch_block_jacobi(int ndim, const int* ptr, const int* idx, const double* R, int n_nodes, double* Dinv,
+                                int* status, cudaStream_t st) {
+  if (ndim == 2) block_jacobi_kernel<4, 4><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status);
+  else block_jacobi_kernel<5, 8><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_block_apply(int ndim, const double* Dinv, const double* v, double* z, int n_nodes, cudaStream_t st) {
+  if (ndim == 2) block_apply_kernel<4><<<kRedBlocks, kRedThreads, 0, st>>>(Dinv, v, z, n_nodes);
+  else block_apply_kernel<5><<<kRedBlocks, kRedThreads, 0, st>>>(Dinv, v, z, n_nodes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_combine_precond(int ndim, double* du, const double* V, size_t ld, const double* y, int m,
+                                   const double* Dinv, int n_nodes, cudaStream_t st) {
+  if (m > 256) return cudaErrorInvalidValue;
+  if (ndim == 2) combine_precond_kernel<4><<<kRedBlocks, kRedThreads, 0, st>>>(du, V, ld, y, m, Dinv, n_nodes);
+  else combine_precond_kernel<5><<<kRedBlocks, kRedThreads, 0, st>>>(du, V, ld, y, m, Dinv, n_nodes);
+  return cudaGetLastError();
+}
+
+}  // namespace cfdv

@@ -48,7 +48,7 @@ class _Params(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("mode", C.c_int), ("m", C.c_int), ("restarts", C.c_int), ("rtol", C.c_double),
-                ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int)]
+                ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int), ("precond", C.c_int)]
 
 
 class _Report(C.Structure):
@@ -59,7 +59,8 @@ class _Report(C.Structure):
 
 class _Stats(C.Structure):
     _fields_ = [("launches", C.c_long), ("total_ms", C.c_double), ("bytes", C.c_double),
-                ("form_launches", C.c_long), ("form_ms", C.c_double), ("kernel_launches", C.c_long)]
+                ("form_launches", C.c_long), ("form_ms", C.c_double), ("kernel_launches", C.c_long),
+                ("solves", C.c_long), ("solve_ms", C.c_double)]
 
 
 _lib = None
@@ -201,9 +202,9 @@ class FDVSolver:
         self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
-    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0):
+    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1):
         return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)),
-                     int(engine))
+                     int(engine), int(precond))
 
     def _report(self, m, restarts):
         est = np.zeros(max(m * max(restarts, 1), 1))
@@ -218,8 +219,8 @@ class FDVSolver:
                 "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
 
     def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False,
-              engine=0):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine)
+              engine=0, precond=True):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond)
         rep, est, fin = self._report(m, restarts)
         self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
         return self._unpack(rep, est, fin)
@@ -233,8 +234,8 @@ class FDVSolver:
         return r
 
     def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-             true_residual=False, engine=0):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine)
+             true_residual=False, engine=0, precond=True):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))
@@ -278,4 +279,4 @@ class FDVSolver:
         self._ck(self.L.cfdv_profile_read(self._ctx, C.byref(s)))
         return {"launches": s.launches, "total_ms": s.total_ms, "bytes": s.bytes,
                 "form_launches": s.form_launches, "form_ms": s.form_ms,
-                "kernel_launches": s.kernel_launches}
+                "kernel_launches": s.kernel_launches, "solves": s.solves, "solve_ms": s.solve_ms}

@@ -54,6 +54,7 @@ int main(int argc, char** argv) {
     o.precision = precision;
     o.true_residual = 0;
     o.engine = 0;
+    o.precond = 1;
     std::vector<double> est((size_t)o.m * o.restarts), gfin(o.restarts);
     cfdv_gmres_report rep;
     std::memset(&rep, 0, sizeof(rep));

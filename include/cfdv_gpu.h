@@ -85,6 +85,9 @@ typedef struct {
   int engine;        /* CORRECT mode: 0 = the whole solve as one persistent cooperative kernel
                         (no host round trip per Arnoldi step), 1 = host-driven (one kernel per
                         pass, Hessenberg column read back every step) */
+  int precond;       /* CORRECT mode: 1 = right node-block Jacobi preconditioning (the inverse of
+                        each node's assembled neqn x neqn diagonal block); the stopping test
+                        stays the true residual of the unpreconditioned system.  0 = none */
 } cfdv_gmres_opts;
 
 typedef struct {
@@ -161,6 +164,8 @@ typedef struct {
   long form_launches;
   double form_ms;
   long kernel_launches; /* every kernel this context launched since cfdv_profile() */
+  long solves;          /* single-launch GMRES solves (engine 0) and their device time */
+  double solve_ms;
 } cfdv_kernel_stats;
 int cfdv_profile(cfdv_ctx* ctx, int enable);
 int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
