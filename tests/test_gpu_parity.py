@@ -29,6 +29,11 @@ TOL_GFINAL = {"cyl4": 1e-6}
 # other case stays below 1e-13.
 TOL_HIST = {"cyl4": 1e-7}
 TOL_U = {"cyl4": 1e-6}
+# The per-field RMS change sqrt(sum U^2 / sum U0^2) - 1 of the cylinder's z-momentum (a
+# field that starts at zero and stays small) amplifies those U differences: the GPU's
+# arithmetic reproduced on the CPU moves the step-1 RMS vector by 0.063 of its max, the GPU
+# by 0.070, and the reference itself, built with FMA contraction, by 0.51 (U by 7.4e-5).
+TOL_RMS = {"cyl4": 0.1}
 
 
 @pytest.fixture(scope="module")
@@ -122,7 +127,7 @@ def test_reference_gmres_matches_golden_history(gpu, name):
             scale = np.abs(g[f"est@{k}"]).max()
             assert np.abs(rep["gfinal"] - g[f"gfinal@{k}"]).max() <= TOL_GFINAL.get(name, 1e-10) * scale
             assert rel_err(s.get_state(), g[f"U@{k}"]) <= TOL_U.get(name, 1e-10)
-            assert rel_err(s.rms(), g[f"rms@{k}"]) <= TOL_U.get(name, 1e-10) * 1e3
+            assert rel_err(s.rms(), g[f"rms@{k}"]) <= TOL_RMS.get(name, 1e-7)
 
 
 def test_reference_mode_long_run_lid32(gpu, oracle_lib):
