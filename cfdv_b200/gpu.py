@@ -20,14 +20,15 @@ PREC_FP64, PREC_MIXED = 0, 1
 GMRES_REFERENCE, GMRES_CORRECT = 0, 1
 
 STATUS = {0: "ok", 1: "bad argument", 2: "CUDA error", 3: "bad mesh", 4: "non-finite value",
-          5: "allocation failed", 6: "call out of order", 7: "not converged"}
+          5: "allocation failed", 6: "call out of order", 7: "not converged",
+          8: "size beyond the static scratch limit"}
 
 # every entry point declared in include/cfdv_gpu.h
 EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error", "cfdv_get_stream",
            "cfdv_set_state", "cfdv_load_node_records", "cfdv_get_state", "cfdv_state_device_ptr", "cfdv_cfl",
            "cfdv_form", "cfdv_set_element_matrices", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
-           "cfdv_profile_read"]
+           "cfdv_profile_read", "cfdv_ebe_matvec_static"]
 
 
 class CfdvError(RuntimeError):
@@ -99,6 +100,7 @@ def lib():
         L.cfdv_matvec.argtypes = [P, P, P, I, I]
         L.cfdv_profile.argtypes = [P, I]
         L.cfdv_profile_read.argtypes = [P, P]
+        L.cfdv_ebe_matvec_static.argtypes = [I, I, I, P, P, P, P, P, P, I, P]
         _lib = L
     return _lib
 

@@ -170,6 +170,39 @@ typedef struct {
 int cfdv_profile(cfdv_ctx* ctx, int enable);
 int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
 
+/* ---- EBE product without device allocation ------------------------------------ */
+/* No counterpart in the reference; it exists for callers of this library that may not
+ * allocate device memory.  Examples: a solver plug-in that runs inside an application
+ * whose own memory pool has already claimed the GPU's free memory, so a cudaMalloc from
+ * the library would fail; or code running between other streams' work, where cudaFree
+ * (and often cudaMalloc) would synchronise the whole device.  A context (cfdv_create)
+ * allocates its buffers, so such callers use this call instead.
+ *
+ * y = A x (transpose = 1: A^T x) for element matrices R [n_elements][Ke*Ke] (column-
+ * major per element, as above), computed by the same element and node passes as
+ * cfdv_matvec.  Every pointer is DEVICE memory owned by the caller:
+ *   conn     [n_elements][nnod] node ids (nnod 4 in 2D, 8 in 3D), as in cfdv_mesh
+ *   node_ptr [n_nodes+1], node_idx [n_elements*nnod]: for node n, the entries
+ *            node_idx[node_ptr[n] .. node_ptr[n+1]) are e*nnod + l for every element e
+ *            and local node l with conn[e*nnod + l] == n, in increasing order
+ *   x, y     [n_nodes*neqn], neqn = ndim + 2; y is overwritten, x and y must not overlap
+ * The element products go to one scratch array compiled into the library, a static
+ * device array of CFDV_STATIC_SCRATCH_DOUBLES doubles (16 MiB) that every GPU which loads
+ * the library keeps until the process exits.  So n_elements * Ke must not exceed
+ * CFDV_STATIC_SCRATCH_DOUBLES (2D quads: 131072 elements, 3D hexes: 52428); a larger
+ * mesh returns CFDV_ERR_TOO_LARGE before any GPU work.  The call allocates nothing.
+ * The first call on a device looks up the array's device address (with that device
+ * current) and keeps it; make that first call before any stream capture begins.  The
+ * work is queued on `stream` (a cudaStream_t; NULL = the default stream) and the call
+ * returns without waiting for it.  All calls share the one array, which keeps the last
+ * call's contents: calls whose work overlaps on a GPU (different streams, or different
+ * host threads, without ordering between them) race on it and give wrong results. */
+#define CFDV_STATIC_SCRATCH_DOUBLES 2097152
+#define CFDV_ERR_TOO_LARGE 8
+int cfdv_ebe_matvec_static(int ndim, int n_nodes, int n_elements, const int* conn, const int* node_ptr,
+                           const int* node_idx, const double* R, const double* x, double* y, int transpose,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif
