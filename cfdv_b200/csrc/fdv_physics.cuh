@@ -106,43 +106,30 @@ CFDV_HD CFDV_INLINE void shape_fn<3>(const double* z, double* Phi, double (*dPxi
   }
 }
 
-// isoparametric Jacobian, physical derivatives dPhi, returns det J; jac[i][j] = dx_i/dxi_j
+// Isoparametric map, split into the pieces a thread block evaluates in parallel:
+//   jac[i][k] = dx_i/dxi_k = sum_N dPxi_N,k x_N,i      (geom_jac_entry, one entry)
+//   det J and, in 3D, the adjugate inv                 (geom_det)
+//   dPhi_N,i from dPxi_N, jac/inv and 1/det            (geom_dphi, one shape function)
+// phys_deriv runs them in sequence for one Gauss point.
+template <int NNOD>
+CFDV_HD CFDV_INLINE double geom_jac_entry(const double (*dPxi)[3], const NodePrim* nd, int i, int k) {
+  double j = 0;
+#pragma unroll
+  for (int N = 0; N < NNOD; N++) j = RN_ADD(j, RN_MUL(dPxi[N][k], nd[N].x[i]));
+  return j;
+}
+
 template <int NDIM>
-CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
-                                             double (*jac)[3]);
+CFDV_HD CFDV_INLINE double geom_det(const double (*j)[3], double (*inv)[3]);
 
 template <>
-CFDV_HD CFDV_INLINE double phys_deriv<2>(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
-                                                double (*jac)[3]) {
-  double j00 = 0, j01 = 0, j10 = 0, j11 = 0;
-#pragma unroll
-  for (int N = 0; N < 4; N++) {
-    j00 = RN_ADD(j00, RN_MUL(dPxi[N][0], nd[N].x[0]));
-    j01 = RN_ADD(j01, RN_MUL(dPxi[N][1], nd[N].x[0]));
-    j10 = RN_ADD(j10, RN_MUL(dPxi[N][0], nd[N].x[1]));
-    j11 = RN_ADD(j11, RN_MUL(dPxi[N][1], nd[N].x[1]));
-  }
-  jac[0][0] = j00; jac[0][1] = j01; jac[1][0] = j10; jac[1][1] = j11;
-  const double J = RN_SUB(RN_MUL(j00, j11), RN_MUL(j10, j01));
-  const double iJ = RN_DIV(1.0, J);
-#pragma unroll
-  for (int N = 0; N < 4; N++) {
-    dPhi[N][0] = RN_MUL(iJ, RN_SUB(RN_MUL(dPxi[N][0], j11), RN_MUL(j10, dPxi[N][1])));
-    dPhi[N][1] = RN_MUL(iJ, RN_SUB(RN_MUL(j00, dPxi[N][1]), RN_MUL(dPxi[N][0], j01)));
-  }
-  return J;
+CFDV_HD CFDV_INLINE double geom_det<2>(const double (*j)[3], double (*inv)[3]) {
+  (void)inv;
+  return RN_SUB(RN_MUL(j[0][0], j[1][1]), RN_MUL(j[1][0], j[0][1]));
 }
 
 template <>
-CFDV_HD CFDV_INLINE double phys_deriv<3>(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
-                                                double (*jac)[3]) {
-  double j[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-#pragma unroll
-  for (int N = 0; N < 8; N++)
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-      for (int k = 0; k < 3; k++) j[i][k] = RN_ADD(j[i][k], RN_MUL(dPxi[N][k], nd[N].x[i]));
+CFDV_HD CFDV_INLINE double geom_det<3>(const double (*j)[3], double (*inv)[3]) {
 #define M3(a, b, c) RN_MUL(RN_MUL(a, b), c)
   const double J = RN_SUB(RN_SUB(RN_SUB(RN_ADD(RN_ADD(M3(j[0][0], j[1][1], j[2][2]), M3(j[0][1], j[1][2], j[2][0])),
                                                M3(j[0][2], j[1][0], j[2][1])),
@@ -151,7 +138,6 @@ CFDV_HD CFDV_INLINE double phys_deriv<3>(const double (*dPxi)[3], const NodePrim
                           M3(j[0][0], j[1][2], j[2][1]));
 #undef M3
 #define D2(a, b, c, d) RN_SUB(RN_MUL(a, b), RN_MUL(c, d))
-  double inv[3][3];
   inv[0][0] = D2(j[1][1], j[2][2], j[1][2], j[2][1]);
   inv[0][1] = -D2(j[1][0], j[2][2], j[1][2], j[2][0]);
   inv[0][2] = D2(j[1][0], j[2][1], j[1][1], j[2][0]);
@@ -162,17 +148,45 @@ CFDV_HD CFDV_INLINE double phys_deriv<3>(const double (*dPxi)[3], const NodePrim
   inv[2][1] = -D2(j[0][0], j[1][2], j[0][2], j[1][0]);
   inv[2][2] = D2(j[0][0], j[1][1], j[0][1], j[1][0]);
 #undef D2
-  const double iJ = RN_DIV(1.0, J);
-#pragma unroll
-  for (int N = 0; N < 8; N++)
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-      dPhi[N][i] = RN_ADD(RN_ADD(RN_MUL(iJ, RN_MUL(inv[i][0], dPxi[N][0])), RN_MUL(iJ, RN_MUL(inv[i][1], dPxi[N][1]))),
-                          RN_MUL(iJ, RN_MUL(inv[i][2], dPxi[N][2])));
+  return J;
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void geom_dphi(const double* dPxi, const double (*j)[3], const double (*inv)[3], double iJ,
+                                   double* dPhi);
+
+template <>
+CFDV_HD CFDV_INLINE void geom_dphi<2>(const double* dPxi, const double (*j)[3], const double (*inv)[3], double iJ,
+                                      double* dPhi) {
+  (void)inv;
+  dPhi[0] = RN_MUL(iJ, RN_SUB(RN_MUL(dPxi[0], j[1][1]), RN_MUL(j[1][0], dPxi[1])));
+  dPhi[1] = RN_MUL(iJ, RN_SUB(RN_MUL(j[0][0], dPxi[1]), RN_MUL(dPxi[0], j[0][1])));
+}
+
+template <>
+CFDV_HD CFDV_INLINE void geom_dphi<3>(const double* dPxi, const double (*j)[3], const double (*inv)[3], double iJ,
+                                      double* dPhi) {
+  (void)j;
 #pragma unroll
   for (int i = 0; i < 3; i++)
+    dPhi[i] = RN_ADD(RN_ADD(RN_MUL(iJ, RN_MUL(inv[i][0], dPxi[0])), RN_MUL(iJ, RN_MUL(inv[i][1], dPxi[1]))),
+                     RN_MUL(iJ, RN_MUL(inv[i][2], dPxi[2])));
+}
+
+// isoparametric Jacobian, physical derivatives dPhi, returns det J; jac[i][j] = dx_i/dxi_j
+template <int NDIM>
+CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
+                                      double (*jac)[3]) {
+  constexpr int NNOD = (NDIM == 2) ? 4 : 8;
 #pragma unroll
-    for (int k = 0; k < 3; k++) jac[i][k] = j[i][k];
+  for (int i = 0; i < NDIM; i++)
+#pragma unroll
+    for (int k = 0; k < NDIM; k++) jac[i][k] = geom_jac_entry<NNOD>(dPxi, nd, i, k);
+  double inv[3][3];
+  const double J = geom_det<NDIM>(jac, inv);
+  const double iJ = RN_DIV(1.0, J);
+#pragma unroll
+  for (int N = 0; N < NNOD; N++) geom_dphi<NDIM>(dPxi[N], jac, inv, iJ, dPhi[N]);
   return J;
 }
 
@@ -240,8 +254,9 @@ template <int NDIM>
 CFDV_HD void jac_a(const GasParams& th, const GpState& f, double* m);
 template <int NDIM>
 CFDV_HD void jac_b(const GasParams& th, const GpState& f, double* m);
+// c(i, j, ., .) for one i (entries i*75 .. i*75+74 of the 3x3 block layout)
 template <int NDIM>
-CFDV_HD void jac_c(const GasParams& th, const GpState& f, double* m);
+CFDV_HD void jac_c_rows(const GasParams& th, const GpState& f, int i, double* m);
 
 template <>
 CFDV_HD CFDV_INLINE void jac_a<2>(const GasParams& th, const GpState& f, double* m) {
@@ -308,43 +323,47 @@ CFDV_HD CFDV_INLINE void jac_b<2>(const GasParams& th, const GpState& f, double*
 }
 
 template <>
-CFDV_HD CFDV_INLINE void jac_c<2>(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < 3 * 3 * 25; i++) m[i] = 0.0;
+CFDV_HD CFDV_INLINE void jac_c_rows<2>(const GasParams& th, const GpState& f, int i, double* m) {
+  double* blk = m + i * 75;
+  for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const double reinv = 1.0 / th.creyn, mu = f.mu;
   const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const double rho = f.U[0], denom = 1. / (rho * rho), denom2 = denom / rho;
   const double l = f.U[1], mv = f.U[2], re = f.U[3];
   const double ll = l * l, lm = l * mv, mm = mv * mv, rv = ll + mm, hkocv = f.k / th.Cv;
-  JC(m, 0, 0, 1, 0) = mu_R * l * denom * reinv;
-  JC(m, 0, 0, 1, 1) = -mu_R / rho * reinv;
-  JC(m, 0, 0, 2, 0) = mu * mv * denom * reinv;
-  JC(m, 0, 0, 2, 2) = -mu / rho * reinv;
-  JC(m, 0, 0, 3, 0) = ((mu_R * ll * denom2 + mu * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
-  JC(m, 0, 0, 3, 1) = (-mu_R + hkocv) * l * denom * reinv;
-  JC(m, 0, 0, 3, 2) = (-mu + hkocv) * mv * denom * reinv;
-  JC(m, 0, 0, 3, 3) = -hkocv / rho * reinv;
-  JC(m, 0, 1, 1, 0) = lambda * mv * denom * reinv;
-  JC(m, 0, 1, 1, 2) = -lambda / rho * reinv;
-  JC(m, 0, 1, 2, 0) = mu * l * denom * reinv;
-  JC(m, 0, 1, 2, 1) = -mu / rho * reinv;
-  JC(m, 0, 1, 3, 0) = (lambda + mu) * lm * denom2 * reinv;
-  JC(m, 0, 1, 3, 1) = -mu * mv * denom * reinv;
-  JC(m, 0, 1, 3, 2) = -lambda * l * denom * reinv;
-  JC(m, 1, 0, 1, 0) = mu * mv * denom * reinv;
-  JC(m, 1, 0, 1, 2) = -mu / rho * reinv;
-  JC(m, 1, 0, 2, 0) = lambda * l * denom * reinv;
-  JC(m, 1, 0, 2, 1) = -lambda / rho * reinv;
-  JC(m, 1, 0, 3, 0) = (mu + lambda) * lm * denom2 * reinv;
-  JC(m, 1, 0, 3, 1) = -lambda * mv * denom * reinv;
-  JC(m, 1, 0, 3, 2) = -mu * l * denom * reinv;
-  JC(m, 1, 1, 1, 0) = mu * l * denom * reinv;
-  JC(m, 1, 1, 1, 1) = -mu / rho * reinv;
-  JC(m, 1, 1, 2, 0) = mu_R * mv * denom * reinv;
-  JC(m, 1, 1, 2, 2) = -mu_R / rho * reinv;
-  JC(m, 1, 1, 3, 0) = ((mu * ll * denom2 + mu_R * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
-  JC(m, 1, 1, 3, 1) = (-mu + hkocv) * l * denom * reinv;
-  JC(m, 1, 1, 3, 2) = (-mu_R + hkocv) * mv * denom * reinv;
-  JC(m, 1, 1, 3, 3) = -hkocv / rho * reinv;
+  if (i == 0) {
+    JC(m, 0, 0, 1, 0) = mu_R * l * denom * reinv;
+    JC(m, 0, 0, 1, 1) = -mu_R / rho * reinv;
+    JC(m, 0, 0, 2, 0) = mu * mv * denom * reinv;
+    JC(m, 0, 0, 2, 2) = -mu / rho * reinv;
+    JC(m, 0, 0, 3, 0) = ((mu_R * ll * denom2 + mu * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+    JC(m, 0, 0, 3, 1) = (-mu_R + hkocv) * l * denom * reinv;
+    JC(m, 0, 0, 3, 2) = (-mu + hkocv) * mv * denom * reinv;
+    JC(m, 0, 0, 3, 3) = -hkocv / rho * reinv;
+    JC(m, 0, 1, 1, 0) = lambda * mv * denom * reinv;
+    JC(m, 0, 1, 1, 2) = -lambda / rho * reinv;
+    JC(m, 0, 1, 2, 0) = mu * l * denom * reinv;
+    JC(m, 0, 1, 2, 1) = -mu / rho * reinv;
+    JC(m, 0, 1, 3, 0) = (lambda + mu) * lm * denom2 * reinv;
+    JC(m, 0, 1, 3, 1) = -mu * mv * denom * reinv;
+    JC(m, 0, 1, 3, 2) = -lambda * l * denom * reinv;
+  } else {
+    JC(m, 1, 0, 1, 0) = mu * mv * denom * reinv;
+    JC(m, 1, 0, 1, 2) = -mu / rho * reinv;
+    JC(m, 1, 0, 2, 0) = lambda * l * denom * reinv;
+    JC(m, 1, 0, 2, 1) = -lambda / rho * reinv;
+    JC(m, 1, 0, 3, 0) = (mu + lambda) * lm * denom2 * reinv;
+    JC(m, 1, 0, 3, 1) = -lambda * mv * denom * reinv;
+    JC(m, 1, 0, 3, 2) = -mu * l * denom * reinv;
+    JC(m, 1, 1, 1, 0) = mu * l * denom * reinv;
+    JC(m, 1, 1, 1, 1) = -mu / rho * reinv;
+    JC(m, 1, 1, 2, 0) = mu_R * mv * denom * reinv;
+    JC(m, 1, 1, 2, 2) = -mu_R / rho * reinv;
+    JC(m, 1, 1, 3, 0) = ((mu * ll * denom2 + mu_R * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+    JC(m, 1, 1, 3, 1) = (-mu + hkocv) * l * denom * reinv;
+    JC(m, 1, 1, 3, 2) = (-mu_R + hkocv) * mv * denom * reinv;
+    JC(m, 1, 1, 3, 3) = -hkocv / rho * reinv;
+  }
 }
 
 template <>
@@ -442,75 +461,103 @@ CFDV_HD CFDV_INLINE void jac_b<3>(const GasParams& th, const GpState& f, double*
 }
 
 template <>
-CFDV_HD CFDV_INLINE void jac_c<3>(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < 225; i++) m[i] = 0.0;
+CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, int i, double* m) {
+  double* blk = m + i * 75;
+  for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const double mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
-  const double rho = f.U[0], denom = 1. / (rho * rho), irho = 1.0;
-  (void)irho;
+  const double rho = f.U[0], denom = 1. / (rho * rho);
   const double l = f.U[1], mv = f.U[2], n = f.U[3], re = f.U[4];
   const double ll = l * l, mm = mv * mv, nn = n * n, hkocv = f.k / th.Cv, TERM1 = f.k / th.Cv * denom;
   const double q = (-re + (ll + mm + nn) / rho);
-  // diagonal (i == j) blocks
-  const double d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
-  JC(m, 0, 0, 1, 0) = mu_R * l * denom; JC(m, 0, 0, 1, 1) = (-mu_R / rho);
-  JC(m, 0, 0, 2, 0) = mu * mv * denom;  JC(m, 0, 0, 2, 2) = (-mu / rho);
-  JC(m, 0, 0, 3, 0) = mu * n * denom;   JC(m, 0, 0, 3, 3) = (-mu / rho);
-  JC(m, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
-  JC(m, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
-  JC(m, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-  JC(m, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-  JC(m, 0, 0, 4, 4) = (-hkocv / rho);
-  const double e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
-  JC(m, 1, 1, 1, 0) = e10; JC(m, 1, 1, 1, 1) = (-mu / rho);
-  JC(m, 1, 1, 2, 0) = e20; JC(m, 1, 1, 2, 2) = (-mu_R / rho);
-  JC(m, 1, 1, 3, 0) = e30; JC(m, 1, 1, 3, 3) = (-mu / rho);
-  JC(m, 1, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
-  JC(m, 1, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-  JC(m, 1, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
-  JC(m, 1, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-  JC(m, 1, 1, 4, 4) = (-hkocv / rho);
-  const double f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
-  JC(m, 2, 2, 1, 0) = f10; JC(m, 2, 2, 1, 1) = (-mu / rho);
-  JC(m, 2, 2, 2, 0) = f20; JC(m, 2, 2, 2, 2) = (-mu / rho);
-  JC(m, 2, 2, 3, 0) = f30; JC(m, 2, 2, 3, 3) = (-mu_R / rho);
-  JC(m, 2, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
-  JC(m, 2, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-  JC(m, 2, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-  JC(m, 2, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
-  JC(m, 2, 2, 4, 4) = (-hkocv / rho);
-  // off-diagonal blocks (i != j)
-  JC(m, 0, 1, 1, 0) = lambda * mv * denom; JC(m, 0, 1, 1, 2) = (-lambda / rho);
-  JC(m, 0, 1, 2, 0) = mu * l * denom;      JC(m, 0, 1, 2, 1) = (-mu / rho);
-  JC(m, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
-  JC(m, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
-  JC(m, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
-  JC(m, 0, 2, 1, 0) = lambda * n * denom;  JC(m, 0, 2, 1, 3) = (-lambda / rho);
-  JC(m, 0, 2, 3, 0) = mu * l * denom;      JC(m, 0, 2, 3, 1) = (-mu / rho);
-  JC(m, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
-  JC(m, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
-  JC(m, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
-  JC(m, 1, 0, 1, 0) = mu * mv * denom;     JC(m, 1, 0, 1, 2) = (-mu / rho);
-  JC(m, 1, 0, 2, 0) = lambda * l * denom;  JC(m, 1, 0, 2, 1) = (-lambda / rho);
-  JC(m, 1, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
-  JC(m, 1, 0, 4, 1) = (mv / rho) * (-lambda / rho);
-  JC(m, 1, 0, 4, 2) = (l / rho) * (-mu / rho);
-  JC(m, 1, 2, 2, 0) = lambda * n * denom;  JC(m, 1, 2, 2, 3) = (-lambda / rho);
-  JC(m, 1, 2, 3, 0) = mu * mv * denom;     JC(m, 1, 2, 3, 2) = (-mu / rho);
-  JC(m, 1, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
-  JC(m, 1, 2, 4, 2) = (n / rho) * (-mu / rho);
-  JC(m, 1, 2, 4, 3) = (mv / rho) * (-lambda / rho);
-  JC(m, 2, 0, 1, 0) = mu * n * denom;      JC(m, 2, 0, 1, 3) = (-mu / rho);
-  JC(m, 2, 0, 3, 0) = lambda * l * denom;  JC(m, 2, 0, 3, 1) = (-lambda / rho);
-  JC(m, 2, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
-  JC(m, 2, 0, 4, 1) = (n / rho) * (-lambda / rho);
-  JC(m, 2, 0, 4, 3) = (l / rho) * (-mu / rho);
-  JC(m, 2, 1, 2, 0) = mu * n * denom;      JC(m, 2, 1, 2, 3) = (-mu / rho);
-  JC(m, 2, 1, 3, 0) = lambda * mv * denom; JC(m, 2, 1, 3, 2) = (-lambda / rho);
-  JC(m, 2, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
-  JC(m, 2, 1, 4, 2) = (n / rho) * (-lambda / rho);
-  JC(m, 2, 1, 4, 3) = (mv / rho) * (-mu / rho);
+  if (i == 0) {
+    const double d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
+    JC(m, 0, 0, 1, 0) = mu_R * l * denom;
+    JC(m, 0, 0, 1, 1) = (-mu_R / rho);
+    JC(m, 0, 0, 2, 0) = mu * mv * denom;
+    JC(m, 0, 0, 2, 2) = (-mu / rho);
+    JC(m, 0, 0, 3, 0) = mu * n * denom;
+    JC(m, 0, 0, 3, 3) = (-mu / rho);
+    JC(m, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
+    JC(m, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
+    JC(m, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+    JC(m, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+    JC(m, 0, 0, 4, 4) = (-hkocv / rho);
+    JC(m, 0, 1, 1, 0) = lambda * mv * denom;
+    JC(m, 0, 1, 1, 2) = (-lambda / rho);
+    JC(m, 0, 1, 2, 0) = mu * l * denom;
+    JC(m, 0, 1, 2, 1) = (-mu / rho);
+    JC(m, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
+    JC(m, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
+    JC(m, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
+    JC(m, 0, 2, 1, 0) = lambda * n * denom;
+    JC(m, 0, 2, 1, 3) = (-lambda / rho);
+    JC(m, 0, 2, 3, 0) = mu * l * denom;
+    JC(m, 0, 2, 3, 1) = (-mu / rho);
+    JC(m, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
+    JC(m, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
+    JC(m, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
+  } else if (i == 1) {
+    const double e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
+    JC(m, 1, 1, 1, 0) = e10;
+    JC(m, 1, 1, 1, 1) = (-mu / rho);
+    JC(m, 1, 1, 2, 0) = e20;
+    JC(m, 1, 1, 2, 2) = (-mu_R / rho);
+    JC(m, 1, 1, 3, 0) = e30;
+    JC(m, 1, 1, 3, 3) = (-mu / rho);
+    JC(m, 1, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
+    JC(m, 1, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+    JC(m, 1, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
+    JC(m, 1, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+    JC(m, 1, 1, 4, 4) = (-hkocv / rho);
+    JC(m, 1, 0, 1, 0) = mu * mv * denom;
+    JC(m, 1, 0, 1, 2) = (-mu / rho);
+    JC(m, 1, 0, 2, 0) = lambda * l * denom;
+    JC(m, 1, 0, 2, 1) = (-lambda / rho);
+    JC(m, 1, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
+    JC(m, 1, 0, 4, 1) = (mv / rho) * (-lambda / rho);
+    JC(m, 1, 0, 4, 2) = (l / rho) * (-mu / rho);
+    JC(m, 1, 2, 2, 0) = lambda * n * denom;
+    JC(m, 1, 2, 2, 3) = (-lambda / rho);
+    JC(m, 1, 2, 3, 0) = mu * mv * denom;
+    JC(m, 1, 2, 3, 2) = (-mu / rho);
+    JC(m, 1, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
+    JC(m, 1, 2, 4, 2) = (n / rho) * (-mu / rho);
+    JC(m, 1, 2, 4, 3) = (mv / rho) * (-lambda / rho);
+  } else {
+    const double f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
+    JC(m, 2, 2, 1, 0) = f10;
+    JC(m, 2, 2, 1, 1) = (-mu / rho);
+    JC(m, 2, 2, 2, 0) = f20;
+    JC(m, 2, 2, 2, 2) = (-mu / rho);
+    JC(m, 2, 2, 3, 0) = f30;
+    JC(m, 2, 2, 3, 3) = (-mu_R / rho);
+    JC(m, 2, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
+    JC(m, 2, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+    JC(m, 2, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+    JC(m, 2, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
+    JC(m, 2, 2, 4, 4) = (-hkocv / rho);
+    JC(m, 2, 0, 1, 0) = mu * n * denom;
+    JC(m, 2, 0, 1, 3) = (-mu / rho);
+    JC(m, 2, 0, 3, 0) = lambda * l * denom;
+    JC(m, 2, 0, 3, 1) = (-lambda / rho);
+    JC(m, 2, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
+    JC(m, 2, 0, 4, 1) = (n / rho) * (-lambda / rho);
+    JC(m, 2, 0, 4, 3) = (l / rho) * (-mu / rho);
+    JC(m, 2, 1, 2, 0) = mu * n * denom;
+    JC(m, 2, 1, 2, 3) = (-mu / rho);
+    JC(m, 2, 1, 3, 0) = lambda * mv * denom;
+    JC(m, 2, 1, 3, 2) = (-lambda / rho);
+    JC(m, 2, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
+    JC(m, 2, 1, 4, 2) = (n / rho) * (-lambda / rho);
+    JC(m, 2, 1, 4, 3) = (mv / rho) * (-mu / rho);
+  }
   const double reinv = 1.0 / th.creyn;
-  for (int i = 0; i < 225; i++) m[i] *= reinv;
+  for (int k = 0; k < 75; k++) blk[k] *= reinv;
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void jac_c(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < NDIM; i++) jac_c_rows<NDIM>(th, f, i, m);
 }
 
 // convective + viscous flux of one node, FG[i*5+r] = F(i,r) + G(i,r).

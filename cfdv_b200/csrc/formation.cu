@@ -10,35 +10,21 @@
 namespace cfdv {
 
 template <int NDIM>
-__global__ void __launch_bounds__(FormTraits<NDIM>::THREADS) fdv_form_kernel(FormArgs a) {
-  using T = FormTraits<NDIM>;
+__global__ void __launch_bounds__(FormTraits<NDIM>::THREADS, FormTraits<NDIM>::MIN_BLOCKS)
+    fdv_form_kernel(FormArgs a) {
   __shared__ FormShared<NDIM> sh;
   __shared__ int bad;
   FormRegs<NDIM> rg;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
   for (int e = blockIdx.x; e < a.n_elements; e += gridDim.x) {
-    phase_load<NDIM>(a, sh, e, tid);
+    form_step<NDIM>(0, a, sh, e, tid, rg, &bad);
     __syncthreads();
-    if (tid < T::Q) phase_domain_gp<NDIM>(a, sh, tid);
-    __syncthreads();
-    phase_hmat<NDIM>(a, sh, T::Q, 1.0, tid);
-    __syncthreads();
-    phase_contract_domain<NDIM>(sh, tid, rg);
-    __syncthreads();
-    const int nf = sh.nfaces;
-    for (int lf = 0; lf < nf; lf++) {
-      if (tid < T::QF) phase_face_gp<NDIM>(a, sh, lf, tid);
-      __syncthreads();
-      phase_hmat<NDIM>(a, sh, T::QF, -1.0, tid);
-      __syncthreads();
-      phase_contract_face<NDIM>(sh, lf, tid, rg);
+    const int n = form_nsteps<NDIM>(sh);
+    for (int k = 1; k < n; k++) {
+      form_step<NDIM>(k, a, sh, e, tid, rg, &bad);
       __syncthreads();
     }
-    phase_stage<NDIM>(sh, tid, rg);
-    __syncthreads();
-    phase_write<NDIM>(a, sh, e, tid, rg, &bad);
-    __syncthreads();
   }
   if (tid == 0 && bad) atomicOr(a.status, STATUS_NONFINITE_MATRIX);
 }

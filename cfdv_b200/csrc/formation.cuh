@@ -38,9 +38,18 @@ struct FormTraits {
   static constexpr int THREADS = NP * SPLIT;         // 64 (2D) / 128 (3D)
   static constexpr int RS = NEQ * NEQ;
   static constexpr int RS_PER = (RS + SPLIT - 1) / SPLIT;  // (r,s) entries per thread
+  static constexpr int MIN_BLOCKS = (NDIM == 2) ? 8 : 5;   // resident blocks per SM (register cap)
 };
 
 // one Gauss point's worth of coefficients
+template <int NDIM>
+struct GpGeom {  // isoparametric map at the Gauss point (dead once the flow state exists)
+  double jac[3][3];  // dx_i / dxi_k
+  double inv[3][3];  // adjugate (3D)
+  double iJ;         // 1 / det
+  double dPxi[FormTraits<NDIM>::NNOD][3];
+};
+
 template <int NDIM>
 struct GpSlot {
   static constexpr int NNOD = FormTraits<NDIM>::NNOD;
@@ -51,9 +60,16 @@ struct GpSlot {
   double en[3];
   double A[NDIM][25];  // a, then a + b
   double D[NDIM][25];  // b, then s2 a + s4 b
-  double X[NDIM][25];  // dt (s1 a + s3 b)
   double H[9][25];     // c, then h (domain) or m (face)
   double P[NDIM][5];   // rhs coefficient per direction and equation
+  union {
+    GpState st;          // flow state (until the Jacobians are formed)
+    double X[NDIM][25];  // dt (s1 a + s3 b)
+  };
+  union {
+    GpGeom<NDIM> g;
+    double F[NDIM + 1][5];  // Fbar(i, r) for i < NDIM, div F(r) in row NDIM
+  };
 };
 
 template <int NDIM>
@@ -82,29 +98,6 @@ CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
   if (ndim == 2) return (f + i) & 3;
   const int tbl[6][4] = {{3, 2, 1, 0}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}, {6, 7, 4, 5}};
   return tbl[f][i];
-}
-
-// ---------------------------------------------------------------------------
-template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_load(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid) {
-  using T = FormTraits<NDIM>;
-  if (tid < T::NNOD) {
-    const int n = a.conn[(size_t)e * T::NNOD + tid];
-    node_unpack<NDIM>(a.gas, a.U + (size_t)n * T::NEQ, a.x + (size_t)n * NDIM, sh.nd[tid]);
-  }
-  if (tid == 0) {
-    int nf = 0;
-    for (int f = 0; f < T::NFACE; f++) {
-      const int c = a.bc[(size_t)e * T::NFACE + f];
-      if (c != 0 && c < 100) {  // FDVGalerkin.h:460
-        sh.faces[nf] = f;
-        sh.codes[nf] = c;
-        nf++;
-      }
-    }
-    sh.nfaces = nf;
-    sh.mask = a.rowmask ? a.rowmask[e] : 0ull;
-  }
 }
 
 // FDVParam.h:15-111 on the element's nodes; s = {s1, s2, s3, s4}
@@ -161,122 +154,296 @@ CFDV_HD CFDV_INLINE void gp_jacobians(const FormArgs& a, const GpState& f, const
       }
 }
 
-// Domain Gauss point q (GaussQuad.h:69-112 loop order: q = (i*2 + j)*2 + k)
+// ---- domain steps ------------------------------------------------------------
+// The domain part of an element runs as block-wide steps separated by barriers.  Each
+// step hands independent values (one Jacobian entry, one state sum, one flux column,
+// one h entry ...) to separate threads; every value is computed by the same expression,
+// in the same order, as a single thread would compute it for the whole Gauss point.
+
+// Gauss point q: natural coordinates, returns the weight (GaussQuad.h:69-112 loop order:
+// q = (i*2 + j)*2 + k)
 template <int NDIM>
-CFDV_HD void phase_domain_gp(const FormArgs& a, FormShared<NDIM>& sh, int q) {
-  using T = FormTraits<NDIM>;
-  constexpr int NNOD = T::NNOD, NEQ = T::NEQ;
-  GpSlot<NDIM>& sl = sh.slot[q];
-  double z[3], w = 1.0;
+CFDV_HD CFDV_INLINE double gp_point(const FormArgs& a, int q, double* z) {
+  double w = 1.0;
   for (int d = 0; d < NDIM; d++) {
     const int bit = (q >> (NDIM - 1 - d)) & 1;
     z[d] = a.gz[bit];
     w *= a.gw[bit];
   }
-  double s[4];
-  fdv_params<NDIM>(a.gas, sh.nd, s);
-  if (q == 0)
-    for (int i = 0; i < 4; i++) sh.s[i] = s[i];
-  double dPxi[NNOD][3], jac[3][3];
-  shape_fn<NDIM>(z, sl.Phi, dPxi);
-  const double J = phys_deriv<NDIM>(dPxi, sh.nd, sl.dPhi, jac);
-  sl.wJ = w * J;
-  const NodePrim* ndp[NNOD];
-  for (int N = 0; N < NNOD; N++) ndp[N] = &sh.nd[N];
-  GpState f;
-  gp_state<NDIM>(a.gas, NNOD, ndp, sl.Phi, sl.dPhi, f);
-  viscous_stress<NDIM>(f);
+  return w;
+}
 
-  double tau = 0.0;
-  for (int N = 0; N < NNOD; N++) sl.Psi[N] = 0.0;
-  if (NDIM == 2) {  // streamline-upwind numerical diffusion (FDVGalerkin.h:225-332)
-    // evaluated in the reference's operation order without contraction (RN_*), because
-    // the exact-zero tests below decide whether a term is present at all
-    const double J_xi = RN_ADD(RN_MUL(jac[0][0], jac[0][0]), RN_MUL(jac[1][0], jac[1][0]));
-    const double J_eta = RN_ADD(RN_MUL(jac[0][1], jac[0][1]), RN_MUL(jac[1][1], jac[1][1]));
-    const double ixi = RN_DIV(1., sqrt(J_xi)), ieta = RN_DIV(1., sqrt(J_eta));
-    const double v_xi = RN_ADD(RN_MUL(f.v[0], RN_MUL(ixi, jac[0][0])), RN_MUL(f.v[1], RN_MUL(ixi, jac[1][0])));
-    const double v_eta = RN_ADD(RN_MUL(f.v[0], RN_MUL(ieta, jac[0][1])), RN_MUL(f.v[1], RN_MUL(ieta, jac[1][1])));
-    const double S = RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]));
-    // element extents between opposite edge midpoints, accumulated node by node with the
-    // edge-midpoint interpolants (the eta extent is taken bottom minus top)
-    const NodePrim* q4 = sh.nd;
-    const double h_xi =
-        RN_SUB(RN_ADD(RN_ADD(-RN_MUL(0.5, q4[0].x[0]), RN_MUL(0.5, q4[1].x[0])), RN_MUL(0.5, q4[2].x[0])),
-               RN_MUL(0.5, q4[3].x[0]));
-    const double h_eta =
-        RN_SUB(RN_SUB(RN_ADD(RN_MUL(0.5, q4[0].x[1]), RN_MUL(0.5, q4[1].x[1])), RN_MUL(0.5, q4[2].x[1])),
-               RN_MUL(0.5, q4[3].x[1]));
-    const double R_xi = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_xi), h_xi), f.mu);
-    const double R_eta = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_eta), h_eta), f.mu);
-    const double al_xi = (R_xi == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_xi / 2.), sinh(R_xi / 2.)), RN_DIV(2., R_xi));
-    const double al_eta = (R_eta == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_eta / 2.), sinh(R_eta / 2.)), RN_DIV(2., R_eta));
-    tau = (S == 0) ? 0.0
-                   : RN_DIV(RN_MUL(0.25, RN_ADD(RN_MUL(RN_MUL(al_xi, h_xi), v_xi), RN_MUL(RN_MUL(al_eta, h_eta), v_eta))),
-                            S);
-    for (int N = 0; N < NNOD; N++)
-      sl.Psi[N] = RN_ADD(RN_MUL(RN_MUL(tau, f.v[0]), sl.dPhi[N][0]), RN_MUL(RN_MUL(tau, f.v[1]), sl.dPhi[N][1]));
-    // discontinuity capturing (FDVGalerkin.h:336-387); in 3D tau = 0 makes it vanish
-    double A[2] = {0, 0};
-    for (int k = 0; k < 2; k++)
-      for (int j = 0; j < 2; j++) A[j] = RN_ADD(A[j], RN_MUL(f.dV[j][k], f.v[k]));
-    const double gam = RN_MUL(sqrt(RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]))),
-                              sqrt(RN_ADD(RN_MUL(A[0], A[0]), RN_MUL(A[1], A[1]))));
-    double tau_b = 0.0;
-    if (gam != 0) {
-      tau_b = RN_ADD(RN_DIV(RN_MUL(RN_MUL(tau, f.v[0]), A[0]), gam), RN_DIV(RN_MUL(RN_MUL(tau, f.v[1]), A[1]), gam));
-      if (RN_SUB(tau_b, tau) < 0) tau_b = tau;
-    }
-    for (int N = 0; N < NNOD; N++)
-      sl.Psi[N] = RN_ADD(RN_ADD(sl.Psi[N], RN_MUL(RN_MUL(tau_b, f.v[0]), sl.dPhi[N][0])),
-                         RN_MUL(RN_MUL(tau_b, f.v[1]), sl.dPhi[N][1]));
+// step 0: node unpack (NodeUnpack.h:185-205), boundary face list, shape functions
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid) {
+  using T = FormTraits<NDIM>;
+  if (tid < T::NNOD) {
+    const int n = a.conn[(size_t)e * T::NNOD + tid];
+    node_unpack<NDIM>(a.gas, a.U + (size_t)n * T::NEQ, a.x + (size_t)n * NDIM, sh.nd[tid]);
   }
+  if (tid == 32 % T::THREADS) {
+    int nf = 0;
+    for (int f = 0; f < T::NFACE; f++) {
+      const int c = a.bc[(size_t)e * T::NFACE + f];
+      if (c != 0 && c < 100) {  // FDVGalerkin.h:460
+        sh.faces[nf] = f;
+        sh.codes[nf] = c;
+        nf++;
+      }
+    }
+    sh.nfaces = nf;
+    sh.mask = a.rowmask ? a.rowmask[e] : 0ull;
+  }
+  const int q = tid - (T::THREADS - T::Q);
+  if (q >= 0) {
+    double z[3];
+    gp_point<NDIM>(a, q, z);
+    shape_fn<NDIM>(z, sh.slot[q].Phi, sh.slot[q].g.dPxi);
+  }
+}
 
-  gp_jacobians<NDIM>(a, f, s, sl);
+// step 1: isoparametric Jacobian entries (q, i, k); FDV parameters of the element
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_geom_jac(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  if (tid < T::Q * NDIM * NDIM) {
+    const int q = tid / (NDIM * NDIM), i = (tid / NDIM) % NDIM, k = tid % NDIM;
+    GpSlot<NDIM>& sl = sh.slot[q];
+    sl.g.jac[i][k] = geom_jac_entry<T::NNOD>(sl.g.dPxi, sh.nd, i, k);
+  }
+  if (tid == T::THREADS - 1) fdv_params<NDIM>(a.gas, sh.nd, sh.s);
+}
 
-  // rhs coefficient: P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s)
-  // with Fbar = sum_b Phi_b FG_b, divF(s) = sum_j sum_b dPhi_bj FG_b(j,s)  (FDVGalerkin.h:549-609, 410-427)
-  double Fbar[NDIM][5], divF[5];
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < 5; r++) Fbar[i][r] = 0.0;
-  for (int r = 0; r < 5; r++) divF[r] = 0.0;
+// step 2: determinant, adjugate, integration weight (one thread per Gauss point)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_geom_det(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  if (tid < FormTraits<NDIM>::Q) {
+    GpSlot<NDIM>& sl = sh.slot[tid];
+    double z[3];
+    const double w = gp_point<NDIM>(a, tid, z);
+    const double J = geom_det<NDIM>(sl.g.jac, sl.g.inv);
+    sl.g.iJ = RN_DIV(1.0, J);
+    sl.wJ = w * J;
+  }
+}
+
+// step 3: physical shape-function derivatives (q, N)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_dphi(FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  if (tid < T::Q * T::NNOD) {
+    GpSlot<NDIM>& sl = sh.slot[tid / T::NNOD];
+    const int N = tid % T::NNOD;
+    geom_dphi<NDIM>(sl.g.dPxi[N], sl.g.jac, sl.g.inv, sl.g.iJ, sl.dPhi[N]);
+  }
+}
+
+// Gauss-point state sums (FDVGalerkin.h:761-797): value v of the state at slot sl is
+// sum_N coef_N * field_N, coef = Phi_N or dPhi_N,c
+template <int NDIM>
+struct StateSums {
+  static constexpr int NEQ = NDIM + 2;
+  static constexpr int COUNT = 2 + NEQ + NEQ * NDIM + NDIM + NDIM + NDIM * NDIM;
+};
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void state_sum(const NodePrim* nd, GpSlot<NDIM>& sl, int v) {
+  constexpr int NEQ = NDIM + 2, NNOD = FormTraits<NDIM>::NNOD;
+  GpState& f = sl.st;
+  double* dst;
+  int c = -1, kind, idx = 0;  // kind: 0 E, 1 T, 2 U[idx], 3 v[idx]
+  if (v == 0) { dst = &f.E; kind = 0; }
+  else if (v == 1) { dst = &f.T; kind = 1; }
+  else if ((v -= 2) < NEQ) { dst = &f.U[v]; kind = 2; idx = v; }
+  else if ((v -= NEQ) < NEQ * NDIM) { idx = v / NDIM; c = v % NDIM; dst = &f.dU[idx][c]; kind = 2; }
+  else if ((v -= NEQ * NDIM) < NDIM) { dst = &f.v[v]; kind = 3; idx = v; }
+  else if ((v -= NDIM) < NDIM) { dst = &f.dT[v]; kind = 1; c = v; }
+  else { v -= NDIM; idx = v / NDIM; c = v % NDIM; dst = &f.dV[idx][c]; kind = 3; }
+  double acc = 0;
+  for (int N = 0; N < NNOD; N++) {
+    const NodePrim& n = nd[N];
+    const double coef = (c < 0) ? sl.Phi[N] : sl.dPhi[N][c];
+    const double val = (kind == 0) ? n.E : (kind == 1) ? n.T : (kind == 2) ? n.U[idx] : n.v[idx];
+    acc = RN_ADD(acc, RN_MUL(coef, val));
+  }
+  *dst = acc;
+}
+
+// step 4: the state sums (q, value)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_state(FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  constexpr int NV = StateSums<NDIM>::COUNT;
+  for (int t = tid; t < T::Q * NV; t += T::THREADS) state_sum<NDIM>(sh.nd, sh.slot[t / NV], t % NV);
+}
+
+// 2D streamline-upwind test function Psi (FDVGalerkin.h:225-332) with discontinuity
+// capturing (FDVGalerkin.h:336-387), evaluated in the reference's operation order without
+// contraction (RN_*), because its exact-zero tests decide whether a term is present at all
+CFDV_HD CFDV_INLINE void supg_psi_2d(const FormShared<2>& sh, GpSlot<2>& sl) {
+  const GpState& f = sl.st;
+  const auto& jac = sl.g.jac;
+  const double J_xi = RN_ADD(RN_MUL(jac[0][0], jac[0][0]), RN_MUL(jac[1][0], jac[1][0]));
+  const double J_eta = RN_ADD(RN_MUL(jac[0][1], jac[0][1]), RN_MUL(jac[1][1], jac[1][1]));
+  const double ixi = RN_DIV(1., sqrt(J_xi)), ieta = RN_DIV(1., sqrt(J_eta));
+  const double v_xi = RN_ADD(RN_MUL(f.v[0], RN_MUL(ixi, jac[0][0])), RN_MUL(f.v[1], RN_MUL(ixi, jac[1][0])));
+  const double v_eta = RN_ADD(RN_MUL(f.v[0], RN_MUL(ieta, jac[0][1])), RN_MUL(f.v[1], RN_MUL(ieta, jac[1][1])));
+  const double S = RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]));
+  // element extents between opposite edge midpoints, accumulated node by node with the
+  // edge-midpoint interpolants (the eta extent is taken bottom minus top)
+  const NodePrim* q4 = sh.nd;
+  const double h_xi =
+      RN_SUB(RN_ADD(RN_ADD(-RN_MUL(0.5, q4[0].x[0]), RN_MUL(0.5, q4[1].x[0])), RN_MUL(0.5, q4[2].x[0])),
+             RN_MUL(0.5, q4[3].x[0]));
+  const double h_eta =
+      RN_SUB(RN_SUB(RN_ADD(RN_MUL(0.5, q4[0].x[1]), RN_MUL(0.5, q4[1].x[1])), RN_MUL(0.5, q4[2].x[1])),
+             RN_MUL(0.5, q4[3].x[1]));
+  const double R_xi = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_xi), h_xi), f.mu);
+  const double R_eta = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_eta), h_eta), f.mu);
+  const double al_xi = (R_xi == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_xi / 2.), sinh(R_xi / 2.)), RN_DIV(2., R_xi));
+  const double al_eta = (R_eta == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_eta / 2.), sinh(R_eta / 2.)), RN_DIV(2., R_eta));
+  const double tau = (S == 0) ? 0.0
+                              : RN_DIV(RN_MUL(0.25, RN_ADD(RN_MUL(RN_MUL(al_xi, h_xi), v_xi),
+                                                            RN_MUL(RN_MUL(al_eta, h_eta), v_eta))),
+                                       S);
+  for (int N = 0; N < 4; N++)
+    sl.Psi[N] = RN_ADD(RN_MUL(RN_MUL(tau, f.v[0]), sl.dPhi[N][0]), RN_MUL(RN_MUL(tau, f.v[1]), sl.dPhi[N][1]));
+  double A[2] = {0, 0};
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++) A[j] = RN_ADD(A[j], RN_MUL(f.dV[j][k], f.v[k]));
+  const double gam = RN_MUL(sqrt(RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]))),
+                            sqrt(RN_ADD(RN_MUL(A[0], A[0]), RN_MUL(A[1], A[1]))));
+  double tau_b = 0.0;
+  if (gam != 0) {
+    tau_b = RN_ADD(RN_DIV(RN_MUL(RN_MUL(tau, f.v[0]), A[0]), gam), RN_DIV(RN_MUL(RN_MUL(tau, f.v[1]), A[1]), gam));
+    if (RN_SUB(tau_b, tau) < 0) tau_b = tau;
+  }
+  for (int N = 0; N < 4; N++)
+    sl.Psi[N] = RN_ADD(RN_ADD(sl.Psi[N], RN_MUL(RN_MUL(tau_b, f.v[0]), sl.dPhi[N][0])),
+                       RN_MUL(RN_MUL(tau_b, f.v[1]), sl.dPhi[N][1]));
+}
+
+// step 5: viscosity, conductivity, stress; the 2D test function (one thread per Gauss point)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_stress(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  if (tid < T::Q) {
+    GpSlot<NDIM>& sl = sh.slot[tid];
+    sl.st.mu = gas_mu(a.gas, sl.st.T);
+    sl.st.k = gas_k(a.gas, sl.st.mu);
+    viscous_stress<NDIM>(sl.st);
+    for (int N = 0; N < T::NNOD; N++) sl.Psi[N] = 0.0;  // 3D: tau = 0, no upwinding
+    if constexpr (NDIM == 2) supg_psi_2d(sh, sl);
+  }
+}
+
+// rhs flux sums for equation r at one Gauss point (FDVGalerkin.h:549-609, 410-427):
+// Fbar(i,r) = sum_b Phi_b FG_b(i,r), divF(r) = sum_b sum_i dPhi_b,i FG_b(i,r)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void flux_sums(const FormArgs& a, const NodePrim* nd, GpSlot<NDIM>& sl, int r) {
+  constexpr int NNOD = FormTraits<NDIM>::NNOD;
+  double Fbar[NDIM], divF = 0.0;
+  for (int i = 0; i < NDIM; i++) Fbar[i] = 0.0;
   const bool withF = (NDIM == 2) || a.physical_3d_flux;
   for (int b = 0; b < NNOD; b++) {
     double FG[15];
-    node_flux<NDIM>(f, sh.nd[b], a.gas.creyn, withF, FG);
-    for (int i = 0; i < NDIM; i++)
-      for (int r = 0; r < NEQ; r++) {
-        Fbar[i][r] += sl.Phi[b] * FG[i * 5 + r];
-        divF[r] += sl.dPhi[b][i] * FG[i * 5 + r];
-      }
-  }
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < NEQ; r++) {
-      double t = 0.0;
-      for (int q2 = 0; q2 < NEQ; q2++) t += sl.A[i][r * 5 + q2] * divF[q2];
-      sl.P[i][r] = a.dt * Fbar[i][r] - a.dtsq_2 * t;
+    node_flux<NDIM>(sl.st, nd[b], a.gas.creyn, withF, FG);
+    for (int i = 0; i < NDIM; i++) {
+      Fbar[i] += sl.Phi[b] * FG[i * 5 + r];
+      divF += sl.dPhi[b][i] * FG[i * 5 + r];
     }
+  }
+  for (int i = 0; i < NDIM; i++) sl.F[i][r] = Fbar[i];
+  sl.F[NDIM][r] = divF;
 }
 
+// step 6: flux Jacobians a, b, c (FDV/NavierStokes2D.h, NavierStokes3D.h) and the rhs flux
+// sums; each kind of task fills whole warps where the block has them
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_jacobians(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  constexpr int Q = T::Q, NEQ = T::NEQ;
+  constexpr int C0 = 0, CN = Q * NDIM;                       // c, one block row i each
+  constexpr int A0 = (NDIM == 3) ? 104 : 8, B0 = 32;         // a, b: one Gauss point each
+  constexpr int F0 = (NDIM == 3) ? 64 : 36, FN = Q * NEQ;    // flux sums: (q, r)
+  static_assert(CN <= A0 && A0 + Q <= T::THREADS && B0 + Q <= F0 && F0 + FN <= T::THREADS &&
+                    (NDIM == 2 || F0 + FN <= A0) && (NDIM == 3 || A0 + Q <= B0),
+                "task ranges overlap");
+  if (tid >= C0 && tid < C0 + CN) {
+    GpSlot<NDIM>& sl = sh.slot[(tid - C0) / NDIM];
+    jac_c_rows<NDIM>(a.gas, sl.st, (tid - C0) % NDIM, &sl.H[0][0]);
+  } else if (tid >= A0 && tid < A0 + Q) {
+    GpSlot<NDIM>& sl = sh.slot[tid - A0];
+    jac_a<NDIM>(a.gas, sl.st, &sl.A[0][0]);
+  } else if (tid >= B0 && tid < B0 + Q) {
+    GpSlot<NDIM>& sl = sh.slot[tid - B0];
+    jac_b<NDIM>(a.gas, sl.st, &sl.D[0][0]);
+  } else if (tid >= F0 && tid < F0 + FN) {
+    flux_sums<NDIM>(a, sh.nd, sh.slot[(tid - F0) / NEQ], (tid - F0) % NEQ);
+  }
+}
+
+// step 7: X = dt (s1 a + s3 b), A = a + b, D = s2 a + s4 b, entry by entry (q, i, r, s)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_coeffs(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ, PER = NDIM * NEQ * NEQ;
+  const double* s = sh.s;
+  for (int t = tid; t < T::Q * PER; t += T::THREADS) {
+    GpSlot<NDIM>& sl = sh.slot[t / PER];
+    const int rem = t % PER, i = rem / (NEQ * NEQ), r = (rem / NEQ) % NEQ, c = rem % NEQ;
+    const int k = r * 5 + c;
+    const double av = sl.A[i][k], bv = sl.D[i][k];
+    sl.X[i][k] = a.dt * (s[0] * av + s[2] * bv);
+    sl.A[i][k] = av + bv;
+    sl.D[i][k] = s[1] * av + s[3] * bv;
+  }
+}
+
+// one entry of h (sign = +1, domain) or m (sign = -1, face):
+// h_ij(r,s) = -dt s3 c_ij(r,s) + dt^2/2 sum_k A_i(r,k) D_j(k,s)  (FDVGalerkin.h:611-628, 698-715)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int it, double sign) {
+  constexpr int NEQ = NDIM + 2;
+  constexpr int PER = NDIM * NDIM * NEQ * NEQ;
+  const double s3_dt = a.dt * sh.s[2];
+  const int q = it / PER;
+  int rem = it % PER;
+  const int ij = rem / (NEQ * NEQ);
+  rem %= NEQ * NEQ;
+  const int r = rem / NEQ, s = rem % NEQ;
+  const int i = ij / NDIM, j = ij % NDIM;
+  GpSlot<NDIM>& sl = sh.slot[q];
+  double t = 0.0;
+  for (int k = 0; k < NEQ; k++) t += sl.A[i][r * 5 + k] * sl.D[j][k * 5 + s];
+  const double c = sl.H[i * 3 + j][r * 5 + s];
+  sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
+}
+
+// step 8: h entries and the rhs coefficient P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_hmat_rhs(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+  using T = FormTraits<NDIM>;
+  constexpr int NEQ = T::NEQ;
+  constexpr int NH = T::Q * NDIM * NDIM * NEQ * NEQ, NP = T::Q * NDIM * NEQ;
+  for (int t = tid; t < NH + NP; t += T::THREADS) {
+    if (t < NH) {
+      hmat_entry<NDIM>(a, sh, t, 1.0);
+    } else {
+      const int p = t - NH, q = p / (NDIM * NEQ), i = (p / NEQ) % NDIM, r = p % NEQ;
+      GpSlot<NDIM>& sl = sh.slot[q];
+      double u = 0.0;
+      for (int q2 = 0; q2 < NEQ; q2++) u += sl.A[i][r * 5 + q2] * sl.F[NDIM][q2];
+      sl.P[i][r] = a.dt * sl.F[i][r] - a.dtsq_2 * u;
+    }
+  }
+}
 // h (sign = +1, domain) or m (sign = -1, face) over nslots slots, all threads
 template <int NDIM>
 CFDV_HD CFDV_INLINE void phase_hmat(const FormArgs& a, FormShared<NDIM>& sh, int nslots, double sign, int tid) {
-  const double s3_dt = a.dt * sh.s[2];
   constexpr int NEQ = NDIM + 2;
   constexpr int PER = NDIM * NDIM * NEQ * NEQ;
-  for (int it = tid; it < nslots * PER; it += FormTraits<NDIM>::THREADS) {
-    const int q = it / PER;
-    int rem = it % PER;
-    const int ij = rem / (NEQ * NEQ);
-    rem %= NEQ * NEQ;
-    const int r = rem / NEQ, s = rem % NEQ;
-    const int i = ij / NDIM, j = ij % NDIM;
-    GpSlot<NDIM>& sl = sh.slot[q];
-    double t = 0.0;
-    for (int k = 0; k < NEQ; k++) t += sl.A[i][r * 5 + k] * sl.D[j][k * 5 + s];
-    const double c = sl.H[i * 3 + j][r * 5 + s];
-    sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
-  }
+  for (int it = tid; it < nslots * PER; it += FormTraits<NDIM>::THREADS) hmat_entry<NDIM>(a, sh, it, sign);
 }
 
 // thread -> (node pair, (r,s) range)
@@ -666,6 +833,49 @@ CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, in
   }
   if (tid == 0 && a.s_out)
     for (int i = 0; i < 4; i++) a.s_out[(size_t)e * 4 + i] = sh.s[i];
+}
+
+// ---- the element as a sequence of block-wide steps --------------------------------
+// Steps 0-9 form the domain integrals, then three steps per boundary face (Gauss-point
+// physics, m, contraction), then staging and the store.  Every step is followed by a
+// block barrier; the CPU emulation runs the same steps thread by thread.
+constexpr int kDomainSteps = 10;
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE int form_nsteps(const FormShared<NDIM>& sh) {
+  return kDomainSteps + 3 * sh.nfaces + 2;
+}
+
+template <int NDIM>
+CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& sh, int e, int tid,
+                                   FormRegs<NDIM>& rg, int* bad) {
+  using T = FormTraits<NDIM>;
+  switch (k) {
+    case 0: step_load<NDIM>(a, sh, e, tid); return;
+    case 1: step_geom_jac<NDIM>(a, sh, tid); return;
+    case 2: step_geom_det<NDIM>(a, sh, tid); return;
+    case 3: step_dphi<NDIM>(sh, tid); return;
+    case 4: step_state<NDIM>(sh, tid); return;
+    case 5: step_stress<NDIM>(a, sh, tid); return;
+    case 6: step_jacobians<NDIM>(a, sh, tid); return;
+    case 7: step_coeffs<NDIM>(a, sh, tid); return;
+    case 8: step_hmat_rhs<NDIM>(a, sh, tid); return;
+    case 9: phase_contract_domain<NDIM>(sh, tid, rg); return;
+    default: break;
+  }
+  const int f = k - kDomainSteps, nf = sh.nfaces;
+  if (f < 3 * nf) {
+    const int lf = f / 3;
+    switch (f % 3) {
+      case 0:
+        if (tid < T::QF) phase_face_gp<NDIM>(a, sh, lf, tid);
+        return;
+      case 1: phase_hmat<NDIM>(a, sh, T::QF, -1.0, tid); return;
+      default: phase_contract_face<NDIM>(sh, lf, tid, rg); return;
+    }
+  }
+  if (f == 3 * nf) phase_stage<NDIM>(sh, tid, rg);
+  else phase_write<NDIM>(a, sh, e, tid, rg, bad);
 }
 
 }  // namespace cfdv

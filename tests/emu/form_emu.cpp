@@ -20,17 +20,10 @@ static int run(const FormArgs& a) {
   FormShared<NDIM>* sh = new FormShared<NDIM>;
   for (int e = 0; e < a.n_elements; e++) {
     std::memset(sh, 0xff, sizeof(*sh));  // garbage in shared memory, as on the device
-    for (int t = 0; t < T::THREADS; t++) phase_load<NDIM>(a, *sh, e, t);
-    for (int q = 0; q < T::Q; q++) phase_domain_gp<NDIM>(a, *sh, q);
-    for (int t = 0; t < T::THREADS; t++) phase_hmat<NDIM>(a, *sh, T::Q, 1.0, t);
-    for (int t = 0; t < T::THREADS; t++) phase_contract_domain<NDIM>(*sh, t, rg[t]);
-    for (int lf = 0; lf < sh->nfaces; lf++) {
-      for (int q = 0; q < T::QF; q++) phase_face_gp<NDIM>(a, *sh, lf, q);
-      for (int t = 0; t < T::THREADS; t++) phase_hmat<NDIM>(a, *sh, T::QF, -1.0, t);
-      for (int t = 0; t < T::THREADS; t++) phase_contract_face<NDIM>(*sh, lf, t, rg[t]);
-    }
-    for (int t = 0; t < T::THREADS; t++) phase_stage<NDIM>(*sh, t, rg[t]);
-    for (int t = 0; t < T::THREADS; t++) phase_write<NDIM>(a, *sh, e, t, rg[t], &bad);
+    for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(0, a, *sh, e, t, rg[t], &bad);
+    const int n = form_nsteps<NDIM>(*sh);
+    for (int k = 1; k < n; k++)
+      for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(k, a, *sh, e, t, rg[t], &bad);
   }
   delete sh;
   return bad;
