@@ -14,15 +14,14 @@ __global__ void __launch_bounds__(FormTraits<NDIM>::THREADS, FormTraits<NDIM>::M
     fdv_form_kernel(FormArgs a) {
   __shared__ FormShared<NDIM> sh;
   __shared__ int bad;
-  FormRegs<NDIM> rg;
   const int tid = threadIdx.x;
   if (tid == 0) bad = 0;
   for (int e = blockIdx.x; e < a.n_elements; e += gridDim.x) {
-    form_step<NDIM>(0, a, sh, e, tid, rg, &bad);
+    form_step<NDIM>(0, a, sh, e, tid, &bad);
     __syncthreads();
     const int n = form_nsteps<NDIM>(sh);
     for (int k = 1; k < n; k++) {
-      form_step<NDIM>(k, a, sh, e, tid, rg, &bad);
+      form_step<NDIM>(k, a, sh, e, tid, &bad);
       __syncthreads();
     }
   }

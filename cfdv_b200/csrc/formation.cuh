@@ -33,11 +33,15 @@ struct FormTraits {
   static constexpr int NBN = (NDIM == 2) ? 2 : 4;    // nodes per face
   static constexpr int QF = (NDIM == 2) ? 2 : 4;     // Gauss points per face
   static constexpr int NFACE = (NDIM == 2) ? 4 : 6;
-  static constexpr int NP = NNOD * NNOD;             // (N, M) node pairs
-  static constexpr int SPLIT = (NDIM == 2) ? 4 : 2;  // threads per node pair
-  static constexpr int THREADS = NP * SPLIT;         // 64 (2D) / 128 (3D)
+  static constexpr int THREADS = (NDIM == 2) ? 64 : 128;
   static constexpr int RS = NEQ * NEQ;
-  static constexpr int RS_PER = (RS + SPLIT - 1) / SPLIT;  // (r,s) entries per thread
+  // contraction: thread `tid` owns the (node N, equation pair r,s) pairs p = tid + k*THREADS,
+  // p = (r*NEQ + s)*NNOD + N, with one accumulator per column node M
+  static constexpr int NPAIR = NNOD * RS;
+  static constexpr int PAIRS = (NPAIR + THREADS - 1) / THREADS;
+  // coefficient rows per Gauss point for the column node M: Phi_M, dPhi_M,j (j < NDIM) and,
+  // in 2D, S_M = sum_j dPhi_M,j for the upwind term
+  static constexpr int NCOEF = 1 + NDIM + (NDIM == 2 ? 1 : 0);
   static constexpr int MIN_BLOCKS = (NDIM == 2) ? 8 : 5;   // resident blocks per SM (register cap)
 };
 
@@ -53,13 +57,12 @@ struct GpGeom {  // isoparametric map at the Gauss point (dead once the flow sta
 template <int NDIM>
 struct GpSlot {
   static constexpr int NNOD = FormTraits<NDIM>::NNOD;
+  alignas(16) double cM[FormTraits<NDIM>::NCOEF][NNOD];  // contraction coefficients, row-major
   double wJ;
   double Phi[NNOD];
   double dPhi[NNOD][3];
   double Psi[NNOD];
   double en[3];
-  double A[NDIM][25];  // a, then a + b
-  double D[NDIM][25];  // b, then s2 a + s4 b
   double H[9][25];     // c, then h (domain) or m (face)
   double P[NDIM][5];   // rhs coefficient per direction and equation
   union {
@@ -80,18 +83,28 @@ struct FormShared {
   int codes[T::NFACE];
   int nfaces;
   uint64_t mask;
-  double s[4];  // s1..s4 of the element (written by Gauss-point thread 0)
+  double s[4];  // s1..s4 of the element
+  double rhs[T::KE];
+  GpSlot<NDIM> slot[T::Q];
   union {
-    GpSlot<NDIM> slot[T::Q];
+    // A(q, i) = a + b and D(q, i) = s2 a + s4 b of the domain Gauss points (a, b until step 7)
+    double AD[T::Q][2][NDIM][25];
+    // the element matrix, column-major, accumulated from the domain contraction on
     double Rt[T::KE * T::KE];
   };
 };
 
+// A and D of a Gauss point: the domain points keep them beside the element matrix; a face
+// point, evaluated after the domain contraction, borrows the h storage of domain slot QF + q
 template <int NDIM>
-struct FormRegs {
-  double acc[FormTraits<NDIM>::RS_PER];
-  double rhs;
-};
+CFDV_HD CFDV_INLINE double (*gp_A(FormShared<NDIM>& sh, int q, bool face))[25] {
+  return face ? sh.slot[FormTraits<NDIM>::QF + q].H : sh.AD[q][0];
+}
+template <int NDIM>
+CFDV_HD CFDV_INLINE double (*gp_D(FormShared<NDIM>& sh, int q, bool face))[25] {
+  return face ? sh.slot[FormTraits<NDIM>::QF + q].H + NDIM : sh.AD[q][1];
+}
+
 
 // hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)
 CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
@@ -138,19 +151,20 @@ CFDV_HD CFDV_INLINE void fdv_params(const GasParams& g, const NodePrim* nd, doub
 
 // a, b, c at the Gauss point -> X, A = a+b, D = s2 a + s4 b (in place), c stays in H
 template <int NDIM>
-CFDV_HD CFDV_INLINE void gp_jacobians(const FormArgs& a, const GpState& f, const double* s, GpSlot<NDIM>& sl) {
+CFDV_HD CFDV_INLINE void gp_jacobians(const FormArgs& a, const GpState& f, const double* s, GpSlot<NDIM>& sl,
+                                      double (*A)[25], double (*D)[25]) {
   constexpr int NEQ = NDIM + 2;
-  jac_a<NDIM>(a.gas, f, &sl.A[0][0]);
-  jac_b<NDIM>(a.gas, f, &sl.D[0][0]);
+  jac_a<NDIM>(a.gas, f, &A[0][0]);
+  jac_b<NDIM>(a.gas, f, &D[0][0]);
   jac_c<NDIM>(a.gas, f, &sl.H[0][0]);
   for (int i = 0; i < NDIM; i++)
     for (int r = 0; r < NEQ; r++)
       for (int q = 0; q < NEQ; q++) {
         const int k = r * 5 + q;
-        const double av = sl.A[i][k], bv = sl.D[i][k];
+        const double av = A[i][k], bv = D[i][k];
         sl.X[i][k] = a.dt * (s[0] * av + s[2] * bv);
-        sl.A[i][k] = av + bv;
-        sl.D[i][k] = s[1] * av + s[3] * bv;
+        A[i][k] = av + bv;
+        D[i][k] = s[1] * av + s[3] * bv;
       }
 }
 
@@ -235,6 +249,13 @@ CFDV_HD CFDV_INLINE void step_dphi(FormShared<NDIM>& sh, int tid) {
     GpSlot<NDIM>& sl = sh.slot[tid / T::NNOD];
     const int N = tid % T::NNOD;
     geom_dphi<NDIM>(sl.g.dPxi[N], sl.g.jac, sl.g.inv, sl.g.iJ, sl.dPhi[N]);
+    sl.cM[0][N] = sl.Phi[N];
+    double sd = 0.0;
+    for (int j = 0; j < NDIM; j++) {
+      sl.cM[1 + j][N] = sl.dPhi[N][j];
+      sd += sl.dPhi[N][j];
+    }
+    if (NDIM == 2) sl.cM[T::NCOEF - 1][N] = sd;
   }
 }
 
@@ -373,11 +394,9 @@ CFDV_HD CFDV_INLINE void step_jacobians(const FormArgs& a, FormShared<NDIM>& sh,
     GpSlot<NDIM>& sl = sh.slot[(tid - C0) / NDIM];
     jac_c_rows<NDIM>(a.gas, sl.st, (tid - C0) % NDIM, &sl.H[0][0]);
   } else if (tid >= A0 && tid < A0 + Q) {
-    GpSlot<NDIM>& sl = sh.slot[tid - A0];
-    jac_a<NDIM>(a.gas, sl.st, &sl.A[0][0]);
+    jac_a<NDIM>(a.gas, sh.slot[tid - A0].st, &sh.AD[tid - A0][0][0][0]);
   } else if (tid >= B0 && tid < B0 + Q) {
-    GpSlot<NDIM>& sl = sh.slot[tid - B0];
-    jac_b<NDIM>(a.gas, sl.st, &sl.D[0][0]);
+    jac_b<NDIM>(a.gas, sh.slot[tid - B0].st, &sh.AD[tid - B0][1][0][0]);
   } else if (tid >= F0 && tid < F0 + FN) {
     flux_sums<NDIM>(a, sh.nd, sh.slot[(tid - F0) / NEQ], (tid - F0) % NEQ);
   }
@@ -390,20 +409,21 @@ CFDV_HD CFDV_INLINE void step_coeffs(const FormArgs& a, FormShared<NDIM>& sh, in
   constexpr int NEQ = T::NEQ, PER = NDIM * NEQ * NEQ;
   const double* s = sh.s;
   for (int t = tid; t < T::Q * PER; t += T::THREADS) {
-    GpSlot<NDIM>& sl = sh.slot[t / PER];
-    const int rem = t % PER, i = rem / (NEQ * NEQ), r = (rem / NEQ) % NEQ, c = rem % NEQ;
+    const int q = t / PER, rem = t % PER, i = rem / (NEQ * NEQ), r = (rem / NEQ) % NEQ, c = rem % NEQ;
     const int k = r * 5 + c;
-    const double av = sl.A[i][k], bv = sl.D[i][k];
-    sl.X[i][k] = a.dt * (s[0] * av + s[2] * bv);
-    sl.A[i][k] = av + bv;
-    sl.D[i][k] = s[1] * av + s[3] * bv;
+    double* A = &sh.AD[q][0][i][k];
+    double* D = &sh.AD[q][1][i][k];
+    const double av = *A, bv = *D;
+    sh.slot[q].X[i][k] = a.dt * (s[0] * av + s[2] * bv);
+    *A = av + bv;
+    *D = s[1] * av + s[3] * bv;
   }
 }
 
 // one entry of h (sign = +1, domain) or m (sign = -1, face):
 // h_ij(r,s) = -dt s3 c_ij(r,s) + dt^2/2 sum_k A_i(r,k) D_j(k,s)  (FDVGalerkin.h:611-628, 698-715)
 template <int NDIM>
-CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int it, double sign) {
+CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int it, double sign, bool face) {
   constexpr int NEQ = NDIM + 2;
   constexpr int PER = NDIM * NDIM * NEQ * NEQ;
   const double s3_dt = a.dt * sh.s[2];
@@ -414,8 +434,10 @@ CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int
   const int r = rem / NEQ, s = rem % NEQ;
   const int i = ij / NDIM, j = ij % NDIM;
   GpSlot<NDIM>& sl = sh.slot[q];
+  const double(*A)[25] = gp_A<NDIM>(sh, q, face);
+  const double(*D)[25] = gp_D<NDIM>(sh, q, face);
   double t = 0.0;
-  for (int k = 0; k < NEQ; k++) t += sl.A[i][r * 5 + k] * sl.D[j][k * 5 + s];
+  for (int k = 0; k < NEQ; k++) t += A[i][r * 5 + k] * D[j][k * 5 + s];
   const double c = sl.H[i * 3 + j][r * 5 + s];
   sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
 }
@@ -428,75 +450,88 @@ CFDV_HD CFDV_INLINE void step_hmat_rhs(const FormArgs& a, FormShared<NDIM>& sh, 
   constexpr int NH = T::Q * NDIM * NDIM * NEQ * NEQ, NP = T::Q * NDIM * NEQ;
   for (int t = tid; t < NH + NP; t += T::THREADS) {
     if (t < NH) {
-      hmat_entry<NDIM>(a, sh, t, 1.0);
+      hmat_entry<NDIM>(a, sh, t, 1.0, false);
     } else {
       const int p = t - NH, q = p / (NDIM * NEQ), i = (p / NEQ) % NDIM, r = p % NEQ;
       GpSlot<NDIM>& sl = sh.slot[q];
       double u = 0.0;
-      for (int q2 = 0; q2 < NEQ; q2++) u += sl.A[i][r * 5 + q2] * sl.F[NDIM][q2];
+      for (int q2 = 0; q2 < NEQ; q2++) u += sh.AD[q][0][i][r * 5 + q2] * sl.F[NDIM][q2];
       sl.P[i][r] = a.dt * sl.F[i][r] - a.dtsq_2 * u;
     }
   }
 }
-// h (sign = +1, domain) or m (sign = -1, face) over nslots slots, all threads
+// m = -h over the face Gauss points, all threads
 template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_hmat(const FormArgs& a, FormShared<NDIM>& sh, int nslots, double sign, int tid) {
+CFDV_HD CFDV_INLINE void phase_hmat_face(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
   constexpr int NEQ = NDIM + 2;
   constexpr int PER = NDIM * NDIM * NEQ * NEQ;
-  for (int it = tid; it < nslots * PER; it += FormTraits<NDIM>::THREADS) hmat_entry<NDIM>(a, sh, it, sign);
+  for (int it = tid; it < FormTraits<NDIM>::QF * PER; it += FormTraits<NDIM>::THREADS)
+    hmat_entry<NDIM>(a, sh, it, -1.0, true);
 }
 
-// thread -> (node pair, (r,s) range)
+// Domain contraction, factored through the row node N:
+//   R(N r, M s) = sum_q [ Phi_M G0 + sum_j dPhi_M,j G1j (+ S_M G2 in 2D) ]  with
+//   G0  = wJ (Phi_N delta_rs - sum_i dPhi_N,i X_i(r,s)),
+//   G1j = wJ sum_i dPhi_N,i h_ij(r,s),   G2 = wJ Psi_N sum_i X_i(r,s),
+// which is sum_k B_k(N,M) C_k(r,s) of FDVGalerkin.h:405-451 regrouped (S_M = sum_j dPhi_M,j).
 template <int NDIM>
-CFDV_HD CFDV_INLINE void thread_pair(int tid, int& N, int& M, int& rs0, int& nrs) {
+CFDV_HD CFDV_INLINE void phase_contract_domain(FormShared<NDIM>& sh, int tid) {
   using T = FormTraits<NDIM>;
-  const int pair = tid % T::NP, split = tid / T::NP;
-  N = pair / T::NNOD;
-  M = pair % T::NNOD;
-  rs0 = split * T::RS_PER;
-  nrs = T::RS - rs0;
-  if (nrs > T::RS_PER) nrs = T::RS_PER;
-}
-
-template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_contract_domain(FormShared<NDIM>& sh, int tid, FormRegs<NDIM>& rg) {
-  using T = FormTraits<NDIM>;
-  constexpr int NEQ = T::NEQ;
-  int N, M, rs0, nrs;
-  thread_pair<NDIM>(tid, N, M, rs0, nrs);
-  for (int k = 0; k < T::RS_PER; k++) rg.acc[k] = 0.0;
+  constexpr int NEQ = T::NEQ, NNOD = T::NNOD, NC = T::NCOEF;
+  double acc[T::PAIRS][NNOD];
+  for (int k = 0; k < T::PAIRS; k++)
+    for (int M = 0; M < NNOD; M++) acc[k][M] = 0.0;
+  const int N = tid % NNOD;  // THREADS is a multiple of NNOD: every pair of this thread has row node N
   for (int q = 0; q < T::Q; q++) {
     const GpSlot<NDIM>& sl = sh.slot[q];
-    const double wJ = sl.wJ;
-    const double B0 = wJ * sl.Phi[N] * sl.Phi[M];
-    double sdM = 0.0;
-    for (int j = 0; j < NDIM; j++) sdM += sl.dPhi[M][j];
-    double Cx[NDIM], Bh[NDIM][NDIM];
-    for (int i = 0; i < NDIM; i++) {
-      Cx[i] = wJ * (sl.Psi[N] * sdM - sl.dPhi[N][i] * sl.Phi[M]);
-      for (int j = 0; j < NDIM; j++) Bh[i][j] = wJ * sl.dPhi[N][i] * sl.dPhi[M][j];
-    }
-    for (int k = 0; k < T::RS_PER; k++) {
-      if (k >= nrs) break;
-      const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
-      double t = (r == s) ? B0 : 0.0;
-      for (int i = 0; i < NDIM; i++) {
-        t += Cx[i] * sl.X[i][idx];
-        for (int j = 0; j < NDIM; j++) t += Bh[i][j] * sl.H[i * 3 + j][idx];
+    const double wJ = sl.wJ, PhiN = sl.Phi[N];
+    double dN[NDIM];
+    for (int i = 0; i < NDIM; i++) dN[i] = sl.dPhi[N][i];
+    for (int k = 0; k < T::PAIRS; k++) {
+      const int p = tid + k * T::THREADS;
+      if (p < T::NPAIR) {
+        const int rs = p / NNOD, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
+        double G[NC];
+        double x = 0.0;
+        for (int i = 0; i < NDIM; i++) x += dN[i] * sl.X[i][idx];
+        G[0] = wJ * (((r == s) ? PhiN : 0.0) - x);
+        for (int j = 0; j < NDIM; j++) {
+          double h = 0.0;
+          for (int i = 0; i < NDIM; i++) h += dN[i] * sl.H[i * 3 + j][idx];
+          G[1 + j] = wJ * h;
+        }
+        if (NDIM == 2) {
+          double sx = 0.0;
+          for (int i = 0; i < NDIM; i++) sx += sl.X[i][idx];
+          G[NC - 1] = wJ * sl.Psi[N] * sx;
+        }
+        for (int M = 0; M < NNOD; M++) {
+          double t = acc[k][M];
+          for (int c = 0; c < NC; c++) t += sl.cM[c][M] * G[c];
+          acc[k][M] = t;
+        }
       }
-      rg.acc[k] += t;
+    }
+  }
+  // the tile aliases A and D, which every thread has finished reading at the last barrier
+  for (int k = 0; k < T::PAIRS; k++) {
+    const int p = tid + k * T::THREADS;
+    if (p < T::NPAIR) {
+      const int rs = p / NNOD, r = rs / NEQ, s = rs % NEQ;
+      for (int M = 0; M < NNOD; M++) sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r] = acc[k][M];
     }
   }
   // rhs(N r) = sum_q wJ sum_i dPhi_Ni P_q(i, r)
-  rg.rhs = 0.0;
   if (tid < T::KE) {
     const int Nn = tid / NEQ, r = tid % NEQ;
+    double rhs = 0.0;
     for (int q = 0; q < T::Q; q++) {
       const GpSlot<NDIM>& sl = sh.slot[q];
       double t = 0.0;
       for (int i = 0; i < NDIM; i++) t += sl.dPhi[Nn][i] * sl.P[i][r];
-      rg.rhs += sl.wJ * t;
+      rhs += sl.wJ * t;
     }
+    sh.rhs[tid] = rhs;
   }
 }
 
@@ -719,11 +754,16 @@ CFDV_HD void phase_face_gp(const FormArgs& a, FormShared<NDIM>& sh, int lf, int 
     }
     for (int i = 0; i < 3; i++) en[i] = nrm[i] * w0 * w1 * det;
   }
+  for (int m = 0; m < NBN; m++) {  // face-local coefficient rows for the contraction
+    sl.cM[0][m] = phib[m];
+    for (int j = 0; j < NDIM; j++) sl.cM[1 + j][m] = dpidx[m][j];
+  }
   GpState fs;
   gp_state<NDIM>(a.gas, NBN, nd, phib, dpidx, fs);
   if (NDIM == 2) edit_face_state_2d(code, fs, nd[0], nd[1], en);
   else edit_face_state_3d(code, fs, en, a.gas.adiabatic);
-  gp_jacobians<NDIM>(a, fs, s, sl);
+  double(*A)[25] = gp_A<NDIM>(sh, qf, true);
+  gp_jacobians<NDIM>(a, fs, s, sl, A, gp_D<NDIM>(sh, qf, true));
   // face rhs: P(i,r) = -dt Fbar(i,r) + dt^2/2 sum_s A_i(r,s) divF(s)   (FDVGalerkin.h:643-680, 720-738)
   double Fbar[NDIM][5], divF[5];
   for (int i = 0; i < NDIM; i++)
@@ -742,7 +782,7 @@ CFDV_HD void phase_face_gp(const FormArgs& a, FormShared<NDIM>& sh, int lf, int 
   for (int i = 0; i < NDIM; i++)
     for (int r = 0; r < NEQ; r++) {
       double t = 0.0;
-      for (int q2 = 0; q2 < NEQ; q2++) t += sl.A[i][r * 5 + q2] * divF[q2];
+      for (int q2 = 0; q2 < NEQ; q2++) t += A[i][r * 5 + q2] * divF[q2];
       sl.P[i][r] = -a.dt * Fbar[i][r] + a.dtsq_2 * t;
     }
 }
@@ -754,31 +794,45 @@ CFDV_HD CFDV_INLINE int face_pos(int f, int node) {
   return -1;
 }
 
+// Face contraction, factored the same way over the face's nodes (local numbering m):
+//   R(N r, M s) += sum_qf Phi_N [ Phi_M sum_i en_i X_i(r,s) + sum_j dPhi_M,j sum_i en_i m_ij(r,s) ]
+// (FDVGalerkin.h:455-533, 643-756)
 template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_contract_face(FormShared<NDIM>& sh, int lf, int tid, FormRegs<NDIM>& rg) {
+CFDV_HD CFDV_INLINE void phase_contract_face(FormShared<NDIM>& sh, int lf, int tid) {
   using T = FormTraits<NDIM>;
-  constexpr int NEQ = T::NEQ;
+  constexpr int NEQ = T::NEQ, NNOD = T::NNOD;
   const int f = sh.faces[lf];
-  int N, M, rs0, nrs;
-  thread_pair<NDIM>(tid, N, M, rs0, nrs);
-  const int fN = face_pos<NDIM>(f, N), fM = face_pos<NDIM>(f, M);
-  if (fN >= 0 && fM >= 0) {
+  const int N = tid % NNOD;
+  const int fN = face_pos<NDIM>(f, N);
+  if (fN >= 0) {
+    int fM[NNOD];
+    for (int M = 0; M < NNOD; M++) fM[M] = face_pos<NDIM>(f, M);
     for (int q = 0; q < T::QF; q++) {
       const GpSlot<NDIM>& sl = sh.slot[q];
-      double Cx[NDIM], Bh[NDIM][NDIM];
-      for (int i = 0; i < NDIM; i++) {
-        Cx[i] = sl.en[i] * sl.Phi[fN] * sl.Phi[fM];
-        for (int j = 0; j < NDIM; j++) Bh[i][j] = sl.en[i] * sl.Phi[fN] * sl.dPhi[fM][j];
-      }
-      for (int k = 0; k < T::RS_PER; k++) {
-        if (k >= nrs) break;
-        const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
-        double t = 0.0;
-        for (int i = 0; i < NDIM; i++) {
-          t += Cx[i] * sl.X[i][idx];
-          for (int j = 0; j < NDIM; j++) t += Bh[i][j] * sl.H[i * 3 + j][idx];
+      const double PhiN = sl.Phi[fN];
+      for (int k = 0; k < T::PAIRS; k++) {
+        const int p = tid + k * T::THREADS;
+        if (p < T::NPAIR) {
+          const int rs = p / NNOD, idx = (rs / NEQ) * 5 + rs % NEQ;
+          double G[1 + NDIM];
+          double x = 0.0;
+          for (int i = 0; i < NDIM; i++) x += sl.en[i] * sl.X[i][idx];
+          G[0] = PhiN * x;
+          for (int j = 0; j < NDIM; j++) {
+            double h = 0.0;
+            for (int i = 0; i < NDIM; i++) h += sl.en[i] * sl.H[i * 3 + j][idx];
+            G[1 + j] = PhiN * h;
+          }
+          const int r = rs / NEQ, s = rs % NEQ;
+          for (int M = 0; M < NNOD; M++) {
+            if (fM[M] >= 0) {  // each (pair, M) entry of the tile belongs to this thread alone
+              double& t = sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r];
+              double v = t;
+              for (int c = 0; c <= NDIM; c++) v += sl.cM[c][fM[M]] * G[c];
+              t = v;
+            }
+          }
         }
-        rg.acc[k] += t;
       }
     }
   }
@@ -786,34 +840,21 @@ CFDV_HD CFDV_INLINE void phase_contract_face(FormShared<NDIM>& sh, int lf, int t
     const int Nn = tid / NEQ, r = tid % NEQ;
     const int fp = face_pos<NDIM>(f, Nn);
     if (fp >= 0) {
+      double rhs = sh.rhs[tid];
       for (int q = 0; q < T::QF; q++) {
         const GpSlot<NDIM>& sl = sh.slot[q];
         double t = 0.0;
         for (int i = 0; i < NDIM; i++) t += sl.en[i] * sl.P[i][r];
-        rg.rhs += sl.Phi[fp] * t;
+        rhs += sl.Phi[fp] * t;
       }
+      sh.rhs[tid] = rhs;
     }
-  }
-}
-
-// accumulators -> column-major staging tile (after the slots are no longer read)
-template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_stage(FormShared<NDIM>& sh, int tid, const FormRegs<NDIM>& rg) {
-  using T = FormTraits<NDIM>;
-  constexpr int NEQ = T::NEQ;
-  int N, M, rs0, nrs;
-  thread_pair<NDIM>(tid, N, M, rs0, nrs);
-  for (int k = 0; k < T::RS_PER; k++) {
-    if (k >= nrs) break;
-    const int rs = rs0 + k, r = rs / NEQ, s = rs % NEQ;
-    sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r] = rg.acc[k];
   }
 }
 
 // ApplyBC (rows of Dirichlet DOFs: zero, diagonal 0.5, rhs 0) and the coalesced store
 template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid,
-                                     const FormRegs<NDIM>& rg, int* bad) {
+CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid, int* bad) {
   using T = FormTraits<NDIM>;
   constexpr int KE = T::KE;
   const uint64_t mk = sh.mask;
@@ -827,7 +868,7 @@ CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, in
     if (a.R32) a.R32[base + k] = (float)v;
   }
   if (tid < KE) {
-    double v = ((mk >> tid) & 1ull) ? 0.0 : rg.rhs;
+    double v = ((mk >> tid) & 1ull) ? 0.0 : sh.rhs[tid];
     if (!(v == v) || v - v != 0.0) *bad = 1;
     a.rhs[(size_t)e * KE + tid] = v;
   }
@@ -836,19 +877,19 @@ CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, in
 }
 
 // ---- the element as a sequence of block-wide steps --------------------------------
-// Steps 0-9 form the domain integrals, then three steps per boundary face (Gauss-point
-// physics, m, contraction), then staging and the store.  Every step is followed by a
+// Steps 0-9 form the domain integrals (step 9 leaves the element matrix in the shared
+// tile), then three steps per boundary face (Gauss-point physics, m, contraction into the
+// tile), then ApplyBC and the store.  Every step is followed by a
 // block barrier; the CPU emulation runs the same steps thread by thread.
 constexpr int kDomainSteps = 10;
 
 template <int NDIM>
 CFDV_HD CFDV_INLINE int form_nsteps(const FormShared<NDIM>& sh) {
-  return kDomainSteps + 3 * sh.nfaces + 2;
+  return kDomainSteps + 3 * sh.nfaces + 1;
 }
 
 template <int NDIM>
-CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& sh, int e, int tid,
-                                   FormRegs<NDIM>& rg, int* bad) {
+CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& sh, int e, int tid, int* bad) {
   using T = FormTraits<NDIM>;
   switch (k) {
     case 0: step_load<NDIM>(a, sh, e, tid); return;
@@ -860,7 +901,7 @@ CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& s
     case 6: step_jacobians<NDIM>(a, sh, tid); return;
     case 7: step_coeffs<NDIM>(a, sh, tid); return;
     case 8: step_hmat_rhs<NDIM>(a, sh, tid); return;
-    case 9: phase_contract_domain<NDIM>(sh, tid, rg); return;
+    case 9: phase_contract_domain<NDIM>(sh, tid); return;
     default: break;
   }
   const int f = k - kDomainSteps, nf = sh.nfaces;
@@ -870,12 +911,11 @@ CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& s
       case 0:
         if (tid < T::QF) phase_face_gp<NDIM>(a, sh, lf, tid);
         return;
-      case 1: phase_hmat<NDIM>(a, sh, T::QF, -1.0, tid); return;
-      default: phase_contract_face<NDIM>(sh, lf, tid, rg); return;
+      case 1: phase_hmat_face<NDIM>(a, sh, tid); return;
+      default: phase_contract_face<NDIM>(sh, lf, tid); return;
     }
   }
-  if (f == 3 * nf) phase_stage<NDIM>(sh, tid, rg);
-  else phase_write<NDIM>(a, sh, e, tid, rg, bad);
+  phase_write<NDIM>(a, sh, e, tid, bad);
 }
 
 }  // namespace cfdv

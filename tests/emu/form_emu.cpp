@@ -16,14 +16,13 @@ template <int NDIM>
 static int run(const FormArgs& a) {
   using T = FormTraits<NDIM>;
   int bad = 0;
-  std::vector<FormRegs<NDIM>> rg(T::THREADS);
   FormShared<NDIM>* sh = new FormShared<NDIM>;
   for (int e = 0; e < a.n_elements; e++) {
     std::memset(sh, 0xff, sizeof(*sh));  // garbage in shared memory, as on the device
-    for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(0, a, *sh, e, t, rg[t], &bad);
+    for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(0, a, *sh, e, t, &bad);
     const int n = form_nsteps<NDIM>(*sh);
     for (int k = 1; k < n; k++)
-      for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(k, a, *sh, e, t, rg[t], &bad);
+      for (int t = 0; t < T::THREADS; t++) form_step<NDIM>(k, a, *sh, e, t, &bad);
   }
   delete sh;
   return bad;
