@@ -196,45 +196,6 @@ struct GpState {
 };
 
 template <int NDIM>
-CFDV_HD CFDV_INLINE void gp_state(const GasParams& g, int nn, const NodePrim* const* nd, const double* Phi,
-                                         const double (*dPhi)[3], GpState& f) {
-  constexpr int NEQ = NDIM + 2;
-  f.E = 0; f.T = 0;
-#pragma unroll
-  for (int i = 0; i < NEQ; i++) {
-    f.U[i] = 0;
-#pragma unroll
-    for (int j = 0; j < NDIM; j++) f.dU[i][j] = 0;
-  }
-#pragma unroll
-  for (int i = 0; i < NDIM; i++) {
-    f.v[i] = 0; f.dT[i] = 0;
-#pragma unroll
-    for (int j = 0; j < NDIM; j++) { f.dV[i][j] = 0; f.tau[i][j] = 0; }
-  }
-  for (int N = 0; N < nn; N++) {
-    const NodePrim& n = *nd[N];
-    f.E = RN_ADD(f.E, RN_MUL(Phi[N], n.E));
-    f.T = RN_ADD(f.T, RN_MUL(Phi[N], n.T));
-#pragma unroll
-    for (int i = 0; i < NEQ; i++) {
-      f.U[i] = RN_ADD(f.U[i], RN_MUL(Phi[N], n.U[i]));
-#pragma unroll
-      for (int j = 0; j < NDIM; j++) f.dU[i][j] = RN_ADD(f.dU[i][j], RN_MUL(dPhi[N][j], n.U[i]));
-    }
-#pragma unroll
-    for (int i = 0; i < NDIM; i++) {
-      f.v[i] = RN_ADD(f.v[i], RN_MUL(Phi[N], n.v[i]));
-      f.dT[i] = RN_ADD(f.dT[i], RN_MUL(dPhi[N][i], n.T));
-#pragma unroll
-      for (int d = 0; d < NDIM; d++) f.dV[i][d] = RN_ADD(f.dV[i][d], RN_MUL(dPhi[N][d], n.v[i]));
-    }
-  }
-  f.mu = gas_mu(g, f.T);
-  f.k = gas_k(g, f.mu);
-}
-
-template <int NDIM>
 CFDV_HD CFDV_INLINE void viscous_stress(GpState& f) {
   double vkk = 0;
 #pragma unroll
@@ -252,8 +213,9 @@ CFDV_HD CFDV_INLINE void viscous_stress(GpState& f) {
 // ---- flux Jacobians ---------------------------------------------------------
 template <int NDIM>
 CFDV_HD void jac_a(const GasParams& th, const GpState& f, double* m);
+// b(i, ., .) for one i (entries i*25 .. i*25+24)
 template <int NDIM>
-CFDV_HD void jac_b(const GasParams& th, const GpState& f, double* m);
+CFDV_HD void jac_b_rows(const GasParams& th, const GpState& f, int i, double* m);
 // c(i, j, ., .) for one i (entries i*75 .. i*75+74 of the 3x3 block layout)
 template <int NDIM>
 CFDV_HD void jac_c_rows(const GasParams& th, const GpState& f, int i, double* m);
@@ -289,8 +251,9 @@ CFDV_HD CFDV_INLINE void jac_a<2>(const GasParams& th, const GpState& f, double*
 }
 
 template <>
-CFDV_HD CFDV_INLINE void jac_b<2>(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < 2 * 25; i++) m[i] = 0.0;
+CFDV_HD CFDV_INLINE void jac_b_rows<2>(const GasParams& th, const GpState& f, int i, double* m) {
+  double* blk = m + i * 25;
+  for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const double reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
   const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const double rho = f.U[0], DENOM = 1. / (rho * rho), TERM1 = f.k * DENOM / th.Cv;
@@ -302,24 +265,35 @@ CFDV_HD CFDV_INLINE void jac_b<2>(const GasParams& th, const GpState& f, double*
   const double b011 = mu_R * drdx * DENOM * reinv, b012 = lambda * drdy * DENOM * reinv;
   const double b020 = (mu * DENOM * (dldy + dmdx - 2. * (u * drdy + v * drdx))) * reinv;
   const double b021 = mu * drdy * DENOM * reinv, b022 = mu * drdx * DENOM * reinv;
-  JA(m, 0, 1, 0) = b010; JA(m, 0, 1, 1) = b011; JA(m, 0, 1, 2) = b012;
-  JA(m, 0, 2, 0) = b020; JA(m, 0, 2, 1) = b021; JA(m, 0, 2, 2) = b022;
-  JA(m, 0, 3, 0) = u * b010 + v * b020 +
-                   ((u * t00 + v * t10) / rho -
-                    TERM1 * (-dedx + (2. * E - 3. * uu - 3. * vv) * drdx + 2. * u * dldx + 2. * v * dmdx)) * reinv;
-  JA(m, 0, 3, 1) = u * b011 + v * b021 + (-t00 / rho - TERM1 * (2. * u * drdx - dldx)) * reinv;
-  JA(m, 0, 3, 2) = u * b012 + v * b022 + (-t10 / rho - TERM1 * (-dmdx + 2. * v * drdx)) * reinv;
-  JA(m, 0, 3, 3) = TERM1 * drdx * reinv;
   const double b120 = (DENOM * (lambda * (dldx + 4. * v * drdy) + mu_R * (u * drdx + dmdy))) * reinv;
   const double b121 = lambda * drdx * DENOM * reinv, b122 = mu_R * drdy * DENOM * reinv;
-  JA(m, 1, 1, 0) = b020; JA(m, 1, 1, 1) = b021; JA(m, 1, 1, 2) = b022;
-  JA(m, 1, 2, 0) = b120; JA(m, 1, 2, 1) = b121; JA(m, 1, 2, 2) = b122;
-  JA(m, 1, 3, 0) = u * b020 + v * b120 +
-                   ((u * t01 + v * t11) / rho -
-                    TERM1 * (-dedy + (2. * E - 3. * uu - 3. * vv) * drdy + 2. * u * dldy + 2. * v * dmdy)) * reinv;
-  JA(m, 1, 3, 1) = u * b021 + v * b121 + (-t10 / rho - TERM1 * (-dldy + 2. * u * drdy)) * reinv;
-  JA(m, 1, 3, 2) = u * b022 + v * b122 + (-t11 / rho - TERM1 * (2. * v * drdy - dmdy)) * reinv;
-  JA(m, 1, 3, 3) = TERM1 * drdy * reinv;
+  if (i == 0) {
+    JA(m, 0, 1, 0) = b010;
+    JA(m, 0, 1, 1) = b011;
+    JA(m, 0, 1, 2) = b012;
+    JA(m, 0, 2, 0) = b020;
+    JA(m, 0, 2, 1) = b021;
+    JA(m, 0, 2, 2) = b022;
+    JA(m, 0, 3, 0) = u * b010 + v * b020 +
+        ((u * t00 + v * t10) / rho -
+        TERM1 * (-dedx + (2. * E - 3. * uu - 3. * vv) * drdx + 2. * u * dldx + 2. * v * dmdx)) * reinv;
+    JA(m, 0, 3, 1) = u * b011 + v * b021 + (-t00 / rho - TERM1 * (2. * u * drdx - dldx)) * reinv;
+    JA(m, 0, 3, 2) = u * b012 + v * b022 + (-t10 / rho - TERM1 * (-dmdx + 2. * v * drdx)) * reinv;
+    JA(m, 0, 3, 3) = TERM1 * drdx * reinv;
+  } else {
+    JA(m, 1, 1, 0) = b020;
+    JA(m, 1, 1, 1) = b021;
+    JA(m, 1, 1, 2) = b022;
+    JA(m, 1, 2, 0) = b120;
+    JA(m, 1, 2, 1) = b121;
+    JA(m, 1, 2, 2) = b122;
+    JA(m, 1, 3, 0) = u * b020 + v * b120 +
+        ((u * t01 + v * t11) / rho -
+        TERM1 * (-dedy + (2. * E - 3. * uu - 3. * vv) * drdy + 2. * u * dldy + 2. * v * dmdy)) * reinv;
+    JA(m, 1, 3, 1) = u * b021 + v * b121 + (-t10 / rho - TERM1 * (-dldy + 2. * u * drdy)) * reinv;
+    JA(m, 1, 3, 2) = u * b022 + v * b122 + (-t11 / rho - TERM1 * (2. * v * drdy - dmdy)) * reinv;
+    JA(m, 1, 3, 3) = TERM1 * drdy * reinv;
+  }
 }
 
 template <>
@@ -402,8 +376,9 @@ CFDV_HD CFDV_INLINE void jac_a<3>(const GasParams& th, const GpState& f, double*
 }
 
 template <>
-CFDV_HD CFDV_INLINE void jac_b<3>(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < 3 * 25; i++) m[i] = 0.0;
+CFDV_HD CFDV_INLINE void jac_b_rows<3>(const GasParams& th, const GpState& f, int i, double* m) {
+  double* blk = m + i * 25;
+  for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const double mu = f.mu, E = f.E;
   const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const double rho = f.U[0], denom = 1. / (rho * rho), TERM1 = f.k * denom / th.Cv;
@@ -420,44 +395,69 @@ CFDV_HD CFDV_INLINE void jac_b<3>(const GasParams& th, const GpState& f, double*
   const double b021 = mu * drdy * denom, b022 = mu * drdx * denom;
   const double b030 = (mu * denom * (dldz + dndx - 2. * (u * drdz + w * drdx)));
   const double b031 = mu * drdz * denom, b033 = mu * drdx * denom;
-  JA(m, 0, 1, 0) = b010; JA(m, 0, 1, 1) = b011; JA(m, 0, 1, 2) = b012; JA(m, 0, 1, 3) = b013;
-  JA(m, 0, 2, 0) = b020; JA(m, 0, 2, 1) = b021; JA(m, 0, 2, 2) = b022;
-  JA(m, 0, 3, 0) = b030; JA(m, 0, 3, 1) = b031; JA(m, 0, 3, 3) = b033;
-  JA(m, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
-                   (denom * (l * t[0][0] + mv * t[0][1] + n * t[0][2]) -
-                    TERM1 * (-dedx + (2. * E - 3. * q2) * drdx + 2. * (u * dldx + v * dmdx + w * dndx)));
-  JA(m, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
-  JA(m, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
-  JA(m, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
-  JA(m, 0, 4, 4) = TERM1 * drdx;
   const double b120 = (denom * (lambda * (dldx + dndz) + mu_R * (dmdy + u * drdx - 2. * v * drdy + w * drdz)));
   const double b121 = lambda * drdx * denom, b122 = mu_R * drdy * denom, b123 = lambda * drdz * denom;
   const double b130 = (mu * denom * (dmdz + dndy - 2. * (v * drdz + w * drdy)));
   const double b132 = mu * denom * drdz, b133 = mu * denom * drdy;
-  JA(m, 1, 1, 0) = b020; JA(m, 1, 1, 1) = b021; JA(m, 1, 1, 2) = b022;
-  JA(m, 1, 2, 0) = b120; JA(m, 1, 2, 1) = b121; JA(m, 1, 2, 2) = b122; JA(m, 1, 2, 3) = b123;
-  JA(m, 1, 3, 0) = b130; JA(m, 1, 3, 2) = b132; JA(m, 1, 3, 3) = b133;
-  JA(m, 1, 4, 0) = u * b020 + v * b120 + w * b130 +
-                   (denom * (l * t[1][0] + mv * t[1][1] + n * t[1][2]) -
-                    TERM1 * (-dedy + (2. * E - 3. * q2) * drdy + 2. * (u * dldy + v * dmdy + w * dndy)));
-  JA(m, 1, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
-  JA(m, 1, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
-  JA(m, 1, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
-  JA(m, 1, 4, 4) = TERM1 * drdy;
   const double b230 = (denom * (mu_R * (dndz + u * drdx + v * drdy - 2. * w * drdz) + lambda * (dldx + dmdy)));
   const double b231 = lambda * drdx * denom, b232 = lambda * drdy * denom, b233 = mu_R * drdz * denom;
-  JA(m, 2, 1, 0) = b030; JA(m, 2, 1, 1) = b031; JA(m, 2, 1, 3) = b033;
-  JA(m, 2, 2, 0) = b130; JA(m, 2, 2, 2) = b132; JA(m, 2, 2, 3) = b133;
-  JA(m, 2, 3, 0) = b230; JA(m, 2, 3, 1) = b231; JA(m, 2, 3, 2) = b232; JA(m, 2, 3, 3) = b233;
-  JA(m, 2, 4, 0) = u * b030 + v * b130 + w * b230 +
-                   (denom * (l * t[2][0] + mv * t[2][1] + n * t[2][2]) -
-                    TERM1 * (-dedz + (2. * E - 3. * q2) * drdz + 2. * (u * dldz + v * dmdz + w * dndz)));
-  JA(m, 2, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
-  JA(m, 2, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
-  JA(m, 2, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
-  JA(m, 2, 4, 4) = TERM1 * drdz;
+  if (i == 0) {
+    JA(m, 0, 1, 0) = b010;
+    JA(m, 0, 1, 1) = b011;
+    JA(m, 0, 1, 2) = b012;
+    JA(m, 0, 1, 3) = b013;
+    JA(m, 0, 2, 0) = b020;
+    JA(m, 0, 2, 1) = b021;
+    JA(m, 0, 2, 2) = b022;
+    JA(m, 0, 3, 0) = b030;
+    JA(m, 0, 3, 1) = b031;
+    JA(m, 0, 3, 3) = b033;
+    JA(m, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
+        (denom * (l * t[0][0] + mv * t[0][1] + n * t[0][2]) -
+        TERM1 * (-dedx + (2. * E - 3. * q2) * drdx + 2. * (u * dldx + v * dmdx + w * dndx)));
+    JA(m, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
+    JA(m, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
+    JA(m, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
+    JA(m, 0, 4, 4) = TERM1 * drdx;
+  } else if (i == 1) {
+    JA(m, 1, 1, 0) = b020;
+    JA(m, 1, 1, 1) = b021;
+    JA(m, 1, 1, 2) = b022;
+    JA(m, 1, 2, 0) = b120;
+    JA(m, 1, 2, 1) = b121;
+    JA(m, 1, 2, 2) = b122;
+    JA(m, 1, 2, 3) = b123;
+    JA(m, 1, 3, 0) = b130;
+    JA(m, 1, 3, 2) = b132;
+    JA(m, 1, 3, 3) = b133;
+    JA(m, 1, 4, 0) = u * b020 + v * b120 + w * b130 +
+        (denom * (l * t[1][0] + mv * t[1][1] + n * t[1][2]) -
+        TERM1 * (-dedy + (2. * E - 3. * q2) * drdy + 2. * (u * dldy + v * dmdy + w * dndy)));
+    JA(m, 1, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
+    JA(m, 1, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
+    JA(m, 1, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
+    JA(m, 1, 4, 4) = TERM1 * drdy;
+  } else {
+    JA(m, 2, 1, 0) = b030;
+    JA(m, 2, 1, 1) = b031;
+    JA(m, 2, 1, 3) = b033;
+    JA(m, 2, 2, 0) = b130;
+    JA(m, 2, 2, 2) = b132;
+    JA(m, 2, 2, 3) = b133;
+    JA(m, 2, 3, 0) = b230;
+    JA(m, 2, 3, 1) = b231;
+    JA(m, 2, 3, 2) = b232;
+    JA(m, 2, 3, 3) = b233;
+    JA(m, 2, 4, 0) = u * b030 + v * b130 + w * b230 +
+        (denom * (l * t[2][0] + mv * t[2][1] + n * t[2][2]) -
+        TERM1 * (-dedz + (2. * E - 3. * q2) * drdz + 2. * (u * dldz + v * dmdz + w * dndz)));
+    JA(m, 2, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
+    JA(m, 2, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
+    JA(m, 2, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
+    JA(m, 2, 4, 4) = TERM1 * drdz;
+  }
   const double reinv = 1.0 / th.creyn;
-  for (int i = 0; i < 75; i++) m[i] *= reinv;
+  for (int k = 0; k < 25; k++) blk[k] *= reinv;
 }
 
 template <>
@@ -556,49 +556,55 @@ CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, in
 }
 
 template <int NDIM>
+CFDV_HD CFDV_INLINE void jac_b(const GasParams& th, const GpState& f, double* m) {
+  for (int i = 0; i < NDIM; i++) jac_b_rows<NDIM>(th, f, i, m);
+}
+
+template <int NDIM>
 CFDV_HD CFDV_INLINE void jac_c(const GasParams& th, const GpState& f, double* m) {
   for (int i = 0; i < NDIM; i++) jac_c_rows<NDIM>(th, f, i, m);
 }
 
-// convective + viscous flux of one node, FG[i*5+r] = F(i,r) + G(i,r).
-// F is the node's own flux; G uses the Gauss-point stress, dT, k with the node velocity.
-// with_F = 0 drops F (the 3D reference evaluates the empty base-class flux).
+// Convective + viscous flux of one node, entry (i, r): F(i,r) + G(i,r).  F is the node's own
+// flux; G uses the Gauss-point stress, dT and k with the node velocity.  with_F = 0 drops F
+// (the 3D reference evaluates the empty base-class flux).  r may be a run-time index:
+// nothing here is an array in registers or local memory.
 template <int NDIM>
-CFDV_HD CFDV_INLINE void node_flux(const GpState& f, const NodePrim& n, double Re, bool with_F, double* FG) {
-  constexpr int NEQ = NDIM + 2;
+CFDV_HD CFDV_INLINE double node_flux_entry(const GpState& f, const NodePrim& n, double Re, bool with_F, int i, int r) {
   const double reinv = 1.0 / Re;
-#pragma unroll
-  for (int i = 0; i < NDIM; i++) {
-    double Gi[5];
-    Gi[0] = 0.0;
-#pragma unroll
-    for (int j = 0; j < NDIM; j++) Gi[1 + j] = -f.tau[i][j] * reinv;
+  double G = 0.0;
+  if (r >= 1 && r <= NDIM) {
+    G = -f.tau[i][r - 1] * reinv;
+  } else if (r == NDIM + 1) {
     double s = -f.tau[i][0] * n.v[0];
 #pragma unroll
     for (int j = 1; j < NDIM; j++) s = s - f.tau[i][j] * n.v[j];
-    Gi[NDIM + 1] = (s - f.k * f.dT[i]) * reinv;
-    double Fi[5] = {0, 0, 0, 0, 0};
-    if (with_F) {
-      if (NDIM == 2) {
-        const double rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
-        const double li = (i == 0) ? l : m;
-        Fi[0] = li;
-        Fi[1] = (i == 0) ? p + l * l / rho : (l * m) / rho;
-        Fi[2] = (i == 0) ? (l * m) / rho : p + m * m / rho;
-        Fi[3] = (p + e) * (li / rho);
+    G = (s - f.k * f.dT[i]) * reinv;
+  }
+  double F = 0.0;
+  if (with_F) {
+    if (NDIM == 2) {
+      const double rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
+      const double li = (i == 0) ? l : m;
+      if (r == 0) F = li;
+      else if (r == 1) F = (i == 0) ? p + l * l / rho : (l * m) / rho;
+      else if (r == 2) F = (i == 0) ? (l * m) / rho : p + m * m / rho;
+      else F = (p + e) * (li / rho);
+    } else {
+      const double rho = n.U[0], p = n.p;
+      const double vi = n.U[1 + i] / n.U[0];
+      if (r == 0) {
+        F = rho * vi;
+      } else if (r <= 3) {
+        const double vj = n.U[r] / n.U[0];
+        F = rho * vi * vj + (i == r - 1 ? p : 0.0);
       } else {
-        const double rho = n.U[0], p = n.p;
-        const double vel[3] = {n.U[1] / n.U[0], n.U[2] / n.U[0], n.U[3] / n.U[0]};
         const double E = n.U[4] / n.U[0];
-        Fi[0] = rho * vel[i];
-#pragma unroll
-        for (int j = 0; j < 3; j++) Fi[1 + j] = rho * vel[i] * vel[j] + (i == j ? p : 0.0);
-        Fi[4] = (rho * E + p) * vel[i];
+        F = (rho * E + p) * vi;
       }
     }
-#pragma unroll
-    for (int r = 0; r < NEQ; r++) FG[i * 5 + r] = Fi[r] + Gi[r];
   }
+  return F + G;
 }
 
 }  // namespace cfdv

@@ -45,6 +45,16 @@ struct FormTraits {
   static constexpr int MIN_BLOCKS = (NDIM == 2) ? 8 : 5;   // resident blocks per SM (register cap)
 };
 
+// hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)
+// hex8 face f lists nodes {3,2,1,0}, {0,1,5,4}, {1,2,6,5}, {2,3,7,6}, {3,0,4,7}, {6,7,4,5},
+// packed four bits per node so that the lookup needs no memory
+CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
+  if (ndim == 2) return (f + i) & 3;
+  const unsigned long long lo = 0x6732562145100123ull, hi = 0x54767403ull;  // faces 0-3, 4-5
+  const unsigned long long w = (f < 4) ? (lo >> (16 * f)) : (hi >> (16 * (f - 4)));
+  return (int)((w >> (4 * i)) & 15ull);
+}
+
 // one Gauss point's worth of coefficients
 template <int NDIM>
 struct GpGeom {  // isoparametric map at the Gauss point (dead once the flow state exists)
@@ -83,7 +93,8 @@ struct FormShared {
   int codes[T::NFACE];
   int nfaces;
   uint64_t mask;
-  double s[4];  // s1..s4 of the element
+  double Mn[T::NNOD], Ren[T::NNOD];  // node Mach and Reynolds numbers
+  double s[4];                        // s1..s4 of the element
   double rhs[T::KE];
   GpSlot<NDIM> slot[T::Q];
   union {
@@ -105,67 +116,52 @@ CFDV_HD CFDV_INLINE double (*gp_D(FormShared<NDIM>& sh, int q, bool face))[25] {
   return face ? sh.slot[FormTraits<NDIM>::QF + q].H + NDIM : sh.AD[q][1];
 }
 
-
-// hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)
-CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
-  if (ndim == 2) return (f + i) & 3;
-  const int tbl[6][4] = {{3, 2, 1, 0}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}, {6, 7, 4, 5}};
-  return tbl[f][i];
+// The Gauss points of a pass: the element's Q domain points over its NNOD nodes, or the
+// QF points of one boundary face over the face's NBN nodes (face-local node numbering)
+template <int NDIM, bool FACE>
+struct Pass {
+  using T = FormTraits<NDIM>;
+  static constexpr int NQ = FACE ? T::QF : T::Q;
+  static constexpr int NN = FACE ? T::NBN : T::NNOD;
+};
+template <int NDIM, bool FACE>
+CFDV_HD CFDV_INLINE const NodePrim& pass_node(const FormShared<NDIM>& sh, int f, int N) {
+  return sh.nd[FACE ? face_node(NDIM, f, N) : N];
 }
 
-// FDVParam.h:15-111 on the element's nodes; s = {s1, s2, s3, s4}
+
+
+// FDVParam.h:15-111, per node: Mach and Reynolds numbers
 template <int NDIM>
-CFDV_HD CFDV_INLINE void fdv_params(const GasParams& g, const NodePrim* nd, double* s) {
-  using T = FormTraits<NDIM>;
-  double M_min = 0, M_max = 0, Re_min = 0, Re_max = 0;
-  for (int b = 0; b < T::NNOD; b++) {
-    double vv = 0;
-    for (int i = 0; i < NDIM; i++) vv = RN_ADD(vv, RN_MUL(nd[b].v[i], nd[b].v[i]));
-    const double V = sqrt(vv);
-    double Tn = nd[b].T;
-    if (Tn < 1.0E-12) Tn = 0;
-    const double snd = sqrt(RN_MUL(RN_MUL(g.gamma, g.cgas), Tn));
-    const double M = (snd < 1.0E-12) ? 0 : RN_DIV(V, snd);
-    const double Re = RN_DIV(RN_MUL(nd[b].rho, V), gas_mu(g, Tn));
-    if (b == 0) { M_max = M; M_min = M; Re_max = Re; Re_min = Re; }
-    M_max = fmax(M_max, M); M_min = fmin(M_min, M);
-    Re_max = fmax(Re_max, Re); Re_min = fmin(Re_min, Re);
+CFDV_HD CFDV_INLINE void node_mach_re(const GasParams& g, const NodePrim& n, double* M, double* Re) {
+  double vv = 0;
+  for (int i = 0; i < NDIM; i++) vv = RN_ADD(vv, RN_MUL(n.v[i], n.v[i]));
+  const double V = sqrt(vv);
+  double Tn = n.T;
+  if (Tn < 1.0E-12) Tn = 0;
+  const double snd = sqrt(RN_MUL(RN_MUL(g.gamma, g.cgas), Tn));
+  *M = (snd < 1.0E-12) ? 0 : RN_DIV(V, snd);
+  *Re = RN_DIV(RN_MUL(n.rho, V), gas_mu(g, Tn));
+}
+
+// FDVParam.h:15-111 over the element's nodes: which = 0 gives s1 and s2 from the Mach
+// numbers, which = 1 gives s3 and s4 from the Reynolds numbers, into s[2*which], s[2*which+1]
+template <int NNOD>
+CFDV_HD CFDV_INLINE void fdv_pair(const double* val, int which, double* s) {
+  double vmin = val[0], vmax = val[0];
+  for (int b = 1; b < NNOD; b++) {
+    vmax = fmax(vmax, val[b]);
+    vmin = fmin(vmin, val[b]);
   }
   const double eps = 0.0000001;
-  // the Mach spread stays in FP64: M_max ~ M_min cancels
-  double r = RN_DIV(sqrt(RN_SUB(RN_MUL(M_max, M_max), RN_MUL(M_min, M_min))), RN_ADD(M_min, eps));
-  double s1 = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
-  if (r > 0.01) s1 = fmin(r, 1.0);
-  else if (r < 0.01 && M_min >= 10E-10) s1 = 0;
-  else if (M_min < 10E-10) s1 = 1.0;
-  r = RN_DIV(sqrt(RN_SUB(RN_MUL(Re_max, Re_max), RN_MUL(Re_min, Re_min))), RN_ADD(Re_min, eps));
-  double s3 = 0.0;
-  if (r > 0.01) s3 = fmin(r, 1.0);
-  else if (r < 0.01 && Re_min >= 10E-10) s3 = 0.0;
-  else if (Re_min <= 10E-10) s3 = 1.0;
-  s[0] = s1;
-  s[1] = 0.5 * (1 + pow(s1, 0.2));
-  s[2] = s3;
-  s[3] = 0.5 * (1 + pow(s3, 0.2));
-}
-
-// a, b, c at the Gauss point -> X, A = a+b, D = s2 a + s4 b (in place), c stays in H
-template <int NDIM>
-CFDV_HD CFDV_INLINE void gp_jacobians(const FormArgs& a, const GpState& f, const double* s, GpSlot<NDIM>& sl,
-                                      double (*A)[25], double (*D)[25]) {
-  constexpr int NEQ = NDIM + 2;
-  jac_a<NDIM>(a.gas, f, &A[0][0]);
-  jac_b<NDIM>(a.gas, f, &D[0][0]);
-  jac_c<NDIM>(a.gas, f, &sl.H[0][0]);
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < NEQ; r++)
-      for (int q = 0; q < NEQ; q++) {
-        const int k = r * 5 + q;
-        const double av = A[i][k], bv = D[i][k];
-        sl.X[i][k] = a.dt * (s[0] * av + s[2] * bv);
-        A[i][k] = av + bv;
-        D[i][k] = s[1] * av + s[3] * bv;
-      }
+  // the spread stays in FP64: max ~ min cancels
+  const double r = RN_DIV(sqrt(RN_SUB(RN_MUL(vmax, vmax), RN_MUL(vmin, vmin))), RN_ADD(vmin, eps));
+  double sv = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
+  if (r > 0.01) sv = fmin(r, 1.0);
+  else if (r < 0.01 && vmin >= 10E-10) sv = 0.0;
+  else if (which == 0 ? (vmin < 10E-10) : (vmin <= 10E-10)) sv = 1.0;
+  s[2 * which] = sv;
+  s[2 * which + 1] = 0.5 * (1 + pow(sv, 0.2));
 }
 
 // ---- domain steps ------------------------------------------------------------
@@ -187,13 +183,15 @@ CFDV_HD CFDV_INLINE double gp_point(const FormArgs& a, int q, double* z) {
   return w;
 }
 
-// step 0: node unpack (NodeUnpack.h:185-205), boundary face list, shape functions
+// step 0: node unpack (NodeUnpack.h:185-205) with the node's Mach and Reynolds numbers,
+// boundary face list, shape functions
 template <int NDIM>
 CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid) {
   using T = FormTraits<NDIM>;
   if (tid < T::NNOD) {
     const int n = a.conn[(size_t)e * T::NNOD + tid];
     node_unpack<NDIM>(a.gas, a.U + (size_t)n * T::NEQ, a.x + (size_t)n * NDIM, sh.nd[tid]);
+    node_mach_re<NDIM>(a.gas, sh.nd[tid], &sh.Mn[tid], &sh.Ren[tid]);
   }
   if (tid == 32 % T::THREADS) {
     int nf = 0;
@@ -216,7 +214,7 @@ CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int 
   }
 }
 
-// step 1: isoparametric Jacobian entries (q, i, k); FDV parameters of the element
+// step 1: isoparametric Jacobian entries (q, i, k); FDV parameters of the element (two threads)
 template <int NDIM>
 CFDV_HD CFDV_INLINE void step_geom_jac(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
   using T = FormTraits<NDIM>;
@@ -225,7 +223,10 @@ CFDV_HD CFDV_INLINE void step_geom_jac(const FormArgs& a, FormShared<NDIM>& sh, 
     GpSlot<NDIM>& sl = sh.slot[q];
     sl.g.jac[i][k] = geom_jac_entry<T::NNOD>(sl.g.dPxi, sh.nd, i, k);
   }
-  if (tid == T::THREADS - 1) fdv_params<NDIM>(a.gas, sh.nd, sh.s);
+  if (tid >= T::THREADS - 2) {
+    const int which = tid - (T::THREADS - 2);
+    fdv_pair<T::NNOD>(which ? sh.Ren : sh.Mn, which, sh.s);
+  }
 }
 
 // step 2: determinant, adjugate, integration weight (one thread per Gauss point)
@@ -267,9 +268,9 @@ struct StateSums {
   static constexpr int COUNT = 2 + NEQ + NEQ * NDIM + NDIM + NDIM + NDIM * NDIM;
 };
 
-template <int NDIM>
-CFDV_HD CFDV_INLINE void state_sum(const NodePrim* nd, GpSlot<NDIM>& sl, int v) {
-  constexpr int NEQ = NDIM + 2, NNOD = FormTraits<NDIM>::NNOD;
+template <int NDIM, bool FACE>
+CFDV_HD CFDV_INLINE void state_sum(const FormShared<NDIM>& sh, int fc, GpSlot<NDIM>& sl, int v) {
+  constexpr int NEQ = NDIM + 2, NN = Pass<NDIM, FACE>::NN;
   GpState& f = sl.st;
   double* dst;
   int c = -1, kind, idx = 0;  // kind: 0 E, 1 T, 2 U[idx], 3 v[idx]
@@ -281,8 +282,8 @@ CFDV_HD CFDV_INLINE void state_sum(const NodePrim* nd, GpSlot<NDIM>& sl, int v) 
   else if ((v -= NDIM) < NDIM) { dst = &f.dT[v]; kind = 1; c = v; }
   else { v -= NDIM; idx = v / NDIM; c = v % NDIM; dst = &f.dV[idx][c]; kind = 3; }
   double acc = 0;
-  for (int N = 0; N < NNOD; N++) {
-    const NodePrim& n = nd[N];
+  for (int N = 0; N < NN; N++) {
+    const NodePrim& n = pass_node<NDIM, FACE>(sh, fc, N);
     const double coef = (c < 0) ? sl.Phi[N] : sl.dPhi[N][c];
     const double val = (kind == 0) ? n.E : (kind == 1) ? n.T : (kind == 2) ? n.U[idx] : n.v[idx];
     acc = RN_ADD(acc, RN_MUL(coef, val));
@@ -290,12 +291,13 @@ CFDV_HD CFDV_INLINE void state_sum(const NodePrim* nd, GpSlot<NDIM>& sl, int v) 
   *dst = acc;
 }
 
-// step 4: the state sums (q, value)
-template <int NDIM>
-CFDV_HD CFDV_INLINE void step_state(FormShared<NDIM>& sh, int tid) {
+// step 4 (and face step 1): the state sums (q, value)
+template <int NDIM, bool FACE>
+CFDV_HD CFDV_INLINE void step_state(FormShared<NDIM>& sh, int lf, int tid) {
   using T = FormTraits<NDIM>;
-  constexpr int NV = StateSums<NDIM>::COUNT;
-  for (int t = tid; t < T::Q * NV; t += T::THREADS) state_sum<NDIM>(sh.nd, sh.slot[t / NV], t % NV);
+  constexpr int NV = StateSums<NDIM>::COUNT, NQ = Pass<NDIM, FACE>::NQ;
+  const int fc = FACE ? sh.faces[lf] : 0;
+  for (int t = tid; t < NQ * NV; t += T::THREADS) state_sum<NDIM, FACE>(sh, fc, sh.slot[t / NV], t % NV);
 }
 
 // 2D streamline-upwind test function Psi (FDVGalerkin.h:225-332) with discontinuity
@@ -360,18 +362,18 @@ CFDV_HD CFDV_INLINE void step_stress(const FormArgs& a, FormShared<NDIM>& sh, in
 
 // rhs flux sums for equation r at one Gauss point (FDVGalerkin.h:549-609, 410-427):
 // Fbar(i,r) = sum_b Phi_b FG_b(i,r), divF(r) = sum_b sum_i dPhi_b,i FG_b(i,r)
-template <int NDIM>
-CFDV_HD CFDV_INLINE void flux_sums(const FormArgs& a, const NodePrim* nd, GpSlot<NDIM>& sl, int r) {
-  constexpr int NNOD = FormTraits<NDIM>::NNOD;
+template <int NDIM, bool FACE>
+CFDV_HD CFDV_INLINE void flux_sums(const FormArgs& a, const FormShared<NDIM>& sh, int fc, GpSlot<NDIM>& sl, int r) {
+  constexpr int NN = Pass<NDIM, FACE>::NN;
   double Fbar[NDIM], divF = 0.0;
   for (int i = 0; i < NDIM; i++) Fbar[i] = 0.0;
   const bool withF = (NDIM == 2) || a.physical_3d_flux;
-  for (int b = 0; b < NNOD; b++) {
-    double FG[15];
-    node_flux<NDIM>(sl.st, nd[b], a.gas.creyn, withF, FG);
+  for (int b = 0; b < NN; b++) {
+    const NodePrim& nb = pass_node<NDIM, FACE>(sh, fc, b);
     for (int i = 0; i < NDIM; i++) {
-      Fbar[i] += sl.Phi[b] * FG[i * 5 + r];
-      divF += sl.dPhi[b][i] * FG[i * 5 + r];
+      const double fg = node_flux_entry<NDIM>(sl.st, nb, a.gas.creyn, withF, i, r);
+      Fbar[i] += sl.Phi[b] * fg;
+      divF += sl.dPhi[b][i] * fg;
     }
   }
   for (int i = 0; i < NDIM; i++) sl.F[i][r] = Fbar[i];
@@ -379,40 +381,43 @@ CFDV_HD CFDV_INLINE void flux_sums(const FormArgs& a, const NodePrim* nd, GpSlot
 }
 
 // step 6: flux Jacobians a, b, c (FDV/NavierStokes2D.h, NavierStokes3D.h) and the rhs flux
-// sums; each kind of task fills whole warps where the block has them
-template <int NDIM>
-CFDV_HD CFDV_INLINE void step_jacobians(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
+// sums; b and c are formed one direction i at a time, and each kind of task fills whole
+// warps where the block has them
+template <int NDIM, bool FACE>
+CFDV_HD CFDV_INLINE void step_jacobians(const FormArgs& a, FormShared<NDIM>& sh, int lf, int tid) {
   using T = FormTraits<NDIM>;
-  constexpr int Q = T::Q, NEQ = T::NEQ;
-  constexpr int C0 = 0, CN = Q * NDIM;                       // c, one block row i each
-  constexpr int A0 = (NDIM == 3) ? 104 : 8, B0 = 32;         // a, b: one Gauss point each
-  constexpr int F0 = (NDIM == 3) ? 64 : 36, FN = Q * NEQ;    // flux sums: (q, r)
-  static_assert(CN <= A0 && A0 + Q <= T::THREADS && B0 + Q <= F0 && F0 + FN <= T::THREADS &&
-                    (NDIM == 2 || F0 + FN <= A0) && (NDIM == 3 || A0 + Q <= B0),
+  constexpr int Q = Pass<NDIM, FACE>::NQ, NEQ = T::NEQ;
+  constexpr int C0 = 0, CN = Q * NDIM;                     // c: (q, i)
+  constexpr int B0 = 32, BN = Q * NDIM;                    // b: (q, i)
+  constexpr int A0 = (NDIM == 3) ? 104 : 8;                // a: q
+  constexpr int F0 = (NDIM == 3) ? 64 : 40, FN = Q * NEQ;  // flux sums: (q, r)
+  static_assert(CN <= B0 && B0 + BN <= F0 && F0 + FN <= T::THREADS && A0 + Q <= T::THREADS &&
+                    (NDIM == 2 ? (CN <= A0 && A0 + Q <= B0) : (F0 + FN <= A0)),
                 "task ranges overlap");
   if (tid >= C0 && tid < C0 + CN) {
     GpSlot<NDIM>& sl = sh.slot[(tid - C0) / NDIM];
     jac_c_rows<NDIM>(a.gas, sl.st, (tid - C0) % NDIM, &sl.H[0][0]);
+  } else if (tid >= B0 && tid < B0 + BN) {
+    const int q = (tid - B0) / NDIM;
+    jac_b_rows<NDIM>(a.gas, sh.slot[q].st, (tid - B0) % NDIM, &gp_D<NDIM>(sh, q, FACE)[0][0]);
   } else if (tid >= A0 && tid < A0 + Q) {
-    jac_a<NDIM>(a.gas, sh.slot[tid - A0].st, &sh.AD[tid - A0][0][0][0]);
-  } else if (tid >= B0 && tid < B0 + Q) {
-    jac_b<NDIM>(a.gas, sh.slot[tid - B0].st, &sh.AD[tid - B0][1][0][0]);
+    jac_a<NDIM>(a.gas, sh.slot[tid - A0].st, &gp_A<NDIM>(sh, tid - A0, FACE)[0][0]);
   } else if (tid >= F0 && tid < F0 + FN) {
-    flux_sums<NDIM>(a, sh.nd, sh.slot[(tid - F0) / NEQ], (tid - F0) % NEQ);
+    flux_sums<NDIM, FACE>(a, sh, FACE ? sh.faces[lf] : 0, sh.slot[(tid - F0) / NEQ], (tid - F0) % NEQ);
   }
 }
 
 // step 7: X = dt (s1 a + s3 b), A = a + b, D = s2 a + s4 b, entry by entry (q, i, r, s)
-template <int NDIM>
+template <int NDIM, bool FACE>
 CFDV_HD CFDV_INLINE void step_coeffs(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
   using T = FormTraits<NDIM>;
   constexpr int NEQ = T::NEQ, PER = NDIM * NEQ * NEQ;
   const double* s = sh.s;
-  for (int t = tid; t < T::Q * PER; t += T::THREADS) {
+  for (int t = tid; t < Pass<NDIM, FACE>::NQ * PER; t += T::THREADS) {
     const int q = t / PER, rem = t % PER, i = rem / (NEQ * NEQ), r = (rem / NEQ) % NEQ, c = rem % NEQ;
     const int k = r * 5 + c;
-    double* A = &sh.AD[q][0][i][k];
-    double* D = &sh.AD[q][1][i][k];
+    double* A = &gp_A<NDIM>(sh, q, FACE)[i][k];
+    double* D = &gp_D<NDIM>(sh, q, FACE)[i][k];
     const double av = *A, bv = *D;
     sh.slot[q].X[i][k] = a.dt * (s[0] * av + s[2] * bv);
     *A = av + bv;
@@ -442,33 +447,27 @@ CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int
   sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
 }
 
-// step 8: h entries and the rhs coefficient P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s)
-template <int NDIM>
+// step 8: h entries and the rhs coefficient P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s);
+// face step 5: m = -h and P with the opposite signs (FDVGalerkin.h:643-680, 698-738)
+template <int NDIM, bool FACE>
 CFDV_HD CFDV_INLINE void step_hmat_rhs(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
   using T = FormTraits<NDIM>;
-  constexpr int NEQ = T::NEQ;
-  constexpr int NH = T::Q * NDIM * NDIM * NEQ * NEQ, NP = T::Q * NDIM * NEQ;
+  constexpr int NEQ = T::NEQ, NQ = Pass<NDIM, FACE>::NQ;
+  constexpr int NH = NQ * NDIM * NDIM * NEQ * NEQ, NP = NQ * NDIM * NEQ;
   for (int t = tid; t < NH + NP; t += T::THREADS) {
     if (t < NH) {
-      hmat_entry<NDIM>(a, sh, t, 1.0, false);
+      hmat_entry<NDIM>(a, sh, t, FACE ? -1.0 : 1.0, FACE);
     } else {
       const int p = t - NH, q = p / (NDIM * NEQ), i = (p / NEQ) % NDIM, r = p % NEQ;
       GpSlot<NDIM>& sl = sh.slot[q];
+      const double(*A)[25] = gp_A<NDIM>(sh, q, FACE);
       double u = 0.0;
-      for (int q2 = 0; q2 < NEQ; q2++) u += sh.AD[q][0][i][r * 5 + q2] * sl.F[NDIM][q2];
-      sl.P[i][r] = a.dt * sl.F[i][r] - a.dtsq_2 * u;
+      for (int q2 = 0; q2 < NEQ; q2++) u += A[i][r * 5 + q2] * sl.F[NDIM][q2];
+      if (FACE) sl.P[i][r] = -a.dt * sl.F[i][r] + a.dtsq_2 * u;
+      else sl.P[i][r] = a.dt * sl.F[i][r] - a.dtsq_2 * u;
     }
   }
 }
-// m = -h over the face Gauss points, all threads
-template <int NDIM>
-CFDV_HD CFDV_INLINE void phase_hmat_face(const FormArgs& a, FormShared<NDIM>& sh, int tid) {
-  constexpr int NEQ = NDIM + 2;
-  constexpr int PER = NDIM * NDIM * NEQ * NEQ;
-  for (int it = tid; it < FormTraits<NDIM>::QF * PER; it += FormTraits<NDIM>::THREADS)
-    hmat_entry<NDIM>(a, sh, it, -1.0, true);
-}
-
 // Domain contraction, factored through the row node N:
 //   R(N r, M s) = sum_q [ Phi_M G0 + sum_j dPhi_M,j G1j (+ S_M G2 in 2D) ]  with
 //   G0  = wJ (Phi_N delta_rs - sum_i dPhi_N,i X_i(r,s)),
@@ -478,48 +477,38 @@ template <int NDIM>
 CFDV_HD CFDV_INLINE void phase_contract_domain(FormShared<NDIM>& sh, int tid) {
   using T = FormTraits<NDIM>;
   constexpr int NEQ = T::NEQ, NNOD = T::NNOD, NC = T::NCOEF;
-  double acc[T::PAIRS][NNOD];
-  for (int k = 0; k < T::PAIRS; k++)
-    for (int M = 0; M < NNOD; M++) acc[k][M] = 0.0;
   const int N = tid % NNOD;  // THREADS is a multiple of NNOD: every pair of this thread has row node N
-  for (int q = 0; q < T::Q; q++) {
-    const GpSlot<NDIM>& sl = sh.slot[q];
-    const double wJ = sl.wJ, PhiN = sl.Phi[N];
-    double dN[NDIM];
-    for (int i = 0; i < NDIM; i++) dN[i] = sl.dPhi[N][i];
-    for (int k = 0; k < T::PAIRS; k++) {
-      const int p = tid + k * T::THREADS;
-      if (p < T::NPAIR) {
-        const int rs = p / NNOD, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
-        double G[NC];
-        double x = 0.0;
-        for (int i = 0; i < NDIM; i++) x += dN[i] * sl.X[i][idx];
-        G[0] = wJ * (((r == s) ? PhiN : 0.0) - x);
-        for (int j = 0; j < NDIM; j++) {
-          double h = 0.0;
-          for (int i = 0; i < NDIM; i++) h += dN[i] * sl.H[i * 3 + j][idx];
-          G[1 + j] = wJ * h;
-        }
-        if (NDIM == 2) {
-          double sx = 0.0;
-          for (int i = 0; i < NDIM; i++) sx += sl.X[i][idx];
-          G[NC - 1] = wJ * sl.Psi[N] * sx;
-        }
-        for (int M = 0; M < NNOD; M++) {
-          double t = acc[k][M];
-          for (int c = 0; c < NC; c++) t += sl.cM[c][M] * G[c];
-          acc[k][M] = t;
-        }
-      }
-    }
-  }
-  // the tile aliases A and D, which every thread has finished reading at the last barrier
   for (int k = 0; k < T::PAIRS; k++) {
     const int p = tid + k * T::THREADS;
-    if (p < T::NPAIR) {
-      const int rs = p / NNOD, r = rs / NEQ, s = rs % NEQ;
-      for (int M = 0; M < NNOD; M++) sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r] = acc[k][M];
+    if (p >= T::NPAIR) break;
+    const int rs = p / NNOD, r = rs / NEQ, s = rs % NEQ, idx = r * 5 + s;
+    double acc[NNOD];
+    for (int M = 0; M < NNOD; M++) acc[M] = 0.0;
+    for (int q = 0; q < T::Q; q++) {
+      const GpSlot<NDIM>& sl = sh.slot[q];
+      const double wJ = sl.wJ;
+      double G[NC];
+      double x = 0.0;
+      for (int i = 0; i < NDIM; i++) x += sl.dPhi[N][i] * sl.X[i][idx];
+      G[0] = wJ * (((r == s) ? sl.Phi[N] : 0.0) - x);
+      for (int j = 0; j < NDIM; j++) {
+        double h = 0.0;
+        for (int i = 0; i < NDIM; i++) h += sl.dPhi[N][i] * sl.H[i * 3 + j][idx];
+        G[1 + j] = wJ * h;
+      }
+      if (NDIM == 2) {
+        double sx = 0.0;
+        for (int i = 0; i < NDIM; i++) sx += sl.X[i][idx];
+        G[NC - 1] = wJ * sl.Psi[N] * sx;
+      }
+      for (int M = 0; M < NNOD; M++) {
+        double t = acc[M];
+        for (int c = 0; c < NC; c++) t += sl.cM[c][M] * G[c];
+        acc[M] = t;
+      }
     }
+    // the tile aliases A and D, which every thread has finished reading at the last barrier
+    for (int M = 0; M < NNOD; M++) sh.Rt[(M * NEQ + s) * T::KE + N * NEQ + r] = acc[M];
   }
   // rhs(N r) = sum_q wJ sum_i dPhi_Ni P_q(i, r)
   if (tid < T::KE) {
@@ -690,16 +679,18 @@ CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim
   if (code == 6) { f.tau[0][0] = 0.; f.tau[1][0] = 0.; }
 }
 
-// face Gauss point qf of face `lf` (index into sh.faces)
+// face step 0: face shape functions, derivatives along the face and the weighted normal
+// en for Gauss point qf (2D TestFunctions1D.h:141-216, 3D calc_TF_norm3D.h:9-167), one
+// thread per face Gauss point
 template <int NDIM>
-CFDV_HD void phase_face_gp(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
+CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
   using T = FormTraits<NDIM>;
-  constexpr int NEQ = T::NEQ, NBN = T::NBN;
+  constexpr int NBN = T::NBN;
+  if (qf >= T::QF) return;
   GpSlot<NDIM>& sl = sh.slot[qf];
-  const int f = sh.faces[lf], code = sh.codes[lf];
+  const int f = sh.faces[lf];
   const NodePrim* nd[NBN];
   for (int i = 0; i < NBN; i++) nd[i] = &sh.nd[face_node(NDIM, f, i)];
-  const double* s = sh.s;
   double* phib = sl.Phi;
   double (*dpidx)[3] = sl.dPhi;
   double* en = sl.en;
@@ -758,33 +749,23 @@ CFDV_HD void phase_face_gp(const FormArgs& a, FormShared<NDIM>& sh, int lf, int 
     sl.cM[0][m] = phib[m];
     for (int j = 0; j < NDIM; j++) sl.cM[1 + j][m] = dpidx[m][j];
   }
-  GpState fs;
-  gp_state<NDIM>(a.gas, NBN, nd, phib, dpidx, fs);
-  if (NDIM == 2) edit_face_state_2d(code, fs, nd[0], nd[1], en);
-  else edit_face_state_3d(code, fs, en, a.gas.adiabatic);
-  double(*A)[25] = gp_A<NDIM>(sh, qf, true);
-  gp_jacobians<NDIM>(a, fs, s, sl, A, gp_D<NDIM>(sh, qf, true));
-  // face rhs: P(i,r) = -dt Fbar(i,r) + dt^2/2 sum_s A_i(r,s) divF(s)   (FDVGalerkin.h:643-680, 720-738)
-  double Fbar[NDIM][5], divF[5];
+}
+
+// face step 2: viscosity and conductivity at the face point, stress zero, then the
+// boundary-condition edits of the state (eval1dboundary.h, eval2dboundary.h)
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_face_edit(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
+  using T = FormTraits<NDIM>;
+  if (qf >= T::QF) return;
+  GpSlot<NDIM>& sl = sh.slot[qf];
+  GpState& fs = sl.st;
+  const int f = sh.faces[lf], code = sh.codes[lf];
+  fs.mu = gas_mu(a.gas, fs.T);
+  fs.k = gas_k(a.gas, fs.mu);
   for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < 5; r++) Fbar[i][r] = 0.0;
-  for (int r = 0; r < 5; r++) divF[r] = 0.0;
-  const bool withF = (NDIM == 2) || a.physical_3d_flux;
-  for (int b = 0; b < NBN; b++) {
-    double FG[15];
-    node_flux<NDIM>(fs, *nd[b], a.gas.creyn, withF, FG);
-    for (int i = 0; i < NDIM; i++)
-      for (int r = 0; r < NEQ; r++) {
-        Fbar[i][r] += phib[b] * FG[i * 5 + r];
-        divF[r] += dpidx[b][i] * FG[i * 5 + r];
-      }
-  }
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < NEQ; r++) {
-      double t = 0.0;
-      for (int q2 = 0; q2 < NEQ; q2++) t += A[i][r * 5 + q2] * divF[q2];
-      sl.P[i][r] = -a.dt * Fbar[i][r] + a.dtsq_2 * t;
-    }
+    for (int j = 0; j < NDIM; j++) fs.tau[i][j] = 0;
+  if (NDIM == 2) edit_face_state_2d(code, fs, &sh.nd[face_node(NDIM, f, 0)], &sh.nd[face_node(NDIM, f, 1)], sl.en);
+  else edit_face_state_3d(code, fs, sl.en, a.gas.adiabatic);
 }
 
 template <int NDIM>
@@ -878,40 +859,43 @@ CFDV_HD CFDV_INLINE void phase_write(const FormArgs& a, FormShared<NDIM>& sh, in
 
 // ---- the element as a sequence of block-wide steps --------------------------------
 // Steps 0-9 form the domain integrals (step 9 leaves the element matrix in the shared
-// tile), then three steps per boundary face (Gauss-point physics, m, contraction into the
-// tile), then ApplyBC and the store.  Every step is followed by a
-// block barrier; the CPU emulation runs the same steps thread by thread.
+// tile), then seven steps per boundary face (geometry, state sums, boundary edits,
+// Jacobians and flux sums, coefficients, m and rhs, contraction into the tile), then
+// ApplyBC and the store.  Every step is followed by a block barrier; the CPU emulation
+// runs the same steps thread by thread.
 constexpr int kDomainSteps = 10;
+constexpr int kFaceSteps = 7;
 
 template <int NDIM>
 CFDV_HD CFDV_INLINE int form_nsteps(const FormShared<NDIM>& sh) {
-  return kDomainSteps + 3 * sh.nfaces + 1;
+  return kDomainSteps + kFaceSteps * sh.nfaces + 1;
 }
 
 template <int NDIM>
 CFDV_HD CFDV_INLINE void form_step(int k, const FormArgs& a, FormShared<NDIM>& sh, int e, int tid, int* bad) {
-  using T = FormTraits<NDIM>;
   switch (k) {
     case 0: step_load<NDIM>(a, sh, e, tid); return;
     case 1: step_geom_jac<NDIM>(a, sh, tid); return;
     case 2: step_geom_det<NDIM>(a, sh, tid); return;
     case 3: step_dphi<NDIM>(sh, tid); return;
-    case 4: step_state<NDIM>(sh, tid); return;
+    case 4: step_state<NDIM, false>(sh, 0, tid); return;
     case 5: step_stress<NDIM>(a, sh, tid); return;
-    case 6: step_jacobians<NDIM>(a, sh, tid); return;
-    case 7: step_coeffs<NDIM>(a, sh, tid); return;
-    case 8: step_hmat_rhs<NDIM>(a, sh, tid); return;
+    case 6: step_jacobians<NDIM, false>(a, sh, 0, tid); return;
+    case 7: step_coeffs<NDIM, false>(a, sh, tid); return;
+    case 8: step_hmat_rhs<NDIM, false>(a, sh, tid); return;
     case 9: phase_contract_domain<NDIM>(sh, tid); return;
     default: break;
   }
   const int f = k - kDomainSteps, nf = sh.nfaces;
-  if (f < 3 * nf) {
-    const int lf = f / 3;
-    switch (f % 3) {
-      case 0:
-        if (tid < T::QF) phase_face_gp<NDIM>(a, sh, lf, tid);
-        return;
-      case 1: phase_hmat_face<NDIM>(a, sh, tid); return;
+  if (f < kFaceSteps * nf) {
+    const int lf = f / kFaceSteps;
+    switch (f % kFaceSteps) {
+      case 0: step_face_geom<NDIM>(a, sh, lf, tid); return;
+      case 1: step_state<NDIM, true>(sh, lf, tid); return;
+      case 2: step_face_edit<NDIM>(a, sh, lf, tid); return;
+      case 3: step_jacobians<NDIM, true>(a, sh, lf, tid); return;
+      case 4: step_coeffs<NDIM, true>(a, sh, tid); return;
+      case 5: step_hmat_rhs<NDIM, true>(a, sh, tid); return;
       default: phase_contract_face<NDIM>(sh, lf, tid); return;
     }
   }
