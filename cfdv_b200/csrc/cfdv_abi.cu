@@ -10,101 +10,17 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cfdv_gpu.h"
+#include "context.h"
 #include "formation.cuh"
 #include "gmres_persistent.h"
 #include "kernels.h"
 
 using namespace cfdv;
-
-struct cfdv_ctx {
-  int dev = 0;
-  int ndim = 0, nnod = 0, neqn = 0, nbnod = 0, nface = 0, n_nodes = 0, n_elements = 0, n_dof = 0, Ke = 0;
-  GasParams gas{};
-  int phys3d = 0;
-  cudaStream_t st = nullptr;
-  // mesh
-  double* d_x = nullptr;
-  int* d_conn = nullptr;
-  int* d_bc = nullptr;
-  uint64_t* d_mask = nullptr;
-  double* d_cleng = nullptr;
-  int* d_csr_ptr = nullptr;
-  int* d_csr_idx = nullptr;
-  // state
-  double* d_U = nullptr;
-  double* d_U0 = nullptr;
-  double* d_du = nullptr;
-  // element data
-  double* d_R64 = nullptr;
-  float* d_R32 = nullptr;
-  double* d_rhs = nullptr;
-  double* d_s = nullptr;
-  double* d_Y64 = nullptr;
-  float* d_Y32 = nullptr;
-  bool formed = false, have32 = false;
-  double dt_formed = 0;
-  // krylov
-  int m_cap = 0;
-  double* d_V = nullptr;
-  double* d_W = nullptr;
-  double* d_b = nullptr;
-  double* d_pa = nullptr;
-  double* d_pb = nullptr;
-  double* d_H = nullptr;   // Hessenberg (m+1) x m column-major + scalars
-  double* d_sc = nullptr;  // scalars: [0] g0/beta, [1] ||b||, [2] dt
-  double* d_y = nullptr;
-  double* d_rms = nullptr;
-  int* d_status = nullptr;
-  double* h_pin = nullptr;  // pinned host staging
-  double* d_pers = nullptr;  // persistent-solve scratch
-  size_t pers_cap = 0;
-  int* d_pers_int = nullptr;
-  double* d_Dinv = nullptr;  // node-block Jacobi inverse [Nn][neqn][neqn]
-  double* d_Z = nullptr;     // preconditioned Krylov vector
-  // profiling
-  bool prof = false;
-  std::vector<cudaEvent_t> ev_pool;
-  size_t ev_used = 0;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_form;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_solve;
-  long mv_launches = 0;
-  long launches = 0;    // kernels launched since the last cfdv_profile()
-  double mv_bytes = 0;  // algorithmic bytes of the timed element passes
-  std::string err;
-};
+using cfdv::ctxi::dalloc;
+using cfdv::ctxi::dfree;
+using cfdv::ctxi::fail;
 
 namespace {
-
-int fail(cfdv_ctx* c, int code, const std::string& msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-#define CK(call)                                                                              \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess) return fail(c, CFDV_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
-
-template <typename T>
-int dalloc(cfdv_ctx* c, T** p, size_t n) {
-  if (*p) { cudaFree(*p); *p = nullptr; }
-  if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(c, CFDV_ERR_ALLOC, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) + " bytes: " +
-                                       cudaGetErrorString(e));
-  }
-  return CFDV_OK;
-}
-
-template <typename T>
-void dfree(T*& p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
 
 void free_all(cfdv_ctx* c) {
   dfree(c->d_x); dfree(c->d_conn); dfree(c->d_bc); dfree(c->d_mask); dfree(c->d_cleng);
@@ -113,6 +29,10 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
+  dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
+  c->adj_state_cap = 0;
+  c->n_wall_elems = 0;
+  c->wall_bc_cached = -1 << 30;
   c->pers_cap = 0;
   if (c->h_pin) cudaFreeHost(c->h_pin);
   c->h_pin = nullptr;
@@ -564,9 +484,12 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
   return CFDV_OK;
 }
 
+}  // namespace
+
 // The same textbook solve as gmres_correct, run as one persistent cooperative kernel
 // (gmres_persistent.cu): one launch and one read-back per solve.
-int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
+int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
+                             int transpose) {
   const int m = o->m;
   const int fp32 = (o->precision == CFDV_PREC_MIXED);
   if (fp32 && !c->have32) return fail(c, CFDV_ERR_STATE, "mixed precision needs cfdv_form(..., CFDV_PREC_MIXED)");
@@ -583,7 +506,18 @@ int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_repor
   if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, 8))) return rc;
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
   double bnorm;
-  if ((rc = compose_b(c, &bnorm))) return rc;
+  if (rhs_vec) {
+    if (rhs_vec != c->d_b)
+      CK(cudaMemcpyAsync(c->d_b, rhs_vec, sizeof(double) * c->n_dof, cudaMemcpyDeviceToDevice, c->st));
+    CK(launch_dot(c->d_b, c->d_b, c->n_dof, c->d_pa, c->st));
+    CK(launch_reduce(c->d_pa, c->d_sc + 1, 1, c->st));
+    c->launches += 2;
+    CK(cudaMemcpyAsync(c->h_pin, c->d_sc + 1, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    bnorm = c->h_pin[0];
+  } else if ((rc = compose_b(c, &bnorm))) {
+    return rc;
+  }
   const double atol = o->rtol * bnorm;
   if (rep) { rep->tol = atol; rep->bnorm = bnorm; }
   if (bnorm == 0.0) { if (rep) rep->true_rel_res = 0.0; return CFDV_OK; }
@@ -592,6 +526,7 @@ int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_repor
   std::memset(&a, 0, sizeof(a));
   a.n_dof = c->n_dof; a.n_elements = c->n_elements; a.m = m; a.max_restarts = o->restarts;
   a.max_blocks = persistent_max_blocks();
+  a.transpose = transpose ? 1 : 0;
   a.atol = atol;
   a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
   a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;
@@ -647,6 +582,8 @@ int gmres_correct_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_repor
   c->mv_launches += (long)res[3];
   return CFDV_OK;
 }
+
+namespace {
 
 int true_residual(cfdv_ctx* c, cfdv_gmres_report* rep) {
   double beta;
@@ -745,6 +682,7 @@ int cfdv_load_node_records(cfdv_ctx* c, const double* rec, size_t n_nodes) {
     u[nd + 1] += 0.5 * v;
     u[nd + 1] *= u[0];
   }
+  if (c->h_records.data() != rec) c->h_records.assign(rec, rec + n_nodes * rs);
   return cfdv_set_state(c, U.data(), U.size());
 }
 
@@ -848,7 +786,7 @@ int cfdv_gmres(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
   } else if (o->engine == 1) {
     rc = gmres_correct(c, o, rep);
   } else {
-    rc = gmres_correct_device(c, o, rep);
+    rc = cfdv::ctxi::solve_device(c, o, rep, nullptr, 0);
   }
   if (rc) return rc;
   if (o->true_residual && rep && o->mode == CFDV_GMRES_REFERENCE) rc = true_residual(c, rep);

@@ -13,12 +13,18 @@
 
 namespace cfdv {
 
-// Nondimensional gas model of the reference (Thermo::set, FDV/Thermo.h:158-169)
-struct GasParams {
+// Nondimensional gas model of the reference (Thermo::set, FDV/Thermo.h:158-169).  The
+// Mach-number-dependent constants Cv, cgas and cmach have the scalar type S, so that the
+// adjoint kernels can differentiate through them (GasT<Dual>); the step uses GasT<double>.
+template <class S>
+struct GasT {
   double gamma, gamm1, gm1d2, gamm3, gm3d2;
-  double Pr, csuth, Cv, cgas, cmach, creyn, Twall;
+  double Pr, csuth;
+  S Cv, cgas, cmach;
+  double creyn, Twall;
   int adiabatic;
 };
+using GasParams = GasT<double>;
 
 inline GasParams make_gas(double gamma, double M, double Re, double Pr, double Tinf, double Tw, int adiabatic) {
   GasParams g;

@@ -13,6 +13,7 @@
 //   a(i,r,s) -> a[(i*5+r)*5+s],  c(i,j,r,s) -> c[((i*3+j)*5+r)*5+s].
 #pragma once
 #include "cfdv_types.h"
+#include "dual.cuh"
 
 namespace cfdv {
 
@@ -20,57 +21,70 @@ namespace cfdv {
 // Gauss-point state feeds exact-zero tests of the reference (gamma == 0, R == 0,
 // S == 0 in FDVGalerkin.h:308-379); evaluating it with the reference's operation
 // order and without contraction makes those decisions agree with the reference.
-#if defined(__CUDA_ARCH__)
-#define RN_MUL(a, b) __dmul_rn((a), (b))
-#define RN_ADD(a, b) __dadd_rn((a), (b))
-#define RN_SUB(a, b) __dsub_rn((a), (b))
-#define RN_DIV(a, b) __ddiv_rn((a), (b))
-#else
-// host: separate calls so that no host compiler setting can fuse them either
-__attribute__((noinline)) inline double rn_mul(double a, double b) { return a * b; }
-__attribute__((noinline)) inline double rn_add(double a, double b) { return a + b; }
-__attribute__((noinline)) inline double rn_sub(double a, double b) { return a - b; }
-__attribute__((noinline)) inline double rn_div(double a, double b) { return a / b; }
+// rn_* (dual.cuh) are the intrinsics for doubles and carry a derivative for duals.
 #define RN_MUL(a, b) ::cfdv::rn_mul((a), (b))
 #define RN_ADD(a, b) ::cfdv::rn_add((a), (b))
 #define RN_SUB(a, b) ::cfdv::rn_sub((a), (b))
 #define RN_DIV(a, b) ::cfdv::rn_div((a), (b))
-#endif
 
 #define JA(t, i, r, s) (t)[((i)*5 + (r)) * 5 + (s)]
 #define JC(t, i, j, r, s) (t)[(((i)*3 + (j)) * 5 + (r)) * 5 + (s)]
 
-CFDV_HD CFDV_INLINE double gas_mu(const GasParams& g, double T) {
-  if (T < 1.0E-12) return 1.0;
+template <class S>
+CFDV_HD CFDV_INLINE S gas_mu(const GasT<S>& g, S T) {
+  if (T < 1.0E-12) return S(1.0);
   return RN_MUL(RN_MUL(RN_DIV(1 + g.csuth, RN_ADD(T, g.csuth)), T), sqrt(T));
 }
-CFDV_HD CFDV_INLINE double gas_k(const GasParams& g, double mu) {
+template <class S>
+CFDV_HD CFDV_INLINE S gas_k(const GasT<S>& g, S mu) {
   return mu / ((g.gamma - 1.0) * (g.cmach * g.cmach) * g.Pr);
 }
 
-// primitive state of a node (NodeUnpack.h:185-205)
-struct NodePrim {
-  double U[5], x[3], v[3];
-  double rho, E, T, p;
+// primitive state of a node (NodeUnpack.h:185-205); coordinates are plain doubles
+template <class S>
+struct NodePrimT {
+  S U[5];
+  double x[3];
+  S v[3];
+  S rho, E, T, p;
 };
+using NodePrim = NodePrimT<double>;
 
-template <int NDIM>
-CFDV_HD CFDV_INLINE void node_unpack(const GasParams& g, const double* U, const double* x, NodePrim& n) {
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void node_unpack(const GasT<S>& g, const S* U, const double* x, NodePrimT<S>& n) {
 #pragma unroll
   for (int k = 0; k < NDIM + 2; k++) n.U[k] = U[k];
 #pragma unroll
   for (int k = 0; k < NDIM; k++) n.x[k] = x[k];
   n.rho = U[0];
-  double vsqr = 0;
+  S vsqr = 0;
 #pragma unroll
   for (int i = 0; i < NDIM; i++) {
     n.v[i] = RN_DIV(U[1 + i], U[0]);
     vsqr = RN_ADD(vsqr, RN_MUL(n.v[i], n.v[i]));
   }
   n.E = RN_DIV(U[NDIM + 1], U[0]);
-  double e = RN_SUB(n.E, RN_MUL(0.5, vsqr));
+  S e = RN_SUB(n.E, RN_MUL(0.5, vsqr));
   n.T = RN_DIV(e, g.Cv);
   n.p = RN_MUL(RN_MUL(n.rho, g.gamma - 1.0), e);
+}
+
+// CFL length of one node of an element (MPI_CFL.h:124-171): cleng / (|v| + sqrt(1.4 cgas T))
+// with T from NodeUnpack (NodeUnpack.h:191-203) clipped at 1e-9; the reference uses 1.4, not
+// gamma.  Returns false (no candidate) where the signal speed is not above 1e-9.
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE bool cfl_node_len(const S* u, double cleng, const GasT<S>& g, S* dxn) {
+  S vv = 0.0;
+  for (int k = 0; k < NDIM; k++) {
+    const S v = RN_DIV(u[1 + k], u[0]);
+    vv = RN_ADD(vv, RN_MUL(v, v));
+  }
+  const S Tn = RN_DIV(RN_SUB(RN_DIV(u[NDIM + 1], u[0]), RN_MUL(0.5, vv)), g.Cv);
+  const S Temp = (Tn > 10E-10) ? Tn : S(0.0);
+  const S sv = sqrt(vv), snd = sqrt(RN_MUL(RN_MUL(1.4, g.cgas), Temp));
+  if (!(RN_ADD(sv, snd) > 10E-10)) return false;
+  *dxn = RN_DIV(S(cleng), RN_ADD(sv, snd));
+  return true;
 }
 
 // shape functions and natural-coordinate derivatives
@@ -111,8 +125,8 @@ CFDV_HD CFDV_INLINE void shape_fn<3>(const double* z, double* Phi, double (*dPxi
 //   det J and, in 3D, the adjugate inv                 (geom_det)
 //   dPhi_N,i from dPxi_N, jac/inv and 1/det            (geom_dphi, one shape function)
 // phys_deriv runs them in sequence for one Gauss point.
-template <int NNOD>
-CFDV_HD CFDV_INLINE double geom_jac_entry(const double (*dPxi)[3], const NodePrim* nd, int i, int k) {
+template <int NNOD, class NP>
+CFDV_HD CFDV_INLINE double geom_jac_entry(const double (*dPxi)[3], const NP* nd, int i, int k) {
   double j = 0;
 #pragma unroll
   for (int N = 0; N < NNOD; N++) j = RN_ADD(j, RN_MUL(dPxi[N][k], nd[N].x[i]));
@@ -174,8 +188,8 @@ CFDV_HD CFDV_INLINE void geom_dphi<3>(const double* dPxi, const double (*j)[3], 
 }
 
 // isoparametric Jacobian, physical derivatives dPhi, returns det J; jac[i][j] = dx_i/dxi_j
-template <int NDIM>
-CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NodePrim* nd, double (*dPhi)[3],
+template <int NDIM, class NP>
+CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NP* nd, double (*dPhi)[3],
                                       double (*jac)[3]) {
   constexpr int NNOD = (NDIM == 2) ? 4 : 8;
 #pragma unroll
@@ -191,39 +205,36 @@ CFDV_HD CFDV_INLINE double phys_deriv(const double (*dPxi)[3], const NodePrim* n
 }
 
 // Gauss-point flow state
-struct GpState {
-  double E, T, U[5], dU[5][3], v[3], dV[3][3], dT[3], mu, k, tau[3][3];
+template <class S>
+struct GpStateT {
+  S E, T, U[5], dU[5][3], v[3], dV[3][3], dT[3], mu, k, tau[3][3];
 };
+using GpState = GpStateT<double>;
 
-template <int NDIM>
-CFDV_HD CFDV_INLINE void viscous_stress(GpState& f) {
-  double vkk = 0;
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void viscous_stress(GpStateT<S>& f) {
+  S vkk = 0;
 #pragma unroll
   for (int k = 0; k < NDIM; k++) vkk = RN_ADD(vkk, f.dV[k][k]);
 #pragma unroll
   for (int i = 0; i < NDIM; i++)
 #pragma unroll
     for (int j = 0; j < NDIM; j++) {
-      double t = RN_MUL(f.mu, RN_ADD(f.dV[i][j], f.dV[j][i]));
+      S t = RN_MUL(f.mu, RN_ADD(f.dV[i][j], f.dV[j][i]));
       if (i == j) t = RN_SUB(t, RN_MUL(RN_MUL(2.0 / 3.0, f.mu), vkk));
       f.tau[i][j] = t;
     }
 }
 
 // ---- flux Jacobians ---------------------------------------------------------
-template <int NDIM>
-CFDV_HD void jac_a(const GasParams& th, const GpState& f, double* m);
-// b(i, ., .) for one i (entries i*25 .. i*25+24)
-template <int NDIM>
-CFDV_HD void jac_b_rows(const GasParams& th, const GpState& f, int i, double* m);
-// c(i, j, ., .) for one i (entries i*75 .. i*75+74 of the 3x3 block layout)
-template <int NDIM>
-CFDV_HD void jac_c_rows(const GasParams& th, const GpState& f, int i, double* m);
+// jac_a<NDIM>: a(i, ., .) for all i; jac_b_rows<NDIM>: b(i, ., .) for one i (entries
+// i*25 .. i*25+24); jac_c_rows<NDIM>: c(i, j, ., .) for one i (entries i*75 .. i*75+74 of
+// the 3x3 block layout).  Each has a 2D and a 3D form below, templated on the scalar.
 
-template <>
-CFDV_HD CFDV_INLINE void jac_a<2>(const GasParams& th, const GpState& f, double* m) {
+template <class S>
+CFDV_HD CFDV_INLINE void jac_a_2d(const GasT<S>& th, const GpStateT<S>& f, S* m) {
   for (int i = 0; i < 2 * 25; i++) m[i] = 0.0;
-  const double u = f.v[0], v = f.v[1], uu = u * u, uv = u * v, vv = v * v, E = f.E;
+  const S u = f.v[0], v = f.v[1], uu = u * u, uv = u * v, vv = v * v, E = f.E;
   JA(m, 0, 0, 1) = 1.0;
   JA(m, 0, 1, 0) = th.gm3d2 * uu + th.gm1d2 * vv;
   JA(m, 0, 1, 1) = -th.gamm3 * u;
@@ -250,23 +261,23 @@ CFDV_HD CFDV_INLINE void jac_a<2>(const GasParams& th, const GpState& f, double*
   JA(m, 1, 3, 3) = th.gamma * v;
 }
 
-template <>
-CFDV_HD CFDV_INLINE void jac_b_rows<2>(const GasParams& th, const GpState& f, int i, double* m) {
-  double* blk = m + i * 25;
+template <class S>
+CFDV_HD CFDV_INLINE void jac_b_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  S* blk = m + i * 25;
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
-  const double reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
-  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
-  const double rho = f.U[0], DENOM = 1. / (rho * rho), TERM1 = f.k * DENOM / th.Cv;
-  const double u = f.v[0], v = f.v[1], uu = u * u, vv = v * v;
-  const double drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dedx = f.dU[3][0];
-  const double drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dedy = f.dU[3][1];
-  const double t00 = f.tau[0][0], t01 = f.tau[0][1], t10 = f.tau[1][0], t11 = f.tau[1][1];
-  const double b010 = (DENOM * (mu_R * dldx + lambda * dmdy - 2. * (mu_R * u * drdx + lambda * v * drdy))) * reinv;
-  const double b011 = mu_R * drdx * DENOM * reinv, b012 = lambda * drdy * DENOM * reinv;
-  const double b020 = (mu * DENOM * (dldy + dmdx - 2. * (u * drdy + v * drdx))) * reinv;
-  const double b021 = mu * drdy * DENOM * reinv, b022 = mu * drdx * DENOM * reinv;
-  const double b120 = (DENOM * (lambda * (dldx + 4. * v * drdy) + mu_R * (u * drdx + dmdy))) * reinv;
-  const double b121 = lambda * drdx * DENOM * reinv, b122 = mu_R * drdy * DENOM * reinv;
+  const S reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
+  const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const S rho = f.U[0], DENOM = 1. / (rho * rho), TERM1 = f.k * DENOM / th.Cv;
+  const S u = f.v[0], v = f.v[1], uu = u * u, vv = v * v;
+  const S drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dedx = f.dU[3][0];
+  const S drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dedy = f.dU[3][1];
+  const S t00 = f.tau[0][0], t01 = f.tau[0][1], t10 = f.tau[1][0], t11 = f.tau[1][1];
+  const S b010 = (DENOM * (mu_R * dldx + lambda * dmdy - 2. * (mu_R * u * drdx + lambda * v * drdy))) * reinv;
+  const S b011 = mu_R * drdx * DENOM * reinv, b012 = lambda * drdy * DENOM * reinv;
+  const S b020 = (mu * DENOM * (dldy + dmdx - 2. * (u * drdy + v * drdx))) * reinv;
+  const S b021 = mu * drdy * DENOM * reinv, b022 = mu * drdx * DENOM * reinv;
+  const S b120 = (DENOM * (lambda * (dldx + 4. * v * drdy) + mu_R * (u * drdx + dmdy))) * reinv;
+  const S b121 = lambda * drdx * DENOM * reinv, b122 = mu_R * drdy * DENOM * reinv;
   if (i == 0) {
     JA(m, 0, 1, 0) = b010;
     JA(m, 0, 1, 1) = b011;
@@ -296,15 +307,15 @@ CFDV_HD CFDV_INLINE void jac_b_rows<2>(const GasParams& th, const GpState& f, in
   }
 }
 
-template <>
-CFDV_HD CFDV_INLINE void jac_c_rows<2>(const GasParams& th, const GpState& f, int i, double* m) {
-  double* blk = m + i * 75;
+template <class S>
+CFDV_HD CFDV_INLINE void jac_c_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  S* blk = m + i * 75;
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
-  const double reinv = 1.0 / th.creyn, mu = f.mu;
-  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
-  const double rho = f.U[0], denom = 1. / (rho * rho), denom2 = denom / rho;
-  const double l = f.U[1], mv = f.U[2], re = f.U[3];
-  const double ll = l * l, lm = l * mv, mm = mv * mv, rv = ll + mm, hkocv = f.k / th.Cv;
+  const S reinv = 1.0 / th.creyn, mu = f.mu;
+  const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const S rho = f.U[0], denom = 1. / (rho * rho), denom2 = denom / rho;
+  const S l = f.U[1], mv = f.U[2], re = f.U[3];
+  const S ll = l * l, lm = l * mv, mm = mv * mv, rv = ll + mm, hkocv = f.k / th.Cv;
   if (i == 0) {
     JC(m, 0, 0, 1, 0) = mu_R * l * denom * reinv;
     JC(m, 0, 0, 1, 1) = -mu_R / rho * reinv;
@@ -340,13 +351,13 @@ CFDV_HD CFDV_INLINE void jac_c_rows<2>(const GasParams& th, const GpState& f, in
   }
 }
 
-template <>
-CFDV_HD CFDV_INLINE void jac_a<3>(const GasParams& th, const GpState& f, double* m) {
+template <class S>
+CFDV_HD CFDV_INLINE void jac_a_3d(const GasT<S>& th, const GpStateT<S>& f, S* m) {
   for (int i = 0; i < 3 * 25; i++) m[i] = 0.0;
-  const double gamma = th.gamma, g1 = th.gamm1, g3 = th.gamm3, gm3d2 = th.gm3d2, gm1d2 = th.gm1d2;
-  const double u = f.v[0], v = f.v[1], w = f.v[2];
-  const double uu = u * u, uv = u * v, vv = v * v, ww = w * w, uw = u * w, vw = v * w, E = f.E;
-  const double q2 = uu + vv + ww;
+  const S gamma = th.gamma, g1 = th.gamm1, g3 = th.gamm3, gm3d2 = th.gm3d2, gm1d2 = th.gm1d2;
+  const S u = f.v[0], v = f.v[1], w = f.v[2];
+  const S uu = u * u, uv = u * v, vv = v * v, ww = w * w, uw = u * w, vw = v * w, E = f.E;
+  const S q2 = uu + vv + ww;
   JA(m, 0, 0, 1) = 1.0;
   JA(m, 0, 1, 0) = gm3d2 * uu + gm1d2 * (vv + ww);
   JA(m, 0, 1, 1) = -g3 * u; JA(m, 0, 1, 2) = -g1 * v; JA(m, 0, 1, 3) = -g1 * w; JA(m, 0, 1, 4) = g1;
@@ -375,32 +386,32 @@ CFDV_HD CFDV_INLINE void jac_a<3>(const GasParams& th, const GpState& f, double*
   JA(m, 2, 4, 4) = gamma * w;
 }
 
-template <>
-CFDV_HD CFDV_INLINE void jac_b_rows<3>(const GasParams& th, const GpState& f, int i, double* m) {
-  double* blk = m + i * 25;
+template <class S>
+CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  S* blk = m + i * 25;
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
-  const double mu = f.mu, E = f.E;
-  const double lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
-  const double rho = f.U[0], denom = 1. / (rho * rho), TERM1 = f.k * denom / th.Cv;
-  const double u = f.v[0], v = f.v[1], w = f.v[2], uu = u * u, vv = v * v, ww = w * w, q2 = uu + vv + ww;
-  const double drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dndx = f.dU[3][0], dedx = f.dU[4][0];
-  const double drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dndy = f.dU[3][1], dedy = f.dU[4][1];
-  const double drdz = f.dU[0][2], dldz = f.dU[1][2], dmdz = f.dU[2][2], dndz = f.dU[3][2], dedz = f.dU[4][2];
-  const double l = f.U[1], mv = f.U[2], n = f.U[3];
+  const S mu = f.mu, E = f.E;
+  const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const S rho = f.U[0], denom = 1. / (rho * rho), TERM1 = f.k * denom / th.Cv;
+  const S u = f.v[0], v = f.v[1], w = f.v[2], uu = u * u, vv = v * v, ww = w * w, q2 = uu + vv + ww;
+  const S drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dndx = f.dU[3][0], dedx = f.dU[4][0];
+  const S drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dndy = f.dU[3][1], dedy = f.dU[4][1];
+  const S drdz = f.dU[0][2], dldz = f.dU[1][2], dmdz = f.dU[2][2], dndz = f.dU[3][2], dedz = f.dU[4][2];
+  const S l = f.U[1], mv = f.U[2], n = f.U[3];
   const auto& t = f.tau;
   // built unscaled, then multiplied by 1/Re (NavierStokes3D.h:331-342)
-  const double b010 = (denom * (mu_R * dldx + lambda * (dmdy + dndz) + mu_R * (-2. * u * drdx + v * drdy + w * drdz)));
-  const double b011 = mu_R * drdx * denom, b012 = lambda * drdy * denom, b013 = lambda * drdz * denom;
-  const double b020 = (mu * denom * (dldy + dmdx - 2. * (u * drdy + v * drdx)));
-  const double b021 = mu * drdy * denom, b022 = mu * drdx * denom;
-  const double b030 = (mu * denom * (dldz + dndx - 2. * (u * drdz + w * drdx)));
-  const double b031 = mu * drdz * denom, b033 = mu * drdx * denom;
-  const double b120 = (denom * (lambda * (dldx + dndz) + mu_R * (dmdy + u * drdx - 2. * v * drdy + w * drdz)));
-  const double b121 = lambda * drdx * denom, b122 = mu_R * drdy * denom, b123 = lambda * drdz * denom;
-  const double b130 = (mu * denom * (dmdz + dndy - 2. * (v * drdz + w * drdy)));
-  const double b132 = mu * denom * drdz, b133 = mu * denom * drdy;
-  const double b230 = (denom * (mu_R * (dndz + u * drdx + v * drdy - 2. * w * drdz) + lambda * (dldx + dmdy)));
-  const double b231 = lambda * drdx * denom, b232 = lambda * drdy * denom, b233 = mu_R * drdz * denom;
+  const S b010 = (denom * (mu_R * dldx + lambda * (dmdy + dndz) + mu_R * (-2. * u * drdx + v * drdy + w * drdz)));
+  const S b011 = mu_R * drdx * denom, b012 = lambda * drdy * denom, b013 = lambda * drdz * denom;
+  const S b020 = (mu * denom * (dldy + dmdx - 2. * (u * drdy + v * drdx)));
+  const S b021 = mu * drdy * denom, b022 = mu * drdx * denom;
+  const S b030 = (mu * denom * (dldz + dndx - 2. * (u * drdz + w * drdx)));
+  const S b031 = mu * drdz * denom, b033 = mu * drdx * denom;
+  const S b120 = (denom * (lambda * (dldx + dndz) + mu_R * (dmdy + u * drdx - 2. * v * drdy + w * drdz)));
+  const S b121 = lambda * drdx * denom, b122 = mu_R * drdy * denom, b123 = lambda * drdz * denom;
+  const S b130 = (mu * denom * (dmdz + dndy - 2. * (v * drdz + w * drdy)));
+  const S b132 = mu * denom * drdz, b133 = mu * denom * drdy;
+  const S b230 = (denom * (mu_R * (dndz + u * drdx + v * drdy - 2. * w * drdz) + lambda * (dldx + dmdy)));
+  const S b231 = lambda * drdx * denom, b232 = lambda * drdy * denom, b233 = mu_R * drdz * denom;
   if (i == 0) {
     JA(m, 0, 1, 0) = b010;
     JA(m, 0, 1, 1) = b011;
@@ -456,21 +467,21 @@ CFDV_HD CFDV_INLINE void jac_b_rows<3>(const GasParams& th, const GpState& f, in
     JA(m, 2, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
     JA(m, 2, 4, 4) = TERM1 * drdz;
   }
-  const double reinv = 1.0 / th.creyn;
+  const S reinv = 1.0 / th.creyn;
   for (int k = 0; k < 25; k++) blk[k] *= reinv;
 }
 
-template <>
-CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, int i, double* m) {
-  double* blk = m + i * 75;
+template <class S>
+CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  S* blk = m + i * 75;
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
-  const double mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
-  const double rho = f.U[0], denom = 1. / (rho * rho);
-  const double l = f.U[1], mv = f.U[2], n = f.U[3], re = f.U[4];
-  const double ll = l * l, mm = mv * mv, nn = n * n, hkocv = f.k / th.Cv, TERM1 = f.k / th.Cv * denom;
-  const double q = (-re + (ll + mm + nn) / rho);
+  const S mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
+  const S rho = f.U[0], denom = 1. / (rho * rho);
+  const S l = f.U[1], mv = f.U[2], n = f.U[3], re = f.U[4];
+  const S ll = l * l, mm = mv * mv, nn = n * n, hkocv = f.k / th.Cv, TERM1 = f.k / th.Cv * denom;
+  const S q = (-re + (ll + mm + nn) / rho);
   if (i == 0) {
-    const double d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
+    const S d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
     JC(m, 0, 0, 1, 0) = mu_R * l * denom;
     JC(m, 0, 0, 1, 1) = (-mu_R / rho);
     JC(m, 0, 0, 2, 0) = mu * mv * denom;
@@ -497,7 +508,7 @@ CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, in
     JC(m, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
     JC(m, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
   } else if (i == 1) {
-    const double e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
+    const S e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
     JC(m, 1, 1, 1, 0) = e10;
     JC(m, 1, 1, 1, 1) = (-mu / rho);
     JC(m, 1, 1, 2, 0) = e20;
@@ -524,7 +535,7 @@ CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, in
     JC(m, 1, 2, 4, 2) = (n / rho) * (-mu / rho);
     JC(m, 1, 2, 4, 3) = (mv / rho) * (-lambda / rho);
   } else {
-    const double f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
+    const S f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
     JC(m, 2, 2, 1, 0) = f10;
     JC(m, 2, 2, 1, 1) = (-mu / rho);
     JC(m, 2, 2, 2, 0) = f20;
@@ -551,55 +562,62 @@ CFDV_HD CFDV_INLINE void jac_c_rows<3>(const GasParams& th, const GpState& f, in
     JC(m, 2, 1, 4, 2) = (n / rho) * (-lambda / rho);
     JC(m, 2, 1, 4, 3) = (mv / rho) * (-mu / rho);
   }
-  const double reinv = 1.0 / th.creyn;
+  const S reinv = 1.0 / th.creyn;
   for (int k = 0; k < 75; k++) blk[k] *= reinv;
 }
 
-template <int NDIM>
-CFDV_HD CFDV_INLINE void jac_b(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < NDIM; i++) jac_b_rows<NDIM>(th, f, i, m);
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void jac_a(const GasT<S>& th, const GpStateT<S>& f, S* m) {
+  if constexpr (NDIM == 2) jac_a_2d(th, f, m);
+  else jac_a_3d(th, f, m);
 }
-
-template <int NDIM>
-CFDV_HD CFDV_INLINE void jac_c(const GasParams& th, const GpState& f, double* m) {
-  for (int i = 0; i < NDIM; i++) jac_c_rows<NDIM>(th, f, i, m);
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void jac_b_rows(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  if constexpr (NDIM == 2) jac_b_rows_2d(th, f, i, m);
+  else jac_b_rows_3d(th, f, i, m);
+}
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void jac_c_rows(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
+  if constexpr (NDIM == 2) jac_c_rows_2d(th, f, i, m);
+  else jac_c_rows_3d(th, f, i, m);
 }
 
 // Convective + viscous flux of one node, entry (i, r): F(i,r) + G(i,r).  F is the node's own
 // flux; G uses the Gauss-point stress, dT and k with the node velocity.  with_F = 0 drops F
 // (the 3D reference evaluates the empty base-class flux).  r may be a run-time index:
 // nothing here is an array in registers or local memory.
-template <int NDIM>
-CFDV_HD CFDV_INLINE double node_flux_entry(const GpState& f, const NodePrim& n, double Re, bool with_F, int i, int r) {
-  const double reinv = 1.0 / Re;
-  double G = 0.0;
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE S node_flux_entry(const GpStateT<S>& f, const NodePrimT<S>& n, double Re, bool with_F, int i,
+                                      int r) {
+  const S reinv = 1.0 / Re;
+  S G = 0.0;
   if (r >= 1 && r <= NDIM) {
     G = -f.tau[i][r - 1] * reinv;
   } else if (r == NDIM + 1) {
-    double s = -f.tau[i][0] * n.v[0];
+    S s = -f.tau[i][0] * n.v[0];
 #pragma unroll
     for (int j = 1; j < NDIM; j++) s = s - f.tau[i][j] * n.v[j];
     G = (s - f.k * f.dT[i]) * reinv;
   }
-  double F = 0.0;
+  S F = 0.0;
   if (with_F) {
     if (NDIM == 2) {
-      const double rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
-      const double li = (i == 0) ? l : m;
+      const S rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
+      const S li = (i == 0) ? l : m;
       if (r == 0) F = li;
       else if (r == 1) F = (i == 0) ? p + l * l / rho : (l * m) / rho;
       else if (r == 2) F = (i == 0) ? (l * m) / rho : p + m * m / rho;
       else F = (p + e) * (li / rho);
     } else {
-      const double rho = n.U[0], p = n.p;
-      const double vi = n.U[1 + i] / n.U[0];
+      const S rho = n.U[0], p = n.p;
+      const S vi = n.U[1 + i] / n.U[0];
       if (r == 0) {
         F = rho * vi;
       } else if (r <= 3) {
-        const double vj = n.U[r] / n.U[0];
+        const S vj = n.U[r] / n.U[0];
         F = rho * vi * vj + (i == r - 1 ? p : 0.0);
       } else {
-        const double E = n.U[4] / n.U[0];
+        const S E = n.U[4] / n.U[0];
         F = (rho * E + p) * vi;
       }
     }

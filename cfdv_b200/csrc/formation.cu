@@ -46,19 +46,8 @@ __global__ void cfl_partial_kernel(const double* __restrict__ U, const int* __re
     double dxele = 1000.0;
     for (int i = 0; i < NNOD; i++) {
       const double* u = U + (size_t)conn[(size_t)e * NNOD + i] * NEQ;
-      double vv = 0.0;
-      for (int k = 0; k < NDIM; k++) {
-        const double v = RN_DIV(u[1 + k], u[0]);
-        vv = RN_ADD(vv, RN_MUL(v, v));
-      }
-      // NodeUnpack (NodeUnpack.h:191-203): e = rhoE/rho - |v|^2/2, T = e / Cv
-      const double Tn = RN_DIV(RN_SUB(RN_DIV(u[NDIM + 1], u[0]), RN_MUL(0.5, vv)), g.Cv);
-      const double Temp = (Tn > 10E-10) ? Tn : 0.0;
-      const double sv = sqrt(vv), snd = sqrt(RN_MUL(RN_MUL(1.4, g.cgas), Temp));  // the reference uses 1.4, not gamma
-      if (RN_ADD(sv, snd) > 10E-10) {
-        const double dxn = RN_DIV(cleng[e], RN_ADD(sv, snd));
-        if (dxn < dxele) dxele = dxn;
-      }
+      double dxn;
+      if (cfl_node_len<NDIM>(u, cleng[e], g, &dxn) && dxn < dxele) dxele = dxn;
     }
     best = fmin(best, dxele);
   }

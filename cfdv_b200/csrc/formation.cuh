@@ -132,32 +132,32 @@ CFDV_HD CFDV_INLINE const NodePrim& pass_node(const FormShared<NDIM>& sh, int f,
 
 
 // FDVParam.h:15-111, per node: Mach and Reynolds numbers
-template <int NDIM>
-CFDV_HD CFDV_INLINE void node_mach_re(const GasParams& g, const NodePrim& n, double* M, double* Re) {
-  double vv = 0;
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE void node_mach_re(const GasT<S>& g, const NodePrimT<S>& n, S* M, S* Re) {
+  S vv = 0;
   for (int i = 0; i < NDIM; i++) vv = RN_ADD(vv, RN_MUL(n.v[i], n.v[i]));
-  const double V = sqrt(vv);
-  double Tn = n.T;
+  const S V = sqrt(vv);
+  S Tn = n.T;
   if (Tn < 1.0E-12) Tn = 0;
-  const double snd = sqrt(RN_MUL(RN_MUL(g.gamma, g.cgas), Tn));
-  *M = (snd < 1.0E-12) ? 0 : RN_DIV(V, snd);
+  const S snd = sqrt(RN_MUL(RN_MUL(g.gamma, g.cgas), Tn));
+  *M = (snd < 1.0E-12) ? S(0) : RN_DIV(V, snd);
   *Re = RN_DIV(RN_MUL(n.rho, V), gas_mu(g, Tn));
 }
 
 // FDVParam.h:15-111 over the element's nodes: which = 0 gives s1 and s2 from the Mach
 // numbers, which = 1 gives s3 and s4 from the Reynolds numbers, into s[2*which], s[2*which+1]
-template <int NNOD>
-CFDV_HD CFDV_INLINE void fdv_pair(const double* val, int which, double* s) {
-  double vmin = val[0], vmax = val[0];
+template <int NNOD, class S>
+CFDV_HD CFDV_INLINE void fdv_pair(const S* val, int which, S* s) {
+  S vmin = val[0], vmax = val[0];
   for (int b = 1; b < NNOD; b++) {
     vmax = fmax(vmax, val[b]);
     vmin = fmin(vmin, val[b]);
   }
   const double eps = 0.0000001;
   // the spread stays in FP64: max ~ min cancels
-  const double r = RN_DIV(sqrt(RN_SUB(RN_MUL(vmax, vmax), RN_MUL(vmin, vmin))), RN_ADD(vmin, eps));
-  double sv = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
-  if (r > 0.01) sv = fmin(r, 1.0);
+  const S r = RN_DIV(sqrt(RN_SUB(RN_MUL(vmax, vmax), RN_MUL(vmin, vmin))), RN_ADD(vmin, eps));
+  S sv = 0.0;  // r == 0.01 exactly: the reference keeps the previous element's value
+  if (r > 0.01) sv = fmin(r, S(1.0));
   else if (r < 0.01 && vmin >= 10E-10) sv = 0.0;
   else if (which == 0 ? (vmin < 10E-10) : (vmin <= 10E-10)) sv = 1.0;
   s[2 * which] = sv;
@@ -300,50 +300,76 @@ CFDV_HD CFDV_INLINE void step_state(FormShared<NDIM>& sh, int lf, int tid) {
   for (int t = tid; t < NQ * NV; t += T::THREADS) state_sum<NDIM, FACE>(sh, fc, sh.slot[t / NV], t % NV);
 }
 
+// SUPG coefficient alpha(R) = coth(R/2) - 2/R with coth = cosh/sinh, in the reference's
+// operation order (FDVGalerkin.h:46-50, 308-319); alpha = 0 at R == 0.
+CFDV_HD CFDV_INLINE double supg_alpha(double R) {
+  return (R == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R / 2.), sinh(R / 2.)), RN_DIV(2., R));
+}
+// The dual form keeps that value; its derivative uses d alpha / dR = 2/R^2 - 1/(2 sinh^2(R/2)),
+// which for |R| < 0.1 is evaluated from its series 1/6 - R^2/120 + R^4/3024 - R^6/86400:
+// the two terms of the closed form cancel to ~R^2 of their size, so at small cell Reynolds
+// numbers their rounding would swamp the derivative.
+CFDV_HD CFDV_INLINE Dual supg_alpha(const Dual& R) {
+  const double r = R.v;
+  double da;
+  if (fabs(r) < 0.1) {
+    const double r2 = r * r;
+    da = 1.0 / 6.0 - r2 / 120.0 + r2 * r2 / 3024.0 - r2 * r2 * r2 / 86400.0;
+  } else {
+    const double sh = sinh(r / 2.);
+    da = 2.0 / (r * r) - 1.0 / (2.0 * sh * sh);
+  }
+  return Dual(supg_alpha(r), (r == 0) ? 0.0 : R.d * da);
+}
+
 // 2D streamline-upwind test function Psi (FDVGalerkin.h:225-332) with discontinuity
 // capturing (FDVGalerkin.h:336-387), evaluated in the reference's operation order without
-// contraction (RN_*), because its exact-zero tests decide whether a term is present at all
-CFDV_HD CFDV_INLINE void supg_psi_2d(const FormShared<2>& sh, GpSlot<2>& sl) {
-  const GpState& f = sl.st;
-  const auto& jac = sl.g.jac;
+// contraction (RN_*), because its exact-zero tests decide whether a term is present at all.
+// jac: isoparametric Jacobian at the point, x4: the element's node coordinates.
+template <class S>
+CFDV_HD CFDV_INLINE void psi_2d(const double (*jac)[3], const double* const* x4, const GpStateT<S>& f,
+                                const double (*dPhi)[3], S* Psi) {
   const double J_xi = RN_ADD(RN_MUL(jac[0][0], jac[0][0]), RN_MUL(jac[1][0], jac[1][0]));
   const double J_eta = RN_ADD(RN_MUL(jac[0][1], jac[0][1]), RN_MUL(jac[1][1], jac[1][1]));
   const double ixi = RN_DIV(1., sqrt(J_xi)), ieta = RN_DIV(1., sqrt(J_eta));
-  const double v_xi = RN_ADD(RN_MUL(f.v[0], RN_MUL(ixi, jac[0][0])), RN_MUL(f.v[1], RN_MUL(ixi, jac[1][0])));
-  const double v_eta = RN_ADD(RN_MUL(f.v[0], RN_MUL(ieta, jac[0][1])), RN_MUL(f.v[1], RN_MUL(ieta, jac[1][1])));
-  const double S = RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]));
+  const S v_xi = RN_ADD(RN_MUL(f.v[0], RN_MUL(ixi, jac[0][0])), RN_MUL(f.v[1], RN_MUL(ixi, jac[1][0])));
+  const S v_eta = RN_ADD(RN_MUL(f.v[0], RN_MUL(ieta, jac[0][1])), RN_MUL(f.v[1], RN_MUL(ieta, jac[1][1])));
+  const S S2 = RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]));
   // element extents between opposite edge midpoints, accumulated node by node with the
   // edge-midpoint interpolants (the eta extent is taken bottom minus top)
-  const NodePrim* q4 = sh.nd;
   const double h_xi =
-      RN_SUB(RN_ADD(RN_ADD(-RN_MUL(0.5, q4[0].x[0]), RN_MUL(0.5, q4[1].x[0])), RN_MUL(0.5, q4[2].x[0])),
-             RN_MUL(0.5, q4[3].x[0]));
+      RN_SUB(RN_ADD(RN_ADD(-RN_MUL(0.5, x4[0][0]), RN_MUL(0.5, x4[1][0])), RN_MUL(0.5, x4[2][0])),
+             RN_MUL(0.5, x4[3][0]));
   const double h_eta =
-      RN_SUB(RN_SUB(RN_ADD(RN_MUL(0.5, q4[0].x[1]), RN_MUL(0.5, q4[1].x[1])), RN_MUL(0.5, q4[2].x[1])),
-             RN_MUL(0.5, q4[3].x[1]));
-  const double R_xi = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_xi), h_xi), f.mu);
-  const double R_eta = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_eta), h_eta), f.mu);
-  const double al_xi = (R_xi == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_xi / 2.), sinh(R_xi / 2.)), RN_DIV(2., R_xi));
-  const double al_eta = (R_eta == 0) ? 0.0 : RN_SUB(RN_DIV(cosh(R_eta / 2.), sinh(R_eta / 2.)), RN_DIV(2., R_eta));
-  const double tau = (S == 0) ? 0.0
-                              : RN_DIV(RN_MUL(0.25, RN_ADD(RN_MUL(RN_MUL(al_xi, h_xi), v_xi),
-                                                            RN_MUL(RN_MUL(al_eta, h_eta), v_eta))),
-                                       S);
+      RN_SUB(RN_SUB(RN_ADD(RN_MUL(0.5, x4[0][1]), RN_MUL(0.5, x4[1][1])), RN_MUL(0.5, x4[2][1])),
+             RN_MUL(0.5, x4[3][1]));
+  const S R_xi = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_xi), h_xi), f.mu);
+  const S R_eta = RN_DIV(RN_MUL(RN_MUL(f.U[0], v_eta), h_eta), f.mu);
+  const S al_xi = supg_alpha(R_xi);
+  const S al_eta = supg_alpha(R_eta);
+  const S tau = (S2 == 0) ? S(0.0)
+                          : RN_DIV(RN_MUL(0.25, RN_ADD(RN_MUL(RN_MUL(al_xi, h_xi), v_xi),
+                                                        RN_MUL(RN_MUL(al_eta, h_eta), v_eta))),
+                                   S2);
   for (int N = 0; N < 4; N++)
-    sl.Psi[N] = RN_ADD(RN_MUL(RN_MUL(tau, f.v[0]), sl.dPhi[N][0]), RN_MUL(RN_MUL(tau, f.v[1]), sl.dPhi[N][1]));
-  double A[2] = {0, 0};
+    Psi[N] = RN_ADD(RN_MUL(RN_MUL(tau, f.v[0]), dPhi[N][0]), RN_MUL(RN_MUL(tau, f.v[1]), dPhi[N][1]));
+  S A[2] = {0, 0};
   for (int k = 0; k < 2; k++)
     for (int j = 0; j < 2; j++) A[j] = RN_ADD(A[j], RN_MUL(f.dV[j][k], f.v[k]));
-  const double gam = RN_MUL(sqrt(RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]))),
-                            sqrt(RN_ADD(RN_MUL(A[0], A[0]), RN_MUL(A[1], A[1]))));
-  double tau_b = 0.0;
+  const S gam = RN_MUL(sqrt(RN_ADD(RN_MUL(f.v[0], f.v[0]), RN_MUL(f.v[1], f.v[1]))),
+                       sqrt(RN_ADD(RN_MUL(A[0], A[0]), RN_MUL(A[1], A[1]))));
+  S tau_b = 0.0;
   if (gam != 0) {
     tau_b = RN_ADD(RN_DIV(RN_MUL(RN_MUL(tau, f.v[0]), A[0]), gam), RN_DIV(RN_MUL(RN_MUL(tau, f.v[1]), A[1]), gam));
     if (RN_SUB(tau_b, tau) < 0) tau_b = tau;
   }
   for (int N = 0; N < 4; N++)
-    sl.Psi[N] = RN_ADD(RN_ADD(sl.Psi[N], RN_MUL(RN_MUL(tau_b, f.v[0]), sl.dPhi[N][0])),
-                       RN_MUL(RN_MUL(tau_b, f.v[1]), sl.dPhi[N][1]));
+    Psi[N] = RN_ADD(RN_ADD(Psi[N], RN_MUL(RN_MUL(tau_b, f.v[0]), dPhi[N][0])), RN_MUL(RN_MUL(tau_b, f.v[1]), dPhi[N][1]));
+}
+
+CFDV_HD CFDV_INLINE void supg_psi_2d(const FormShared<2>& sh, GpSlot<2>& sl) {
+  const double* x4[4] = {sh.nd[0].x, sh.nd[1].x, sh.nd[2].x, sh.nd[3].x};
+  psi_2d<double>(sl.g.jac, x4, sl.st, sl.dPhi, sl.Psi);
 }
 
 // step 5: viscosity, conductivity, stress; the 2D test function (one thread per Gauss point)
@@ -525,7 +551,8 @@ CFDV_HD CFDV_INLINE void phase_contract_domain(FormShared<NDIM>& sh, int tid) {
 }
 
 // 3D boundary-state edits (eval2dboundary.h:14-371); tau enters as zero
-CFDV_HD CFDV_INLINE void edit_face_state_3d(int code, GpState& f, const double* en, int adiabatic) {
+template <class S>
+CFDV_HD CFDV_INLINE void edit_face_state_3d(int code, GpStateT<S>& f, const double* en, int adiabatic) {
   switch (code) {
     case 2:
     case 12:
@@ -574,11 +601,11 @@ CFDV_HD CFDV_INLINE void edit_face_state_3d(int code, GpState& f, const double* 
     case 4: {
       f.v[0] = 0; f.v[1] = 0; f.v[2] = 0;
       const double* n = en;  // the weighted normal, not a unit vector
-      const double dud = f.dV[0][0] * n[0] + f.dV[0][1] * n[1] + f.dV[0][2] * n[2];
-      const double dvd = f.dV[1][0] * n[0] + f.dV[1][1] * n[1] + f.dV[1][2] * n[2];
-      const double dtd = f.dT[0] * n[0] + f.dT[1] * n[1] + f.dT[2] * n[2];
+      const S dud = f.dV[0][0] * n[0] + f.dV[0][1] * n[1] + f.dV[0][2] * n[2];
+      const S dvd = f.dV[1][0] * n[0] + f.dV[1][1] * n[1] + f.dV[1][2] * n[2];
+      const S dtd = f.dT[0] * n[0] + f.dT[1] * n[1] + f.dT[2] * n[2];
       for (int j = 0; j < 3; j++) { f.dV[0][j] -= dud * n[j]; f.dV[1][j] -= dvd * n[j]; f.dT[j] -= dtd * n[j]; }
-      double dUd[3];
+      S dUd[3];
       for (int i = 0; i < 3; i++) dUd[i] = f.dU[i][0] * n[0] + f.dU[i][1] * n[1] + f.dU[i][2] * n[2];
       for (int i = 0; i < 3; i++)  // only the first three equations (loop bound dU.jmax() = 3)
         for (int j = 0; j < 3; j++) f.dU[i][j] -= dUd[i] * n[j];
@@ -596,15 +623,16 @@ CFDV_HD CFDV_INLINE void edit_face_state_3d(int code, GpState& f, const double* 
   }
 }
 
-// 2D boundary-state edits (eval1dboundary.h:9-251)
-CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim* n0, const NodePrim* n1,
+// 2D boundary-state edits (eval1dboundary.h:9-251); x0, x1: the edge's node coordinates
+template <class S>
+CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpStateT<S>& f, const double* x0, const double* x1,
                                             const double* en) {
   const double len = sqrt(en[0] * en[0] + en[1] * en[1]);
   const double n[2] = {en[0] / len, en[1] / len};
   switch (code) {
     case 2:
     case 12: {
-      double d = f.v[0] * n[0] + f.v[1] * n[1];
+      S d = f.v[0] * n[0] + f.v[1] * n[1];
       f.v[0] -= d * n[0];
       d = f.v[0] * n[0] + f.v[1] * n[1];  // re-evaluated after the first component
       f.v[1] -= d * n[1];
@@ -615,7 +643,7 @@ CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim
     } break;
     case 1:
     case 51: {
-      double d = f.dT[0] * n[0] + f.dT[1] * n[1];
+      S d = f.dT[0] * n[0] + f.dT[1] * n[1];
       f.dT[0] -= d * n[0];
       d = f.dT[0] * n[0] + f.dT[1] * n[1];
       f.dT[1] -= d * n[1];
@@ -643,17 +671,17 @@ CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim
         nn[0] = en[0]; nn[1] = en[1];
       } else {  // fixed 10 degree ramp direction scaled by the edge height
         const double alpha = 10 * (3.14159 / 180.0);
-        const double dl = fabs(n1->x[1] - n0->x[1]);
+        const double dl = fabs(x1[1] - x0[1]);
         nn[0] = cos(alpha) * dl;
         nn[1] = sin(alpha) * dl;
       }
-      const double dud = f.dV[0][0] * nn[0] + f.dV[0][1] * nn[1];
-      const double dvd = f.dV[1][0] * nn[0] + f.dV[1][1] * nn[1];
-      const double dtd = f.dT[0] * nn[0] + f.dT[1] * nn[1];
+      const S dud = f.dV[0][0] * nn[0] + f.dV[0][1] * nn[1];
+      const S dvd = f.dV[1][0] * nn[0] + f.dV[1][1] * nn[1];
+      const S dtd = f.dT[0] * nn[0] + f.dT[1] * nn[1];
       f.dV[0][0] -= dud * nn[0]; f.dV[0][1] -= dud * nn[1];
       f.dV[1][0] -= dvd * nn[0]; f.dV[1][1] -= dvd * nn[1];
       f.dT[0] -= dtd * nn[0]; f.dT[1] -= dtd * nn[1];
-      double dUd[4];
+      S dUd[4];
       for (int i = 0; i < 4; i++) dUd[i] = f.dU[i][0] * nn[0] + f.dU[i][1] * nn[1];
       for (int i = 0; i < 4; i++)
         for (int j = 0; j < 2; j++) f.dU[i][j] -= dUd[i] * nn[j];
@@ -679,43 +707,35 @@ CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpState& f, const NodePrim
   if (code == 6) { f.tau[0][0] = 0.; f.tau[1][0] = 0.; }
 }
 
-// face step 0: face shape functions, derivatives along the face and the weighted normal
-// en for Gauss point qf (2D TestFunctions1D.h:141-216, 3D calc_TF_norm3D.h:9-167), one
-// thread per face Gauss point
+// Face shape functions phib, derivatives along the face dpidx and the weighted normal en
+// at face Gauss point qf (2D TestFunctions1D.h:141-216, 3D calc_TF_norm3D.h:9-167); xf
+// holds the coordinates of the face's NBN nodes in face order.
 template <int NDIM>
-CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
-  using T = FormTraits<NDIM>;
-  constexpr int NBN = T::NBN;
-  if (qf >= T::QF) return;
-  GpSlot<NDIM>& sl = sh.slot[qf];
-  const int f = sh.faces[lf];
-  const NodePrim* nd[NBN];
-  for (int i = 0; i < NBN; i++) nd[i] = &sh.nd[face_node(NDIM, f, i)];
-  double* phib = sl.Phi;
-  double (*dpidx)[3] = sl.dPhi;
-  double* en = sl.en;
+CFDV_HD CFDV_INLINE void face_point_geom(const double* gz, const double* gw, const double* const* xf, int qf,
+                                         double* phib, double (*dpidx)[3], double* en) {
+  constexpr int NBN = FormTraits<NDIM>::NBN;
   for (int i = 0; i < NBN; i++)
     for (int j = 0; j < 3; j++) dpidx[i][j] = 0.0;
   en[2] = 0.0;
   if (NDIM == 2) {  // TestFunctions1D.h:141-216
-    const double z = a.gz[qf], w = a.gw[qf];
+    const double z = gz[qf], w = gw[qf];
     phib[0] = 0.5 * (1 - z);
     phib[1] = 0.5 * (1 + z);
-    const double dxds = -0.5 * nd[0]->x[0] + 0.5 * nd[1]->x[0];
-    const double dyds = -0.5 * nd[0]->x[1] + 0.5 * nd[1]->x[1];
+    const double dxds = -0.5 * xf[0][0] + 0.5 * xf[1][0];
+    const double dyds = -0.5 * xf[0][1] + 0.5 * xf[1][1];
     en[0] = dyds * w;
     en[1] = -dxds * w;
-    const double delx = nd[1]->x[0] - nd[0]->x[0], dely = nd[1]->x[1] - nd[0]->x[1];
+    const double delx = xf[1][0] - xf[0][0], dely = xf[1][1] - xf[0][1];
     if (!(fabs(delx) < 1.0E-12)) { dpidx[0][0] = -1.0 / delx; dpidx[1][0] = 1.0 / delx; }
     if (!(fabs(dely) < 1.0E-12)) { dpidx[0][1] = -1.0 / dely; dpidx[1][1] = 1.0 / dely; }
   } else {  // calc_TF_norm3D.h:9-167
-    const double z[2] = {a.gz[qf >> 1], a.gz[qf & 1]};
-    const double w0 = a.gw[qf >> 1], w1 = a.gw[qf & 1];
+    const double z[2] = {gz[qf >> 1], gz[qf & 1]};
+    const double w0 = gw[qf >> 1], w1 = gw[qf & 1];
     double ph[4], dpxi[4][3];
     shape_fn<2>(z, ph, dpxi);
     for (int i = 0; i < 4; i++) phib[i] = ph[i];
     double L[3], Mu[3];
-    for (int i = 0; i < 3; i++) { L[i] = nd[1]->x[i] - nd[0]->x[i]; Mu[i] = nd[3]->x[i] - nd[0]->x[i]; }
+    for (int i = 0; i < 3; i++) { L[i] = xf[1][i] - xf[0][i]; Mu[i] = xf[3][i] - xf[0][i]; }
     for (int j = 0; j < 3; j++) {  // magnitude re-evaluated after each component
       L[j] /= sqrt(L[0] * L[0] + L[1] * L[1] + L[2] * L[2]);
       Mu[j] /= sqrt(Mu[0] * Mu[0] + Mu[1] * Mu[1] + Mu[2] * Mu[2]);
@@ -730,7 +750,7 @@ CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh,
     double dxd[3][2] = {{0, 0}, {0, 0}, {0, 0}};
     for (int N = 0; N < 4; N++)
       for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 2; j++) dxd[i][j] += dpxi[N][j] * nd[N]->x[i];
+        for (int j = 0; j < 2; j++) dxd[i][j] += dpxi[N][j] * xf[N][i];
     double tr[2][2];
     for (int j = 0; j < 2; j++) {
       tr[0][j] = L[0] * dxd[0][j] + L[1] * dxd[1][j] + L[2] * dxd[2][j];
@@ -745,9 +765,23 @@ CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh,
     }
     for (int i = 0; i < 3; i++) en[i] = nrm[i] * w0 * w1 * det;
   }
-  for (int m = 0; m < NBN; m++) {  // face-local coefficient rows for the contraction
-    sl.cM[0][m] = phib[m];
-    for (int j = 0; j < NDIM; j++) sl.cM[1 + j][m] = dpidx[m][j];
+}
+
+// face step 0: the face geometry of Gauss point qf (one thread per face Gauss point) and
+// the face-local coefficient rows of the contraction
+template <int NDIM>
+CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh, int lf, int qf) {
+  using T = FormTraits<NDIM>;
+  constexpr int NBN = T::NBN;
+  if (qf >= T::QF) return;
+  GpSlot<NDIM>& sl = sh.slot[qf];
+  const int f = sh.faces[lf];
+  const double* xf[NBN];
+  for (int i = 0; i < NBN; i++) xf[i] = sh.nd[face_node(NDIM, f, i)].x;
+  face_point_geom<NDIM>(a.gz, a.gw, xf, qf, sl.Phi, sl.dPhi, sl.en);
+  for (int m = 0; m < NBN; m++) {
+    sl.cM[0][m] = sl.Phi[m];
+    for (int j = 0; j < NDIM; j++) sl.cM[1 + j][m] = sl.dPhi[m][j];
   }
 }
 
@@ -764,7 +798,7 @@ CFDV_HD CFDV_INLINE void step_face_edit(const FormArgs& a, FormShared<NDIM>& sh,
   fs.k = gas_k(a.gas, fs.mu);
   for (int i = 0; i < NDIM; i++)
     for (int j = 0; j < NDIM; j++) fs.tau[i][j] = 0;
-  if (NDIM == 2) edit_face_state_2d(code, fs, &sh.nd[face_node(NDIM, f, 0)], &sh.nd[face_node(NDIM, f, 1)], sl.en);
+  if (NDIM == 2) edit_face_state_2d(code, fs, sh.nd[face_node(NDIM, f, 0)].x, sh.nd[face_node(NDIM, f, 1)].x, sl.en);
   else edit_face_state_3d(code, fs, sl.en, a.gas.adiabatic);
 }
 

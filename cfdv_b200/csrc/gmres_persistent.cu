@@ -1,15 +1,21 @@
 // Restarted GMRES(m) to a relative tolerance as ONE persistent cooperative kernel.
 //
-// For meshes whose per-product work is a few microseconds (the 2D cases fit in L2),
-// launching one kernel per MGS pass and reading every Hessenberg column back to the
-// host costs more than the arithmetic.  This kernel keeps the whole solve on the
-// device: every restart recomputes r = b - A du with the FP64 matrices, then runs
-// the Arnoldi cycle with MGS (dots reduced from fixed block partials, so every block
-// derives the same scalar), block 0 applies the Givens rotations and tests
-// |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver), back-substitutes
-// the small triangular system and all blocks add V y to du.  Products use the FP64
-// matrices, or the FP32 matrices with FP32 accumulation for the mixed form (the
-// restart residual stays FP64: GMRES-based iterative refinement).
+// Launching one kernel per MGS pass and reading every Hessenberg column back to the
+// host costs more than the arithmetic on the 2D cases (they fit in L2), and on the 3D
+// cases the host round trips still idle the GPU between passes.  This kernel keeps the
+// whole solve on the device: every restart recomputes r = b - A du with the FP64
+// matrices, then runs the Arnoldi cycle with MGS (dots reduced from fixed block
+// partials, so every block derives the same scalar), block 0 applies the Givens
+// rotations and tests |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver),
+// back-substitutes the small triangular system and all blocks add V y to du.  Products
+// use the FP64 matrices, or the FP32 matrices with FP32 accumulation for the mixed form
+// (the restart residual stays FP64: GMRES-based iterative refinement).  With
+// `transpose` every product is A^T x (the adjoint system) and the node-block
+// preconditioner is applied transposed.
+//
+// Shape: 512-thread blocks, two per SM, so that the element pass keeps as many matrix
+// loads in flight as the stand-alone element kernel (each thread owns one row of one
+// element and issues its Ke loads back to back).
 //
 // Phases are separated by a grid barrier.  Its spin is bounded: a block that waits
 // longer than the limit sets an error flag and every block returns at the next
@@ -27,6 +33,8 @@ namespace cfdv {
 namespace {
 
 constexpr long long kSpinLimit = 1ll << 27;  // ~ seconds of polling: far above any barrier
+constexpr int kThreads = 512;
+constexpr int kBlocksPerSm = 2;
 
 struct Barrier {
   unsigned int* count;
@@ -91,74 +99,73 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
   return block_sum(v);
 }
 
-// z_d = sum_s Dinv[n][r][s] * (w[n*NEQ + s] / scale), d = n*NEQ + r, with the same
-// division as the stored v so that z = Dinv v exactly
+// z_d = sum_s P[r][s] * (w[n*NEQ + s] / scale), d = n*NEQ + r, P = Dinv (or Dinv^T), with
+// the same division as the stored v so that z = P v exactly
 template <int NEQ>
-__device__ __forceinline__ double precond_at(const double* Dinv, const double* w, int d, double scale) {
+__device__ __forceinline__ double precond_at(const double* Dinv, const double* w, int d, double scale, bool trans) {
   const int n = d / NEQ, r = d % NEQ;
-  const double* D = Dinv + (size_t)n * NEQ * NEQ + r * NEQ;
+  const double* D = Dinv + (size_t)n * NEQ * NEQ;
   double t = 0.0;
 #pragma unroll
-  for (int s = 0; s < NEQ; s++) t += D[s] * (__ldcg(w + (size_t)n * NEQ + s) / scale);
+  for (int s = 0; s < NEQ; s++)
+    t += D[trans ? s * NEQ + r : r * NEQ + s] * (__ldcg(w + (size_t)n * NEQ + s) / scale);
   return t;
+}
+
+// Element pass Y_e = R_e x_e (TRANS: R_e^T x_e) over the grid: thread (le, i) owns row i of
+// element le of each block iteration; x_e is gathered into a double-buffered shared tile.
+template <int KE, int NEQ, int NNOD, typename TM>
+__device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* __restrict__ conn, const double* x,
+                                          TM* Y, int E, bool trans, TM (*xs)[kThreads / KE][KE]) {
+  constexpr int EPB = kThreads / KE;
+  const int le = threadIdx.x / KE, i = threadIdx.x % KE;
+  int buf = 0;
+  for (int e0 = blockIdx.x * EPB; e0 < E; e0 += gridDim.x * EPB) {
+    const int e = e0 + le;
+    const bool act = le < EPB && e < E;
+    if (act) xs[buf][le][i] = (TM)__ldcg(x + (size_t)__ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ);
+    __syncthreads();  // the other buffer was last read before the previous barrier
+    if (act) {
+      const TM* Re = R + (size_t)e * KE * KE;
+      TM acc = 0;
+      if (!trans) {
+#pragma unroll
+        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[buf][le][j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < KE; j++) acc += __ldg(Re + i * KE + j) * xs[buf][le][j];
+      }
+      Y[(size_t)e * KE + i] = acc;
+    }
+    buf ^= 1;
+  }
 }
 
 }  // namespace
 
 template <int KE, int NEQ, int NNOD, typename TR>
-__global__ void gmres_persistent_kernel(PersistentArgs a) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kernel(PersistentArgs a) {
   const unsigned int nb = gridDim.x;
   const int tid = threadIdx.x, bid = blockIdx.x;
-  const int nthr = blockDim.x;
-  const int gtid = bid * nthr + tid, gstride = nb * nthr;
+  const int gtid = bid * kThreads + tid, gstride = nb * kThreads;
   const int n = a.n_dof;
+  const bool tr = a.transpose != 0;
   Barrier bar{a.bar_count, a.bar_gen, a.err};
-  constexpr int EPB = 256 / KE;  // elements per block-iteration of the element pass
-  __shared__ TR xs[EPB > 0 ? EPB : 1][KE];
-  __shared__ double xs64[EPB > 0 ? EPB : 1][KE];
+  constexpr int EPB = kThreads / KE;
+  __shared__ double xs64[2][EPB][KE];
+  __shared__ TR xs[2][EPB][KE];
   double* V = a.V;
   double* W = a.W;
   double* pa = a.part0;
   double* pb = a.part1;
 
-  // element pass: Y = R x (FP64 matrices, or FP32 matrices with FP32 accumulation)
   auto elem_pass64 = [&](const double* x) {
-    const int le = tid / KE, i = tid % KE;
-    for (int e0 = bid * EPB; e0 < a.n_elements; e0 += nb * EPB) {
-      const int e = e0 + le;
-      if (le < EPB && e < a.n_elements)
-        xs64[le][i] = __ldcg(x + (size_t)a.conn[(size_t)e * NNOD + i / NEQ] * NEQ + i % NEQ);
-      __syncthreads();
-      if (le < EPB && e < a.n_elements) {
-        const double* Re = a.R64 + (size_t)e * KE * KE;
-        double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs64[le][j];
-        a.Y64[(size_t)e * KE + i] = acc;
-      }
-      __syncthreads();
-    }
+    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, tr, xs64);
   };
+  // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
-    if (sizeof(TR) == 8) {
-      elem_pass64(x);
-      return;
-    }
-    const int le = tid / KE, i = tid % KE;
-    for (int e0 = bid * EPB; e0 < a.n_elements; e0 += nb * EPB) {
-      const int e = e0 + le;
-      if (le < EPB && e < a.n_elements)
-        xs[le][i] = (TR)__ldcg(x + (size_t)a.conn[(size_t)e * NNOD + i / NEQ] * NEQ + i % NEQ);
-      __syncthreads();
-      if (le < EPB && e < a.n_elements) {
-        const TR* Re = (const TR*)a.R32 + (size_t)e * KE * KE;
-        TR acc = 0;
-#pragma unroll 8
-        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[le][j];
-        a.Y32[(size_t)e * KE + i] = (float)acc;
-      }
-      __syncthreads();
-    }
+    if (sizeof(TR) == 8) elem_pass64(x);
+    else elem_pass<KE, NEQ, NNOD, TR>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, tr, xs);
   };
   // node pass: out = gather(Y) (mode 0) or b - gather(Y) (mode 1); partial of out . dotv
   auto node_pass = [&](bool fp32, int mode, double* out, const double* dotv, double* part) {
@@ -166,9 +173,9 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     for (int d = gtid; d < n; d += gstride) {
       const int nd = d / NEQ, k = d % NEQ;
       double s = 0.0;
-      const int p1 = a.csr_ptr[nd + 1];
-      for (int p = a.csr_ptr[nd]; p < p1; p++) {
-        const int v = a.csr_idx[p];
+      const int p1 = __ldg(a.csr_ptr + nd + 1);
+      for (int p = __ldg(a.csr_ptr + nd); p < p1; p++) {
+        const int v = __ldg(a.csr_idx + p);
         const size_t yi = (size_t)(v / NNOD) * KE + (v % NNOD) * NEQ + k;
         s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
       }
@@ -189,10 +196,7 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     // r = b - A64 du, beta = ||r||
     elem_pass64(a.du);
     if (!grid_sync(bar, nb)) return;
-    {
-      const bool f32 = false;
-      node_pass(f32, 1, W, nullptr, pa);
-    }
+    node_pass(false, 1, W, nullptr, pa);
     mv++;
     if (!grid_sync(bar, nb)) return;
     beta = sqrt(sum_partials(pa, nb));
@@ -206,7 +210,7 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     }
     for (int d = gtid; d < n; d += gstride) {
       V[d] = __ldcg(W + d) / beta;
-      if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, beta);
+      if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, beta, tr);
     }
     if (bid == 0 && tid == 0) {
       for (int i = 0; i <= m; i++) a.g[i] = 0.0;
@@ -215,7 +219,7 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     if (!grid_sync(bar, nb)) return;
     int k = 0;
     for (int j = 0; j < m; j++) {
-      const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A Dinv v_j
+      const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A P v_j
       elem_pass_op(xj);
       if (!grid_sync(bar, nb)) return;
       node_pass(sizeof(TR) == 4, 0, W, V, pa);
@@ -223,11 +227,14 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
       if (!grid_sync(bar, nb)) return;
       double* Hj = H + (size_t)j * (m + 1);
       for (int i = 0; i <= j; i++) {
+        // MGS step i: h = <w, v_i> (reduced from the partials of the previous pass),
+        // w -= h v_i, and the partial of the next dot <w, v_{i+1}> (or ||w||^2)
         const double h = sum_partials(pa, nb);
         if (bid == 0 && tid == 0) Hj[i] = h;
         const double* vi = V + (size_t)i * n;
         const double* nx = (i < j) ? V + (size_t)(i + 1) * n : nullptr;
         double acc = 0.0;
+#pragma unroll 4
         for (int d = gtid; d < n; d += gstride) {
           const double wn = __ldcg(W + d) - h * __ldcg(vi + d);
           W[d] = wn;
@@ -242,7 +249,7 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
       double* vn = V + (size_t)(j + 1) * n;
       for (int d = gtid; d < n; d += gstride) {
         vn[d] = __ldcg(W + d) / nrm;
-        if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, nrm);
+        if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, nrm, tr);
       }
       if (bid == 0 && tid == 0) {
         // Givens QR of column j (rotations of earlier columns are stored in cs/sn)
@@ -268,7 +275,7 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
       if (!grid_sync(bar, nb)) return;
       if (*(volatile int*)a.stop) break;
     }
-    // y from the upper-triangular system, du += V y
+    // y from the upper-triangular system, du += P V y
     if (bid == 0 && tid == 0) {
       for (int i = k - 1; i >= 0; i--) {
         double s = a.g[i];
@@ -279,14 +286,14 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
     }
     if (!grid_sync(bar, nb)) return;
     for (int d = gtid; d < n; d += gstride) {
-      if (a.Dinv) {  // du += Dinv (V y)
+      if (a.Dinv) {  // du += P (V y), P = Dinv or Dinv^T
         const int nd = d / NEQ, r = d % NEQ;
         double acc = 0.0;
 #pragma unroll
         for (int s2 = 0; s2 < NEQ; s2++) {
           double t = 0.0;
           for (int i = 0; i < k; i++) t += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + (size_t)nd * NEQ + s2);
-          acc += a.Dinv[(size_t)nd * NEQ * NEQ + r * NEQ + s2] * t;
+          acc += a.Dinv[(size_t)nd * NEQ * NEQ + (tr ? s2 * NEQ + r : r * NEQ + s2)] * t;
         }
         a.du[d] += acc;
       } else {
@@ -316,21 +323,20 @@ __global__ void gmres_persistent_kernel(PersistentArgs a) {
 
 template <int KE, int NEQ, int NNOD, typename TR>
 static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
-  constexpr int THREADS = (256 / KE) * KE;
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_persistent_kernel<KE, NEQ, NNOD, TR>,
-                                                                THREADS, 0);
+                                                                kThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidConfiguration;
-  // few blocks keep the grid barrier short; large systems take two per SM for bandwidth
-  int blocks = sms * (a.n_dof > (1 << 20) ? 2 : 1);
-  if (blocks > sms * per_sm) blocks = sms * per_sm;
+  // every co-resident block: on the 2D plate (81k unknowns, L2-resident) and the 3D ramp
+  // (1.4M unknowns) alike, fewer blocks made each barrier cheaper but every pass slower
+  int blocks = sms * (per_sm < kBlocksPerSm ? per_sm : kBlocksPerSm);
   if (blocks > a.max_blocks) blocks = a.max_blocks;
   PersistentArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR>, dim3(blocks), dim3(THREADS),
+  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR>, dim3(blocks), dim3(kThreads),
                                      params, 0, st);
 }
 

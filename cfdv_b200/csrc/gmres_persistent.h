@@ -6,6 +6,7 @@ namespace cfdv {
 
 struct PersistentArgs {
   int n_dof, n_elements, m, max_restarts, max_blocks;
+  int transpose;               // 1: solve A^T x = b (products with R_e^T, preconditioner transposed)
   double atol;                 // stop when ||b - A du|| < atol (true residual, FP64 matrices)
   const int* conn;
   const int* csr_ptr;

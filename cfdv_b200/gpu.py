@@ -28,7 +28,8 @@ EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error",
            "cfdv_set_state", "cfdv_load_node_records", "cfdv_get_state", "cfdv_state_device_ptr", "cfdv_cfl",
            "cfdv_form", "cfdv_set_element_matrices", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
-           "cfdv_profile_read", "cfdv_ebe_matvec_static"]
+           "cfdv_profile_read", "cfdv_vjp", "cfdv_jvp", "cfdv_element_functional", "cfdv_wall_force",
+           "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static"]
 
 
 class CfdvError(RuntimeError):
@@ -62,6 +63,18 @@ class _Stats(C.Structure):
     _fields_ = [("launches", C.c_long), ("total_ms", C.c_double), ("bytes", C.c_double),
                 ("form_launches", C.c_long), ("form_ms", C.c_double), ("kernel_launches", C.c_long),
                 ("solves", C.c_long), ("solve_ms", C.c_double)]
+
+
+class _AdjOpts(C.Structure):
+    _fields_ = [("n_steps", C.c_int), ("checkpoint_every", C.c_int), ("cfl", C.c_double), ("m", C.c_int),
+                ("restarts", C.c_int), ("rtol", C.c_double), ("precision", C.c_int), ("wall_bc", C.c_int)]
+
+
+class _AdjResult(C.Structure):
+    _fields_ = [("J", C.c_double), ("dJ_dmach", C.c_double), ("dJ_dtwall", C.c_double), ("n_wall_nodes", C.c_int),
+                ("wall_capacity", C.c_int), ("wall_nodes", C.c_void_p), ("dJ_dtnode", C.c_void_p),
+                ("forward_ms", C.c_double), ("backward_ms", C.c_double), ("forward_matvecs", C.c_int),
+                ("adjoint_matvecs", C.c_int)]
 
 
 _lib = None
@@ -100,6 +113,13 @@ def lib():
         L.cfdv_matvec.argtypes = [P, P, P, I, I]
         L.cfdv_profile.argtypes = [P, I]
         L.cfdv_profile_read.argtypes = [P, P]
+        L.cfdv_vjp.argtypes = [P, P, P, P, P, P]
+        L.cfdv_jvp.argtypes = [P, P, P, D, D, P]
+        L.cfdv_element_functional.argtypes = [P, P, P, P]
+        L.cfdv_wall_force.argtypes = [P, I, P, P, P]
+        L.cfdv_wall_nodes.argtypes = [P, I, P, I, P]
+        L.cfdv_adjoint.argtypes = [P, P, P]
+        L.cfdv_tangent.argtypes = [P, P, D, P, P, P]
         L.cfdv_ebe_matvec_static.argtypes = [I, I, I, P, P, P, P, P, P, I, P]
         _lib = L
     return _lib
@@ -282,3 +302,70 @@ class FDVSolver:
         return {"launches": s.launches, "total_ms": s.total_ms, "bytes": s.bytes,
                 "form_launches": s.form_launches, "form_ms": s.form_ms,
                 "kernel_launches": s.kernel_launches, "solves": s.solves, "solve_ms": s.solve_ms}
+
+    # -- discrete adjoint and tangent --
+    def vjp(self, mu, du):
+        """(dr/dU)^T mu assembled, mu^T dr/ddt, mu^T dr/dMach at the current U and formed dt."""
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        g = np.zeros(self.n_dof)
+        gd, gm = C.c_double(), C.c_double()
+        self._ck(self.L.cfdv_vjp(self._ctx, _p(mu), _p(du), _p(g), C.byref(gd), C.byref(gm)))
+        return g, gd.value, gm.value
+
+    def jvp(self, du, tU, t_dt=0.0, t_mach=0.0):
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        tU = np.ascontiguousarray(tU, dtype=np.float64)
+        dr = np.zeros(self.n_dof)
+        self._ck(self.L.cfdv_jvp(self._ctx, _p(du), _p(tU), float(t_dt), float(t_mach), _p(dr)))
+        return dr
+
+    def element_functional(self, mu, du):
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        L = np.zeros(self.n_elements)
+        self._ck(self.L.cfdv_element_functional(self._ctx, _p(mu), _p(du), _p(L)))
+        return L
+
+    def wall_force(self, wall_bc=1, grad=False):
+        F = C.c_double()
+        dm = C.c_double()
+        g = np.zeros(self.n_dof) if grad else None
+        self._ck(self.L.cfdv_wall_force(self._ctx, int(wall_bc), C.byref(F), _p(g) if grad else None,
+                                        C.byref(dm)))
+        return (F.value, g, dm.value) if grad else F.value
+
+    def wall_nodes(self, wall_bc=1):
+        n = C.c_int()
+        self._ck(self.L.cfdv_wall_nodes(self._ctx, int(wall_bc), None, 0, C.byref(n)))
+        ids = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._ck(self.L.cfdv_wall_nodes(self._ctx, int(wall_bc), _p(ids), ids.size, C.byref(n)))
+        return ids[: n.value].copy()
+
+    @staticmethod
+    def _adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc):
+        return _AdjOpts(int(n_steps), int(checkpoint_every), float(cfl), int(m), int(restarts), float(rtol),
+                        int(precision), int(wall_bc))
+
+    def adjoint(self, n_steps, cfl, checkpoint_every=50, m=30, restarts=200, rtol=1e-10, precision=PREC_FP64,
+                wall_bc=1):
+        """Gradient of J = mean_{n=1..N} F_x(U_n) w.r.t. Mach, wall temperature and each wall-node T0."""
+        o = self._adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc)
+        nw = len(self.wall_nodes(wall_bc))
+        ids = np.zeros(max(nw, 1), dtype=np.int32)
+        gT = np.zeros(max(nw, 1))
+        r = _AdjResult(0, 0, 0, 0, nw, _p(ids).value, _p(gT).value, 0, 0, 0, 0)
+        self._ck(self.L.cfdv_adjoint(self._ctx, C.byref(o), C.byref(r)))
+        return {"J": r.J, "dJ_dmach": r.dJ_dmach, "dJ_dtwall": r.dJ_dtwall, "wall_nodes": ids[:nw].copy(),
+                "dJ_dtnode": gT[:nw].copy(), "forward_ms": r.forward_ms, "backward_ms": r.backward_ms,
+                "forward_matvecs": r.forward_matvecs, "adjoint_matvecs": r.adjoint_matvecs}
+
+    def tangent(self, n_steps, cfl, dmach=0.0, dT_wall=None, m=30, restarts=200, rtol=1e-10, precision=PREC_FP64,
+                wall_bc=1):
+        """FP64 tangent-linear run: (J, dJ) along (dmach, dT_wall per wall node)."""
+        o = self._adj_opts(n_steps, 1, cfl, m, restarts, rtol, precision, wall_bc)
+        J, dJ = C.c_double(), C.c_double()
+        dT = None if dT_wall is None else np.ascontiguousarray(dT_wall, dtype=np.float64)
+        self._ck(self.L.cfdv_tangent(self._ctx, C.byref(o), float(dmach), _p(dT) if dT is not None else None,
+                                     C.byref(J), C.byref(dJ)))
+        return J.value, dJ.value

@@ -170,6 +170,67 @@ typedef struct {
 int cfdv_profile(cfdv_ctx* ctx, int enable);
 int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
 
+/* ---- discrete adjoint and tangent of the step ------------------------------------- */
+/* The reference has no adjoint; these entry points differentiate the CORRECT-mode step
+ * (dt = CFL(U), A(U,dt) dU = b(U,dt), U += dU) exactly, through the same physics as
+ * cfdv_form, by forward-mode dual numbers per element.  The element residual is
+ * r_e = rhs_e - R_e dU_e with dU fixed; Dirichlet rows (ApplyBC) are constant.
+ *
+ * Objective: the wall x-force F_x = sum over element faces with boundary code wall_bc of
+ * the face integral of p n_x - (1/Re) tau_xj n_j (2-point Gauss per face direction; n the
+ * outward normal of the fluid element, p and T interpolated from the nodes, tau from the
+ * element's velocity gradient at the face point), and J = (1/N) sum_{n=1..N} F_x(U_n) over
+ * an N-step run from the loaded node records.  Parameters: the Mach number (gas constants
+ * Cv, cgas, cmach and the initial rho E through Cv) and the initial temperature of each
+ * wall node (the nodes of the wall_bc faces; an isothermal wall keeps it through the
+ * Dirichlet energy row). */
+typedef struct {
+  int n_steps;          /* N steps from the records of cfdv_load_node_records */
+  int checkpoint_every; /* k: the forward run keeps U every k steps; the backward sweep
+                           recomputes each segment's states from its checkpoint and
+                           re-forms the element matrices instead of storing them */
+  double cfl;
+  int m, restarts;      /* GMRES(m), at most `restarts` cycles, CORRECT mode, node-block */
+  double rtol;          /* Jacobi; forward, tangent and adjoint solves to this rtol */
+  int precision;        /* cfdv_precision of every solve (MIXED: FP32 inner products) */
+  int wall_bc;          /* boundary code of the wall faces */
+} cfdv_adjoint_opts;
+
+typedef struct {
+  double J;             /* (1/N) sum_{n=1..N} F_x(U_n) */
+  double dJ_dmach;
+  double dJ_dtwall;     /* all wall-node temperatures moved together */
+  int n_wall_nodes;     /* written: number of wall nodes */
+  int wall_capacity;    /* size of the two caller buffers below (may be 0) */
+  int* wall_nodes;      /* node ids of the wall nodes, ascending */
+  double* dJ_dtnode;    /* dJ / d T0 of each wall node */
+  double forward_ms;    /* device time of the forward run */
+  double backward_ms;   /* device time of the backward sweep, recomputation included */
+  int forward_matvecs;  /* EBE products of all forward solves (recomputation included) */
+  int adjoint_matvecs;  /* EBE products of the transposed solves */
+} cfdv_adjoint_result;
+
+/* Vector-Jacobian product of the element residuals at the current U and the dt of the
+ * last cfdv_form: gU = sum_e P_e^T (d r_e / d U_e)^T mu_e (host vectors [n_nodes*neqn]),
+ * g_dt = mu^T dr/ddt, g_mach = mu^T dr/dMach, for the step solution du. */
+int cfdv_vjp(cfdv_ctx* ctx, const double* mu, const double* du, double* gU, double* g_dt, double* g_mach);
+/* Jacobian-vector product: dr = (dr/dU) tU + (dr/ddt) t_dt + (dr/dMach) t_mach, assembled. */
+int cfdv_jvp(cfdv_ctx* ctx, const double* du, const double* tU, double t_dt, double t_mach, double* dr);
+/* L_e = sum over unmasked rows of mu_e (rhs_e - R_e du_e) per element [n_elements] (checks). */
+int cfdv_element_functional(cfdv_ctx* ctx, const double* mu, const double* du, double* L);
+/* F_x at the current U; dF_dU [n_nodes*neqn] and dF_dmach may be NULL. */
+int cfdv_wall_force(cfdv_ctx* ctx, int wall_bc, double* F, double* dF_dU, double* dF_dmach);
+/* The wall nodes of wall_bc (ascending ids, up to capacity) and their number. */
+int cfdv_wall_nodes(cfdv_ctx* ctx, int wall_bc, int* ids, int capacity, int* n);
+/* Forward run with checkpoints, then the reverse sweep: lambda_N = (1/N) dF/dU(U_N),
+ * mu_n = A_n^-T lambda_{n+1}, lambda_n = lambda_{n+1} + (dr_n/dU)^T mu_n
+ * + (mu_n^T dr_n/ddt) d dt_n/dU + [n >= 1] (1/N) dF/dU(U_n); gradients from lambda_0.
+ * The context's state is U_N afterwards. */
+int cfdv_adjoint(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, cfdv_adjoint_result* res);
+/* FP64 tangent-linear run along (dmach, dT_wall[n_wall_nodes], NULL = 0): J and dJ. */
+int cfdv_tangent(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, double dmach, const double* dT_wall, double* J,
+                 double* dJ);
+
 /* ---- EBE product without device allocation ------------------------------------ */
 /* No counterpart in the reference; it exists for callers of this library that may not
  * allocate device memory.  Examples: a solver plug-in that runs inside an application

@@ -1,0 +1,57 @@
+// Test-only CPU build of the adjoint element functionals (cfdv_b200/csrc/adjoint.cuh).
+//
+// Evaluates, on the host, exactly the per-thread functions the adjoint kernels run on the
+// device: the weighted element residual L_e with its dual-number derivative along one seed
+// direction, and the wall x-force of an element.  Used only by tests/test_adjoint_emulated.py
+// to check the functionals against the oracle's formation and against finite differences.
+#include <cstring>
+
+#include "../../cfdv_b200/csrc/adjoint.cuh"
+
+using namespace cfdv;
+
+// mode 0: out[e*(Ke+2)+k] = d L_e / d(direction k) (k < Ke unknowns, Ke: dt, Ke+1: Mach),
+//         val[e] = L_e;   mode 1: out[e*Ke + row] = d r_e(row) along (tU, t_dt, t_mach)
+extern "C" void emu_functional(int ndim, int n_elements, const double* U, const double* x, const int* conn,
+                               const int* bc, const uint64_t* rowmask, double gamma, double M, double Re, double Pr,
+                               double Tinf, double Tw, int adiabatic, double dt, int physical_3d_flux, int mode,
+                               const double* dU, const double* w, const double* tU, double t_dt, double t_mach,
+                               double* out, double* val) {
+  FunctionalArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.gas = make_gas(gamma, M, Re, Pr, Tinf, Tw, adiabatic);
+  a.dt = dt;
+  gauss_legendre(2, a.gz, a.gw);
+  a.n_elements = n_elements;
+  a.physical_3d_flux = physical_3d_flux;
+  a.mode = mode;
+  a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
+  a.dU = dU; a.w = w; a.tU = tU; a.t_dt = t_dt; a.t_mach = t_mach;
+  const int Ke = (ndim == 2) ? 16 : 40;
+  const int nd = mode == 0 ? Ke + 2 : Ke;
+  for (int e = 0; e < n_elements; e++)
+    for (int k = 0; k < nd; k++) {
+      const Dual L = (ndim == 2) ? element_functional<2>(a, e, k) : element_functional<3>(a, e, k);
+      out[(size_t)e * nd + k] = L.d;
+      if (k == 0 && val) val[e] = L.v;
+    }
+}
+
+// F_x of each element's wall faces and its gradient: out[e*(Ke+1) + k], k == Ke: Mach
+extern "C" void emu_wall_force(int ndim, int n_elements, const double* U, const double* x, const int* conn,
+                               const int* bc, double gamma, double M, double Re, double Pr, double Tinf, double Tw,
+                               int adiabatic, int wall_bc, double* out, double* val) {
+  ForceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.gas = make_gas(gamma, M, Re, Pr, Tinf, Tw, adiabatic);
+  gauss_legendre(2, a.gz, a.gw);
+  a.wall_bc = wall_bc;
+  a.U = U; a.x = x; a.conn = conn; a.bc = bc;
+  const int Ke = (ndim == 2) ? 16 : 40;
+  for (int e = 0; e < n_elements; e++)
+    for (int k = 0; k <= Ke; k++) {
+      const Dual F = (ndim == 2) ? wall_force_element<2>(a, e, k) : wall_force_element<3>(a, e, k);
+      out[(size_t)e * (Ke + 1) + k] = F.d;
+      if (k == 0) val[e] = F.v;
+    }
+}
