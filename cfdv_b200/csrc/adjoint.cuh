@@ -156,7 +156,7 @@ CFDV_HD CFDV_INLINE Dual pass_terms(const GasT<Dual>& g, const GpStateT<Dual>& f
     jac_b_rows<NDIM>(g, f, i, J);
     for (int r = 0; r < NEQ; r++)
       for (int c = 0; c < NEQ; c++) {
-        const Dual& bv = J[i * 25 + r * 5 + c];
+        const Dual& bv = J[r * 5 + c];
         abar[c] += wi[i][r] * bv;
         vb1[r] += bv * u1[i][c];
         Sb += wi[i][r] * (bv * u0[c]);
@@ -165,13 +165,13 @@ CFDV_HD CFDV_INLINE Dual pass_terms(const GasT<Dual>& g, const GpStateT<Dual>& f
   }
   // c: the bilinear form, one direction i at a time
   {
-    Dual C[NDIM * 75];
+    Dual C[75];
     for (int i = 0; i < NDIM; i++) {
       jac_c_rows<NDIM>(g, f, i, C);
       for (int j = 0; j < NDIM; j++)
         for (int r = 0; r < NEQ; r++) {
           Dual t = 0.0;
-          for (int c = 0; c < NEQ; c++) t += C[(i * 3 + j) * 25 + r * 5 + c] * u1[j][c];
+          for (int c = 0; c < NEQ; c++) t += C[j * 25 + r * 5 + c] * u1[j][c];
           Gam += wi[i][r] * t;
         }
     }

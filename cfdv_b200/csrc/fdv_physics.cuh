@@ -227,9 +227,9 @@ CFDV_HD CFDV_INLINE void viscous_stress(GpStateT<S>& f) {
 }
 
 // ---- flux Jacobians ---------------------------------------------------------
-// jac_a<NDIM>: a(i, ., .) for all i; jac_b_rows<NDIM>: b(i, ., .) for one i (entries
-// i*25 .. i*25+24); jac_c_rows<NDIM>: c(i, j, ., .) for one i (entries i*75 .. i*75+74 of
-// the 3x3 block layout).  Each has a 2D and a 3D form below, templated on the scalar.
+// jac_a<NDIM>: a(i, ., .) for all i at m[i*25 + r*5 + s]; jac_b_rows<NDIM>: b(i, ., .) for
+// one i at m[r*5 + s]; jac_c_rows<NDIM>: c(i, j, ., .) for one i at m[j*25 + r*5 + s].  Each
+// has a 2D and a 3D form below, templated on the scalar.
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_a_2d(const GasT<S>& th, const GpStateT<S>& f, S* m) {
@@ -263,7 +263,7 @@ CFDV_HD CFDV_INLINE void jac_a_2d(const GasT<S>& th, const GpStateT<S>& f, S* m)
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_b_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
-  S* blk = m + i * 25;
+  S* blk = m;
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const S reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -279,37 +279,37 @@ CFDV_HD CFDV_INLINE void jac_b_rows_2d(const GasT<S>& th, const GpStateT<S>& f, 
   const S b120 = (DENOM * (lambda * (dldx + 4. * v * drdy) + mu_R * (u * drdx + dmdy))) * reinv;
   const S b121 = lambda * drdx * DENOM * reinv, b122 = mu_R * drdy * DENOM * reinv;
   if (i == 0) {
-    JA(m, 0, 1, 0) = b010;
-    JA(m, 0, 1, 1) = b011;
-    JA(m, 0, 1, 2) = b012;
-    JA(m, 0, 2, 0) = b020;
-    JA(m, 0, 2, 1) = b021;
-    JA(m, 0, 2, 2) = b022;
-    JA(m, 0, 3, 0) = u * b010 + v * b020 +
+    JA(blk, 0, 1, 0) = b010;
+    JA(blk, 0, 1, 1) = b011;
+    JA(blk, 0, 1, 2) = b012;
+    JA(blk, 0, 2, 0) = b020;
+    JA(blk, 0, 2, 1) = b021;
+    JA(blk, 0, 2, 2) = b022;
+    JA(blk, 0, 3, 0) = u * b010 + v * b020 +
         ((u * t00 + v * t10) / rho -
         TERM1 * (-dedx + (2. * E - 3. * uu - 3. * vv) * drdx + 2. * u * dldx + 2. * v * dmdx)) * reinv;
-    JA(m, 0, 3, 1) = u * b011 + v * b021 + (-t00 / rho - TERM1 * (2. * u * drdx - dldx)) * reinv;
-    JA(m, 0, 3, 2) = u * b012 + v * b022 + (-t10 / rho - TERM1 * (-dmdx + 2. * v * drdx)) * reinv;
-    JA(m, 0, 3, 3) = TERM1 * drdx * reinv;
+    JA(blk, 0, 3, 1) = u * b011 + v * b021 + (-t00 / rho - TERM1 * (2. * u * drdx - dldx)) * reinv;
+    JA(blk, 0, 3, 2) = u * b012 + v * b022 + (-t10 / rho - TERM1 * (-dmdx + 2. * v * drdx)) * reinv;
+    JA(blk, 0, 3, 3) = TERM1 * drdx * reinv;
   } else {
-    JA(m, 1, 1, 0) = b020;
-    JA(m, 1, 1, 1) = b021;
-    JA(m, 1, 1, 2) = b022;
-    JA(m, 1, 2, 0) = b120;
-    JA(m, 1, 2, 1) = b121;
-    JA(m, 1, 2, 2) = b122;
-    JA(m, 1, 3, 0) = u * b020 + v * b120 +
+    JA(blk, 0, 1, 0) = b020;
+    JA(blk, 0, 1, 1) = b021;
+    JA(blk, 0, 1, 2) = b022;
+    JA(blk, 0, 2, 0) = b120;
+    JA(blk, 0, 2, 1) = b121;
+    JA(blk, 0, 2, 2) = b122;
+    JA(blk, 0, 3, 0) = u * b020 + v * b120 +
         ((u * t01 + v * t11) / rho -
         TERM1 * (-dedy + (2. * E - 3. * uu - 3. * vv) * drdy + 2. * u * dldy + 2. * v * dmdy)) * reinv;
-    JA(m, 1, 3, 1) = u * b021 + v * b121 + (-t10 / rho - TERM1 * (-dldy + 2. * u * drdy)) * reinv;
-    JA(m, 1, 3, 2) = u * b022 + v * b122 + (-t11 / rho - TERM1 * (2. * v * drdy - dmdy)) * reinv;
-    JA(m, 1, 3, 3) = TERM1 * drdy * reinv;
+    JA(blk, 0, 3, 1) = u * b021 + v * b121 + (-t10 / rho - TERM1 * (-dldy + 2. * u * drdy)) * reinv;
+    JA(blk, 0, 3, 2) = u * b022 + v * b122 + (-t11 / rho - TERM1 * (2. * v * drdy - dmdy)) * reinv;
+    JA(blk, 0, 3, 3) = TERM1 * drdy * reinv;
   }
 }
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_c_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
-  S* blk = m + i * 75;
+  S* blk = m;
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const S reinv = 1.0 / th.creyn, mu = f.mu;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -317,37 +317,37 @@ CFDV_HD CFDV_INLINE void jac_c_rows_2d(const GasT<S>& th, const GpStateT<S>& f, 
   const S l = f.U[1], mv = f.U[2], re = f.U[3];
   const S ll = l * l, lm = l * mv, mm = mv * mv, rv = ll + mm, hkocv = f.k / th.Cv;
   if (i == 0) {
-    JC(m, 0, 0, 1, 0) = mu_R * l * denom * reinv;
-    JC(m, 0, 0, 1, 1) = -mu_R / rho * reinv;
-    JC(m, 0, 0, 2, 0) = mu * mv * denom * reinv;
-    JC(m, 0, 0, 2, 2) = -mu / rho * reinv;
-    JC(m, 0, 0, 3, 0) = ((mu_R * ll * denom2 + mu * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
-    JC(m, 0, 0, 3, 1) = (-mu_R + hkocv) * l * denom * reinv;
-    JC(m, 0, 0, 3, 2) = (-mu + hkocv) * mv * denom * reinv;
-    JC(m, 0, 0, 3, 3) = -hkocv / rho * reinv;
-    JC(m, 0, 1, 1, 0) = lambda * mv * denom * reinv;
-    JC(m, 0, 1, 1, 2) = -lambda / rho * reinv;
-    JC(m, 0, 1, 2, 0) = mu * l * denom * reinv;
-    JC(m, 0, 1, 2, 1) = -mu / rho * reinv;
-    JC(m, 0, 1, 3, 0) = (lambda + mu) * lm * denom2 * reinv;
-    JC(m, 0, 1, 3, 1) = -mu * mv * denom * reinv;
-    JC(m, 0, 1, 3, 2) = -lambda * l * denom * reinv;
+    JC(blk, 0, 0, 1, 0) = mu_R * l * denom * reinv;
+    JC(blk, 0, 0, 1, 1) = -mu_R / rho * reinv;
+    JC(blk, 0, 0, 2, 0) = mu * mv * denom * reinv;
+    JC(blk, 0, 0, 2, 2) = -mu / rho * reinv;
+    JC(blk, 0, 0, 3, 0) = ((mu_R * ll * denom2 + mu * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+    JC(blk, 0, 0, 3, 1) = (-mu_R + hkocv) * l * denom * reinv;
+    JC(blk, 0, 0, 3, 2) = (-mu + hkocv) * mv * denom * reinv;
+    JC(blk, 0, 0, 3, 3) = -hkocv / rho * reinv;
+    JC(blk, 0, 1, 1, 0) = lambda * mv * denom * reinv;
+    JC(blk, 0, 1, 1, 2) = -lambda / rho * reinv;
+    JC(blk, 0, 1, 2, 0) = mu * l * denom * reinv;
+    JC(blk, 0, 1, 2, 1) = -mu / rho * reinv;
+    JC(blk, 0, 1, 3, 0) = (lambda + mu) * lm * denom2 * reinv;
+    JC(blk, 0, 1, 3, 1) = -mu * mv * denom * reinv;
+    JC(blk, 0, 1, 3, 2) = -lambda * l * denom * reinv;
   } else {
-    JC(m, 1, 0, 1, 0) = mu * mv * denom * reinv;
-    JC(m, 1, 0, 1, 2) = -mu / rho * reinv;
-    JC(m, 1, 0, 2, 0) = lambda * l * denom * reinv;
-    JC(m, 1, 0, 2, 1) = -lambda / rho * reinv;
-    JC(m, 1, 0, 3, 0) = (mu + lambda) * lm * denom2 * reinv;
-    JC(m, 1, 0, 3, 1) = -lambda * mv * denom * reinv;
-    JC(m, 1, 0, 3, 2) = -mu * l * denom * reinv;
-    JC(m, 1, 1, 1, 0) = mu * l * denom * reinv;
-    JC(m, 1, 1, 1, 1) = -mu / rho * reinv;
-    JC(m, 1, 1, 2, 0) = mu_R * mv * denom * reinv;
-    JC(m, 1, 1, 2, 2) = -mu_R / rho * reinv;
-    JC(m, 1, 1, 3, 0) = ((mu * ll * denom2 + mu_R * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
-    JC(m, 1, 1, 3, 1) = (-mu + hkocv) * l * denom * reinv;
-    JC(m, 1, 1, 3, 2) = (-mu_R + hkocv) * mv * denom * reinv;
-    JC(m, 1, 1, 3, 3) = -hkocv / rho * reinv;
+    JC(blk, 0, 0, 1, 0) = mu * mv * denom * reinv;
+    JC(blk, 0, 0, 1, 2) = -mu / rho * reinv;
+    JC(blk, 0, 0, 2, 0) = lambda * l * denom * reinv;
+    JC(blk, 0, 0, 2, 1) = -lambda / rho * reinv;
+    JC(blk, 0, 0, 3, 0) = (mu + lambda) * lm * denom2 * reinv;
+    JC(blk, 0, 0, 3, 1) = -lambda * mv * denom * reinv;
+    JC(blk, 0, 0, 3, 2) = -mu * l * denom * reinv;
+    JC(blk, 0, 1, 1, 0) = mu * l * denom * reinv;
+    JC(blk, 0, 1, 1, 1) = -mu / rho * reinv;
+    JC(blk, 0, 1, 2, 0) = mu_R * mv * denom * reinv;
+    JC(blk, 0, 1, 2, 2) = -mu_R / rho * reinv;
+    JC(blk, 0, 1, 3, 0) = ((mu * ll * denom2 + mu_R * mm * denom2) - hkocv * (-re * denom + rv * denom2)) * reinv;
+    JC(blk, 0, 1, 3, 1) = (-mu + hkocv) * l * denom * reinv;
+    JC(blk, 0, 1, 3, 2) = (-mu_R + hkocv) * mv * denom * reinv;
+    JC(blk, 0, 1, 3, 3) = -hkocv / rho * reinv;
   }
 }
 
@@ -388,7 +388,7 @@ CFDV_HD CFDV_INLINE void jac_a_3d(const GasT<S>& th, const GpStateT<S>& f, S* m)
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
-  S* blk = m + i * 25;
+  S* blk = m;
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const S mu = f.mu, E = f.E;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -413,59 +413,59 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
   const S b230 = (denom * (mu_R * (dndz + u * drdx + v * drdy - 2. * w * drdz) + lambda * (dldx + dmdy)));
   const S b231 = lambda * drdx * denom, b232 = lambda * drdy * denom, b233 = mu_R * drdz * denom;
   if (i == 0) {
-    JA(m, 0, 1, 0) = b010;
-    JA(m, 0, 1, 1) = b011;
-    JA(m, 0, 1, 2) = b012;
-    JA(m, 0, 1, 3) = b013;
-    JA(m, 0, 2, 0) = b020;
-    JA(m, 0, 2, 1) = b021;
-    JA(m, 0, 2, 2) = b022;
-    JA(m, 0, 3, 0) = b030;
-    JA(m, 0, 3, 1) = b031;
-    JA(m, 0, 3, 3) = b033;
-    JA(m, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
+    JA(blk, 0, 1, 0) = b010;
+    JA(blk, 0, 1, 1) = b011;
+    JA(blk, 0, 1, 2) = b012;
+    JA(blk, 0, 1, 3) = b013;
+    JA(blk, 0, 2, 0) = b020;
+    JA(blk, 0, 2, 1) = b021;
+    JA(blk, 0, 2, 2) = b022;
+    JA(blk, 0, 3, 0) = b030;
+    JA(blk, 0, 3, 1) = b031;
+    JA(blk, 0, 3, 3) = b033;
+    JA(blk, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
         (denom * (l * t[0][0] + mv * t[0][1] + n * t[0][2]) -
         TERM1 * (-dedx + (2. * E - 3. * q2) * drdx + 2. * (u * dldx + v * dmdx + w * dndx)));
-    JA(m, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
-    JA(m, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
-    JA(m, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
-    JA(m, 0, 4, 4) = TERM1 * drdx;
+    JA(blk, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
+    JA(blk, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
+    JA(blk, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
+    JA(blk, 0, 4, 4) = TERM1 * drdx;
   } else if (i == 1) {
-    JA(m, 1, 1, 0) = b020;
-    JA(m, 1, 1, 1) = b021;
-    JA(m, 1, 1, 2) = b022;
-    JA(m, 1, 2, 0) = b120;
-    JA(m, 1, 2, 1) = b121;
-    JA(m, 1, 2, 2) = b122;
-    JA(m, 1, 2, 3) = b123;
-    JA(m, 1, 3, 0) = b130;
-    JA(m, 1, 3, 2) = b132;
-    JA(m, 1, 3, 3) = b133;
-    JA(m, 1, 4, 0) = u * b020 + v * b120 + w * b130 +
+    JA(blk, 0, 1, 0) = b020;
+    JA(blk, 0, 1, 1) = b021;
+    JA(blk, 0, 1, 2) = b022;
+    JA(blk, 0, 2, 0) = b120;
+    JA(blk, 0, 2, 1) = b121;
+    JA(blk, 0, 2, 2) = b122;
+    JA(blk, 0, 2, 3) = b123;
+    JA(blk, 0, 3, 0) = b130;
+    JA(blk, 0, 3, 2) = b132;
+    JA(blk, 0, 3, 3) = b133;
+    JA(blk, 0, 4, 0) = u * b020 + v * b120 + w * b130 +
         (denom * (l * t[1][0] + mv * t[1][1] + n * t[1][2]) -
         TERM1 * (-dedy + (2. * E - 3. * q2) * drdy + 2. * (u * dldy + v * dmdy + w * dndy)));
-    JA(m, 1, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
-    JA(m, 1, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
-    JA(m, 1, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
-    JA(m, 1, 4, 4) = TERM1 * drdy;
+    JA(blk, 0, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
+    JA(blk, 0, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
+    JA(blk, 0, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
+    JA(blk, 0, 4, 4) = TERM1 * drdy;
   } else {
-    JA(m, 2, 1, 0) = b030;
-    JA(m, 2, 1, 1) = b031;
-    JA(m, 2, 1, 3) = b033;
-    JA(m, 2, 2, 0) = b130;
-    JA(m, 2, 2, 2) = b132;
-    JA(m, 2, 2, 3) = b133;
-    JA(m, 2, 3, 0) = b230;
-    JA(m, 2, 3, 1) = b231;
-    JA(m, 2, 3, 2) = b232;
-    JA(m, 2, 3, 3) = b233;
-    JA(m, 2, 4, 0) = u * b030 + v * b130 + w * b230 +
+    JA(blk, 0, 1, 0) = b030;
+    JA(blk, 0, 1, 1) = b031;
+    JA(blk, 0, 1, 3) = b033;
+    JA(blk, 0, 2, 0) = b130;
+    JA(blk, 0, 2, 2) = b132;
+    JA(blk, 0, 2, 3) = b133;
+    JA(blk, 0, 3, 0) = b230;
+    JA(blk, 0, 3, 1) = b231;
+    JA(blk, 0, 3, 2) = b232;
+    JA(blk, 0, 3, 3) = b233;
+    JA(blk, 0, 4, 0) = u * b030 + v * b130 + w * b230 +
         (denom * (l * t[2][0] + mv * t[2][1] + n * t[2][2]) -
         TERM1 * (-dedz + (2. * E - 3. * q2) * drdz + 2. * (u * dldz + v * dmdz + w * dndz)));
-    JA(m, 2, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
-    JA(m, 2, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
-    JA(m, 2, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
-    JA(m, 2, 4, 4) = TERM1 * drdz;
+    JA(blk, 0, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
+    JA(blk, 0, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
+    JA(blk, 0, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
+    JA(blk, 0, 4, 4) = TERM1 * drdz;
   }
   const S reinv = 1.0 / th.creyn;
   for (int k = 0; k < 25; k++) blk[k] *= reinv;
@@ -473,7 +473,7 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
-  S* blk = m + i * 75;
+  S* blk = m;
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const S mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const S rho = f.U[0], denom = 1. / (rho * rho);
@@ -482,85 +482,85 @@ CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
   const S q = (-re + (ll + mm + nn) / rho);
   if (i == 0) {
     const S d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
-    JC(m, 0, 0, 1, 0) = mu_R * l * denom;
-    JC(m, 0, 0, 1, 1) = (-mu_R / rho);
-    JC(m, 0, 0, 2, 0) = mu * mv * denom;
-    JC(m, 0, 0, 2, 2) = (-mu / rho);
-    JC(m, 0, 0, 3, 0) = mu * n * denom;
-    JC(m, 0, 0, 3, 3) = (-mu / rho);
-    JC(m, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
-    JC(m, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
-    JC(m, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-    JC(m, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-    JC(m, 0, 0, 4, 4) = (-hkocv / rho);
-    JC(m, 0, 1, 1, 0) = lambda * mv * denom;
-    JC(m, 0, 1, 1, 2) = (-lambda / rho);
-    JC(m, 0, 1, 2, 0) = mu * l * denom;
-    JC(m, 0, 1, 2, 1) = (-mu / rho);
-    JC(m, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
-    JC(m, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
-    JC(m, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
-    JC(m, 0, 2, 1, 0) = lambda * n * denom;
-    JC(m, 0, 2, 1, 3) = (-lambda / rho);
-    JC(m, 0, 2, 3, 0) = mu * l * denom;
-    JC(m, 0, 2, 3, 1) = (-mu / rho);
-    JC(m, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
-    JC(m, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
-    JC(m, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
+    JC(blk, 0, 0, 1, 0) = mu_R * l * denom;
+    JC(blk, 0, 0, 1, 1) = (-mu_R / rho);
+    JC(blk, 0, 0, 2, 0) = mu * mv * denom;
+    JC(blk, 0, 0, 2, 2) = (-mu / rho);
+    JC(blk, 0, 0, 3, 0) = mu * n * denom;
+    JC(blk, 0, 0, 3, 3) = (-mu / rho);
+    JC(blk, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
+    JC(blk, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
+    JC(blk, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+    JC(blk, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+    JC(blk, 0, 0, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 1, 1, 0) = lambda * mv * denom;
+    JC(blk, 0, 1, 1, 2) = (-lambda / rho);
+    JC(blk, 0, 1, 2, 0) = mu * l * denom;
+    JC(blk, 0, 1, 2, 1) = (-mu / rho);
+    JC(blk, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
+    JC(blk, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
+    JC(blk, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
+    JC(blk, 0, 2, 1, 0) = lambda * n * denom;
+    JC(blk, 0, 2, 1, 3) = (-lambda / rho);
+    JC(blk, 0, 2, 3, 0) = mu * l * denom;
+    JC(blk, 0, 2, 3, 1) = (-mu / rho);
+    JC(blk, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
+    JC(blk, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
+    JC(blk, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
   } else if (i == 1) {
     const S e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
-    JC(m, 1, 1, 1, 0) = e10;
-    JC(m, 1, 1, 1, 1) = (-mu / rho);
-    JC(m, 1, 1, 2, 0) = e20;
-    JC(m, 1, 1, 2, 2) = (-mu_R / rho);
-    JC(m, 1, 1, 3, 0) = e30;
-    JC(m, 1, 1, 3, 3) = (-mu / rho);
-    JC(m, 1, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
-    JC(m, 1, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-    JC(m, 1, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
-    JC(m, 1, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-    JC(m, 1, 1, 4, 4) = (-hkocv / rho);
-    JC(m, 1, 0, 1, 0) = mu * mv * denom;
-    JC(m, 1, 0, 1, 2) = (-mu / rho);
-    JC(m, 1, 0, 2, 0) = lambda * l * denom;
-    JC(m, 1, 0, 2, 1) = (-lambda / rho);
-    JC(m, 1, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
-    JC(m, 1, 0, 4, 1) = (mv / rho) * (-lambda / rho);
-    JC(m, 1, 0, 4, 2) = (l / rho) * (-mu / rho);
-    JC(m, 1, 2, 2, 0) = lambda * n * denom;
-    JC(m, 1, 2, 2, 3) = (-lambda / rho);
-    JC(m, 1, 2, 3, 0) = mu * mv * denom;
-    JC(m, 1, 2, 3, 2) = (-mu / rho);
-    JC(m, 1, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
-    JC(m, 1, 2, 4, 2) = (n / rho) * (-mu / rho);
-    JC(m, 1, 2, 4, 3) = (mv / rho) * (-lambda / rho);
+    JC(blk, 0, 1, 1, 0) = e10;
+    JC(blk, 0, 1, 1, 1) = (-mu / rho);
+    JC(blk, 0, 1, 2, 0) = e20;
+    JC(blk, 0, 1, 2, 2) = (-mu_R / rho);
+    JC(blk, 0, 1, 3, 0) = e30;
+    JC(blk, 0, 1, 3, 3) = (-mu / rho);
+    JC(blk, 0, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
+    JC(blk, 0, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+    JC(blk, 0, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
+    JC(blk, 0, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
+    JC(blk, 0, 1, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 0, 1, 0) = mu * mv * denom;
+    JC(blk, 0, 0, 1, 2) = (-mu / rho);
+    JC(blk, 0, 0, 2, 0) = lambda * l * denom;
+    JC(blk, 0, 0, 2, 1) = (-lambda / rho);
+    JC(blk, 0, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
+    JC(blk, 0, 0, 4, 1) = (mv / rho) * (-lambda / rho);
+    JC(blk, 0, 0, 4, 2) = (l / rho) * (-mu / rho);
+    JC(blk, 0, 2, 2, 0) = lambda * n * denom;
+    JC(blk, 0, 2, 2, 3) = (-lambda / rho);
+    JC(blk, 0, 2, 3, 0) = mu * mv * denom;
+    JC(blk, 0, 2, 3, 2) = (-mu / rho);
+    JC(blk, 0, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
+    JC(blk, 0, 2, 4, 2) = (n / rho) * (-mu / rho);
+    JC(blk, 0, 2, 4, 3) = (mv / rho) * (-lambda / rho);
   } else {
     const S f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
-    JC(m, 2, 2, 1, 0) = f10;
-    JC(m, 2, 2, 1, 1) = (-mu / rho);
-    JC(m, 2, 2, 2, 0) = f20;
-    JC(m, 2, 2, 2, 2) = (-mu / rho);
-    JC(m, 2, 2, 3, 0) = f30;
-    JC(m, 2, 2, 3, 3) = (-mu_R / rho);
-    JC(m, 2, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
-    JC(m, 2, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-    JC(m, 2, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-    JC(m, 2, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
-    JC(m, 2, 2, 4, 4) = (-hkocv / rho);
-    JC(m, 2, 0, 1, 0) = mu * n * denom;
-    JC(m, 2, 0, 1, 3) = (-mu / rho);
-    JC(m, 2, 0, 3, 0) = lambda * l * denom;
-    JC(m, 2, 0, 3, 1) = (-lambda / rho);
-    JC(m, 2, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
-    JC(m, 2, 0, 4, 1) = (n / rho) * (-lambda / rho);
-    JC(m, 2, 0, 4, 3) = (l / rho) * (-mu / rho);
-    JC(m, 2, 1, 2, 0) = mu * n * denom;
-    JC(m, 2, 1, 2, 3) = (-mu / rho);
-    JC(m, 2, 1, 3, 0) = lambda * mv * denom;
-    JC(m, 2, 1, 3, 2) = (-lambda / rho);
-    JC(m, 2, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
-    JC(m, 2, 1, 4, 2) = (n / rho) * (-lambda / rho);
-    JC(m, 2, 1, 4, 3) = (mv / rho) * (-mu / rho);
+    JC(blk, 0, 2, 1, 0) = f10;
+    JC(blk, 0, 2, 1, 1) = (-mu / rho);
+    JC(blk, 0, 2, 2, 0) = f20;
+    JC(blk, 0, 2, 2, 2) = (-mu / rho);
+    JC(blk, 0, 2, 3, 0) = f30;
+    JC(blk, 0, 2, 3, 3) = (-mu_R / rho);
+    JC(blk, 0, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
+    JC(blk, 0, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
+    JC(blk, 0, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
+    JC(blk, 0, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
+    JC(blk, 0, 2, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 0, 1, 0) = mu * n * denom;
+    JC(blk, 0, 0, 1, 3) = (-mu / rho);
+    JC(blk, 0, 0, 3, 0) = lambda * l * denom;
+    JC(blk, 0, 0, 3, 1) = (-lambda / rho);
+    JC(blk, 0, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
+    JC(blk, 0, 0, 4, 1) = (n / rho) * (-lambda / rho);
+    JC(blk, 0, 0, 4, 3) = (l / rho) * (-mu / rho);
+    JC(blk, 0, 1, 2, 0) = mu * n * denom;
+    JC(blk, 0, 1, 2, 3) = (-mu / rho);
+    JC(blk, 0, 1, 3, 0) = lambda * mv * denom;
+    JC(blk, 0, 1, 3, 2) = (-lambda / rho);
+    JC(blk, 0, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
+    JC(blk, 0, 1, 4, 2) = (n / rho) * (-lambda / rho);
+    JC(blk, 0, 1, 4, 3) = (mv / rho) * (-mu / rho);
   }
   const S reinv = 1.0 / th.creyn;
   for (int k = 0; k < 75; k++) blk[k] *= reinv;

@@ -422,10 +422,11 @@ CFDV_HD CFDV_INLINE void step_jacobians(const FormArgs& a, FormShared<NDIM>& sh,
                 "task ranges overlap");
   if (tid >= C0 && tid < C0 + CN) {
     GpSlot<NDIM>& sl = sh.slot[(tid - C0) / NDIM];
-    jac_c_rows<NDIM>(a.gas, sl.st, (tid - C0) % NDIM, &sl.H[0][0]);
+    const int i = (tid - C0) % NDIM;
+    jac_c_rows<NDIM>(a.gas, sl.st, i, &sl.H[i * 3][0]);
   } else if (tid >= B0 && tid < B0 + BN) {
-    const int q = (tid - B0) / NDIM;
-    jac_b_rows<NDIM>(a.gas, sh.slot[q].st, (tid - B0) % NDIM, &gp_D<NDIM>(sh, q, FACE)[0][0]);
+    const int q = (tid - B0) / NDIM, i = (tid - B0) % NDIM;
+    jac_b_rows<NDIM>(a.gas, sh.slot[q].st, i, &gp_D<NDIM>(sh, q, FACE)[i][0]);
   } else if (tid >= A0 && tid < A0 + Q) {
     jac_a<NDIM>(a.gas, sh.slot[tid - A0].st, &gp_A<NDIM>(sh, tid - A0, FACE)[0][0]);
   } else if (tid >= F0 && tid < F0 + FN) {

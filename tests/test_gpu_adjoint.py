@@ -1,0 +1,235 @@
+"""Discrete adjoint and tangent of the step on the GPU (through the C ABI).
+
+* The element functionals run by the CUDA kernels agree with the same functionals built
+  for the CPU (tests/emu/adj_emu.cpp), which tests/test_adjoint_emulated.py checks
+  against the oracle and finite differences.
+* The adjoint gradient of J = mean_{n=1..N} F_x(U_n) agrees with the FP64 tangent-linear
+  run along the same parameter directions (both are exact derivatives of the same
+  discrete map, so they agree to the solve tolerance: 1e-8 relative here).
+* It agrees with central finite differences, step 1e-6 relative, of the GPU's own FP64
+  forward run and of the oracle's CPU solve (the restatement pinned to the reference,
+  textbook mode), to 1e-5 relative, for the Mach number and the wall temperature; single
+  wall nodes are checked against unit tangent runs (see the test for why).
+* Checkpoint spacing does not change the gradient; the mixed-precision adjoint agrees
+  with FP64 to 1e-6."""
+import numpy as np
+import pytest
+
+from conftest import get_case
+from test_adjoint_emulated import Setup, _force, _p
+
+pytestmark = pytest.mark.gpu
+
+ADJ_CASE = "cyl4"     # the O-grid cylinder with an isothermal wall (bc 1)
+N_STEPS, CFL, M_GMRES, RTOL = 6, 0.5, 40, 1e-12
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    from cfdv_b200 import gpu as G
+    return G
+
+
+@pytest.fixture(scope="module")
+def emu():
+    return _load_emu()
+
+
+def _load_emu():
+    import ctypes as C
+    import os
+    import subprocess
+    from conftest import ROOT
+    src = os.path.join(ROOT, "tests", "emu", "adj_emu.cpp")
+    lib = os.path.join(ROOT, "tests", "emu", "libadj_emu.so")
+    if not os.path.exists(lib):
+        subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wno-unknown-pragmas", src, "-o", lib],
+                       check=True)
+    L = C.CDLL(lib)
+    P, D, I = C.c_void_p, C.c_double, C.c_int
+    L.emu_functional.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, I, P, P, P, D, D, P, P]
+    L.emu_wall_force.argtypes = [I, I, P, P, P, P, D, D, D, D, D, D, I, I, P, P]
+    return L
+
+
+def gather(s, rows):
+    """Node vector sum_e P_e^T rows_e from per-element rows [E][Ke]."""
+    g = np.zeros(s.o.n_dof)
+    for e in range(s.E):
+        np.add.at(g, s.idx(e), rows[e])
+    return g
+
+
+# The lid's cell Reynolds numbers are small enough that the reference's SUPG coefficient
+# coth(R/2) - 2/R (FDVGalerkin.h:46-50) keeps only a few significant digits: moving cosh up
+# and sinh down by two ulps in the CPU build shifts its assembled gradient by 1.4e-4 and its
+# tangent by 1.2e-4 relative (values by 1.4e-10), and CUDA's cosh/sinh are not glibc's.  The
+# other cases, and the 3D path (no SUPG term), agree to rounding.
+TOL_VAL = {"lid8": 1e-9}
+TOL_DER = {"lid8": 1e-3}
+
+
+@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
+def test_functionals_match_cpu_build(gpu, emu, oracle_lib, name):
+    s = Setup(oracle_lib, name)
+    with gpu.FDVSolver(s.case) as g:
+        g.set_state(s.U)
+        g.form(s.dt)
+        L = g.element_functional(s.w, s.du)
+        gU, gdt, gm = g.vjp(s.w, s.du)
+        rng = np.random.default_rng(3)
+        tU = rng.standard_normal(s.o.n_dof) * np.abs(s.U).max() * 1e-2
+        dr = g.jvp(s.du, tU, 0.2 * s.dt, 0.01)
+        walls = (s.case.bc == 1).any()
+        F = g.wall_force(1, grad=True) if walls else None
+    tv, td = TOL_VAL.get(name, 1e-11), TOL_DER.get(name, 1e-10)
+    ge, Le = s.emu(emu)
+    assert np.abs(L - Le).max() <= tv * np.abs(Le).max()
+    ref = gather(s, ge[:, : s.Ke])
+    assert np.abs(gU - ref).max() <= td * np.abs(ref).max()
+    assert gdt == pytest.approx(ge[:, s.Ke].sum(), rel=td, abs=1e-12 * np.abs(ge[:, s.Ke]).max())
+    assert gm == pytest.approx(ge[:, s.Ke + 1].sum(), rel=td, abs=1e-12 * np.abs(ge[:, s.Ke + 1]).max())
+    je, _ = s.emu(emu, mode=1, tU=tU, tdt=0.2 * s.dt, tM=0.01)
+    jref = gather(s, je)
+    assert np.abs(dr - jref).max() <= td * np.abs(jref).max()
+    if F is not None:
+        fe, fv = _force(emu, s, s.U)
+        assert F[0] == pytest.approx(fv.sum(), rel=1e-12)
+        fref = gather(s, fe[:, : s.Ke])
+        assert np.abs(F[1] - fref).max() <= 1e-10 * np.abs(fref).max()
+        assert F[2] == pytest.approx(fe[:, s.Ke].sum(), rel=1e-10)
+
+
+def _solver(G, case):
+    s = G.FDVSolver(case)
+    s.load_node_records()
+    return s
+
+
+@pytest.fixture(scope="module")
+def adj(gpu):
+    case = get_case(ADJ_CASE)
+    with _solver(gpu, case) as s:
+        r = s.adjoint(N_STEPS, CFL, checkpoint_every=2, m=M_GMRES, rtol=RTOL)
+    assert len(r["wall_nodes"]) > 0
+    return r
+
+
+def test_adjoint_matches_tangent_linear(gpu, adj):
+    case = get_case(ADJ_CASE)
+    rng = np.random.default_rng(11)
+    v = rng.standard_normal(len(adj["wall_nodes"]))
+    with _solver(gpu, case) as s:
+        J, dJm = s.tangent(N_STEPS, CFL, dmach=1.0, m=M_GMRES, rtol=RTOL)
+        J2, dJt = s.tangent(N_STEPS, CFL, dT_wall=v, m=M_GMRES, rtol=RTOL)
+    assert J == pytest.approx(adj["J"], rel=1e-12)
+    assert J2 == pytest.approx(adj["J"], rel=1e-12)
+    assert adj["dJ_dmach"] == pytest.approx(dJm, rel=1e-8)
+    assert float(adj["dJ_dtnode"] @ v) == pytest.approx(dJt, rel=1e-8)
+    assert adj["dJ_dtwall"] == pytest.approx(adj["dJ_dtnode"].sum(), rel=1e-14)
+
+
+def _with_mach(case, M):
+    import copy
+    c = copy.deepcopy(case)
+    c.aero = dict(case.aero)
+    c.aero["M"] = M
+    return c
+
+
+def _with_wall_T(case, wall, dT):
+    import copy
+    c = copy.deepcopy(case)
+    c.nodes = case.nodes.copy()
+    c.nodes[wall, 2 * case.ndim + 1] += dT
+    return c
+
+
+def _gpu_J(G, case):
+    with _solver(G, case) as s:
+        J, _ = s.tangent(N_STEPS, CFL, dmach=0.0, m=M_GMRES, rtol=RTOL)
+    return J
+
+
+def test_adjoint_matches_gpu_finite_differences(gpu, adj):
+    case = get_case(ADJ_CASE)
+    M = float(case.aero["M"])
+    h = 1e-6 * M
+    fd = (_gpu_J(gpu, _with_mach(case, M + h)) - _gpu_J(gpu, _with_mach(case, M - h))) / (2 * h)
+    assert adj["dJ_dmach"] == pytest.approx(fd, rel=1e-5)
+    wall = adj["wall_nodes"]
+    h = 1e-6
+    fd = (_gpu_J(gpu, _with_wall_T(case, wall, h)) - _gpu_J(gpu, _with_wall_T(case, wall, -h))) / (2 * h)
+    assert adj["dJ_dtwall"] == pytest.approx(fd, rel=1e-5)
+
+
+def test_per_node_gradient_matches_unit_tangents(gpu, adj):
+    """Single wall nodes are checked against tangent runs along unit directions, not against
+    differences: the wall starts at rest at one temperature, so the CFL minimum
+    (MPI_CFL.h:124-171) is attained at many wall nodes at once, and moving one node's
+    temperature breaks the tie on one side only (dt = cfl * min is not differentiable
+    there).  Both the adjoint and the tangent give the whole dt sensitivity to the first
+    arg-min node in element order."""
+    case = get_case(ADJ_CASE)
+    g = adj["dJ_dtnode"]
+    picks = {int(np.argmax(np.abs(g))), int(np.argmin(np.abs(g))), len(g) // 2}
+    with _solver(gpu, case) as s:
+        for k in sorted(picks):
+            e = np.zeros(len(g))
+            e[k] = 1.0
+            _, dJ = s.tangent(N_STEPS, CFL, dT_wall=e, m=M_GMRES, rtol=RTOL)
+            assert g[k] == pytest.approx(dJ, rel=1e-8, abs=1e-10 * np.abs(g).max())
+
+
+def _oracle_J(O, emu, case):
+    """J of the oracle's textbook-mode CPU solve, with the wall force of the CPU build."""
+    s = Setup.__new__(Setup)
+    s.case = case
+    s.o = o = O.Oracle(case)
+    s.x = np.ascontiguousarray(case.nodes[:, : case.ndim])
+    s.conn = np.ascontiguousarray(case.conn, np.int32)
+    s.bc = np.ascontiguousarray(case.bc, np.int32)
+    a = case.aero
+    s.gas = (float(a["gamma"]), float(a["M"]), float(a["Re"]), float(a["Pr"]), float(a["Tinf"]), float(a["Twall"]),
+             int(a["Adiabatic"]))
+    s.E, s.Ke = case.n_elements, o.Ke
+    U = o.init_U()
+    cl = o.cleng()
+    J = 0.0
+    for _ in range(N_STEPS):
+        U = o.step(U, CFL, M_GMRES, 200, mode=1, rtol=RTOL, cleng=cl)[0]
+        J += _force(emu, s, U)[1].sum()
+    return J / N_STEPS
+
+
+def test_adjoint_matches_oracle_finite_differences(emu, oracle_lib, adj):
+    case = get_case(ADJ_CASE)
+    M = float(case.aero["M"])
+    h = 1e-6 * M
+    assert _oracle_J(oracle_lib, emu, case) == pytest.approx(adj["J"], rel=1e-10)
+    fd = (_oracle_J(oracle_lib, emu, _with_mach(case, M + h)) -
+          _oracle_J(oracle_lib, emu, _with_mach(case, M - h))) / (2 * h)
+    assert adj["dJ_dmach"] == pytest.approx(fd, rel=1e-5)
+    wall = adj["wall_nodes"]
+    h = 1e-6
+    fd = (_oracle_J(oracle_lib, emu, _with_wall_T(case, wall, h)) -
+          _oracle_J(oracle_lib, emu, _with_wall_T(case, wall, -h))) / (2 * h)
+    assert adj["dJ_dtwall"] == pytest.approx(fd, rel=1e-5)
+
+
+def test_checkpoint_spacing_and_mixed_precision(gpu, adj):
+    case = get_case(ADJ_CASE)
+    with _solver(gpu, case) as s:
+        r1 = s.adjoint(N_STEPS, CFL, checkpoint_every=1, m=M_GMRES, rtol=RTOL)
+        rN = s.adjoint(N_STEPS, CFL, checkpoint_every=N_STEPS, m=M_GMRES, rtol=RTOL)
+        s.load_node_records()
+        rm = s.adjoint(N_STEPS, CFL, checkpoint_every=3, m=M_GMRES, rtol=1e-10, precision=gpu.PREC_MIXED)
+    for r in (r1, rN):
+        assert r["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-13)
+        assert np.abs(r["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-13 * np.abs(adj["dJ_dtnode"]).max()
+    # mixed precision: the same gradient to 1e-6 (its states differ from FP64 by ~1e-10, which
+    # can move the CFL tie to another wall node: that moves the dt share, ~1e-5 of the
+    # largest entry, between tied nodes and leaves the totals unchanged)
+    assert rm["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-6)
+    assert rm["dJ_dtwall"] == pytest.approx(adj["dJ_dtwall"], rel=1e-6)
+    assert np.abs(rm["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-4 * np.abs(adj["dJ_dtnode"]).max()
