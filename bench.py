@@ -186,6 +186,43 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
     return out
 
 
+def solve_roofline(r, peak, peak_kind, label, traffic=None):
+    """The single-launch GMRES solve (the step's dominant kernel): algorithmic bytes of its
+    products and Krylov passes over its CUDA-event time."""
+    st = r["stats"]
+    if st["solve_ms"] <= 0 or st["solves"] == 0:
+        return None
+    achieved = st["solve_bytes"] / (st["solve_ms"] / 1e3) / 1e9
+    return {"kernel": label, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "bytes_per_launch": st["solve_bytes"] / st["solves"], "launches": st["solves"],
+            "avg_launch_us": 1e3 * st["solve_ms"] / st["solves"]}
+
+
+def measure_adjoint(args, ws, max_over_ranks):
+    """Discrete adjoint on the O-grid cylinder: forward run with checkpoints, reverse sweep;
+    device time of each phase from the library's own CUDA events."""
+    from cfdv_b200 import gpu as G, meshgen as mg
+    case = mg.cylinder(96, 128, 16)
+    s = G.FDVSolver(case)
+    out = {"workload": f"3D cylinder O-grid 96x128x16 hex8 ({case.n_elements} elements), M=0.3, Re=150, isothermal "
+                       "wall; J = mean_n wall x-force; gradient w.r.t. Mach, wall temperature and each wall-node "
+                       "temperature", "elements": case.n_elements, "steps": args.adj_steps,
+           "checkpoint_every": 2, "gmres": "GMRES(40) to 1e-8 (forward, tangent and adjoint solves)"}
+    for name, prec in (("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)):
+        s.load_node_records()
+        s.adjoint(2, 0.5, checkpoint_every=1, m=40, rtol=1e-8, precision=prec)  # warm-up
+        s.load_node_records()
+        r = s.adjoint(args.adj_steps, 0.5, checkpoint_every=2, m=40, rtol=1e-8, precision=prec)
+        f, b = max_over_ranks(r["forward_ms"]), max_over_ranks(r["backward_ms"])
+        out[name] = {"forward_ms_per_step": f / args.adj_steps, "backward_ms_per_step": b / args.adj_steps,
+                     "backward_over_forward": b / f, "forward_matvecs": r["forward_matvecs"],
+                     "adjoint_matvecs": r["adjoint_matvecs"], "J": r["J"], "dJ_dmach": r["dJ_dmach"],
+                     "dJ_dtwall": r["dJ_dtwall"], "wall_nodes": int(len(r["wall_nodes"]))}
+    s.close()
+    return out
+
+
 def ebe_roofline(r, peak, peak_kind, label, traffic=None):
     e = r["ebe"]
     if e["total_ms"] <= 0 or e["launches"] == 0:
@@ -274,7 +311,8 @@ def bench_gpu(args, ws, rank, local):
     mixed, fp64 = head["mixed"], head["fp64"]
     err = float(np.abs(mixed["state"] - fp64["state"]).max() / np.abs(fp64["state"]).max())
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "ebe_traffic.json")
+    # DRAM bytes per launch of the solve kernel from an ncu capture (profiles/*.md)
+    tfile = os.path.join(ROOT, "profiles", "solve_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             traffic = json.load(f).get(args.workload)
@@ -300,16 +338,20 @@ def bench_gpu(args, ws, rank, local):
         "mixed": {"true_rel_res_max": mixed["true_rel_res_max"], "matvecs_per_step": mixed["matvecs_per_step"],
                   "form_ms": mixed["form_ms"], "solve_ms": mixed["solve_ms"], "max_field_diff_vs_fp64": err},
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
-        "roofline": ebe_roofline(mixed, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.workload + ")",
-                                 traffic),
-        "roofline_fp64": ebe_roofline(fp64, peak, peak_kind, "ebe_elem_kernel, FP64 matrices (" + args.workload + ")"),
+        "roofline": solve_roofline(mixed, peak, peak_kind,
+                                   "gmres_persistent_kernel, mixed (" + args.workload + "; data L2-resident)"
+                                   if args.workload in ("plate", "lid") else
+                                   "gmres_persistent_kernel, mixed (" + args.workload + ")", traffic),
+        "roofline_ebe": ebe_roofline(mixed, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.workload + ")"),
+        "roofline_ebe_fp64": ebe_roofline(fp64, peak, peak_kind,
+                                          "ebe_elem_kernel, FP64 matrices (" + args.workload + ")"),
         "e2e": {"value": ws * args.steps / e2e_s, "unit": "FDV steps/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": head["clocks"],
     }
     del head
-    if args.secondary and args.secondary != args.workload:
+    if args.secondary in WORKLOADS and args.secondary != args.workload:
         sec = measure_workload(args, args.secondary, 3, 3, flush, ws, barrier, max_over_ranks)
         sec["solver"].close()
         s_m, s_f = sec["mixed"], sec["fp64"]
@@ -327,11 +369,15 @@ def bench_gpu(args, ws, rank, local):
                      "true_rel_res_max": s_f["true_rel_res_max"], "matvecs_per_step": s_f["matvecs_per_step"],
                      "form_ms": s_f["form_ms"], "solve_ms": s_f["solve_ms"]},
             "mixed_over_fp64": s_m["steps_per_s"] / s_f["steps_per_s"],
-            "roofline": ebe_roofline(s_m, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.secondary + ")",
-                                     stile),
-            "roofline_fp64": ebe_roofline(s_f, peak, peak_kind,
-                                          "ebe_elem_kernel, FP64 matrices (" + args.secondary + ")"),
+            "roofline": solve_roofline(s_m, peak, peak_kind, "gmres_persistent_kernel, mixed (" + args.secondary + ")",
+                                       stile),
+            "roofline_ebe": ebe_roofline(s_m, peak, peak_kind,
+                                         "ebe_elem_kernel, FP32 matrices (" + args.secondary + ")"),
+            "roofline_ebe_fp64": ebe_roofline(s_f, peak, peak_kind,
+                                              "ebe_elem_kernel, FP64 matrices (" + args.secondary + ")"),
         }
+    if args.adj_steps > 0:
+        line["adjoint"] = measure_adjoint(args, ws, max_over_ranks)
     if rank == 0:
         if not args.no_cpu_baseline:
             k = 2
@@ -376,7 +422,8 @@ def main():
     ap.add_argument("--workload", default="plate", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", choices=["fp64", "mixed"], help="time one form only (profiling runs)")
-    ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('' to skip)")
+    ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('none' to skip)")
+    ap.add_argument("--adj-steps", type=int, default=4, help="steps of the adjoint leg on the cylinder (0 to skip)")
     args = ap.parse_args()
     ws, rank, local = dist_info()
     if args.impl == "reference":

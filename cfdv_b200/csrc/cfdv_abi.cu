@@ -497,8 +497,8 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
   if (rc) return rc;
   const int est_cap = std::max(1, m * std::max(o->restarts, 1));
   const int gf_cap = std::max(1, o->restarts);
-  // scratch: g, cs, sn, y (m+1 each) | est | gfinal | result(4)
-  const size_t need = 4 * (size_t)(m + 1) + est_cap + gf_cap + 4;
+  // scratch: g, cs, sn, y (m+1 each) | est | gfinal | result(8)
+  const size_t need = 4 * (size_t)(m + 1) + est_cap + gf_cap + 8;
   if (need > c->pers_cap) {
     if ((rc = dalloc(c, &c->d_pers, need))) return rc;
     c->pers_cap = need;
@@ -558,9 +558,9 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
   }
   c->launches++;
   int hi[8];
-  double res[4];
+  double res[6];
   CK(cudaMemcpyAsync(hi, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaMemcpyAsync(res, a.result, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(res, a.result, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (hi[2] & 1) return fail(c, CFDV_ERR_CUDA, "persistent GMRES: grid barrier timed out");
   if (hi[2] & 2) return fail(c, CFDV_ERR_NONFINITE, "persistent GMRES: non-finite residual");
@@ -580,6 +580,10 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
     }
   }
   c->mv_launches += (long)res[3];
+  if (c->prof) {  // algorithmic bytes: each product streams the matrices once, reads x, writes y
+    const double sr = fp32 ? 4.0 : 8.0, E = c->n_elements, K2 = (double)c->Ke * c->Ke, n8 = 8.0 * c->n_dof;
+    c->solve_bytes += res[4] * (E * K2 * 8.0 + 2 * n8) + (res[3] - res[4]) * (E * K2 * sr + 2 * n8) + res[5] * n8;
+  }
   return CFDV_OK;
 }
 
@@ -895,6 +899,7 @@ int cfdv_profile(cfdv_ctx* c, int enable) {
   c->ev_used = 0;
   c->mv_launches = 0;
   c->mv_bytes = 0;
+  c->solve_bytes = 0;
   c->launches = 0;
   c->prof = enable != 0;
   return CFDV_OK;
@@ -924,6 +929,7 @@ int cfdv_profile_read(cfdv_ctx* c, cfdv_kernel_stats* out) {
     out->solves++;
   }
   out->bytes = c->mv_bytes;
+  out->solve_bytes = c->solve_bytes;
   out->kernel_launches = c->launches;
   return CFDV_OK;
 }

@@ -73,6 +73,7 @@ struct cfdv_ctx {
   long mv_launches = 0;
   long launches = 0;    // kernels launched since the last cfdv_profile()
   double mv_bytes = 0;  // algorithmic bytes of the timed element passes
+  double solve_bytes = 0;  // algorithmic bytes of the timed single-launch solves
   std::string err;
 };
 

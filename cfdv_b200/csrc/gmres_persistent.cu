@@ -189,7 +189,8 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
 
   const int m = a.m;
   double* H = a.H;  // (m+1) x m column-major, rotated in place by block 0
-  int total_est = 0, mv = 0;
+  int total_est = 0, mv = 0, mv64 = 0;
+  long passes = 0;  // algorithmic DOF-vector passes of the orthogonalisation and combination
   bool converged = false;
   double beta = 0.0;
   for (int cycle = 0; cycle < a.max_restarts; cycle++) {
@@ -198,6 +199,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
     if (!grid_sync(bar, nb)) return;
     node_pass(false, 1, W, nullptr, pa);
     mv++;
+    mv64++;
     if (!grid_sync(bar, nb)) return;
     beta = sqrt(sum_partials(pa, nb));
     if (!(beta == beta)) {
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
         *a.stop = (fabs(a.g[j + 1]) < a.atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
       }
       total_est++;
+      passes += j + 2;  // v_0 .. v_j read once, v_{j+1} written
       k = j + 1;
       if (!grid_sync(bar, nb)) return;
       if (*(volatile int*)a.stop) break;
@@ -303,6 +306,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
       }
     }
     if (!grid_sync(bar, nb)) return;
+    passes += k + 2;  // du += V y: k basis vectors read, du read and written
     if (bid == 0 && tid == 0) a.out[0] = cycle + 1;
   }
   if (!converged) {  // residual after the last cycle
@@ -310,6 +314,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
     if (!grid_sync(bar, nb)) return;
     node_pass(false, 1, W, nullptr, pa);
     mv++;
+    mv64++;
     if (!grid_sync(bar, nb)) return;
     beta = sqrt(sum_partials(pa, nb));
   }
@@ -318,6 +323,8 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
     a.result[1] = converged ? 1.0 : 0.0;
     a.result[2] = (double)total_est;
     a.result[3] = (double)mv;
+    a.result[4] = (double)mv64;
+    a.result[5] = (double)passes;
   }
 }
 

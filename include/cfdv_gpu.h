@@ -166,6 +166,8 @@ typedef struct {
   long kernel_launches; /* every kernel this context launched since cfdv_profile() */
   long solves;          /* single-launch GMRES solves (engine 0) and their device time */
   double solve_ms;
+  double solve_bytes;   /* algorithmic bytes of those solves: per product E*Ke^2*s_R + 2*DOF*8,
+                           per Arnoldi step (j+2) DOF vectors, per cycle (k+2) DOF vectors */
 } cfdv_kernel_stats;
 int cfdv_profile(cfdv_ctx* ctx, int enable);
 int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
