@@ -29,6 +29,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
+  dfree(c->d_pm);
   dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
   c->adj_state_cap = 0;
   c->n_wall_elems = 0;
@@ -527,6 +528,11 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
   a.n_dof = c->n_dof; a.n_elements = c->n_elements; a.m = m; a.max_restarts = o->restarts;
   a.max_blocks = persistent_max_blocks();
   a.transpose = transpose ? 1 : 0;
+  a.orth = o->orth;
+  if (o->orth == 0) {
+    if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 64))) return rc;
+    a.partm = c->d_pm;
+  }
   a.atol = atol;
   a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
   a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;

@@ -55,6 +55,7 @@ struct cfdv_ctx {
   int* d_pers_int = nullptr;
   double* d_Dinv = nullptr;  // node-block Jacobi inverse [Nn][neqn][neqn]
   double* d_Z = nullptr;     // preconditioned Krylov vector
+  double* d_pm = nullptr;    // CGS2 multi-dot partials [blocks][64]
   // adjoint and tangent runs (adjoint.cu)
   std::vector<double> h_records;   // node records of cfdv_load_node_records: the initial state
   double* d_adj_e = nullptr;       // [E][Ke + 3] per-element gradient rows, d/ddt, d/dMach

@@ -4,14 +4,20 @@
 // host costs more than the arithmetic on the 2D cases (they fit in L2), and on the 3D
 // cases the host round trips still idle the GPU between passes.  This kernel keeps the
 // whole solve on the device: every restart recomputes r = b - A du with the FP64
-// matrices, then runs the Arnoldi cycle with MGS (dots reduced from fixed block
-// partials, so every block derives the same scalar), block 0 applies the Givens
-// rotations and tests |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver),
-// back-substitutes the small triangular system and all blocks add V y to du.  Products
-// use the FP64 matrices, or the FP32 matrices with FP32 accumulation for the mixed form
-// (the restart residual stays FP64: GMRES-based iterative refinement).  With
-// `transpose` every product is A^T x (the adjoint system) and the node-block
-// preconditioner is applied transposed.
+// matrices, then runs the Arnoldi cycle (dots reduced from fixed block partials, so every
+// block derives the same scalars), block 0 applies the Givens rotations and tests
+// |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver), back-substitutes the
+// small triangular system and all blocks add V y to du.  Products use the FP64 matrices,
+// or the FP32 matrices with FP32 accumulation for the mixed form (the restart residual
+// stays FP64: GMRES-based iterative refinement).  With `transpose` every product is A^T x
+// (the adjoint system) and the node-block preconditioner is applied transposed.
+//
+// Orthogonalisation: classical Gram-Schmidt applied twice (CGS2, the default) or modified
+// Gram-Schmidt (MGS), both with FP64 dots and norms.  MGS reduces one projection at a time:
+// j+3 grid barriers for Arnoldi step j.  CGS2 reduces the j+1 projections of a pass at once
+// and repeats the pass once ("twice is enough": orthogonality to working precision, as with
+// MGS): 4 grid barriers per step.  On the L2-resident 2D cases the solve is bound by that
+// chain of barriers.
 //
 // Shape: 512-thread blocks, two per SM, so that the element pass keeps as many matrix
 // loads in flight as the stand-alone element kernel (each thread owns one row of one
@@ -141,6 +147,53 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
   }
 }
 
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxBasis = 64;  // CGS2 runs for m + 1 <= 64; larger m falls back to MGS
+
+// part[bid * ld + i] = this block's share of <V_i, w>, i < nv: a warp sum per i into
+// red[warp][i], then one sum over the warps per i (fixed order)
+__device__ __forceinline__ void multi_dot_partials(const double* V, const double* w, int n, int nv, double* part,
+                                                   int ld, double (*red)[kMaxBasis]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int gtid = blockIdx.x * kThreads + threadIdx.x, gstride = gridDim.x * kThreads;
+  for (int i = 0; i < nv; i++) {
+    const double* vi = V + (size_t)i * n;
+    double acc = 0.0;
+    for (int d = gtid; d < n; d += gstride) acc += __ldcg(vi + d) * __ldcg(w + d);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[wid][i] = acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nv; i += kThreads) {
+    double t = 0.0;
+    for (int k = 0; k < kWarps; k++) t += red[k][i];
+    part[(size_t)blockIdx.x * ld + i] = t;
+  }
+}
+
+// hs[i] = sum over the nb blocks of part[b * ld + i], i < nv, the same bits in every block:
+// the threads split the blocks into `slices` fixed ranges per i, and the slice sums are
+// added in slice order.  stage holds kThreads doubles.
+__device__ __forceinline__ void reduce_multi(const double* part, int ld, int nv, int nb, double* hs, double* stage) {
+  const int slices = kThreads / nv;
+  const int t = threadIdx.x, i = t % nv, sl = t / nv;
+  double acc = 0.0;
+  if (sl < slices) {
+    const int per = (nb + slices - 1) / slices;
+    const int b1 = min(nb, (sl + 1) * per);
+    for (int b = sl * per; b < b1; b++) acc += __ldcg(part + (size_t)b * ld + i);
+  }
+  stage[t] = acc;
+  __syncthreads();
+  if (t < nv) {
+    double s = 0.0;
+    for (int k = 0; k < slices; k++) s += stage[k * nv + t];
+    hs[t] = s;
+  }
+  __syncthreads();
+}
+
 }  // namespace
 
 template <int KE, int NEQ, int NNOD, typename TR>
@@ -158,6 +211,9 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
   double* W = a.W;
   double* pa = a.part0;
   double* pb = a.part1;
+  const bool cgs = a.orth == 0 && a.m + 1 <= kMaxBasis && a.partm != nullptr;
+  __shared__ double red[kWarps][kMaxBasis];  // CGS2: per-warp dot partials
+  __shared__ double hs1[kMaxBasis], hs2[kMaxBasis], stage[kThreads];
 
   auto elem_pass64 = [&](const double* x) {
     elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, tr, xs64);
@@ -224,10 +280,40 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
       const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A P v_j
       elem_pass_op(xj);
       if (!grid_sync(bar, nb)) return;
+      double* Hj = H + (size_t)j * (m + 1);
+      if (cgs) {
+        // CGS2.  Every thread owns the same unknowns d = gtid + k*gstride in all passes, so
+        // the node pass's w feeds this thread's first dots without a grid barrier.
+        const int nv = j + 1, ld = m + 1;
+        node_pass(sizeof(TR) == 4, 0, W, nullptr, pa);
+        mv++;
+        multi_dot_partials(V, W, n, nv, a.partm, ld, red);  // h1 = V^T w
+        if (!grid_sync(bar, nb)) return;
+        reduce_multi(a.partm, ld, nv, nb, hs1, stage);
+        for (int d = gtid; d < n; d += gstride) {  // w -= V h1
+          double w = __ldcg(W + d);
+          for (int i = 0; i < nv; i++) w -= hs1[i] * __ldcg(V + (size_t)i * n + d);
+          W[d] = w;
+        }
+        multi_dot_partials(V, W, n, nv, a.partm, ld, red);  // h2 = V^T w (the second pass)
+        if (!grid_sync(bar, nb)) return;
+        reduce_multi(a.partm, ld, nv, nb, hs2, stage);
+        if (bid == 0)
+          for (int i = tid; i < nv; i += kThreads) Hj[i] = hs1[i] + hs2[i];
+        double acc = 0.0;
+        for (int d = gtid; d < n; d += gstride) {  // w -= V h2, ||w||^2
+          double w = __ldcg(W + d);
+          for (int i = 0; i < nv; i++) w -= hs2[i] * __ldcg(V + (size_t)i * n + d);
+          W[d] = w;
+          acc += w * w;
+        }
+        acc = block_sum(acc);
+        if (tid == 0) pa[bid] = acc;
+        if (!grid_sync(bar, nb)) return;
+      } else {
       node_pass(sizeof(TR) == 4, 0, W, V, pa);
       mv++;
       if (!grid_sync(bar, nb)) return;
-      double* Hj = H + (size_t)j * (m + 1);
       for (int i = 0; i <= j; i++) {
         // MGS step i: h = <w, v_i> (reduced from the partials of the previous pass),
         // w -= h v_i, and the partial of the next dot <w, v_{i+1}> (or ||w||^2)
@@ -246,6 +332,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
         if (tid == 0) pb[bid] = acc;
         double* t = pa; pa = pb; pb = t;
         if (!grid_sync(bar, nb)) return;
+      }
       }
       const double nrm = sqrt(sum_partials(pa, nb));
       double* vn = V + (size_t)(j + 1) * n;

@@ -50,7 +50,8 @@ class _Params(C.Structure):
 
 class _Opts(C.Structure):
     _fields_ = [("mode", C.c_int), ("m", C.c_int), ("restarts", C.c_int), ("rtol", C.c_double),
-                ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int), ("precond", C.c_int)]
+                ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int), ("precond", C.c_int),
+                ("orth", C.c_int)]
 
 
 class _Report(C.Structure):
@@ -224,9 +225,9 @@ class FDVSolver:
         self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
-    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1):
+    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1, orth=0):
         return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)),
-                     int(engine), int(precond))
+                     int(engine), int(precond), int(orth))
 
     def _report(self, m, restarts):
         est = np.zeros(max(m * max(restarts, 1), 1))
@@ -241,8 +242,8 @@ class FDVSolver:
                 "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
 
     def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False,
-              engine=0, precond=True):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond)
+              engine=0, precond=True, orth=0):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
         rep, est, fin = self._report(m, restarts)
         self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
         return self._unpack(rep, est, fin)
@@ -256,8 +257,8 @@ class FDVSolver:
         return r
 
     def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-             true_residual=False, engine=0, precond=True):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond)
+             true_residual=False, engine=0, precond=True, orth=0):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))

@@ -88,6 +88,9 @@ typedef struct {
   int precond;       /* CORRECT mode: 1 = right node-block Jacobi preconditioning (the inverse of
                         each node's assembled neqn x neqn diagonal block); the stopping test
                         stays the true residual of the unpreconditioned system.  0 = none */
+  int orth;          /* CORRECT mode, engine 0: 0 = classical Gram-Schmidt applied twice (4 grid
+                        barriers per Arnoldi step; m <= 63), 1 = modified Gram-Schmidt as the
+                        reference's Arnoldi (MPI_GMRES.h:164-181; j+3 barriers per step j) */
 } cfdv_gmres_opts;
 
 typedef struct {

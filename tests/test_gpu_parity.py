@@ -175,20 +175,27 @@ def test_correct_gmres_fp64_and_mixed(gpu, oracle_lib, name):
 
 @pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_persistent_engine_matches_host_driven(gpu, name, prec):
-    """The single-launch cooperative solve against the one-kernel-per-pass solve."""
+@pytest.mark.parametrize("orth", ["cgs2", "mgs"])
+def test_persistent_engine_matches_host_driven(gpu, name, prec, orth):
+    """The single-launch cooperative solve, with either orthogonalisation, against the
+    one-kernel-per-pass MGS solve: same stopping point, same solution to the tolerance."""
     case = get_case(name)
     p = gpu.PREC_MIXED if prec == "mixed" else gpu.PREC_FP64
     with solver(gpu, case) as s:
         dt = s.cfl(float(case.control["cfl"]))
         s.form(dt, precision=gpu.PREC_MIXED)
-        r0 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=0)
+        r0 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=0,
+                     orth=0 if orth == "cgs2" else 1)
         d0 = s.du()
         r1 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=1)
         d1 = s.du()
     assert r0["true_rel_res"] < 1e-8 and r1["true_rel_res"] < 1e-8
     assert rel_err(d0, d1) <= 1e-6
     assert r0["restarts"] == r1["restarts"]
+    # the Givens estimates of the two Arnoldi processes agree to rounding of the basis
+    n = min(len(r0["est"]), len(r1["est"]))
+    assert abs(len(r0["est"]) - len(r1["est"])) <= 1
+    assert rel_err(np.abs(r0["est"][:n]), np.abs(r1["est"][:n])) <= 1e-6
 
 
 @pytest.mark.parametrize("name", ["lid8", "ramp4", "cyl4"])
