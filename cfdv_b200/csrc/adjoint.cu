@@ -22,12 +22,16 @@ namespace cfdv {
 template <int NDIM>
 __global__ void __launch_bounds__(128) functional_kernel(FunctionalArgs a) {
   constexpr int KE = FormTraits<NDIM>::KE;
-  const int ndir = (a.mode == 0) ? KE + 2 : KE;
+  const int ndir = (a.mode == 0) ? KE + 2 : (a.mode == 1) ? KE : 2;
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = (int)(t / ndir), k = (int)(t % ndir);
+  const int e = (int)(t / ndir), k = (int)(t % ndir) + (a.mode == 2 ? KE : 0);
   if (e >= a.n_elements) return;
   const Dual L = element_functional<NDIM>(a, e, k);
-  if (a.mode == 0) {
+  if (a.mode == 2) {
+    if (k == KE) a.out_dt[e] = L.d;
+    else a.out_mach[e] = L.d;
+    if (k == KE && a.out_val) a.out_val[e] = L.v;
+  } else if (a.mode == 0) {
     if (k < KE) a.out[(size_t)e * KE + k] = L.d;
     else if (k == KE) a.out_dt[e] = L.d;
     else a.out_mach[e] = L.d;
@@ -35,6 +39,15 @@ __global__ void __launch_bounds__(128) functional_kernel(FunctionalArgs a) {
   } else {
     a.out[(size_t)e * KE + k] = L.d;
   }
+}
+
+// reverse mode: the gradient over the element's Ke unknowns, one thread per element
+template <int NDIM>
+__global__ void __launch_bounds__(64) vjp_rev_kernel(FunctionalArgs a) {
+  constexpr int KE = FormTraits<NDIM>::KE;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= a.n_elements) return;
+  element_vjp_rev<NDIM>(a, e, a.out + (size_t)e * KE);
 }
 
 template <int NDIM>
@@ -133,7 +146,7 @@ FunctionalArgs functional_args(cfdv_ctx* c, double dt) {
 }
 
 cudaError_t launch_functional(cfdv_ctx* c, const FunctionalArgs& a) {
-  const int ndir = (a.mode == 0) ? c->Ke + 2 : c->Ke;
+  const int ndir = (a.mode == 0) ? c->Ke + 2 : (a.mode == 1) ? c->Ke : 2;
   const long threads = (long)c->n_elements * ndir;
   const int grid = (int)((threads + kThreadsFn - 1) / kThreadsFn);
   if (c->ndim == 2) functional_kernel<2><<<grid, kThreadsFn, 0, c->st>>>(a);
@@ -149,7 +162,7 @@ int vjp_device(cfdv_ctx* c, double dt, const double* d_w, const double* d_du, do
   if (rc) return rc;
   const size_t E = c->n_elements, Ke = c->Ke;
   FunctionalArgs a = functional_args(c, dt);
-  a.mode = 0;
+  a.mode = 2;  // forward mode for dt and the Mach number
   a.dU = d_du;
   a.w = d_w;
   a.out = c->d_adj_e;
@@ -157,6 +170,13 @@ int vjp_device(cfdv_ctx* c, double dt, const double* d_w, const double* d_du, do
   a.out_mach = c->d_adj_e + E * (Ke + 1);
   a.out_val = d_val;
   CK(launch_functional(c, a));
+  {  // reverse mode for the element's unknowns
+    const int grid = (int)((E + 63) / 64);
+    if (c->ndim == 2) vjp_rev_kernel<2><<<grid, 64, 0, c->st>>>(a);
+    else vjp_rev_kernel<3><<<grid, 64, 0, c->st>>>(a);
+    c->launches++;
+    CK(cudaGetLastError());
+  }
   CK(launch_compose_rhs(ebe_of(c), a.out, d_g, c->d_pa, c->st));
   c->launches++;
   rc = CFDV_OK;
