@@ -40,6 +40,8 @@ WORKLOADS = {
                  make=lambda mg: mg.ramp(128, 64, 32), m=50, cfl=0.25),
     "ramp64": dict(desc="3D compression ramp 64x32x32 hex8 (profiling size), M=2.5, Re=1e5, GMRES(50) to 1e-8",
                    make=lambda mg: mg.ramp(64, 32, 32), m=50, cfl=0.25),
+    "duct": dict(desc="3D duct 200x100x50 hex8 (1,000,000 elements, jittered), M=0.8, Re=5e4, GMRES(40) to 1e-8",
+                 make=lambda mg: mg.duct(200, 100, 50), m=40, cfl=0.5),
 }
 
 
@@ -60,7 +62,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms during the timed region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -74,7 +76,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -261,6 +263,11 @@ def bench_gpu(args, ws, rank, local):
 
     peak, peak_kind = peaks()
     sampler = ClockSampler(local)
+    if args.only == "adjoint":  # profiling runs of the adjoint leg alone
+        out = measure_adjoint(args, ws, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(out))
+        return
     head = measure_workload(args, args.workload, args.steps, args.warmup, flush, ws, barrier, max_over_ranks, sampler)
     solver, case = head["solver"], head["case"]
     if args.only:  # profiling runs: one form, no end-to-end loop, no JSON line
@@ -416,12 +423,13 @@ def bench_reference(args, ws, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cfdv_b200", choices=["cfdv_b200", "reference"])
     ap.add_argument("--workload", default="plate", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--only", choices=["fp64", "mixed"], help="time one form only (profiling runs)")
+    ap.add_argument("--only", choices=["fp64", "mixed", "adjoint"], help="time one form or the adjoint leg only "
+                                                                         "(profiling runs)")
     ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('none' to skip)")
     ap.add_argument("--adj-steps", type=int, default=4, help="steps of the adjoint leg on the cylinder (0 to skip)")
     args = ap.parse_args()

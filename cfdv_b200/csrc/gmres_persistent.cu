@@ -120,9 +120,9 @@ __device__ __forceinline__ double precond_at(const double* Dinv, const double* w
 
 // Element pass Y_e = R_e x_e (TRANS: R_e^T x_e) over the grid: thread (le, i) owns row i of
 // element le of each block iteration; x_e is gathered into a double-buffered shared tile.
-template <int KE, int NEQ, int NNOD, typename TM>
+template <int KE, int NEQ, int NNOD, typename TM, bool TRANS>
 __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* __restrict__ conn, const double* x,
-                                          TM* Y, int E, bool trans, TM (*xs)[kThreads / KE][KE]) {
+                                          TM* Y, int E, TM (*xs)[kThreads / KE][KE]) {
   constexpr int EPB = kThreads / KE;
   const int le = threadIdx.x / KE, i = threadIdx.x % KE;
   int buf = 0;
@@ -134,10 +134,10 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
     if (act) {
       const TM* Re = R + (size_t)e * KE * KE;
       TM acc = 0;
-      if (!trans) {
+      if constexpr (!TRANS) {
 #pragma unroll
         for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[buf][le][j];
-      } else {
+      } else {  // row i of R_e^T is R_e's contiguous column i (served by L1 across j)
 #pragma unroll
         for (int j = 0; j < KE; j++) acc += __ldg(Re + i * KE + j) * xs[buf][le][j];
       }
@@ -196,13 +196,13 @@ __device__ __forceinline__ void reduce_multi(const double* part, int ld, int nv,
 
 }  // namespace
 
-template <int KE, int NEQ, int NNOD, typename TR>
+template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kernel(PersistentArgs a) {
   const unsigned int nb = gridDim.x;
   const int tid = threadIdx.x, bid = blockIdx.x;
   const int gtid = bid * kThreads + tid, gstride = nb * kThreads;
   const int n = a.n_dof;
-  const bool tr = a.transpose != 0;
+  constexpr bool tr = TRANS;
   Barrier bar{a.bar_count, a.bar_gen, a.err};
   constexpr int EPB = kThreads / KE;
   __shared__ double xs64[2][EPB][KE];
@@ -216,12 +216,12 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
   __shared__ double hs1[kMaxBasis], hs2[kMaxBasis], stage[kThreads];
 
   auto elem_pass64 = [&](const double* x) {
-    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, tr, xs64);
+    elem_pass<KE, NEQ, NNOD, double, TRANS>(a.R64, a.conn, x, a.Y64, a.n_elements, xs64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
     if (sizeof(TR) == 8) elem_pass64(x);
-    else elem_pass<KE, NEQ, NNOD, TR>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, tr, xs);
+    else elem_pass<KE, NEQ, NNOD, TR, TRANS>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, xs);
   };
   // node pass: out = gather(Y) (mode 0) or b - gather(Y) (mode 1); partial of out . dotv
   auto node_pass = [&](bool fp32, int mode, double* out, const double* dotv, double* part) {
@@ -415,12 +415,12 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
   }
 }
 
-template <int KE, int NEQ, int NNOD, typename TR>
+template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
 static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_persistent_kernel<KE, NEQ, NNOD, TR>,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS>,
                                                                 kThreads, 0);
   if (e != cudaSuccess) return e;
   if (per_sm <= 0) return cudaErrorInvalidConfiguration;
@@ -430,13 +430,18 @@ static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   if (blocks > a.max_blocks) blocks = a.max_blocks;
   PersistentArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR>, dim3(blocks), dim3(kThreads),
+  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS>, dim3(blocks), dim3(kThreads),
                                      params, 0, st);
 }
 
+template <bool TRANS>
+static cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
+  if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float, TRANS>(a, st) : launch_one<16, 4, 4, double, TRANS>(a, st);
+  return fp32 ? launch_one<40, 5, 8, float, TRANS>(a, st) : launch_one<40, 5, 8, double, TRANS>(a, st);
+}
+
 cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
-  if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float>(a, st) : launch_one<16, 4, 4, double>(a, st);
-  return fp32 ? launch_one<40, 5, 8, float>(a, st) : launch_one<40, 5, 8, double>(a, st);
+  return a.transpose ? launch_dim<true>(ndim, fp32, a, st) : launch_dim<false>(ndim, fp32, a, st);
 }
 
 int persistent_max_blocks() { return kRedBlocks; }

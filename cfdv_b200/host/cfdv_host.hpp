@@ -8,9 +8,11 @@
 //                (Utility/Solvers/GMRESbase.h:8-23: iterate(), update())
 //   TecplotOut   tecplot_<iter>.plt      (Utility/IO/MPI_TecplotOut.h:186-373)
 //   RmsLog       RMSError.txt            (FDV/Function/MPI_RMSError.h:56-75)
+//   save_case    <iter>/ checkpoints     (MPIBinaryConfiguration.h:148-161, SaveBinary.h)
 #pragma once
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <iomanip>
 #include <map>
@@ -225,6 +227,59 @@ inline void tecplot_write(const std::string& path, const BinaryCase& c, const cf
     for (int k = 0; k < c.nnod; k++) t << c.conn[(size_t)e * c.nnod + k] + 1 << " ";
     t << std::endl;
   }
+}
+
+// Checkpoint of the state (MPIBinaryConfiguration.h:148-161, SaveBinary.h:34-150): the case
+// directory <dir>/<iter>/ with binarynodes {x[ndim], rho, v[ndim], T} from NodeUnpack of U,
+// binaryelements {node[nnod], bc[nface]}, the aero file, a single-rank MPIBreakdown, and the
+// control file with iter = <iter>, so that the run resumes from it (main.cpp:177, control
+// "iter").  The reference writes its 3D records with the 2D struct (SaveBinary.h:48-52,
+// 110-116); here both layouts are the ones LoadBinary reads (LoadBinary.h:20-48).
+inline void save_case(const std::string& dir, int iter, const BinaryCase& c, const CaseConfig& cfg,
+                      const cfdv_params& p, const std::vector<double>& U) {
+  const std::string out = dir + "/" + std::to_string(iter);
+  if (std::system(("mkdir -p '" + out + "'").c_str()) != 0) throw std::runtime_error("cannot create " + out);
+  const int nd = c.ndim, ne = nd + 2, rs = 2 * nd + 2;
+  const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
+  std::vector<double> rec((size_t)c.n_nodes * rs);
+  for (int n = 0; n < c.n_nodes; n++) {  // NodeUnpack.h:185-205
+    const double* u = &U[(size_t)n * ne];
+    double* r = &rec[(size_t)n * rs];
+    for (int k = 0; k < nd; k++) r[k] = c.x[(size_t)n * nd + k];
+    r[nd] = u[0];
+    double vsqr = 0;
+    for (int k = 0; k < nd; k++) {
+      r[nd + 1 + k] = u[1 + k] / u[0];
+      vsqr += r[nd + 1 + k] * r[nd + 1 + k];
+    }
+    r[2 * nd + 1] = (u[nd + 1] / u[0] - 0.5 * vsqr) / Cv;
+  }
+  std::vector<int> el((size_t)c.n_elements * (c.nnod + c.nface));
+  for (int e = 0; e < c.n_elements; e++) {
+    for (int k = 0; k < c.nnod; k++) el[(size_t)e * (c.nnod + c.nface) + k] = c.conn[(size_t)e * c.nnod + k];
+    for (int k = 0; k < c.nface; k++) el[(size_t)e * (c.nnod + c.nface) + c.nnod + k] = c.bc[(size_t)e * c.nface + k];
+  }
+  auto write = [&](const std::string& name, const void* data, size_t bytes) {
+    FILE* f = std::fopen((out + "/" + name).c_str(), "wb");
+    if (!f) throw std::runtime_error("cannot write " + out + "/" + name);
+    const size_t put = std::fwrite(data, 1, bytes, f);
+    std::fclose(f);
+    if (put != bytes) throw std::runtime_error("short write of " + out + "/" + name);
+  };
+  write("binarynodes", rec.data(), rec.size() * sizeof(double));
+  write("binaryelements", el.data(), el.size() * sizeof(int));
+  auto kv = [&](const std::string& name, std::map<std::string, std::string> m) {
+    std::ofstream f((out + "/" + name).c_str());
+    for (const auto& it : m) f << it.first << " = " << it.second << "\n";
+  };
+  std::map<std::string, std::string> ctl = cfg.control;
+  ctl["iter"] = std::to_string(iter);
+  kv("control", ctl);
+  kv("aero", cfg.aero);
+  std::ofstream b((out + "/MPIBreakdown").c_str());  // one rank (MPI_Breakdown.h:23-70)
+  b << "1\n";
+  b << "elemin, elemax, nodemin, nodemax, nedgenode_l, nedgenode_r, NodeIteratorMin, NodeIteratorMax\n";
+  b << "0 " << c.n_elements << " 0 " << c.n_nodes - 1 << " 0 0 0 " << c.n_nodes - 1 << "\n";
 }
 
 // one "iter\t(rms) " line per step (MPI_RMSError.h:56-69)

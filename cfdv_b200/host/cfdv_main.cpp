@@ -1,13 +1,16 @@
 // cfdv_gpu: the CFDV time loop (src/main.cpp:162-206) with the per-step path on a B200.
 //
 //   cfdv_gpu <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed]
-//            [--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR]
+//            [--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K]
 //
 // Reads the reference case directory (control, aero, binarynodes, binaryelements) and
 // runs, per iteration, the reference's call order: CFL (main.cpp:179), Tecplot output
 // every 100 iterations (:183), element formation + ApplyBC (:185-194), GMRES iterate and
 // update (:196-197), RMSErr (:198).  Output files are the reference's: tecplot_<iter>.plt
-// and RMSError.txt, written to --out (default: the working directory).
+// and RMSError.txt, written to --out (default: the working directory), and the checkpoint
+// case directories <out>/<iter>/ every --save-every iterations (default 1000, main.cpp:177)
+// and after the last one (main.cpp:208); running the driver on such a directory resumes
+// the run at its iteration.
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -20,12 +23,12 @@ int main(int argc, char** argv) {
   if (argc < 2) {
     std::fprintf(stderr,
                  "usage: %s <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed] "
-                 "[--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR]\n",
+                 "[--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K]\n",
                  argv[0]);
     return 2;
   }
   std::string dir = argv[1], out = ".";
-  int steps = -1, restarts = -1, phys = 0;
+  int steps = -1, restarts = -1, phys = 0, save_every = 1000;
   int mode = CFDV_GMRES_REFERENCE, precision = CFDV_PREC_FP64;
   double rtol = 1e-8;
   for (int i = 2; i < argc; i++) {
@@ -37,6 +40,7 @@ int main(int argc, char** argv) {
     else if (a == "--restarts" && i + 1 < argc) restarts = std::atoi(argv[++i]);
     else if (a == "--physical-3d-flux") phys = 1;
     else if (a == "--out" && i + 1 < argc) out = argv[++i];
+    else if (a == "--save-every" && i + 1 < argc) save_every = std::atoi(argv[++i]);
   }
   try {
     cfdv_host::CaseConfig cfg(dir);
@@ -66,6 +70,7 @@ int main(int argc, char** argv) {
     double t = 0;
     auto t0 = std::chrono::steady_clock::now();
     for (int iter = iter0; iter < itermax; iter++) {
+      if (save_every > 0 && iter % save_every == 0) cfdv_host::save_case(out, iter, c, cfg, p, fdv.state());
       const double dt = fdv.cfl(cfl);
       fdv.form(dt, precision);
       if (iter % 100 == 0) {  // written from this step's state, before the solve
@@ -78,6 +83,7 @@ int main(int argc, char** argv) {
       t += dt;
       std::printf("iter %d dt %.6e restarts %d matvecs %d\n", iter, dt, rep.n_restarts, rep.n_matvec);
     }
+    if (save_every > 0) cfdv_host::save_case(out, itermax, c, cfg, p, fdv.state());
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::printf("%d steps in %.3f s (%.2f steps/s)\n", itermax - iter0, secs, (itermax - iter0) / secs);
   } catch (const std::exception& e) {

@@ -38,3 +38,28 @@ def test_driver_outputs_match_reference(name, steps):
         assert a[0] == b[0]
         # 6 significant digits are printed; allow one unit in the last place
         np.testing.assert_allclose(np.array(a[1:], float), np.array(b[1:], float), rtol=2e-5, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["lid8", "ramp4"])
+def test_driver_checkpoint_restart(name):
+    """The driver saves <out>/<iter>/ every --save-every iterations and at the end; run on a
+    checkpoint directory it resumes there (control iter) and reaches the state of the
+    uninterrupted run, to the rounding of the record round trip."""
+    from cfdv_b200 import meshgen as mg
+    case = get_case(name)
+    with tempfile.TemporaryDirectory() as d:
+        cdir = os.path.join(d, "case")
+        mg.write_case(case, cdir)
+        a, b = os.path.join(d, "a"), os.path.join(d, "b")
+        os.makedirs(a)
+        os.makedirs(b)
+        common = ["--mode", "correct", "--rtol", "1e-12", "--save-every", "3"]
+        subprocess.run([DRIVER, cdir, "--steps", "6", "--out", a] + common, check=True, capture_output=True)
+        assert sorted(os.listdir(a)) >= ["0", "3", "6"]
+        subprocess.run([DRIVER, os.path.join(a, "3"), "--steps", "3", "--out", b] + common, check=True,
+                       capture_output=True)
+        full = mg.read_case(os.path.join(a, "6"))
+        resumed = mg.read_case(os.path.join(b, "6"))
+    assert int(full.control["iter"]) == 6 and int(resumed.control["iter"]) == 6
+    scale = np.abs(full.nodes).max(axis=0)
+    assert (np.abs(resumed.nodes - full.nodes).max(axis=0) <= 1e-10 * scale + 1e-14).all()
