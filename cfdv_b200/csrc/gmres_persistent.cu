@@ -156,13 +156,23 @@ __device__ __forceinline__ void multi_dot_partials(const double* V, const double
                                                    int ld, double (*red)[kMaxBasis]) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int gtid = blockIdx.x * kThreads + threadIdx.x, gstride = gridDim.x * kThreads;
-  for (int i = 0; i < nv; i++) {
-    const double* vi = V + (size_t)i * n;
-    double acc = 0.0;
-    for (int d = gtid; d < n; d += gstride) acc += __ldcg(vi + d) * __ldcg(w + d);
+  // four projections at a time: their loads and butterfly sums overlap
+  for (int i0 = 0; i0 < nv; i0 += 4) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int d = gtid; d < n; d += gstride) {
+      const double wd = __ldcg(w + d);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) red[wid][i] = acc;
+      for (int q = 0; q < 4; q++)
+        if (i0 + q < nv) acc[q] += __ldcg(V + (size_t)(i0 + q) * n + d) * wd;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (i0 + q < nv) red[wid][i0 + q] = acc[q];
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nv; i += kThreads) {
@@ -292,6 +302,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
         reduce_multi(a.partm, ld, nv, nb, hs1, stage);
         for (int d = gtid; d < n; d += gstride) {  // w -= V h1
           double w = __ldcg(W + d);
+#pragma unroll 8
           for (int i = 0; i < nv; i++) w -= hs1[i] * __ldcg(V + (size_t)i * n + d);
           W[d] = w;
         }
@@ -303,6 +314,7 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
         double acc = 0.0;
         for (int d = gtid; d < n; d += gstride) {  // w -= V h2, ||w||^2
           double w = __ldcg(W + d);
+#pragma unroll 8
           for (int i = 0; i < nv; i++) w -= hs2[i] * __ldcg(V + (size_t)i * n + d);
           W[d] = w;
           acc += w * w;
