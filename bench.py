@@ -52,6 +52,33 @@ def dist_info():
     return ws, rank, local
 
 
+class Ranks:
+    """Replica bookkeeping across ranks (the path is not partitioned: every rank runs its own
+    replica).  The barrier and the max over ranks use the process group when there is one:
+    NCCL with CUDA tensors on the GPU box, gloo with CPU tensors in the tests."""
+
+    def __init__(self, ws, device):
+        self.ws, self.device = ws, device
+
+    def barrier(self):
+        if self.ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, v):
+        if self.ws == 1:
+            return v
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def throughput(self, steps, seconds_max):
+        """Whole-job steps per second: every replica's steps over the slowest replica's time."""
+        return self.ws * steps / seconds_max
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -245,18 +272,8 @@ def bench_gpu(args, ws, rank, local):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    def barrier():
-        if ws > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if ws == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(ws, "cuda")
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     peak, peak_kind = peaks()
     sampler = ClockSampler(local)
