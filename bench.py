@@ -333,6 +333,11 @@ def bench_gpu(args, ws, rank, local):
 
     mixed, fp64 = head["mixed"], head["fp64"]
     err = float(np.abs(mixed["state"] - fp64["state"]).max() / np.abs(fp64["state"]).max())
+    # per conserved field: max |U_mixed - U_fp64| / max |U_fp64| over the nodes
+    neq = case.neqn
+    names = ["rho", "rho_u", "rho_v", "rho_w", "rho_E"] if neq == 5 else ["rho", "rho_u", "rho_v", "rho_E"]
+    per_field = {nm: float(np.abs(mixed["state"][k::neq] - fp64["state"][k::neq]).max() /
+                           max(np.abs(fp64["state"][k::neq]).max(), 1e-300)) for k, nm in enumerate(names)}
     traffic = None
     # DRAM bytes per launch of the solve kernel from an ncu capture (profiles/*.md)
     tfile = os.path.join(ROOT, "profiles", "solve_traffic.json")
@@ -359,7 +364,9 @@ def bench_gpu(args, ws, rank, local):
                  "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"],
                  "form_ms": fp64["form_ms"], "solve_ms": fp64["solve_ms"]},
         "mixed": {"true_rel_res_max": mixed["true_rel_res_max"], "matvecs_per_step": mixed["matvecs_per_step"],
-                  "form_ms": mixed["form_ms"], "solve_ms": mixed["solve_ms"], "max_field_diff_vs_fp64": err},
+                  "form_ms": mixed["form_ms"], "solve_ms": mixed["solve_ms"], "max_field_diff_vs_fp64": err,
+                  "field_diff_vs_fp64": per_field,
+                  "after_steps": args.warmup + args.steps},
         "mixed_over_fp64": mixed["steps_per_s"] / fp64["steps_per_s"],
         "roofline": solve_roofline(mixed, peak, peak_kind,
                                    "gmres_persistent_kernel, mixed (" + args.workload + "; data L2-resident)"
