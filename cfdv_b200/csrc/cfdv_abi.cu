@@ -550,7 +550,7 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
   a.result = a.gfinal + gf_cap;
   int* pi = c->d_pers_int;
   a.stop = pi; a.out = pi + 1; a.err = pi + 2;
-  a.bar_count = (unsigned int*)(pi + 3); a.bar_gen = (unsigned int*)(pi + 4);
+  a.bar_count = (unsigned int*)(pi + 3);
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
   if (c->prof) {
     cudaEventCreate(&ev.first);

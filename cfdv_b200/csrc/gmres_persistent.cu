@@ -4,31 +4,41 @@
 // host costs more than the arithmetic on the 2D cases (they fit in L2), and on the 3D
 // cases the host round trips still idle the GPU between passes.  This kernel keeps the
 // whole solve on the device: every restart recomputes r = b - A du with the FP64
-// matrices, then runs the Arnoldi cycle (dots reduced from fixed block partials, so every
-// block derives the same scalars), block 0 applies the Givens rotations and tests
+// matrices, then runs the Arnoldi cycle, applies the Givens rotations, tests
 // |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver), back-substitutes the
-// small triangular system and all blocks add V y to du.  Products use the FP64 matrices,
-// or the FP32 matrices with FP32 accumulation for the mixed form (the restart residual
-// stays FP64: GMRES-based iterative refinement).  With `transpose` every product is A^T x
-// (the adjoint system) and the node-block preconditioner is applied transposed.
+// small triangular system and adds P V y to du.  Products use the FP64 matrices, or the
+// FP32 matrices with FP32 accumulation for the mixed form (the restart residual stays
+// FP64: GMRES-based iterative refinement).  With `transpose` every product is A^T x (the
+// adjoint system) and the node-block preconditioner is applied transposed.
+//
+// Ownership.  One 1024-thread block per SM.  Block b owns a contiguous range of whole
+// nodes; every Krylov vector entry, w, z = P v and du of those unknowns is written only by
+// b, so the orthogonalisation, normalisation and update passes need no grid barrier of
+// their own.  Only the element pass (it gathers x at the nodes of its elements) and the
+// node pass (it gathers the element products of the node's elements) read other blocks'
+// data.  When the block's share of the basis fits in shared memory (the 2D cases) it is
+// kept there as well ("resident"), and the Gram-Schmidt passes run out of shared memory.
+//
+// Scalars.  Dot products are reduced from per-block partials in a fixed order, so every
+// block derives the same bits; every block then applies the Givens rotations, keeps the
+// triangular factor and back-substitutes on its own (redundantly, in shared memory), so
+// no block waits for another to publish those scalars.  Block 0 alone records H, the
+// residual estimates and the counters.
 //
 // Orthogonalisation: classical Gram-Schmidt applied twice (CGS2, the default) or modified
-// Gram-Schmidt (MGS), both with FP64 dots and norms.  MGS reduces one projection at a time:
-// j+3 grid barriers for Arnoldi step j.  CGS2 reduces the j+1 projections of a pass at once
-// and repeats the pass once ("twice is enough": orthogonality to working precision, as with
-// MGS): 4 grid barriers per step.  On the L2-resident 2D cases the solve is bound by that
-// chain of barriers.
+// Gram-Schmidt (MGS), both with FP64 dots and norms.  CGS2 reduces the j+1 projections of
+// a pass at once and repeats the pass once ("twice is enough": orthogonality to working
+// precision, as with MGS).  The norm of the new vector comes from the second pass's
+// partials, ||w2||^2 = ||w1||^2 - ||h2||^2 (w2 = w1 - V h2 with V orthonormal); when that
+// difference loses more than four digits to cancellation it is recomputed directly, with
+// one more grid barrier.  That gives 4 grid barriers per Arnoldi step (MGS: j+3).
 //
-// Shape: 512-thread blocks, two per SM, so that the element pass keeps as many matrix
-// loads in flight as the stand-alone element kernel (each thread owns one row of one
-// element and issues its Ke loads back to back).
-//
-// Phases are separated by a grid barrier.  Its spin is bounded: a block that waits
-// longer than the limit sets an error flag and every block returns at the next
-// barrier, so a broken launch ends instead of hanging.  The launch is cooperative,
-// which guarantees that all blocks are resident.  Data written by other blocks in the
-// same launch is read through L2 (__ldcg): L1 is not coherent across SMs.
-#include <cooperative_groups.h>
+// Grid barrier: one arrival counter per launch; barrier k completes when the count reaches
+// k * blocks.  Its wait is bounded in time: a block that waits longer than the limit sets
+// the failure bit and every block returns at its next barrier, so a broken launch ends
+// instead of hanging.  The launch is cooperative, which guarantees that all blocks are
+// resident.  Data written by other blocks in the same launch is read through L2 (__ldcg):
+// L1 is not coherent across SMs.
 #include <cuda_runtime.h>
 
 #include "gmres_persistent.h"
@@ -38,60 +48,70 @@ namespace cfdv {
 
 namespace {
 
-constexpr long long kSpinLimit = 1ll << 27;  // ~ seconds of polling: far above any barrier
-constexpr int kThreads = 512;
-constexpr int kBlocksPerSm = 2;
+constexpr int kThreads = 1024;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxBasis = 64;         // CGS2 partial slots: m + 1 projections and ||w||^2
+constexpr int kPartLd = kRedBlocks;   // partm[i * kPartLd + block]
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s: far above any barrier wait
+constexpr double kPythMin = 1e-4;     // ||w2||^2 / ||w1||^2 below this: recompute the norm
+
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct Barrier {
-  unsigned int* count;
-  unsigned int* gen;
+  unsigned int* count;  // arrivals since the launch (zero before it); bit 31: failure
   int* err;
+  unsigned int target;
 };
 
-// sense-counting barrier over all blocks; returns false if this or another block failed
-__device__ __forceinline__ bool grid_sync(const Barrier& b, unsigned int nblocks) {
-  __syncthreads();
+// every block: returns false if this or another block gave up waiting
+__device__ __forceinline__ bool grid_sync(Barrier& b) {
   __shared__ int ok;
+  __syncthreads();
+  b.target += gridDim.x;
   if (threadIdx.x == 0) {
-    ok = 1;
-    const unsigned int g = *(volatile unsigned int*)b.gen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(b.count, 1u) + 1u;
-    if (arrived == nblocks) {
-      *(volatile unsigned int*)b.count = 0u;
-      __threadfence();
-      atomicAdd(b.gen, 1u);
-    } else {
-      long long spins = 0;
-      while (*(volatile unsigned int*)b.gen == g) {
-        if (++spins > kSpinLimit) {
+    unsigned int v;
+    // release: this block's writes (ordered before by the block barrier) precede the arrival
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], 1;" : "=r"(v) : "l"(b.count) : "memory");
+    v += 1u;
+    if ((v & 0x7fffffffu) < b.target && !(v & 0x80000000u)) {
+      const unsigned long long t0 = now_ns();
+      unsigned int polls = 0;
+      do {
+        if (++polls > 16) __nanosleep(32);
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(b.count) : "memory");
+        if ((polls & 255u) == 0 && now_ns() - t0 > kWaitNs) {
+          atomicOr(b.count, 0x80000000u);
           atomicOr(b.err, 1);
-          break;
+          v = 0x80000000u;
         }
-        __nanosleep(20);
-      }
+      } while ((v & 0x7fffffffu) < b.target && !(v & 0x80000000u));
     }
-    __threadfence();
-    if (*(volatile int*)b.err) ok = 0;
+    ok = (v & 0x80000000u) ? 0 : 1;
   }
   __syncthreads();
   return ok != 0;
 }
 
+__device__ __forceinline__ double xor_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __device__ __forceinline__ double block_sum(double v) {
-  __shared__ double ws[32];
+  __shared__ double ws[kWarps];
   __shared__ double res;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  v = xor_sum(v);
   __syncthreads();
   if (lane == 0) ws[wid] = v;
   __syncthreads();
   if (wid == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-    v = (lane < nw) ? ws[lane] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    v = xor_sum(ws[lane]);
     if (lane == 0) res = v;
   }
   __syncthreads();
@@ -101,21 +121,8 @@ __device__ __forceinline__ double block_sum(double v) {
 // the same partials summed in the same order by every block
 __device__ __forceinline__ double sum_partials(const double* p, int n) {
   double v = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) v += __ldcg(p + i);
+  for (int i = threadIdx.x; i < n; i += kThreads) v += __ldcg(p + i);
   return block_sum(v);
-}
-
-// z_d = sum_s P[r][s] * (w[n*NEQ + s] / scale), d = n*NEQ + r, P = Dinv (or Dinv^T), with
-// the same division as the stored v so that z = P v exactly
-template <int NEQ>
-__device__ __forceinline__ double precond_at(const double* Dinv, const double* w, int d, double scale, bool trans) {
-  const int n = d / NEQ, r = d % NEQ;
-  const double* D = Dinv + (size_t)n * NEQ * NEQ;
-  double t = 0.0;
-#pragma unroll
-  for (int s = 0; s < NEQ; s++)
-    t += D[trans ? s * NEQ + r : r * NEQ + s] * (__ldcg(w + (size_t)n * NEQ + s) / scale);
-  return t;
 }
 
 // Element pass Y_e = R_e x_e (TRANS: R_e^T x_e) over the grid: thread (le, i) owns row i of
@@ -147,83 +154,63 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
   }
 }
 
-constexpr int kWarps = kThreads / 32;
-constexpr int kMaxBasis = 64;  // CGS2 runs for m + 1 <= 64; larger m falls back to MGS
-
-// part[bid * ld + i] = this block's share of <V_i, w>, i < nv: a warp sum per i into
-// red[warp][i], then one sum over the warps per i (fixed order)
-__device__ __forceinline__ void multi_dot_partials(const double* V, const double* w, int n, int nv, double* part,
-                                                   int ld, double (*red)[kMaxBasis]) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int gtid = blockIdx.x * kThreads + threadIdx.x, gstride = gridDim.x * kThreads;
-  // four projections at a time: their loads and butterfly sums overlap
-  for (int i0 = 0; i0 < nv; i0 += 4) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int d = gtid; d < n; d += gstride) {
-      const double wd = __ldcg(w + d);
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (i0 + q < nv) acc[q] += __ldcg(V + (size_t)(i0 + q) * n + d) * wd;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
-    if (lane == 0)
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (i0 + q < nv) red[wid][i0 + q] = acc[q];
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nv; i += kThreads) {
-    double t = 0.0;
-    for (int k = 0; k < kWarps; k++) t += red[k][i];
-    part[(size_t)blockIdx.x * ld + i] = t;
-  }
-}
-
-// hs[i] = sum over the nb blocks of part[b * ld + i], i < nv, the same bits in every block:
-// the threads split the blocks into `slices` fixed ranges per i, and the slice sums are
-// added in slice order.  stage holds kThreads doubles.
-__device__ __forceinline__ void reduce_multi(const double* part, int ld, int nv, int nb, double* hs, double* stage) {
-  const int slices = kThreads / nv;
-  const int t = threadIdx.x, i = t % nv, sl = t / nv;
-  double acc = 0.0;
-  if (sl < slices) {
-    const int per = (nb + slices - 1) / slices;
-    const int b1 = min(nb, (sl + 1) * per);
-    for (int b = sl * per; b < b1; b++) acc += __ldcg(part + (size_t)b * ld + i);
-  }
-  stage[t] = acc;
-  __syncthreads();
-  if (t < nv) {
-    double s = 0.0;
-    for (int k = 0; k < slices; k++) s += stage[k * nv + t];
-    hs[t] = s;
-  }
-  __syncthreads();
-}
-
 }  // namespace
 
-template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
-__global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kernel(PersistentArgs a) {
-  const unsigned int nb = gridDim.x;
-  const int tid = threadIdx.x, bid = blockIdx.x;
-  const int gtid = bid * kThreads + tid, gstride = nb * kThreads;
-  const int n = a.n_dof;
+// Shared memory beyond the static arrays, in doubles (the host sizes the launch with it):
+// g (m+1), cs (m), sn (m), col (m+1), y (m), the packed triangular factor m(m+1)/2, then
+// either the resident basis and w ((m+1)*S + S, S = unknowns per block) or the per-warp dot
+// partials of the streaming passes (kWarps * kMaxBasis).
+__host__ __device__ inline size_t persistent_dyn_doubles(int m, int S, bool resident) {
+  const size_t base = (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2;
+  return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kMaxBasis);
+}
+
+template <int KE, int NEQ, int NNOD, typename TR, bool TRANS, bool RES>
+__global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(PersistentArgs a) {
+  extern __shared__ __align__(16) double dyn[];
+  const int nb = gridDim.x, tid = threadIdx.x, bid = blockIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int n = a.n_dof, m = a.m;
   constexpr bool tr = TRANS;
-  Barrier bar{a.bar_count, a.bar_gen, a.err};
+  // own unknowns [lo, lo + ns): whole nodes, S per block
+  const int pn = (n / NEQ + nb - 1) / nb, S = pn * NEQ;
+  const int lo = min(n, bid * S), ns = min(n, lo + S) - lo;
+  Barrier bar{a.bar_count, a.err, 0u};
   constexpr int EPB = kThreads / KE;
   __shared__ double xs64[2][EPB][KE];
   __shared__ TR xs[2][EPB][KE];
+  __shared__ double hs1[kMaxBasis], hs2[kMaxBasis];
+  __shared__ int s_stop;
+  double* g = dyn;             // Givens right-hand side
+  double* cs = g + (m + 1);    // rotations
+  double* sn = cs + m;
+  double* col = sn + m;        // Hessenberg column being rotated
+  double* y = col + (m + 1);   // least-squares solution
+  double* tri = y + m;         // R column j at tri[j (j+1) / 2 + i], i <= j
+  double* rest = tri + (size_t)m * (m + 1) / 2;
+  double* sV = rest;                          // resident: (m+1) x S own-slice basis
+  double* sW = rest + (size_t)(m + 1) * S;    // resident: own slice of w
+  double (*red)[kMaxBasis] = reinterpret_cast<double (*)[kMaxBasis]>(rest);  // streaming: per-warp dots
   double* V = a.V;
   double* W = a.W;
-  double* pa = a.part0;
-  double* pb = a.part1;
-  const bool cgs = a.orth == 0 && a.m + 1 <= kMaxBasis && a.partm != nullptr;
-  __shared__ double red[kWarps][kMaxBasis];  // CGS2: per-warp dot partials
-  __shared__ double hs1[kMaxBasis], hs2[kMaxBasis], stage[kThreads];
+  const bool cgs = a.orth == 0 && m + 2 <= kMaxBasis && a.partm != nullptr;
+
+  // own-slice accessors: basis entry i, w
+  auto vld = [&](int i, int dl) -> double {
+    if constexpr (RES) return sV[(size_t)i * S + dl];
+    else return __ldcg(V + (size_t)i * n + lo + dl);
+  };
+  auto wld = [&](int dl) -> double {
+    if constexpr (RES) return sW[dl];
+    else return W[lo + dl];  // written by this block only
+  };
+  auto wst = [&](int dl, double v) {
+    if constexpr (RES) sW[dl] = v;
+    else W[lo + dl] = v;
+  };
+  auto vst = [&](int i, int dl, double v) {
+    V[(size_t)i * n + lo + dl] = v;  // the element pass gathers it when there is no preconditioner
+    if constexpr (RES) sV[(size_t)i * S + dl] = v;
+  };
 
   auto elem_pass64 = [&](const double* x) {
     elem_pass<KE, NEQ, NNOD, double, TRANS>(a.R64, a.conn, x, a.Y64, a.n_elements, xs64);
@@ -233,11 +220,12 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
     if (sizeof(TR) == 8) elem_pass64(x);
     else elem_pass<KE, NEQ, NNOD, TR, TRANS>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, xs);
   };
-  // node pass: out = gather(Y) (mode 0) or b - gather(Y) (mode 1); partial of out . dotv
-  auto node_pass = [&](bool fp32, int mode, double* out, const double* dotv, double* part) {
+  // node pass over the own unknowns: w = gather(Y) (mode 0) or b - gather(Y) (mode 1);
+  // returns this thread's share of <w, dotv> (dotv null: ||w||^2)
+  auto node_pass = [&](bool fp32, int mode, const double* dotv) -> double {
     double acc = 0.0;
-    for (int d = gtid; d < n; d += gstride) {
-      const int nd = d / NEQ, k = d % NEQ;
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      const int d = lo + dl, nd = d / NEQ, k = d % NEQ;
       double s = 0.0;
       const int p1 = __ldg(a.csr_ptr + nd + 1);
       for (int p = __ldg(a.csr_ptr + nd); p < p1; p++) {
@@ -246,28 +234,131 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
         s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
       }
       const double val = mode ? a.b[d] - s : s;
-      out[d] = val;
+      wst(dl, val);
       acc += val * (dotv ? __ldcg(dotv + d) : val);
     }
-    acc = block_sum(acc);
-    if (tid == 0) part[bid] = acc;
+    return acc;
+  };
+  // z = P v on the own nodes from the stored v_i (P = Dinv, or Dinv^T for the adjoint)
+  auto precond_slice = [&](int i) {
+    __syncthreads();  // v_i of the whole node is written
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      const int d = lo + dl, nd = d / NEQ, r = d % NEQ, base = dl - r;
+      const double* D = a.Dinv + (size_t)nd * NEQ * NEQ;
+      double t = 0.0;
+#pragma unroll
+      for (int s = 0; s < NEQ; s++) t += D[tr ? s * NEQ + r : r * NEQ + s] * vld(i, base + s);
+      a.Z[d] = t;
+    }
+  };
+  // partm[i][bid] = <v_i, w> over the own unknowns, i < nv; with `norm` also ||w||^2 at i = nv
+  auto dots = [&](int nv, bool norm) {
+    const int nt = nv + (norm ? 1 : 0);
+    if constexpr (RES) {  // warp per projection, out of shared memory
+      __syncthreads();    // w written by other threads
+      for (int i = wid; i < nt; i += kWarps) {
+        const double* vi = i < nv ? sV + (size_t)i * S : sW;
+        double acc = 0.0;
+        for (int dl = lane; dl < ns; dl += 32) acc += vi[dl] * sW[dl];
+        acc = xor_sum(acc);
+        if (lane == 0) a.partm[(size_t)i * kPartLd + bid] = acc;
+      }
+    } else {  // streaming: each thread its own unknowns, four projections per load batch
+      for (int i0 = 0; i0 < nt; i0 += 4) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int dl = tid; dl < ns; dl += kThreads) {
+          const double wd = wld(dl);
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (i0 + q < nt) acc[q] += (i0 + q < nv ? vld(i0 + q, dl) : wd) * wd;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[q] = xor_sum(acc[q]);
+        if (lane == 0)
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (i0 + q < nt) red[wid][i0 + q] = acc[q];
+      }
+      __syncthreads();
+      for (int i = tid; i < nt; i += kThreads) {
+        double t = 0.0;
+        for (int k = 0; k < kWarps; k++) t += red[k][i];
+        a.partm[(size_t)i * kPartLd + bid] = t;
+      }
+    }
+  };
+  // hs[i] = sum over the blocks of partm[i][b], i < nt, in the same order in every block
+  auto reduce_parts = [&](int nt, double* hs) {
+    for (int i = wid; i < nt; i += kWarps) {
+      double acc = 0.0;
+#pragma unroll 4
+      for (int b = lane; b < nb; b += 32) acc += __ldcg(a.partm + (size_t)i * kPartLd + b);
+      acc = xor_sum(acc);
+      if (lane == 0) hs[i] = acc;
+    }
+    __syncthreads();
+  };
+  // w -= V h over the own unknowns; returns this thread's share of ||w||^2, and with `scale`
+  // (nrm > 0) stores v_{j+1} = w / nrm instead of w
+  auto update = [&](int nv, const double* h, int jn, double nrm) -> double {
+    double acc = 0.0;
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      double w = wld(dl);
+#pragma unroll 8
+      for (int i = 0; i < nv; i++) w -= h[i] * vld(i, dl);
+      if (jn >= 0) vst(jn, dl, w / nrm);
+      else wst(dl, w);
+      acc += w * w;
+    }
+    return acc;
+  };
+  // Givens QR of Hessenberg column j (col[0..j], subdiagonal nrm) with the stored rotations,
+  // by one thread of every block; sets s_stop
+  int total_est = 0;
+  auto givens = [&](int j, double nrm) {
+    if (tid == kThreads - 1) {
+      double* Rj = tri + (size_t)j * (j + 1) / 2;
+      double hi = col[0];
+      for (int i = 0; i < j; i++) {
+        const double h1 = col[i + 1];
+        Rj[i] = cs[i] * hi + sn[i] * h1;
+        hi = -sn[i] * hi + cs[i] * h1;
+      }
+      const double den = hypot(hi, nrm);
+      const double c = den > 0 ? hi / den : 1.0, s = den > 0 ? nrm / den : 0.0;
+      cs[j] = c;
+      sn[j] = s;
+      Rj[j] = den;
+      g[j + 1] = -s * g[j];
+      g[j] = c * g[j];
+      const int stop = (fabs(g[j + 1]) < a.atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
+      s_stop = stop;
+      if (bid == 0) {
+        double* Hj = a.H + (size_t)j * (m + 1);
+        for (int i = 0; i <= j; i++) Hj[i] = Rj[i];
+        Hj[j + 1] = 0.0;
+        if (total_est < a.est_capacity) a.est[total_est] = g[j + 1];
+        *a.stop = stop;
+      }
+    }
   };
 
-  const int m = a.m;
-  double* H = a.H;  // (m+1) x m column-major, rotated in place by block 0
-  int total_est = 0, mv = 0, mv64 = 0;
+  int mv = 0, mv64 = 0;
   long passes = 0;  // algorithmic DOF-vector passes of the orthogonalisation and combination
   bool converged = false;
   double beta = 0.0;
   for (int cycle = 0; cycle < a.max_restarts; cycle++) {
     // r = b - A64 du, beta = ||r||
     elem_pass64(a.du);
-    if (!grid_sync(bar, nb)) return;
-    node_pass(false, 1, W, nullptr, pa);
+    if (!grid_sync(bar)) return;
+    {
+      const double acc = block_sum(node_pass(false, 1, nullptr));
+      if (tid == 0) a.part0[bid] = acc;
+    }
     mv++;
     mv64++;
-    if (!grid_sync(bar, nb)) return;
-    beta = sqrt(sum_partials(pa, nb));
+    if (!grid_sync(bar)) return;
+    beta = sqrt(sum_partials(a.part0, nb));
     if (!(beta == beta)) {
       if (bid == 0 && tid == 0) atomicOr(a.err, 2);
       return;
@@ -276,146 +367,124 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
       converged = true;
       break;
     }
-    for (int d = gtid; d < n; d += gstride) {
-      V[d] = __ldcg(W + d) / beta;
-      if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, beta, tr);
-    }
-    if (bid == 0 && tid == 0) {
-      for (int i = 0; i <= m; i++) a.g[i] = 0.0;
-      a.g[0] = beta;
-    }
-    if (!grid_sync(bar, nb)) return;
+    for (int dl = tid; dl < ns; dl += kThreads) vst(0, dl, wld(dl) / beta);
+    if (a.Dinv) precond_slice(0);
+    for (int i = tid; i <= m; i += kThreads) g[i] = i == 0 ? beta : 0.0;
+    if (!grid_sync(bar)) return;
     int k = 0;
     for (int j = 0; j < m; j++) {
       const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A P v_j
       elem_pass_op(xj);
-      if (!grid_sync(bar, nb)) return;
-      double* Hj = H + (size_t)j * (m + 1);
+      if (!grid_sync(bar)) return;
+      const int nv = j + 1;
+      double nrm;
       if (cgs) {
-        // CGS2.  Every thread owns the same unknowns d = gtid + k*gstride in all passes, so
-        // the node pass's w feeds this thread's first dots without a grid barrier.
-        const int nv = j + 1, ld = m + 1;
-        node_pass(sizeof(TR) == 4, 0, W, nullptr, pa);
+        // CGS2: h1 = V^T w, w1 = w - V h1, h2 = V^T w1, w2 = w1 - V h2, H(:, j) = h1 + h2
+        node_pass(sizeof(TR) == 4, 0, nullptr);
         mv++;
-        multi_dot_partials(V, W, n, nv, a.partm, ld, red);  // h1 = V^T w
-        if (!grid_sync(bar, nb)) return;
-        reduce_multi(a.partm, ld, nv, nb, hs1, stage);
-        for (int d = gtid; d < n; d += gstride) {  // w -= V h1
-          double w = __ldcg(W + d);
-#pragma unroll 8
-          for (int i = 0; i < nv; i++) w -= hs1[i] * __ldcg(V + (size_t)i * n + d);
-          W[d] = w;
+        dots(nv, false);
+        if (!grid_sync(bar)) return;
+        reduce_parts(nv, hs1);
+        update(nv, hs1, -1, 0.0);
+        dots(nv, true);
+        if (!grid_sync(bar)) return;
+        reduce_parts(nv + 1, hs2);
+        double hh = 0.0;
+        for (int i = 0; i < nv; i++) hh += hs2[i] * hs2[i];
+        const double w1n2 = hs2[nv], n2 = w1n2 - hh;
+        for (int i = tid; i < nv; i += kThreads) col[i] = hs1[i] + hs2[i];
+        if (n2 > kPythMin * w1n2) {  // the same decision in every block
+          nrm = sqrt(n2);
+          update(nv, hs2, j + 1, nrm);
+        } else {
+          const double acc = block_sum(update(nv, hs2, -1, 0.0));
+          if (tid == 0) a.part0[bid] = acc;
+          if (!grid_sync(bar)) return;
+          nrm = sqrt(sum_partials(a.part0, nb));
+          for (int dl = tid; dl < ns; dl += kThreads) vst(j + 1, dl, wld(dl) / nrm);
         }
-        multi_dot_partials(V, W, n, nv, a.partm, ld, red);  // h2 = V^T w (the second pass)
-        if (!grid_sync(bar, nb)) return;
-        reduce_multi(a.partm, ld, nv, nb, hs2, stage);
-        if (bid == 0)
-          for (int i = tid; i < nv; i += kThreads) Hj[i] = hs1[i] + hs2[i];
-        double acc = 0.0;
-        for (int d = gtid; d < n; d += gstride) {  // w -= V h2, ||w||^2
-          double w = __ldcg(W + d);
-#pragma unroll 8
-          for (int i = 0; i < nv; i++) w -= hs2[i] * __ldcg(V + (size_t)i * n + d);
-          W[d] = w;
-          acc += w * w;
-        }
-        acc = block_sum(acc);
-        if (tid == 0) pa[bid] = acc;
-        if (!grid_sync(bar, nb)) return;
       } else {
-      node_pass(sizeof(TR) == 4, 0, W, V, pa);
-      mv++;
-      if (!grid_sync(bar, nb)) return;
-      for (int i = 0; i <= j; i++) {
-        // MGS step i: h = <w, v_i> (reduced from the partials of the previous pass),
-        // w -= h v_i, and the partial of the next dot <w, v_{i+1}> (or ||w||^2)
-        const double h = sum_partials(pa, nb);
-        if (bid == 0 && tid == 0) Hj[i] = h;
-        const double* vi = V + (size_t)i * n;
-        const double* nx = (i < j) ? V + (size_t)(i + 1) * n : nullptr;
-        double acc = 0.0;
-#pragma unroll 4
-        for (int d = gtid; d < n; d += gstride) {
-          const double wn = __ldcg(W + d) - h * __ldcg(vi + d);
-          W[d] = wn;
-          acc += wn * (nx ? __ldcg(nx + d) : wn);
+        // MGS: h_i = <w, v_i> reduced from the partials of the previous pass, w -= h_i v_i
+        double* pa = a.part0;
+        double* pb = a.part1;
+        {
+          const double acc = block_sum(node_pass(sizeof(TR) == 4, 0, V));
+          if (tid == 0) pa[bid] = acc;
         }
-        acc = block_sum(acc);
-        if (tid == 0) pb[bid] = acc;
-        double* t = pa; pa = pb; pb = t;
-        if (!grid_sync(bar, nb)) return;
-      }
-      }
-      const double nrm = sqrt(sum_partials(pa, nb));
-      double* vn = V + (size_t)(j + 1) * n;
-      for (int d = gtid; d < n; d += gstride) {
-        vn[d] = __ldcg(W + d) / nrm;
-        if (a.Dinv) a.Z[d] = precond_at<NEQ>(a.Dinv, W, d, nrm, tr);
-      }
-      if (bid == 0 && tid == 0) {
-        // Givens QR of column j (rotations of earlier columns are stored in cs/sn)
-        Hj[j + 1] = nrm;
-        for (int i = 0; i < j; i++) {
-          const double t0 = a.cs[i] * Hj[i] + a.sn[i] * Hj[i + 1];
-          Hj[i + 1] = -a.sn[i] * Hj[i] + a.cs[i] * Hj[i + 1];
-          Hj[i] = t0;
+        mv++;
+        if (!grid_sync(bar)) return;
+        for (int i = 0; i <= j; i++) {
+          const double h = sum_partials(pa, nb);
+          if (tid == 0) col[i] = h;
+          const double* nx = (i < j) ? V + (size_t)(i + 1) * n : nullptr;
+          double acc = 0.0;
+          for (int dl = tid; dl < ns; dl += kThreads) {
+            const double wn = wld(dl) - h * vld(i, dl);
+            wst(dl, wn);
+            acc += wn * (nx ? __ldcg(nx + lo + dl) : wn);
+          }
+          acc = block_sum(acc);
+          if (tid == 0) pb[bid] = acc;
+          double* t = pa; pa = pb; pb = t;
+          if (!grid_sync(bar)) return;
         }
-        const double den = hypot(Hj[j], Hj[j + 1]);
-        const double c = den > 0 ? Hj[j] / den : 1.0, s = den > 0 ? Hj[j + 1] / den : 0.0;
-        a.cs[j] = c;
-        a.sn[j] = s;
-        Hj[j] = den;
-        Hj[j + 1] = 0.0;
-        a.g[j + 1] = -s * a.g[j];
-        a.g[j] = c * a.g[j];
-        if (total_est < a.est_capacity) a.est[total_est] = a.g[j + 1];
-        *a.stop = (fabs(a.g[j + 1]) < a.atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
+        nrm = sqrt(sum_partials(pa, nb));
+        for (int dl = tid; dl < ns; dl += kThreads) vst(j + 1, dl, wld(dl) / nrm);
       }
+      if (a.Dinv) precond_slice(j + 1);
+      __syncthreads();  // col complete
+      givens(j, nrm);
       total_est++;
       passes += j + 2;  // v_0 .. v_j read once, v_{j+1} written
       k = j + 1;
-      if (!grid_sync(bar, nb)) return;
-      if (*(volatile int*)a.stop) break;
+      if (!grid_sync(bar)) return;
+      if (s_stop) break;
     }
-    // y from the upper-triangular system, du += P V y
-    if (bid == 0 && tid == 0) {
+    // y from R y = g (column-oriented back substitution by one warp of every block)
+    if (wid == 0) {
       for (int i = k - 1; i >= 0; i--) {
-        double s = a.g[i];
-        for (int jj = i + 1; jj < k; jj++) s -= H[(size_t)jj * (m + 1) + i] * a.y[jj];
-        a.y[i] = s / H[(size_t)i * (m + 1) + i];
+        const double* Ri = tri + (size_t)i * (i + 1) / 2;
+        const double yi = g[i] / Ri[i];
+        __syncwarp();
+        for (int r = lane; r < i; r += 32) g[r] -= Ri[r] * yi;
+        if (lane == 0) y[i] = yi;
+        __syncwarp();
       }
-      if (cycle < a.gfinal_capacity) a.gfinal[cycle] = a.g[k];
     }
-    if (!grid_sync(bar, nb)) return;
-    for (int d = gtid; d < n; d += gstride) {
-      if (a.Dinv) {  // du += P (V y), P = Dinv or Dinv^T
-        const int nd = d / NEQ, r = d % NEQ;
+    if (bid == 0 && tid == 0 && cycle < a.gfinal_capacity) a.gfinal[cycle] = g[k];
+    __syncthreads();
+    // du += P V y over the own unknowns
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      const int d = lo + dl;
+      if (a.Dinv) {
+        const int nd = d / NEQ, r = d % NEQ, base = dl - r;
         double acc = 0.0;
 #pragma unroll
         for (int s2 = 0; s2 < NEQ; s2++) {
           double t = 0.0;
-          for (int i = 0; i < k; i++) t += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + (size_t)nd * NEQ + s2);
+          for (int i = 0; i < k; i++) t += y[i] * vld(i, base + s2);
           acc += a.Dinv[(size_t)nd * NEQ * NEQ + (tr ? s2 * NEQ + r : r * NEQ + s2)] * t;
         }
         a.du[d] += acc;
       } else {
         double z = 0.0;
-        for (int i = 0; i < k; i++) z += __ldcg(a.y + i) * __ldcg(V + (size_t)i * n + d);
+        for (int i = 0; i < k; i++) z += y[i] * vld(i, dl);
         a.du[d] += z;
       }
     }
-    if (!grid_sync(bar, nb)) return;
+    if (!grid_sync(bar)) return;
     passes += k + 2;  // du += V y: k basis vectors read, du read and written
     if (bid == 0 && tid == 0) a.out[0] = cycle + 1;
   }
   if (!converged) {  // residual after the last cycle
     elem_pass64(a.du);
-    if (!grid_sync(bar, nb)) return;
-    node_pass(false, 1, W, nullptr, pa);
+    if (!grid_sync(bar)) return;
+    const double acc = block_sum(node_pass(false, 1, nullptr));
+    if (tid == 0) a.part0[bid] = acc;
     mv++;
     mv64++;
-    if (!grid_sync(bar, nb)) return;
-    beta = sqrt(sum_partials(pa, nb));
+    if (!grid_sync(bar)) return;
+    beta = sqrt(sum_partials(a.part0, nb));
   }
   if (bid == 0 && tid == 0) {
     a.result[0] = beta;
@@ -427,30 +496,52 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) gmres_persistent_kerne
   }
 }
 
-template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
-static cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS>,
-                                                                kThreads, 0);
+namespace {
+
+template <int KE, int NEQ, int NNOD, typename TR, bool TRANS, bool RES>
+cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, cudaStream_t st) {
+  auto* k = gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, RES>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_bytes);
   if (e != cudaSuccess) return e;
-  if (per_sm <= 0) return cudaErrorInvalidConfiguration;
-  // every co-resident block: on the 2D plate (81k unknowns, L2-resident) and the 3D ramp
-  // (1.4M unknowns) alike, fewer blocks made each barrier cheaper but every pass slower
-  int blocks = sms * (per_sm < kBlocksPerSm ? per_sm : kBlocksPerSm);
-  if (blocks > a.max_blocks) blocks = a.max_blocks;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, dyn_bytes);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
   PersistentArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((void*)gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS>, dim3(blocks), dim3(kThreads),
-                                     params, 0, st);
+  return cudaLaunchCooperativeKernel((void*)k, dim3(blocks), dim3(kThreads), params, dyn_bytes, st);
+}
+
+// resident basis when the block's share of it fits next to the static arrays
+template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
+cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
+  int dev = 0, sms = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int blocks = sms < a.max_blocks ? sms : a.max_blocks;
+  const int pn = (a.n_dof / NEQ + blocks - 1) / blocks, S = pn * NEQ;
+  const bool cgs = a.orth == 0 && a.m + 2 <= kMaxBasis && a.partm != nullptr;
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, true>);
+  if (e != cudaSuccess) return e;
+  const size_t res_bytes = sizeof(double) * persistent_dyn_doubles(a.m, S, true);
+  if (cgs && fa.sharedSizeBytes + res_bytes <= (size_t)optin)
+    return launch_cfg<KE, NEQ, NNOD, TR, TRANS, true>(a, blocks, res_bytes, st);
+  e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, false>);
+  if (e != cudaSuccess) return e;
+  const size_t str_bytes = sizeof(double) * persistent_dyn_doubles(a.m, S, false);
+  if (fa.sharedSizeBytes + str_bytes > (size_t)optin) return cudaErrorInvalidValue;  // m too large
+  return launch_cfg<KE, NEQ, NNOD, TR, TRANS, false>(a, blocks, str_bytes, st);
 }
 
 template <bool TRANS>
-static cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
+cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
   if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float, TRANS>(a, st) : launch_one<16, 4, 4, double, TRANS>(a, st);
   return fp32 ? launch_one<40, 5, 8, float, TRANS>(a, st) : launch_one<40, 5, 8, double, TRANS>(a, st);
 }
+
+}  // namespace
 
 cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
   return a.transpose ? launch_dim<true>(ndim, fp32, a, st) : launch_dim<false>(ndim, fp32, a, st);

@@ -38,8 +38,7 @@ struct PersistentArgs {
   int* out;                    // [0] cycles run
   double* result;              // [0] final ||r||, [1] converged, [2] estimates, [3] products,
                                // [4] FP64 products, [5] algorithmic vector passes
-  unsigned int* bar_count;     // grid barrier state, zero before launch
-  unsigned int* bar_gen;
+  unsigned int* bar_count;     // grid barrier arrivals, zero before launch
   int* err;                    // bit 0: barrier timeout, bit 1: non-finite residual
 };
 
