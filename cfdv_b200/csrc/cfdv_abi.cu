@@ -488,9 +488,12 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
 }  // namespace
 
 // The same textbook solve as gmres_correct, run as one persistent cooperative kernel
-// (gmres_persistent.cu): one launch and one read-back per solve.
-int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
-                             int transpose) {
+// (gmres_persistent.cu): one launch per solve.  solve_launch enqueues the launch and the
+// read-back of its results into pinned memory without waiting; solve_finish waits and
+// fills the report, so a caller can enqueue more work (the state update of a step) in
+// between.  The kernel computes ||b|| itself.
+int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double* rhs_vec, int transpose,
+                             SolveLaunch* L) {
   const int m = o->m;
   const int fp32 = (o->precision == CFDV_PREC_MIXED);
   if (fp32 && !c->have32) return fail(c, CFDV_ERR_STATE, "mixed precision needs cfdv_form(..., CFDV_PREC_MIXED)");
@@ -506,22 +509,13 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
   }
   if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, 8))) return rc;
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
-  double bnorm;
   if (rhs_vec) {
     if (rhs_vec != c->d_b)
       CK(cudaMemcpyAsync(c->d_b, rhs_vec, sizeof(double) * c->n_dof, cudaMemcpyDeviceToDevice, c->st));
-    CK(launch_dot(c->d_b, c->d_b, c->n_dof, c->d_pa, c->st));
-    CK(launch_reduce(c->d_pa, c->d_sc + 1, 1, c->st));
-    c->launches += 2;
-    CK(cudaMemcpyAsync(c->h_pin, c->d_sc + 1, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    bnorm = c->h_pin[0];
-  } else if ((rc = compose_b(c, &bnorm))) {
-    return rc;
+  } else {
+    CK(launch_compose_rhs(ebe_args(c), c->d_rhs, c->d_b, c->d_pa, c->st));
+    c->launches++;
   }
-  const double atol = o->rtol * bnorm;
-  if (rep) { rep->tol = atol; rep->bnorm = bnorm; }
-  if (bnorm == 0.0) { if (rep) rep->true_rel_res = 0.0; return CFDV_OK; }
   CK(cudaMemsetAsync(c->d_pers_int, 0, sizeof(int) * 8, c->st));
   PersistentArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -533,7 +527,7 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
     if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 64))) return rc;
     a.partm = c->d_pm;
   }
-  a.atol = atol;
+  a.rtol = o->rtol;
   a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
   a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;
   a.b = c->d_b; a.du = c->d_du; a.V = c->d_V; a.W = c->d_W; a.part0 = c->d_pa; a.part1 = c->d_pb;
@@ -563,34 +557,54 @@ int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_r
     c->ev_solve.push_back(ev);
   }
   c->launches++;
-  int hi[8];
-  double res[6];
-  CK(cudaMemcpyAsync(hi, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaMemcpyAsync(res, a.result, sizeof(double) * 6, cudaMemcpyDeviceToHost, c->st));
+  double* hp = c->h_pin + cfdv::ctxi::kPinSolve;
+  CK(cudaMemcpyAsync(hp, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(hp + 4, a.result, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
+  L->est = a.est; L->gfinal = a.gfinal; L->est_cap = est_cap; L->gf_cap = gf_cap;
+  L->err = a.err; L->fp32 = fp32;
+  return CFDV_OK;
+}
+
+int cfdv::ctxi::solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_report* rep) {
   CK(cudaStreamSynchronize(c->st));
+  const double* hp = c->h_pin + kPinSolve;
+  int hi[8];
+  double res[8];
+  std::memcpy(hi, hp, sizeof(hi));
+  std::memcpy(res, hp + 4, sizeof(res));
   if (hi[2] & 1) return fail(c, CFDV_ERR_CUDA, "persistent GMRES: grid barrier timed out");
   if (hi[2] & 2) return fail(c, CFDV_ERR_NONFINITE, "persistent GMRES: non-finite residual");
+  const double bnorm = res[6];
   if (rep) {
     const int nest = (int)res[2];
+    rep->tol = res[7];
+    rep->bnorm = bnorm;
     rep->n_est = nest;
     rep->n_restarts = hi[1];
     rep->n_matvec += (int)res[3];
-    rep->true_rel_res = res[0] / bnorm;
+    rep->true_rel_res = bnorm > 0.0 ? res[0] / bnorm : 0.0;
     if (rep->est && rep->est_capacity > 0) {
-      const int k = std::min(std::min(nest, rep->est_capacity), est_cap);
-      if (k > 0) CK(cudaMemcpy(rep->est, a.est, sizeof(double) * k, cudaMemcpyDeviceToHost));
+      const int k = std::min(std::min(nest, rep->est_capacity), L.est_cap);
+      if (k > 0) CK(cudaMemcpy(rep->est, L.est, sizeof(double) * k, cudaMemcpyDeviceToHost));
     }
     if (rep->gfinal && rep->gfinal_capacity > 0) {
-      const int k = std::min(std::min(hi[1], rep->gfinal_capacity), gf_cap);
-      if (k > 0) CK(cudaMemcpy(rep->gfinal, a.gfinal, sizeof(double) * k, cudaMemcpyDeviceToHost));
+      const int k = std::min(std::min(hi[1], rep->gfinal_capacity), L.gf_cap);
+      if (k > 0) CK(cudaMemcpy(rep->gfinal, L.gfinal, sizeof(double) * k, cudaMemcpyDeviceToHost));
     }
   }
   c->mv_launches += (long)res[3];
   if (c->prof) {  // algorithmic bytes: each product streams the matrices once, reads x, writes y
-    const double sr = fp32 ? 4.0 : 8.0, E = c->n_elements, K2 = (double)c->Ke * c->Ke, n8 = 8.0 * c->n_dof;
+    const double sr = L.fp32 ? 4.0 : 8.0, E = c->n_elements, K2 = (double)c->Ke * c->Ke, n8 = 8.0 * c->n_dof;
     c->solve_bytes += res[4] * (E * K2 * 8.0 + 2 * n8) + (res[3] - res[4]) * (E * K2 * sr + 2 * n8) + res[5] * n8;
   }
   return CFDV_OK;
+}
+
+int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
+                             int transpose) {
+  SolveLaunch L;
+  const int rc = solve_launch(c, o, rhs_vec, transpose, &L);
+  return rc ? rc : solve_finish(c, L, rep);
 }
 
 namespace {
@@ -724,10 +738,12 @@ int cfdv_cfl(cfdv_ctx* c, double cfl, double* dt) {
   return CFDV_OK;
 }
 
-int cfdv_form(cfdv_ctx* c, double dt, int precision) {
-  if (!c) return CFDV_ERR_ARG;
-  if (!(dt > 0) || !std::isfinite(dt)) return fail(c, CFDV_ERR_ARG, "form: dt must be positive and finite");
-  cudaSetDevice(c->dev);
+}  // extern "C"
+
+namespace {
+
+// formation launch without the status read-back; dt_dev (device) overrides dt when set
+int form_enqueue(cfdv_ctx* c, double dt, const double* dt_dev, int precision) {
   if (precision == CFDV_PREC_MIXED && !c->d_R32) {
     int rc = dalloc(c, &c->d_R32, (size_t)c->n_elements * c->Ke * c->Ke);
     if (rc) return rc;
@@ -737,6 +753,7 @@ int cfdv_form(cfdv_ctx* c, double dt, int precision) {
   a.gas = c->gas;
   a.dt = dt;
   a.dtsq_2 = std::pow(dt, 2.0) / 2.0;
+  a.dt_dev = dt_dev;
   gauss_legendre(2, a.gz, a.gw);
   a.n_elements = c->n_elements;
   a.physical_3d_flux = c->phys3d;
@@ -760,7 +777,19 @@ int cfdv_form(cfdv_ctx* c, double dt, int precision) {
   c->formed = true;
   c->have32 = (precision == CFDV_PREC_MIXED);
   c->dt_formed = dt;
-  return read_status(c);
+  return CFDV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cfdv_form(cfdv_ctx* c, double dt, int precision) {
+  if (!c) return CFDV_ERR_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(c, CFDV_ERR_ARG, "form: dt must be positive and finite");
+  cudaSetDevice(c->dev);
+  const int rc = form_enqueue(c, dt, nullptr, precision);
+  return rc ? rc : read_status(c);
 }
 
 int cfdv_set_element_matrices(cfdv_ctx* c, const double* R, const double* rhs, int precision) {
@@ -829,12 +858,42 @@ int cfdv_rms(cfdv_ctx* c, double* rms) {
 
 int cfdv_step(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, double* dt) {
   if (!c || !o) return CFDV_ERR_ARG;
-  double d;
-  int rc = cfdv_cfl(c, cfl, &d);
+  int rc;
+  if (o->mode == CFDV_GMRES_REFERENCE || o->engine == 1) {  // host-driven solvers
+    double d;
+    if ((rc = cfdv_cfl(c, cfl, &d))) return rc;
+    if ((rc = cfdv_form(c, d, o->precision))) return rc;
+    if ((rc = cfdv_gmres(c, o, rep))) return rc;
+    if ((rc = cfdv_update(c))) return rc;
+    if (dt) *dt = d;
+    return CFDV_OK;
+  }
+  // persistent solve: CFL, formation (dt read on the device), solve and state update are
+  // enqueued back to back and the host waits once; the update skips itself on the device
+  // when dt, the formation or the solve failed, and the errors are reported in that order
+  if (o->m <= 0 || o->restarts < 0) return fail(c, CFDV_ERR_ARG, "gmres: m > 0, restarts >= 0");
+  cudaSetDevice(c->dev);
+  if (rep) { rep->n_est = 0; rep->n_restarts = 0; rep->n_matvec = 0; rep->true_rel_res = -1.0; }
+  double* d_dt = c->d_sc + 2;
+  CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, kRedBlocks, d_dt,
+                c->st));
+  c->launches += 2;
+  if ((rc = form_enqueue(c, 0.0, d_dt, o->precision))) return rc;
+  cfdv::ctxi::SolveLaunch L;
+  if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L))) return rc;
+  CK(launch_state_update_guarded(c->d_U, c->d_U0, c->d_du, c->n_dof, L.err, c->d_status, d_dt, c->st));
+  c->launches++;
+  double* hs = c->h_pin + cfdv::ctxi::kPinStep;
+  CK(cudaMemcpyAsync(hs, d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(hs + 1, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  rc = cfdv::ctxi::solve_finish(c, L, rep);  // waits for the stream
+  const double d = hs[0];
+  int status;
+  std::memcpy(&status, hs + 1, sizeof(int));
+  if (!(d > 0) || !std::isfinite(d)) return fail(c, CFDV_ERR_NONFINITE, "CFL: no finite positive time step");
+  c->dt_formed = d;
+  if (status & STATUS_NONFINITE_MATRIX) return fail(c, CFDV_ERR_NONFINITE, "non-finite entry in an element matrix or rhs");
   if (rc) return rc;
-  if ((rc = cfdv_form(c, d, o->precision))) return rc;
-  if ((rc = cfdv_gmres(c, o, rep))) return rc;
-  if ((rc = cfdv_update(c))) return rc;
   if (dt) *dt = d;
   return CFDV_OK;
 }

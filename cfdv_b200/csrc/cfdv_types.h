@@ -80,6 +80,7 @@ inline void gauss_legendre(int N, double* zeta, double* w) {
 struct FormArgs {
   GasParams gas;
   double dt, dtsq_2;
+  const double* dt_dev;      // when set, dt is read from device memory (dtsq_2 = dt^2 / 2)
   double gz[2], gw[2];       // 2-point Gauss-Legendre points and weights
   int n_elements;
   int physical_3d_flux;      // 1: evaluate the 3D convective flux the reference drops

@@ -118,5 +118,20 @@ inline void dfree(T*& p) {
 int solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
                  int transpose);
 
+// solve_device in two halves: solve_launch enqueues the persistent launch and the read-back
+// of its results into c->h_pin + kPinSolve without waiting; solve_finish waits for the
+// stream and fills the report.
+constexpr int kPinSolve = 4000;  // 4 doubles of int flags, 8 results
+constexpr int kPinStep = 4016;   // dt, formation status of a step
+struct SolveLaunch {
+  double* est;
+  double* gfinal;
+  int est_cap, gf_cap;
+  int* err;   // device error flags of the launch (bit 0 barrier timeout, bit 1 non-finite)
+  int fp32;
+};
+int solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double* rhs_vec, int transpose, SolveLaunch* L);
+int solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_report* rep);
+
 }  // namespace ctxi
 }  // namespace cfdv

@@ -95,6 +95,7 @@ struct FormShared {
   uint64_t mask;
   double Mn[T::NNOD], Ren[T::NNOD];  // node Mach and Reynolds numbers
   double s[4];                        // s1..s4 of the element
+  double dt, dtsq_2;                  // time step of the formation and dt^2 / 2
   double rhs[T::KE];
   GpSlot<NDIM> slot[T::Q];
   union {
@@ -205,6 +206,8 @@ CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int 
     }
     sh.nfaces = nf;
     sh.mask = a.rowmask ? a.rowmask[e] : 0ull;
+    sh.dt = a.dt_dev ? *a.dt_dev : a.dt;
+    sh.dtsq_2 = a.dt_dev ? sh.dt * sh.dt / 2.0 : a.dtsq_2;
   }
   const int q = tid - (T::THREADS - T::Q);
   if (q >= 0) {
@@ -446,7 +449,7 @@ CFDV_HD CFDV_INLINE void step_coeffs(const FormArgs& a, FormShared<NDIM>& sh, in
     double* A = &gp_A<NDIM>(sh, q, FACE)[i][k];
     double* D = &gp_D<NDIM>(sh, q, FACE)[i][k];
     const double av = *A, bv = *D;
-    sh.slot[q].X[i][k] = a.dt * (s[0] * av + s[2] * bv);
+    sh.slot[q].X[i][k] = sh.dt * (s[0] * av + s[2] * bv);
     *A = av + bv;
     *D = s[1] * av + s[3] * bv;
   }
@@ -458,7 +461,7 @@ template <int NDIM>
 CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int it, double sign, bool face) {
   constexpr int NEQ = NDIM + 2;
   constexpr int PER = NDIM * NDIM * NEQ * NEQ;
-  const double s3_dt = a.dt * sh.s[2];
+  const double s3_dt = sh.dt * sh.s[2];
   const int q = it / PER;
   int rem = it % PER;
   const int ij = rem / (NEQ * NEQ);
@@ -471,7 +474,7 @@ CFDV_HD CFDV_INLINE void hmat_entry(const FormArgs& a, FormShared<NDIM>& sh, int
   double t = 0.0;
   for (int k = 0; k < NEQ; k++) t += A[i][r * 5 + k] * D[j][k * 5 + s];
   const double c = sl.H[i * 3 + j][r * 5 + s];
-  sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + a.dtsq_2 * t);
+  sl.H[i * 3 + j][r * 5 + s] = sign * (-s3_dt * c + sh.dtsq_2 * t);
 }
 
 // step 8: h entries and the rhs coefficient P(i,r) = dt Fbar(i,r) - dt^2/2 sum_s A_i(r,s) divF(s);
@@ -490,8 +493,8 @@ CFDV_HD CFDV_INLINE void step_hmat_rhs(const FormArgs& a, FormShared<NDIM>& sh, 
       const double(*A)[25] = gp_A<NDIM>(sh, q, FACE);
       double u = 0.0;
       for (int q2 = 0; q2 < NEQ; q2++) u += A[i][r * 5 + q2] * sl.F[NDIM][q2];
-      if (FACE) sl.P[i][r] = -a.dt * sl.F[i][r] + a.dtsq_2 * u;
-      else sl.P[i][r] = a.dt * sl.F[i][r] - a.dtsq_2 * u;
+      if (FACE) sl.P[i][r] = -sh.dt * sl.F[i][r] + sh.dtsq_2 * u;
+      else sl.P[i][r] = sh.dt * sl.F[i][r] - sh.dtsq_2 * u;
     }
   }
 }

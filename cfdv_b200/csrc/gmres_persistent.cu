@@ -125,30 +125,146 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
   return block_sum(v);
 }
 
-// Element pass Y_e = R_e x_e (TRANS: R_e^T x_e) over the grid: thread (le, i) owns row i of
-// element le of each block iteration; x_e is gathered into a double-buffered shared tile.
+// Element pass Y_e = R_e x_e (TRANS: R_e^T x_e), thread (le, i) owning row i of element le.
+// 2D (L2-resident, latency-bound): the block's warps form groups of G = lcm(Ke, 32) / 32
+// warps (one warp, two elements) that each take U = 3 waves of their elements at once from
+// the block's contiguous range (the block's whole share in one chunk), synchronising only
+// within the group.  3D (streamed from HBM): waves of kThreads / Ke elements interleaved over
+// the grid with a block barrier per wave; this kept more of the HBM bandwidth than
+// independent groups or bulk L2 prefetches of the next waves did.  x_e of a wave is gathered
+// into a shared tile; the gather offsets of the first chunk are kept from launch start
+// (`first`, shared memory).
+template <int KE>
+struct ElemGroups {
+  static constexpr int L = KE % 32 == 0 ? KE : (KE == 16 ? 32 : (KE == 40 ? 160 : 32 * KE));  // lcm(KE, 32)
+  static constexpr int G = L / 32;            // warps per group
+  static constexpr int EPG = L / KE;          // elements per wave of a group
+  static constexpr int NG = kWarps / G;       // groups per block
+  static constexpr int U = KE <= 16 ? 3 : 1;  // waves per chunk
+  static constexpr int CH = U * EPG;          // elements per chunk of a group
+  static constexpr int TILE = 2 * U * EPG * KE;  // tile entries per group (double-buffered)
+  static constexpr int EPW = kThreads / KE;      // 3D: elements per block wave
+  static constexpr int TILES = (U > 1 ? NG * TILE : 2 * EPW * KE);  // tile entries of the block
+  static_assert(L % KE == 0 && L % 32 == 0 && NG >= 1 && (G == 1 || NG <= 15), "element groups");  // named barriers 1..15
+};
+
+// chunk k of group g of this block covers elements [first_e + k * stride, + CH), elements < end
+template <int KE>
+struct ElemChunks {
+  int first_e, stride, end;
+  __device__ __forceinline__ ElemChunks(int E, int g) {
+    using EG = ElemGroups<KE>;
+    if constexpr (EG::U > 1) {
+      const int per = (E + gridDim.x - 1) / gridDim.x;
+      const int e0 = min(E, (int)blockIdx.x * per);
+      end = min(E, e0 + per);
+      first_e = e0 + g * EG::CH;
+      stride = EG::NG * EG::CH;
+    } else {
+      end = E;
+      first_e = ((int)blockIdx.x * EG::NG + g) * EG::CH;
+      stride = gridDim.x * EG::NG * EG::CH;
+    }
+  }
+};
+
+__device__ __forceinline__ void group_sync(int g, int nthreads) {
+  if (nthreads == 32) __syncwarp();
+  else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(nthreads) : "memory");
+}
+
+template <int KE, int NEQ, int NNOD>
+__device__ __forceinline__ void elem_first(const int* __restrict__ conn, int E, int (*first)[kThreads]) {
+  using EG = ElemGroups<KE>;
+  if constexpr (EG::U == 1) {
+    const int le = threadIdx.x / KE, i = threadIdx.x % KE, e = blockIdx.x * EG::EPW + le;
+    first[0][threadIdx.x] = (le < EG::EPW && e < E) ? __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ : -1;
+    return;
+  }
+  const int g = threadIdx.x / (32 * EG::G), t = threadIdx.x % (32 * EG::G), le = t / KE, i = t % KE;
+  const ElemChunks<KE> ch(E, g);
+#pragma unroll
+  for (int u = 0; u < EG::U; u++) {
+    const int e = ch.first_e + u * EG::EPG + le;
+    first[u][threadIdx.x] =
+        (g < EG::NG && e < ch.end) ? __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ : -1;
+  }
+}
+
 template <int KE, int NEQ, int NNOD, typename TM, bool TRANS>
 __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* __restrict__ conn, const double* x,
-                                          TM* Y, int E, TM (*xs)[kThreads / KE][KE]) {
-  constexpr int EPB = kThreads / KE;
-  const int le = threadIdx.x / KE, i = threadIdx.x % KE;
-  int buf = 0;
-  for (int e0 = blockIdx.x * EPB; e0 < E; e0 += gridDim.x * EPB) {
-    const int e = e0 + le;
-    const bool act = le < EPB && e < E;
-    if (act) xs[buf][le][i] = (TM)__ldcg(x + (size_t)__ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ);
-    __syncthreads();  // the other buffer was last read before the previous barrier
-    if (act) {
-      const TM* Re = R + (size_t)e * KE * KE;
-      TM acc = 0;
-      if constexpr (!TRANS) {
-#pragma unroll
-        for (int j = 0; j < KE; j++) acc += __ldg(Re + j * KE + i) * xs[buf][le][j];
-      } else {  // row i of R_e^T is R_e's contiguous column i (served by L1 across j)
-#pragma unroll
-        for (int j = 0; j < KE; j++) acc += __ldg(Re + i * KE + j) * xs[buf][le][j];
+                                          TM* Y, int E, const int (*first)[kThreads], TM* tiles) {
+  using EG = ElemGroups<KE>;
+  constexpr int U = EG::U, EPG = EG::EPG;
+  if constexpr (U == 1) {
+    constexpr int EPW = EG::EPW;
+    const int le = threadIdx.x / KE, i = threadIdx.x % KE;
+    const bool lact = le < EPW;
+    int buf = 0;
+    for (int e0 = blockIdx.x * EPW; e0 < E; e0 += gridDim.x * EPW) {
+      const int e = e0 + le;
+      const bool act = lact && e < E;
+      TM* tb = tiles + (size_t)buf * EPW * KE;
+      if (act) {
+        const int f = e0 == (int)blockIdx.x * EPW ? first[0][threadIdx.x]
+                                                  : __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ;
+        tb[le * KE + i] = (TM)__ldcg(x + f);
       }
-      Y[(size_t)e * KE + i] = acc;
+      __syncthreads();  // the other buffer was last read before the previous barrier
+      if (act) {
+        const TM* Re = R + (size_t)e * KE * KE;
+        TM acc = 0;
+#pragma unroll
+        for (int j = 0; j < KE; j++)
+          acc += (TRANS ? __ldg(Re + i * KE + j) : __ldg(Re + j * KE + i)) * tb[le * KE + j];
+        Y[(size_t)e * KE + i] = acc;
+      }
+      buf ^= 1;
+    }
+    return;
+  }
+  const int g = threadIdx.x / (32 * EG::G), t = threadIdx.x % (32 * EG::G), le = t / KE, i = t % KE;
+  if (g >= EG::NG) return;  // warps left over by the grouping
+  const ElemChunks<KE> ch(E, g);
+  const int e1 = ch.end;
+  TM* tile = tiles + (size_t)g * EG::TILE;  // [2][U][EPG][KE]
+  TM nx[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const int f = first[u][threadIdx.x];
+    nx[u] = f >= 0 ? (TM)__ldcg(x + f) : TM(0);
+  }
+  int buf = 0;
+  for (int c0 = ch.first_e; c0 < e1; c0 += ch.stride) {
+    TM* tb = tile + (size_t)buf * U * EPG * KE;
+    if (c0 != ch.first_e)
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int e = c0 + u * EPG + le;
+        nx[u] = e < e1 ? (TM)__ldcg(x + (size_t)__ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ) : TM(0);
+      }
+#pragma unroll
+    for (int u = 0; u < U; u++) tb[(u * EPG + le) * KE + i] = nx[u];
+    group_sync(g, 32 * EG::G);  // the other buffer was last read before the previous chunk's barrier
+    const TM* Ru[U];
+    TM acc[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      Ru[u] = R + (size_t)min(c0 + u * EPG + le, e1 - 1) * KE * KE;  // clamped: rows past the range are not stored
+      acc[u] = 0;
+    }
+#pragma unroll
+    for (int j = 0; j < KE; j++)
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        // TRANS: row i of R_e^T is R_e's contiguous column i (served by L1 across j)
+        const TM rv = TRANS ? __ldg(Ru[u] + i * KE + j) : __ldg(Ru[u] + j * KE + i);
+        acc[u] += rv * tb[(u * EPG + le) * KE + j];
+      }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int e = c0 + u * EPG + le;
+      if (e < e1) Y[(size_t)e * KE + i] = acc[u];
     }
     buf ^= 1;
   }
@@ -156,12 +272,19 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
 
 }  // namespace
 
-// Shared memory beyond the static arrays, in doubles (the host sizes the launch with it):
-// g (m+1), cs (m), sn (m), col (m+1), y (m), the packed triangular factor m(m+1)/2, then
-// either the resident basis and w ((m+1)*S + S, S = unknowns per block) or the per-warp dot
-// partials of the streaming passes (kWarps * kMaxBasis).
-__host__ __device__ inline size_t persistent_dyn_doubles(int m, int S, bool resident) {
-  const size_t base = (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2;
+// Element tiles of all groups (in doubles, enough for FP64) and first-chunk gather offsets
+template <int KE>
+constexpr size_t tile_doubles() {
+  return (size_t)ElemGroups<KE>::TILES + (size_t)ElemGroups<KE>::U * kThreads / 2;
+}
+
+// Dynamic shared memory in doubles (the host sizes the launch with it): the element tile and
+// gather offsets, g (m+1), cs (m), sn (m), col (m+1), y (m), the packed triangular factor
+// m(m+1)/2, then either the resident basis and w ((m+1)*S + S, S = unknowns per block) or
+// the per-warp dot partials of the streaming passes (kWarps * kMaxBasis).
+template <int KE>
+size_t persistent_dyn_doubles(int m, int S, bool resident) {
+  const size_t base = tile_doubles<KE>() + (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2;
   return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kMaxBasis);
 }
 
@@ -175,12 +298,14 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   const int pn = (n / NEQ + nb - 1) / nb, S = pn * NEQ;
   const int lo = min(n, bid * S), ns = min(n, lo + S) - lo;
   Barrier bar{a.bar_count, a.err, 0u};
-  constexpr int EPB = kThreads / KE;
-  __shared__ double xs64[2][EPB][KE];
-  __shared__ TR xs[2][EPB][KE];
+  // one tile area for both products (FP64 restart residual, TR Arnoldi products)
+  double* tile64 = dyn;
+  TR* tileR = reinterpret_cast<TR*>(dyn);
+  auto* first = reinterpret_cast<int (*)[kThreads]>(dyn + (size_t)ElemGroups<KE>::TILES);
+  elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
   __shared__ double hs1[kMaxBasis], hs2[kMaxBasis];
   __shared__ int s_stop;
-  double* g = dyn;             // Givens right-hand side
+  double* g = dyn + tile_doubles<KE>();  // Givens right-hand side
   double* cs = g + (m + 1);    // rotations
   double* sn = cs + m;
   double* col = sn + m;        // Hessenberg column being rotated
@@ -213,12 +338,12 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   };
 
   auto elem_pass64 = [&](const double* x) {
-    elem_pass<KE, NEQ, NNOD, double, TRANS>(a.R64, a.conn, x, a.Y64, a.n_elements, xs64);
+    elem_pass<KE, NEQ, NNOD, double, TRANS>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
     if (sizeof(TR) == 8) elem_pass64(x);
-    else elem_pass<KE, NEQ, NNOD, TR, TRANS>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, xs);
+    else elem_pass<KE, NEQ, NNOD, TR, TRANS>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, first, tileR);
   };
   // node pass over the own unknowns: w = gather(Y) (mode 0) or b - gather(Y) (mode 1);
   // returns this thread's share of <w, dotv> (dotv null: ||w||^2)
@@ -312,6 +437,24 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     }
     return acc;
   };
+  // ||b|| over the own unknowns, then the stopping threshold rtol ||b|| (the same bits in
+  // every block)
+  {
+    double acc = 0.0;
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      const double v = a.b[lo + dl];
+      acc += v * v;
+    }
+    acc = block_sum(acc);
+    if (tid == 0) a.part1[bid] = acc;
+  }
+  if (!grid_sync(bar)) return;
+  const double bnorm = sqrt(sum_partials(a.part1, nb));
+  const double atol = a.rtol * bnorm;
+  if (!(bnorm == bnorm)) {
+    if (bid == 0 && tid == 0) atomicOr(a.err, 2);
+    return;
+  }
   // Givens QR of Hessenberg column j (col[0..j], subdiagonal nrm) with the stored rotations,
   // by one thread of every block; sets s_stop
   int total_est = 0;
@@ -331,7 +474,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       Rj[j] = den;
       g[j + 1] = -s * g[j];
       g[j] = c * g[j];
-      const int stop = (fabs(g[j + 1]) < a.atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
+      const int stop = (fabs(g[j + 1]) < atol || nrm == 0.0 || !(nrm == nrm)) ? 1 : 0;
       s_stop = stop;
       if (bid == 0) {
         double* Hj = a.H + (size_t)j * (m + 1);
@@ -345,9 +488,9 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
 
   int mv = 0, mv64 = 0;
   long passes = 0;  // algorithmic DOF-vector passes of the orthogonalisation and combination
-  bool converged = false;
+  bool converged = bnorm == 0.0;  // b = 0: du = 0 is the solution
   double beta = 0.0;
-  for (int cycle = 0; cycle < a.max_restarts; cycle++) {
+  for (int cycle = 0; cycle < a.max_restarts && !converged; cycle++) {
     // r = b - A64 du, beta = ||r||
     elem_pass64(a.du);
     if (!grid_sync(bar)) return;
@@ -363,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       if (bid == 0 && tid == 0) atomicOr(a.err, 2);
       return;
     }
-    if (beta < a.atol) {
+    if (beta < atol) {
       converged = true;
       break;
     }
@@ -493,6 +636,8 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     a.result[3] = (double)mv;
     a.result[4] = (double)mv64;
     a.result[5] = (double)passes;
+    a.result[6] = bnorm;
+    a.result[7] = atol;
   }
 }
 
@@ -525,12 +670,12 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, true>);
   if (e != cudaSuccess) return e;
-  const size_t res_bytes = sizeof(double) * persistent_dyn_doubles(a.m, S, true);
+  const size_t res_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, true);
   if (cgs && fa.sharedSizeBytes + res_bytes <= (size_t)optin)
     return launch_cfg<KE, NEQ, NNOD, TR, TRANS, true>(a, blocks, res_bytes, st);
   e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, false>);
   if (e != cudaSuccess) return e;
-  const size_t str_bytes = sizeof(double) * persistent_dyn_doubles(a.m, S, false);
+  const size_t str_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, false);
   if (fa.sharedSizeBytes + str_bytes > (size_t)optin) return cudaErrorInvalidValue;  // m too large
   return launch_cfg<KE, NEQ, NNOD, TR, TRANS, false>(a, blocks, str_bytes, st);
 }

@@ -9,7 +9,7 @@ struct PersistentArgs {
   int transpose;               // 1: solve A^T x = b (products with R_e^T, preconditioner transposed)
   int orth;                    // 0: classical Gram-Schmidt twice (CGS2), 1: modified Gram-Schmidt
   double* partm;               // CGS2 multi-dot partials [gridDim.x][m+1]
-  double atol;                 // stop when ||b - A du|| < atol (true residual, FP64 matrices)
+  double rtol;                 // stop when ||b - A du|| < rtol ||b|| (true residual, FP64 matrices)
   const int* conn;
   const int* csr_ptr;
   const int* csr_idx;
@@ -37,7 +37,8 @@ struct PersistentArgs {
   int* stop;
   int* out;                    // [0] cycles run
   double* result;              // [0] final ||r||, [1] converged, [2] estimates, [3] products,
-                               // [4] FP64 products, [5] algorithmic vector passes
+                               // [4] FP64 products, [5] algorithmic vector passes, [6] ||b||,
+                               // [7] the stopping threshold rtol ||b||
   unsigned int* bar_count;     // grid barrier arrivals, zero before launch
   int* err;                    // bit 0: barrier timeout, bit 1: non-finite residual
 };

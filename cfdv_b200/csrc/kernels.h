@@ -116,6 +116,10 @@ cudaError_t launch_combine_precond(int ndim, double* du, const double* V, size_t
                                    const double* Dinv, int n_nodes, cudaStream_t st);
 // U0 = U ; U += du
 cudaError_t launch_state_update(double* U, double* U0, const double* du, int n, cudaStream_t st);
+// the update, skipped on the device when *err != 0, the formation status flags a non-finite
+// entry, or *dt is not finite and positive
+cudaError_t launch_state_update_guarded(double* U, double* U0, const double* du, int n, const int* err,
+                                        const int* status, const double* dt, cudaStream_t st);
 // per-field sums of U^2 and U0^2 -> partial[blk][2*neqn]
 cudaError_t launch_rms_partial(const double* U, const double* U0, int n_nodes, int neqn, double* partial,
                                cudaStream_t st);

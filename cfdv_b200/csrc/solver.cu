@@ -161,6 +161,18 @@ __global__ void state_update_kernel(double* U, double* U0, const double* __restr
   }
 }
 
+// the same update, skipped when the solve (err), the formation (status) or the time step failed
+__global__ void state_update_guarded_kernel(double* U, double* U0, const double* __restrict__ du, int n,
+                                            const int* err, const int* status, const double* dt) {
+  const double d = *dt;
+  if (*err != 0 || (*status & STATUS_NONFINITE_MATRIX) || !(d > 0.0) || !isfinite(d)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double u = U[i];
+    U0[i] = u;
+    U[i] = u + du[i];
+  }
+}
+
 __global__ void __launch_bounds__(kRedThreads) rms_partial_kernel(const double* __restrict__ U,
                                                                   const double* __restrict__ U0, int n_nodes,
                                                                   int neqn, double* partial) {
@@ -213,6 +225,11 @@ cudaError_t launch_combine(double* x, const double* V, int n, const double* y, i
 }
 cudaError_t launch_state_update(double* U, double* U0, const double* du, int n, cudaStream_t st) {
   state_update_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(U, U0, du, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_state_update_guarded(double* U, double* U0, const double* du, int n, const int* err,
+                                        const int* status, const double* dt, cudaStream_t st) {
+  state_update_guarded_kernel<<<kRedBlocks, kRedThreads, 0, st>>>(U, U0, du, n, err, status, dt);
   return cudaGetLastError();
 }
 cudaError_t launch_rms_partial(const double* U, const double* U0, int n_nodes, int neqn, double* partial,
