@@ -45,6 +45,10 @@ WORKLOADS = {
 }
 
 
+# orthogonalisation of the persistent solve (cfdv_gmres_opts.orth)
+ORTH = {"cgs2": 0, "mgs": 1, "dcgs2": 2}
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -170,7 +174,8 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
     for prec_name, prec in forms:
         solver.load_node_records()
         for _ in range(warmup):
-            solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec)
+            solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec,
+                        orth=ORTH[args.orth])
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -184,7 +189,8 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(ext)
-            rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec)
+            rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec,
+                              orth=ORTH[args.orth])
             with torch.cuda.stream(ext):
                 e1.record(ext)
             e1.synchronize()
@@ -304,7 +310,8 @@ def bench_gpu(args, ws, rank, local):
     solver.profile(True)
     for _ in range(2):
         solver.set_state(host.numpy())
-        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED)
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED,
+                    orth=ORTH[args.orth])
         solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(outb.numpy()), None, n))
         host.copy_(outb)
     torch.cuda.synchronize()
@@ -318,7 +325,8 @@ def bench_gpu(args, ws, rank, local):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(ext)
         solver.set_state(host.numpy())
-        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED)
+        solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=G.PREC_MIXED,
+                    orth=ORTH[args.orth])
         solver._ck(solver.L.cfdv_get_state(solver._ctx, G._p(outb.numpy()), None, n))
         with torch.cuda.stream(ext):
             e1.record(ext)
@@ -358,7 +366,8 @@ def bench_gpu(args, ws, rank, local):
         "dtype": "f32 matrices/f64 vectors (mixed); f64",
         "data": "synthetic",
         "config": {"workload": head["desc"], "elements": case.n_elements, "dof": n,
-                   "gmres": f"restarted GMRES({m}), MGS, right node-block Jacobi, to true relative residual {rtol:g}",
+                   "gmres": f"restarted GMRES({m}), {args.orth.upper()}, right node-block Jacobi, to true relative "
+                            f"residual {rtol:g}",
                    "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
         "fp64": {"value": fp64["steps_per_s"], "ms_per_step": fp64["ms_per_step"],
                  "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"],
@@ -455,6 +464,7 @@ def main():
                                                                          "(profiling runs)")
     ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('none' to skip)")
     ap.add_argument("--adj-steps", type=int, default=4, help="steps of the adjoint leg on the cylinder (0 to skip)")
+    ap.add_argument("--orth", default="dcgs2", choices=sorted(ORTH), help="Gram-Schmidt of the persistent GMRES solve")
     args = ap.parse_args()
     ws, rank, local = dist_info()
     if args.impl == "reference":

@@ -325,6 +325,7 @@ cfdv_gmres_opts solve_opts(const cfdv_adjoint_opts* o) {
   g.precision = o->precision;
   g.engine = 0;
   g.precond = 1;
+  g.orth = 2;  // delayed CGS2
   return g;
 }
 

@@ -523,8 +523,8 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   a.max_blocks = persistent_max_blocks();
   a.transpose = transpose ? 1 : 0;
   a.orth = o->orth;
-  if (o->orth == 0) {
-    if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 64))) return rc;
+  if (o->orth == 0 || o->orth == 2) {
+    if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 128))) return rc;
     a.partm = c->d_pm;
   }
   a.rtol = o->rtol;

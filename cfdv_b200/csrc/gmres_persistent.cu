@@ -50,7 +50,8 @@ namespace {
 
 constexpr int kThreads = 1024;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxBasis = 64;         // CGS2 partial slots: m + 1 projections and ||w||^2
+constexpr int kMaxBasis = 64;         // CGS2 / DCGS2: m + 2 <= kMaxBasis
+constexpr int kSlots = 128;           // partial slots of one reduction (DCGS2: 2j + 3)
 constexpr int kPartLd = kRedBlocks;   // partm[i * kPartLd + block]
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s: far above any barrier wait
 constexpr double kPythMin = 1e-4;     // ||w2||^2 / ||w1||^2 below this: recompute the norm
@@ -280,12 +281,13 @@ constexpr size_t tile_doubles() {
 
 // Dynamic shared memory in doubles (the host sizes the launch with it): the element tile and
 // gather offsets, g (m+1), cs (m), sn (m), col (m+1), y (m), the packed triangular factor
-// m(m+1)/2, then either the resident basis and w ((m+1)*S + S, S = unknowns per block) or
-// the per-warp dot partials of the streaming passes (kWarps * kMaxBasis).
+// m(m+1)/2, the unrotated Hessenberg matrix (m+1) m and a pending column (m+1) of DCGS2,
+// then either the resident basis and w ((m+1)*S + S, S = unknowns per block) or the
+// per-warp dot partials of the streaming passes (kWarps * kSlots).
 template <int KE>
 size_t persistent_dyn_doubles(int m, int S, bool resident) {
-  const size_t base = tile_doubles<KE>() + (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2;
-  return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kMaxBasis);
+  const size_t base = tile_doubles<KE>() + (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2 + (size_t)(m + 1) * (m + 1);
+  return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kSlots);
 }
 
 template <int KE, int NEQ, int NNOD, typename TR, bool TRANS, bool RES>
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   TR* tileR = reinterpret_cast<TR*>(dyn);
   auto* first = reinterpret_cast<int (*)[kThreads]>(dyn + (size_t)ElemGroups<KE>::TILES);
   elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
-  __shared__ double hs1[kMaxBasis], hs2[kMaxBasis];
+  __shared__ double hs1[kSlots], hs2[kMaxBasis], sc[4];
   __shared__ int s_stop;
   double* g = dyn + tile_doubles<KE>();  // Givens right-hand side
   double* cs = g + (m + 1);    // rotations
@@ -311,13 +313,16 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* col = sn + m;        // Hessenberg column being rotated
   double* y = col + (m + 1);   // least-squares solution
   double* tri = y + m;         // R column j at tri[j (j+1) / 2 + i], i <= j
-  double* rest = tri + (size_t)m * (m + 1) / 2;
+  double* Hf = tri + (size_t)m * (m + 1) / 2;  // DCGS2: unrotated column j at Hf[j (m+1) + i]
+  double* pend = Hf + (size_t)(m + 1) * m;      // DCGS2: pending column (m+1)
+  double* rest = pend + (m + 1);
   double* sV = rest;                          // resident: (m+1) x S own-slice basis
   double* sW = rest + (size_t)(m + 1) * S;    // resident: own slice of w
-  double (*red)[kMaxBasis] = reinterpret_cast<double (*)[kMaxBasis]>(rest);  // streaming: per-warp dots
+  double (*red)[kSlots] = reinterpret_cast<double (*)[kSlots]>(rest);  // streaming: per-warp dots
   double* V = a.V;
   double* W = a.W;
   const bool cgs = a.orth == 0 && m + 2 <= kMaxBasis && a.partm != nullptr;
+  const bool dcgs = a.orth == 2 && m + 2 <= kMaxBasis && a.partm != nullptr;
 
   // own-slice accessors: basis entry i, w
   auto vld = [&](int i, int dl) -> double {
@@ -437,6 +442,131 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     }
     return acc;
   };
+  // DCGS2 pass A: partm[s][bid] over the own unknowns of, with u~ = slot j of V,
+  //   s < j: <q_s, u~>;  with w: j <= s < 2j: <q_{s-j}, w>, 2j: <u~, u~>, 2j+1: <u~, w>,
+  //   2j+2: <w, w>;  without w: j: <u~, u~>
+  auto dots_d = [&](int j, bool with_w) {
+    const int nt = with_w ? 2 * j + 3 : j + 1, s0 = with_w ? 2 * j : j;
+    if constexpr (RES) {
+      __syncthreads();  // w and u~ written by other threads
+      const double* sU = sV + (size_t)j * S;
+      for (int sl = wid; sl < nt; sl += kWarps) {
+        const double *x, *yv;
+        if (sl < j) { x = sV + (size_t)sl * S; yv = sU; }
+        else if (sl < s0) { x = sV + (size_t)(sl - j) * S; yv = sW; }
+        else { const int r = sl - s0; x = r == 2 ? sW : sU; yv = r == 0 ? sU : sW; }
+        double acc = 0.0;
+        for (int dl = lane; dl < ns; dl += 32) acc += x[dl] * yv[dl];
+        acc = xor_sum(acc);
+        if (lane == 0) a.partm[(size_t)sl * kPartLd + bid] = acc;
+      }
+    } else {  // streaming: each thread its own unknowns, four basis vectors per load batch
+      for (int i0 = 0; i0 < j; i0 += 4) {
+        double au[4] = {0.0, 0.0, 0.0, 0.0}, aw[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int dl = tid; dl < ns; dl += kThreads) {
+          const double u = vld(j, dl), w = with_w ? wld(dl) : 0.0;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (i0 + q < j) {
+              const double v = vld(i0 + q, dl);
+              au[q] += v * u;
+              aw[q] += v * w;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          au[q] = xor_sum(au[q]);
+          aw[q] = xor_sum(aw[q]);
+        }
+        if (lane == 0)
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (i0 + q < j) {
+              red[wid][i0 + q] = au[q];
+              if (with_w) red[wid][j + i0 + q] = aw[q];
+            }
+      }
+      double uu = 0.0, uw = 0.0, ww = 0.0;
+      for (int dl = tid; dl < ns; dl += kThreads) {
+        const double u = vld(j, dl);
+        uu += u * u;
+        if (with_w) {
+          const double w = wld(dl);
+          uw += u * w;
+          ww += w * w;
+        }
+      }
+      uu = xor_sum(uu);
+      uw = xor_sum(uw);
+      ww = xor_sum(ww);
+      if (lane == 0) {
+        red[wid][s0] = uu;
+        if (with_w) {
+          red[wid][s0 + 1] = uw;
+          red[wid][s0 + 2] = ww;
+        }
+      }
+      __syncthreads();
+      for (int sl = tid; sl < nt; sl += kThreads) {
+        double t = 0.0;
+        for (int k = 0; k < kWarps; k++) t += red[k][sl];
+        a.partm[(size_t)sl * kPartLd + bid] = t;
+      }
+    }
+  };
+  // DCGS2 pass B over the own unknowns, with c = hs1[0..j), p = hs1[j..2j) ++ pj:
+  //   q_j = (u~_j - Q_j c) / nu  (final, into slot j),  u = w - Q_j p[0..j) - pj q_j,
+  //   slot j+1 = u / sigma (sigma > 0), or u kept in w (sigma = 0); returns the share of ||u||^2
+  auto pass_b = [&](int j, double nu, double pj, double sigma) -> double {
+    double acc = 0.0;
+    for (int dl = tid; dl < ns; dl += kThreads) {
+      double su = 0.0, sw = 0.0;
+#pragma unroll 4
+      for (int i = 0; i < j; i++) {
+        const double q = vld(i, dl);
+        su += hs1[i] * q;
+        sw += hs1[j + i] * q;
+      }
+      const double qj = (vld(j, dl) - su) / nu;
+      const double u = wld(dl) - sw - pj * qj;
+      vst(j, dl, qj);
+      if (sigma > 0.0) vst(j + 1, dl, u / sigma);
+      else wst(dl, u);
+      acc += u * u;
+    }
+    return acc;
+  };
+  // DCGS2 scalars from the reduced slots (warp 0, the same order in every block):
+  // sc[0] = nu = sqrt(<u~,u~> - |c|^2), sc[1] = pj = (<u~,w> - c.p) / nu, sc[2] = <w,w> - |p|^2
+  auto dcgs_scalars = [&](int j, bool with_w) {
+    if (wid == 0) {
+      double cc = 0.0, cp = 0.0, pp = 0.0;
+      for (int i = lane; i < j; i += 32) {
+        const double c = hs1[i];
+        cc += c * c;
+        if (with_w) {
+          const double p = hs1[j + i];
+          cp += c * p;
+          pp += p * p;
+        }
+      }
+      cc = xor_sum(cc);
+      cp = xor_sum(cp);
+      pp = xor_sum(pp);
+      if (lane == 0) {
+        const int s0 = with_w ? 2 * j : j;
+        const double nu = sqrt(hs1[s0] - cc);
+        sc[0] = nu;
+        if (with_w) {
+          const double pj = (hs1[s0 + 1] - cp) / nu;
+          sc[1] = pj;
+          sc[2] = hs1[s0 + 2] - (pp + pj * pj);
+          sc[3] = hs1[s0 + 2];
+        }
+      }
+    }
+    __syncthreads();
+  };
   // ||b|| over the own unknowns, then the stopping threshold rtol ||b|| (the same bits in
   // every block)
   {
@@ -515,7 +645,90 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     for (int i = tid; i <= m; i += kThreads) g[i] = i == 0 ? beta : 0.0;
     if (!grid_sync(bar)) return;
     int k = 0;
-    for (int j = 0; j < m; j++) {
+    if (dcgs) {
+      // DCGS2 (delayed CGS2, one reduction per step): slot j of V holds the candidate u~_j,
+      // projected once and normalised; its second projection happens in step j's pass B, with
+      // the coefficients of that step's single reduction, and column j-1 of H is completed
+      // then: A P q_{j-1} = Q_j (a + t c) + t nu q_j with the pending (a, t) of step j-1.
+      double tpend = 0.0;
+      bool done = false;
+      for (int j = 0; j < m && !done; j++) {
+        elem_pass_op(a.Dinv ? a.Z : V + (size_t)j * n);  // A P u~_j
+        if (!grid_sync(bar)) return;
+        node_pass(sizeof(TR) == 4, 0, nullptr);
+        mv++;
+        dots_d(j, true);
+        if (!grid_sync(bar)) return;
+        reduce_parts(2 * j + 3, hs1);
+        dcgs_scalars(j, true);
+        const double nu = sc[0], pj = sc[1], s2 = sc[2], w2 = sc[3];
+        if (j == 0) {
+          if (tid == 0) g[0] = beta * nu;  // r = beta u~_0 = beta nu q_0
+        } else {  // complete column j-1 and rotate it
+          for (int r = tid; r <= j; r += kThreads) {
+            const double h = r < j ? pend[r] + tpend * hs1[r] : tpend * nu;
+            col[r] = h;
+            Hf[(size_t)(j - 1) * (m + 1) + r] = h;
+          }
+          __syncthreads();
+          givens(j - 1, tpend * nu);
+          total_est++;
+          __syncthreads();
+          if (s_stop) {
+            k = j;
+            break;
+          }
+        }
+        // pending column j: a = (p - H_j c) / nu (rows 0..j), t = sigma / nu
+        for (int r = tid; r <= j; r += kThreads) {
+          double hc = 0.0;
+          for (int cj = r > 0 ? r - 1 : 0; cj < j; cj++) hc += Hf[(size_t)cj * (m + 1) + r] * hs1[cj];
+          pend[r] = ((r < j ? hs1[j + r] : pj) - hc) / nu;
+        }
+        double sigma;
+        if (s2 > kPythMin * w2) {  // the same decision in every block
+          sigma = sqrt(s2);
+          pass_b(j, nu, pj, sigma);
+        } else {  // cancellation: the norm of the projected w directly
+          const double acc = block_sum(pass_b(j, nu, pj, 0.0));
+          if (tid == 0) a.part0[bid] = acc;
+          if (!grid_sync(bar)) return;
+          sigma = sqrt(sum_partials(a.part0, nb));
+          if (sigma > 0.0)
+            for (int dl = tid; dl < ns; dl += kThreads) vst(j + 1, dl, wld(dl) / sigma);
+        }
+        passes += j + 2;
+        if (!(sigma > 0.0)) {  // invariant subspace (or a non-finite norm): column j is final
+          __syncthreads();
+          for (int r = tid; r <= j; r += kThreads) col[r] = pend[r];
+          __syncthreads();
+          givens(j, 0.0);
+          total_est++;
+          k = j + 1;
+          done = true;
+          if (!grid_sync(bar)) return;
+          break;
+        }
+        tpend = sigma / nu;
+        if (a.Dinv) precond_slice(j + 1);
+        k = j + 1;
+        if (!grid_sync(bar)) return;
+      }
+      if (!done && k == m) {
+        // the cycle ran to m: complete the last column from u~_m's coefficients
+        dots_d(m, false);
+        if (!grid_sync(bar)) return;
+        reduce_parts(m + 1, hs1);
+        dcgs_scalars(m, false);
+        const double nu = sc[0];
+        for (int r = tid; r < m; r += kThreads) col[r] = pend[r] + tpend * hs1[r];
+        __syncthreads();
+        givens(m - 1, tpend * nu);
+        total_est++;
+        __syncthreads();
+      }
+    }
+    for (int j = 0; j < m && !dcgs; j++) {
       const double* xj = a.Dinv ? a.Z : V + (size_t)j * n;  // right preconditioning: A P v_j
       elem_pass_op(xj);
       if (!grid_sync(bar)) return;
@@ -666,7 +879,7 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int blocks = sms < a.max_blocks ? sms : a.max_blocks;
   const int pn = (a.n_dof / NEQ + blocks - 1) / blocks, S = pn * NEQ;
-  const bool cgs = a.orth == 0 && a.m + 2 <= kMaxBasis && a.partm != nullptr;
+  const bool cgs = (a.orth == 0 || a.orth == 2) && a.m + 2 <= kMaxBasis && a.partm != nullptr;
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, true>);
   if (e != cudaSuccess) return e;

@@ -225,7 +225,7 @@ class FDVSolver:
         self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
-    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1, orth=0):
+    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1, orth=2):
         return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)),
                      int(engine), int(precond), int(orth))
 
@@ -242,7 +242,7 @@ class FDVSolver:
                 "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
 
     def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False,
-              engine=0, precond=True, orth=0):
+              engine=0, precond=True, orth=2):
         o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
         rep, est, fin = self._report(m, restarts)
         self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
@@ -257,7 +257,7 @@ class FDVSolver:
         return r
 
     def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-             true_residual=False, engine=0, precond=True, orth=0):
+             true_residual=False, engine=0, precond=True, orth=2):
         o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()

@@ -59,7 +59,7 @@ int main(int argc, char** argv) {
     o.true_residual = 0;
     o.engine = 0;
     o.precond = 1;
-    o.orth = 0;
+    o.orth = 2;  // delayed CGS2 (one reduction per Arnoldi step)
     std::vector<double> est((size_t)o.m * o.restarts), gfin(o.restarts);
     cfdv_gmres_report rep;
     std::memset(&rep, 0, sizeof(rep));

@@ -89,8 +89,11 @@ typedef struct {
                         each node's assembled neqn x neqn diagonal block); the stopping test
                         stays the true residual of the unpreconditioned system.  0 = none */
   int orth;          /* CORRECT mode, engine 0: 0 = classical Gram-Schmidt applied twice (4 grid
-                        barriers per Arnoldi step; m <= 63), 1 = modified Gram-Schmidt as the
-                        reference's Arnoldi (MPI_GMRES.h:164-181; j+3 barriers per step j) */
+                        barriers per Arnoldi step; m <= 62), 1 = modified Gram-Schmidt as the
+                        reference's Arnoldi (MPI_GMRES.h:164-181; j+3 barriers per step j),
+                        2 = delayed CGS2: the second projection of a step's vector is taken in
+                        the next step's single reduction (3 grid barriers and two passes over
+                        the basis per step; m <= 62) */
 } cfdv_gmres_opts;
 
 typedef struct {

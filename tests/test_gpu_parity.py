@@ -175,7 +175,7 @@ def test_correct_gmres_fp64_and_mixed(gpu, oracle_lib, name):
 
 @pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-@pytest.mark.parametrize("orth", ["cgs2", "mgs"])
+@pytest.mark.parametrize("orth", ["cgs2", "mgs", "dcgs2"])
 def test_persistent_engine_matches_host_driven(gpu, name, prec, orth):
     """The single-launch cooperative solve, with either orthogonalisation, against the
     one-kernel-per-pass MGS solve: same stopping point, same solution to the tolerance."""
@@ -185,7 +185,7 @@ def test_persistent_engine_matches_host_driven(gpu, name, prec, orth):
         dt = s.cfl(float(case.control["cfl"]))
         s.form(dt, precision=gpu.PREC_MIXED)
         r0 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=0,
-                     orth=0 if orth == "cgs2" else 1)
+                     orth={"cgs2": 0, "mgs": 1, "dcgs2": 2}[orth])
         d0 = s.du()
         r1 = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=1)
         d1 = s.du()
