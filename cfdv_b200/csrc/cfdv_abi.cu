@@ -521,7 +521,6 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   std::memset(&a, 0, sizeof(a));
   a.n_dof = c->n_dof; a.n_elements = c->n_elements; a.m = m; a.max_restarts = o->restarts;
   a.max_blocks = persistent_max_blocks();
-  a.transpose = transpose ? 1 : 0;
   a.orth = o->orth;
   if (o->orth == 0 || o->orth == 2) {
     if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 128))) return rc;
@@ -531,8 +530,18 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   a.conn = c->d_conn; a.csr_ptr = c->d_csr_ptr; a.csr_idx = c->d_csr_idx;
   a.R64 = c->d_R64; a.R32 = c->d_R32; a.Y64 = c->d_Y64; a.Y32 = c->d_Y32;
   a.b = c->d_b; a.du = c->d_du; a.V = c->d_V; a.W = c->d_W; a.part0 = c->d_pa; a.part1 = c->d_pb;
+  // A^T: transpose every element block in place (restored after the launch), so the kernel's
+  // coalesced row loads stream R_e^T and the block Jacobi inverse is that of A^T
+  float* r32 = c->have32 ? c->d_R32 : nullptr;
+  if (transpose) {
+    CK(launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st));
+    c->launches += r32 ? 2 : 1;
+  }
   if (o->precond) {
-    if ((rc = build_block_jacobi(c))) return rc;
+    if ((rc = build_block_jacobi(c))) {
+      if (transpose) launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st);
+      return rc;
+    }
     a.Dinv = c->d_Dinv;
     a.Z = c->d_Z;
   }
@@ -557,6 +566,10 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
     c->ev_solve.push_back(ev);
   }
   c->launches++;
+  if (transpose) {
+    CK(launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st));
+    c->launches += r32 ? 2 : 1;
+  }
   double* hp = c->h_pin + cfdv::ctxi::kPinSolve;
   CK(cudaMemcpyAsync(hp, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(hp + 4, a.result, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));

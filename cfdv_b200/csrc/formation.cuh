@@ -42,7 +42,7 @@ struct FormTraits {
   // coefficient rows per Gauss point for the column node M: Phi_M, dPhi_M,j (j < NDIM) and,
   // in 2D, S_M = sum_j dPhi_M,j for the upwind term
   static constexpr int NCOEF = 1 + NDIM + (NDIM == 2 ? 1 : 0);
-  static constexpr int MIN_BLOCKS = (NDIM == 2) ? 8 : 5;   // resident blocks per SM (register cap)
+  static constexpr int MIN_BLOCKS = (NDIM == 2) ? 12 : 5;  // resident blocks per SM (register cap)
 };
 
 // hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)

@@ -8,8 +8,8 @@
 // |g_{j+1}| < rtol ||b|| (the stopping rule of the textbook solver), back-substitutes the
 // small triangular system and adds P V y to du.  Products use the FP64 matrices, or the
 // FP32 matrices with FP32 accumulation for the mixed form (the restart residual stays
-// FP64: GMRES-based iterative refinement).  With `transpose` every product is A^T x (the
-// adjoint system) and the node-block preconditioner is applied transposed.
+// FP64: GMRES-based iterative refinement).  The adjoint system A^T x = b runs through the same
+// kernel: the host transposes every element block in place around the launch.
 //
 // Ownership.  One 1024-thread block per SM.  Block b owns a contiguous range of whole
 // nodes; every Krylov vector entry, w, z = P v and du of those unknowns is written only by
@@ -126,7 +126,7 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
   return block_sum(v);
 }
 
-// Element pass Y_e = R_e x_e (TRANS: R_e^T x_e), thread (le, i) owning row i of element le.
+// Element pass Y_e = R_e x_e, thread (le, i) owning row i of element le.
 // 2D (L2-resident, latency-bound): the block's warps form groups of G = lcm(Ke, 32) / 32
 // warps (one warp, two elements) that each take U = 3 waves of their elements at once from
 // the block's contiguous range (the block's whole share in one chunk), synchronising only
@@ -192,7 +192,7 @@ __device__ __forceinline__ void elem_first(const int* __restrict__ conn, int E, 
   }
 }
 
-template <int KE, int NEQ, int NNOD, typename TM, bool TRANS>
+template <int KE, int NEQ, int NNOD, typename TM>
 __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* __restrict__ conn, const double* x,
                                           TM* Y, int E, const int (*first)[kThreads], TM* tiles) {
   using EG = ElemGroups<KE>;
@@ -217,7 +217,7 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
         TM acc = 0;
 #pragma unroll
         for (int j = 0; j < KE; j++)
-          acc += (TRANS ? __ldg(Re + i * KE + j) : __ldg(Re + j * KE + i)) * tb[le * KE + j];
+          acc += __ldg(Re + j * KE + i) * tb[le * KE + j];
         Y[(size_t)e * KE + i] = acc;
       }
       buf ^= 1;
@@ -258,8 +258,7 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
     for (int j = 0; j < KE; j++)
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        // TRANS: row i of R_e^T is R_e's contiguous column i (served by L1 across j)
-        const TM rv = TRANS ? __ldg(Ru[u] + i * KE + j) : __ldg(Ru[u] + j * KE + i);
+        const TM rv = __ldg(Ru[u] + j * KE + i);
         acc[u] += rv * tb[(u * EPG + le) * KE + j];
       }
 #pragma unroll
@@ -290,12 +289,11 @@ size_t persistent_dyn_doubles(int m, int S, bool resident) {
   return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kSlots);
 }
 
-template <int KE, int NEQ, int NNOD, typename TR, bool TRANS, bool RES>
+template <int KE, int NEQ, int NNOD, typename TR, bool RES>
 __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(PersistentArgs a) {
   extern __shared__ __align__(16) double dyn[];
   const int nb = gridDim.x, tid = threadIdx.x, bid = blockIdx.x, lane = tid & 31, wid = tid >> 5;
   const int n = a.n_dof, m = a.m;
-  constexpr bool tr = TRANS;
   // own unknowns [lo, lo + ns): whole nodes, S per block
   const int pn = (n / NEQ + nb - 1) / nb, S = pn * NEQ;
   const int lo = min(n, bid * S), ns = min(n, lo + S) - lo;
@@ -343,12 +341,12 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   };
 
   auto elem_pass64 = [&](const double* x) {
-    elem_pass<KE, NEQ, NNOD, double, TRANS>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
+    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
     if (sizeof(TR) == 8) elem_pass64(x);
-    else elem_pass<KE, NEQ, NNOD, TR, TRANS>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, first, tileR);
+    else elem_pass<KE, NEQ, NNOD, TR>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, first, tileR);
   };
   // node pass over the own unknowns: w = gather(Y) (mode 0) or b - gather(Y) (mode 1);
   // returns this thread's share of <w, dotv> (dotv null: ||w||^2)
@@ -377,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       const double* D = a.Dinv + (size_t)nd * NEQ * NEQ;
       double t = 0.0;
 #pragma unroll
-      for (int s = 0; s < NEQ; s++) t += D[tr ? s * NEQ + r : r * NEQ + s] * vld(i, base + s);
+      for (int s = 0; s < NEQ; s++) t += D[r * NEQ + s] * vld(i, base + s);
       a.Z[d] = t;
     }
   };
@@ -819,7 +817,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
         for (int s2 = 0; s2 < NEQ; s2++) {
           double t = 0.0;
           for (int i = 0; i < k; i++) t += y[i] * vld(i, base + s2);
-          acc += a.Dinv[(size_t)nd * NEQ * NEQ + (tr ? s2 * NEQ + r : r * NEQ + s2)] * t;
+          acc += a.Dinv[(size_t)nd * NEQ * NEQ + r * NEQ + s2] * t;
         }
         a.du[d] += acc;
       } else {
@@ -856,9 +854,9 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
 
 namespace {
 
-template <int KE, int NEQ, int NNOD, typename TR, bool TRANS, bool RES>
+template <int KE, int NEQ, int NNOD, typename TR, bool RES>
 cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, cudaStream_t st) {
-  auto* k = gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, RES>;
+  auto* k = gmres_persistent_kernel<KE, NEQ, NNOD, TR, RES>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_bytes);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -871,7 +869,7 @@ cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, cu
 }
 
 // resident basis when the block's share of it fits next to the static arrays
-template <int KE, int NEQ, int NNOD, typename TR, bool TRANS>
+template <int KE, int NEQ, int NNOD, typename TR>
 cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   int dev = 0, sms = 0, optin = 0;
   cudaGetDevice(&dev);
@@ -881,28 +879,27 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   const int pn = (a.n_dof / NEQ + blocks - 1) / blocks, S = pn * NEQ;
   const bool cgs = (a.orth == 0 || a.orth == 2) && a.m + 2 <= kMaxBasis && a.partm != nullptr;
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, true>);
+  cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, true>);
   if (e != cudaSuccess) return e;
   const size_t res_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, true);
   if (cgs && fa.sharedSizeBytes + res_bytes <= (size_t)optin)
-    return launch_cfg<KE, NEQ, NNOD, TR, TRANS, true>(a, blocks, res_bytes, st);
-  e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, TRANS, false>);
+    return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes, st);
+  e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, false>);
   if (e != cudaSuccess) return e;
   const size_t str_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, false);
   if (fa.sharedSizeBytes + str_bytes > (size_t)optin) return cudaErrorInvalidValue;  // m too large
-  return launch_cfg<KE, NEQ, NNOD, TR, TRANS, false>(a, blocks, str_bytes, st);
+  return launch_cfg<KE, NEQ, NNOD, TR, false>(a, blocks, str_bytes, st);
 }
 
-template <bool TRANS>
 cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
-  if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float, TRANS>(a, st) : launch_one<16, 4, 4, double, TRANS>(a, st);
-  return fp32 ? launch_one<40, 5, 8, float, TRANS>(a, st) : launch_one<40, 5, 8, double, TRANS>(a, st);
+  if (ndim == 2) return fp32 ? launch_one<16, 4, 4, float>(a, st) : launch_one<16, 4, 4, double>(a, st);
+  return fp32 ? launch_one<40, 5, 8, float>(a, st) : launch_one<40, 5, 8, double>(a, st);
 }
 
 }  // namespace
 
 cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {
-  return a.transpose ? launch_dim<true>(ndim, fp32, a, st) : launch_dim<false>(ndim, fp32, a, st);
+  return launch_dim(ndim, fp32, a, st);
 }
 
 int persistent_max_blocks() { return kRedBlocks; }

@@ -6,7 +6,6 @@ namespace cfdv {
 
 struct PersistentArgs {
   int n_dof, n_elements, m, max_restarts, max_blocks;
-  int transpose;               // 1: solve A^T x = b (products with R_e^T, preconditioner transposed)
   int orth;                    // 0: classical Gram-Schmidt twice (CGS2), 1: modified Gram-Schmidt
   double* partm;               // CGS2 multi-dot partials [gridDim.x][m+1]
   double rtol;                 // stop when ||b - A du|| < rtol ||b|| (true residual, FP64 matrices)

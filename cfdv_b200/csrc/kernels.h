@@ -106,6 +106,8 @@ cudaError_t launch_reduce(const double* pin, double* out, int do_sqrt, cudaStrea
 cudaError_t launch_combine(double* x, const double* V, int n, const double* y, int m, cudaStream_t st);
 // out[i] = (float) in[i]
 cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t st);
+// transpose every element block of R64 and R32 (either may be null) in place; ke = 16 or 40
+cudaError_t launch_transpose_blocks(int ke, double* R64, float* R32, int E, cudaStream_t st);
 // node-block Jacobi: Dinv_n = (sum of the node's diagonal element blocks)^-1, FP64
 cudaError_t launch_block_jacobi(int ndim, const int* ptr, const int* idx, const double* R, int n_nodes, double* Dinv,
                                 int* status, cudaStream_t st);

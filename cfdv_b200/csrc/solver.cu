@@ -190,6 +190,37 @@ __global__ void __launch_bounds__(kRedThreads) rms_partial_kernel(const double* 
   }
 }
 
+// In-place transpose of every element's Ke x Ke block (entry (r, c) at c*Ke + r becomes
+// entry (c, r)): the adjoint solve then streams R_e^T with the same coalesced row loads as the
+// forward solve.  One block per element at a time; the block is staged in shared memory with
+// a padded row stride.
+template <int KE, typename T>
+__global__ void __launch_bounds__(256) transpose_blocks_kernel(T* R, int E) {
+  __shared__ T tile[KE * (KE + 1)];
+  for (int e = blockIdx.x; e < E; e += gridDim.x) {
+    T* M = R + (size_t)e * KE * KE;
+    for (int k = threadIdx.x; k < KE * KE; k += blockDim.x) tile[(k / KE) * (KE + 1) + k % KE] = M[k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < KE * KE; k += blockDim.x) M[k] = tile[(k % KE) * (KE + 1) + k / KE];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_transpose_blocks(int ke, double* R64, float* R32, int E, cudaStream_t st) {
+  const int grid = E < 16 * kRedBlocks ? E : 16 * kRedBlocks;
+  if (E <= 0) return cudaSuccess;
+  if (ke == 16) {
+    if (R64) transpose_blocks_kernel<16, double><<<grid, 256, 0, st>>>(R64, E);
+    if (R32) transpose_blocks_kernel<16, float><<<grid, 256, 0, st>>>(R32, E);
+  } else if (ke == 40) {
+    if (R64) transpose_blocks_kernel<40, double><<<grid, 256, 0, st>>>(R64, E);
+    if (R32) transpose_blocks_kernel<40, float><<<grid, 256, 0, st>>>(R32, E);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 __global__ void to_float_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     out[i] = (float)in[i];
