@@ -9,6 +9,7 @@
 //   TecplotOut   tecplot_<iter>.plt      (Utility/IO/MPI_TecplotOut.h:186-373)
 //   RmsLog       RMSError.txt            (FDV/Function/MPI_RMSError.h:56-75)
 //   save_case    <iter>/ checkpoints     (MPIBinaryConfiguration.h:148-161, SaveBinary.h)
+//   EnsightSeries EnSight Gold output    (new: the reference's EnsightOut.h:9-13 is a stub)
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -281,6 +282,109 @@ inline void save_case(const std::string& dir, int iter, const BinaryCase& c, con
   b << "elemin, elemax, nodemin, nodemax, nedgenode_l, nedgenode_r, NodeIteratorMin, NodeIteratorMax\n";
   b << "0 " << c.n_elements << " 0 " << c.n_nodes - 1 << " 0 0 0 " << c.n_nodes - 1 << "\n";
 }
+
+// EnSight Gold ASCII time series (the reference's EnsightOut.h:9-13 is an empty stub): one
+// geometry file (one part, quad4 or hexa8, z = 0 in 2D), per output step the node
+// variables rho, velocity (3 components), T and p from NodeUnpack of U and the element
+// variables s1..s4, and a case file listing every step written so far.
+//   <dir>/cfdv.case, <dir>/cfdv.geo, <dir>/cfdv.<var>.<00000..>
+class EnsightSeries {
+ public:
+  EnsightSeries(const std::string& dir, const BinaryCase& c) : dir_(dir), c_(c) {
+    if (std::system(("mkdir -p '" + dir_ + "'").c_str()) != 0) throw std::runtime_error("cannot create " + dir_);
+    std::ofstream g((dir_ + "/cfdv.geo").c_str());
+    if (!g) throw std::runtime_error("cannot write " + dir_ + "/cfdv.geo");
+    g << "CFDV FDV solution\n" << c.ndim << "D unstructured mesh\n";
+    g << "node id off\nelement id off\n";
+    g << "part\n" << std::setw(10) << 1 << "\nflow field\ncoordinates\n" << std::setw(10) << c.n_nodes << "\n";
+    g << std::scientific << std::setprecision(5);
+    for (int k = 0; k < 3; k++)
+      for (int n = 0; n < c.n_nodes; n++) g << std::setw(12) << (k < c.ndim ? c.x[(size_t)n * c.ndim + k] : 0.0) << "\n";
+    g << element_type() << "\n" << std::setw(10) << c.n_elements << "\n";
+    for (int e = 0; e < c.n_elements; e++) {
+      for (int k = 0; k < c.nnod; k++) g << std::setw(10) << c.conn[(size_t)e * c.nnod + k] + 1;
+      g << "\n";
+    }
+  }
+
+  void write(double time, const cfdv_params& p, const std::vector<double>& U, const std::vector<double>* s) {
+    const int nd = c_.ndim, ne = nd + 2, Nn = c_.n_nodes, step = (int)times_.size();
+    const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
+    std::vector<double> rho(Nn), T(Nn), pr(Nn), v((size_t)Nn * 3, 0.0);
+    for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:185-205
+      const double* u = &U[(size_t)n * ne];
+      rho[n] = u[0];
+      double vsqr = 0;
+      for (int i = 0; i < nd; i++) {
+        v[(size_t)i * Nn + n] = u[1 + i] / u[0];
+        vsqr += v[(size_t)i * Nn + n] * v[(size_t)i * Nn + n];
+      }
+      const double e = u[nd + 1] / u[0] - 0.5 * vsqr;
+      T[n] = e / Cv;
+      pr[n] = rho[n] * (p.gamma - 1.0) * e;
+    }
+    node_var("rho", step, rho);
+    node_var("velocity", step, v);
+    node_var("T", step, T);
+    node_var("p", step, pr);
+    if (s) {
+      has_s_ = true;
+      for (int k = 0; k < 4; k++) {
+        std::vector<double> sk(c_.n_elements);
+        for (int e = 0; e < c_.n_elements; e++) sk[e] = (*s)[(size_t)e * 4 + k];
+        element_var("s" + std::to_string(k + 1), step, sk);
+      }
+    }
+    times_.push_back(time);
+    write_case();
+  }
+
+  static std::string var_file(const std::string& var, int step) {
+    std::ostringstream f;
+    f << "cfdv." << var << "." << std::setw(5) << std::setfill('0') << step;
+    return f.str();
+  }
+
+ private:
+  const char* element_type() const { return c_.ndim == 2 ? "quad4" : "hexa8"; }
+
+  // scalar (values.size() == n_nodes) or 3-component vector (component-major)
+  void node_var(const std::string& var, int step, const std::vector<double>& values) {
+    std::ofstream f((dir_ + "/" + var_file(var, step)).c_str());
+    if (!f) throw std::runtime_error("cannot write " + dir_ + "/" + var_file(var, step));
+    f << var << " at step " << step << "\npart\n" << std::setw(10) << 1 << "\ncoordinates\n";
+    f << std::scientific << std::setprecision(5);
+    for (double x : values) f << std::setw(12) << x << "\n";
+  }
+
+  void element_var(const std::string& var, int step, const std::vector<double>& values) {
+    std::ofstream f((dir_ + "/" + var_file(var, step)).c_str());
+    if (!f) throw std::runtime_error("cannot write " + dir_ + "/" + var_file(var, step));
+    f << var << " at step " << step << "\npart\n" << std::setw(10) << 1 << "\n" << element_type() << "\n";
+    f << std::scientific << std::setprecision(5);
+    for (double x : values) f << std::setw(12) << x << "\n";
+  }
+
+  void write_case() const {
+    std::ofstream f((dir_ + "/cfdv.case").c_str());
+    f << "FORMAT\ntype: ensight gold\n\nGEOMETRY\nmodel: cfdv.geo\n\nVARIABLE\n";
+    f << "scalar per node: 1 rho cfdv.rho.*****\n";
+    f << "vector per node: 1 velocity cfdv.velocity.*****\n";
+    f << "scalar per node: 1 T cfdv.T.*****\n";
+    f << "scalar per node: 1 p cfdv.p.*****\n";
+    if (has_s_)
+      for (int k = 1; k <= 4; k++) f << "scalar per element: 1 s" << k << " cfdv.s" << k << ".*****\n";
+    f << "\nTIME\ntime set: 1\nnumber of steps: " << times_.size() << "\nfilename start number: 0\n";
+    f << "filename increment: 1\ntime values:\n";
+    f << std::scientific << std::setprecision(9);
+    for (double t : times_) f << t << "\n";
+  }
+
+  std::string dir_;
+  const BinaryCase& c_;
+  std::vector<double> times_;
+  bool has_s_ = false;
+};
 
 // one "iter\t(rms) " line per step (MPI_RMSError.h:56-69)
 inline void rms_append(const std::string& path, int iter, const std::vector<double>& rms) {

@@ -2,6 +2,7 @@
 //
 //   cfdv_gpu <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed]
 //            [--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K]
+//            [--ensight DIR]
 //
 // Reads the reference case directory (control, aero, binarynodes, binaryelements) and
 // runs, per iteration, the reference's call order: CFL (main.cpp:179), Tecplot output
@@ -14,6 +15,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -23,11 +25,11 @@ int main(int argc, char** argv) {
   if (argc < 2) {
     std::fprintf(stderr,
                  "usage: %s <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed] "
-                 "[--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K]\n",
+                 "[--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K] [--ensight DIR]\n",
                  argv[0]);
     return 2;
   }
-  std::string dir = argv[1], out = ".";
+  std::string dir = argv[1], out = ".", ensight_dir;
   int steps = -1, restarts = -1, phys = 0, save_every = 1000;
   int mode = CFDV_GMRES_REFERENCE, precision = CFDV_PREC_FP64;
   double rtol = 1e-8;
@@ -41,6 +43,7 @@ int main(int argc, char** argv) {
     else if (a == "--physical-3d-flux") phys = 1;
     else if (a == "--out" && i + 1 < argc) out = argv[++i];
     else if (a == "--save-every" && i + 1 < argc) save_every = std::atoi(argv[++i]);
+    else if (a == "--ensight" && i + 1 < argc) ensight_dir = argv[++i];
   }
   try {
     cfdv_host::CaseConfig cfg(dir);
@@ -68,6 +71,8 @@ int main(int argc, char** argv) {
     rep.gfinal = gfin.data();
     rep.gfinal_capacity = (int)gfin.size();
     double t = 0;
+    std::unique_ptr<cfdv_host::EnsightSeries> ensight;
+    if (!ensight_dir.empty()) ensight.reset(new cfdv_host::EnsightSeries(ensight_dir, c));
     auto t0 = std::chrono::steady_clock::now();
     for (int iter = iter0; iter < itermax; iter++) {
       if (save_every > 0 && iter % save_every == 0) cfdv_host::save_case(out, iter, c, cfg, p, fdv.state());
@@ -76,6 +81,7 @@ int main(int argc, char** argv) {
       if (iter % 100 == 0) {  // written from this step's state, before the solve
         std::vector<double> U = fdv.state(), s = fdv.fdv_params();
         cfdv_host::tecplot_write(out + "/" + cfdv_host::tecplot_name(iter), c, p, U, &s, t);
+        if (ensight) ensight->write(t, p, U, &s);
       }
       fdv.iterate(o, &rep);
       fdv.update();

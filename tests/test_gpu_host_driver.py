@@ -63,3 +63,27 @@ def test_driver_checkpoint_restart(name):
     assert int(full.control["iter"]) == 6 and int(resumed.control["iter"]) == 6
     scale = np.abs(full.nodes).max(axis=0)
     assert (np.abs(resumed.nodes - full.nodes).max(axis=0) <= 1e-10 * scale + 1e-14).all()
+
+
+@pytest.mark.parametrize("name", ["lid8", "ramp4"])
+def test_driver_ensight_series(name):
+    """--ensight writes an EnSight Gold series beside the Tecplot files (every 100th
+    iteration): geometry once, one set of variable files per output step, and the case file's
+    time values are the simulation times of those steps."""
+    from cfdv_b200 import meshgen as mg
+    case = get_case(name)
+    with tempfile.TemporaryDirectory() as d:
+        cdir = os.path.join(d, "case")
+        mg.write_case(case, cdir)
+        out, ens = os.path.join(d, "out"), os.path.join(d, "ens")
+        os.makedirs(out)
+        subprocess.run([DRIVER, cdir, "--steps", "101", "--mode", "correct", "--out", out, "--ensight", ens,
+                        "--save-every", "0"], check=True, capture_output=True)
+        files = sorted(os.listdir(ens))
+        with open(os.path.join(ens, "cfdv.case")) as f:
+            text = f.read()
+    assert "cfdv.geo" in files and "cfdv.case" in files
+    for var in ("rho", "velocity", "T", "p", "s1", "s2", "s3", "s4"):
+        assert f"cfdv.{var}.00000" in files and f"cfdv.{var}.00001" in files
+    times = [float(v) for v in text.split("time values:\n")[1].split()]
+    assert len(times) == 2 and times[0] == 0.0 and times[1] > 0.0
