@@ -39,6 +39,11 @@ class Case:
     elements: np.ndarray  # (E, nnod+nface) int32: node ids then bc codes
     control: dict = field(default_factory=dict)
     aero: dict = field(default_factory=dict)
+    # adaptive (hanging-node) elements: ids, refine levels and Hnm[N, M] (nnod x nnod), as the
+    # reference's "adap" file holds them (LoadBinary.h:246-260, Element.h:39-40)
+    adap_elements: np.ndarray | None = None
+    adap_levels: np.ndarray | None = None
+    adap_hnm: np.ndarray | None = None
 
     @property
     def nnod(self) -> int:
@@ -67,6 +72,13 @@ class Case:
     @property
     def bc(self) -> np.ndarray:
         return self.elements[:, self.nnod:]
+
+    def hnm_index(self) -> np.ndarray:
+        """Per element the row of ``adap_hnm`` that applies, -1 for a plain element."""
+        idx = np.full(self.n_elements, -1, dtype=np.int32)
+        if self.adap_elements is not None:
+            idx[self.adap_elements] = np.arange(len(self.adap_elements), dtype=np.int32)
+        return idx
 
 
 def _control(ndim, Nn, E, cfl, m, restart=1, itermax=1000):
@@ -337,6 +349,44 @@ SMALL = {
 }
 
 
+def with_adaptive(case: Case, elements, hnm, levels=None) -> Case:
+    """A copy of ``case`` whose ``elements`` carry the hanging-node matrices ``hnm``
+    ((n, nnod, nnod), Hnm[N, M]); written with control adap = 1 and an "adap" file."""
+    import copy
+    c = copy.copy(case)
+    c.control = dict(case.control)
+    c.control["adap"] = 1
+    c.adap_elements = np.asarray(elements, dtype=np.int32)
+    c.adap_hnm = np.asarray(hnm, dtype=np.float64).reshape(len(c.adap_elements), case.nnod, case.nnod)
+    c.adap_levels = np.ones(len(c.adap_elements), dtype=np.int32) if levels is None else np.asarray(levels, np.int32)
+    c.name = case.name + "_adap"
+    return c
+
+
+def adaptive_demo(case: Case) -> Case:
+    """Every third element of ``case`` (boundary elements included) made adaptive with a
+    hanging-node style Hnm: the identity with one or two local nodes moved to the midpoint
+    of an edge they share with a neighbour, or a quarter of the way along it (rows of Hnm
+    sum to one, so the shape functions keep the partition of unity and the element stays
+    valid).  Entries are exact in six significant digits, the precision at which the
+    reference writes and reads them."""
+    nnod = case.nnod
+    edges = [(0, 1), (1, 2), (2, 3), (3, 0)] if case.ndim == 2 else [(0, 1), (1, 2), (2, 3), (3, 0), (4, 5), (5, 6)]
+    els, hs = [], []
+    for k, e in enumerate(range(0, case.n_elements, 3)):
+        H = np.eye(nnod)
+        a, b = edges[k % len(edges)]
+        H[a, a], H[a, b] = 0.5, 0.5  # local node a at the midpoint of edge a-b
+        if k % 2:
+            c, d = edges[(k + 2) % len(edges)]
+            if c not in (a, b):
+                H[c] = 0.0
+                H[c, c], H[c, d] = 0.75, 0.25
+        els.append(e)
+        hs.append(H)
+    return with_adaptive(case, els, hs)
+
+
 def write_case(case: Case, path: str) -> str:
     """Write ``case`` as a reference case directory at ``path`` (created if needed)."""
     os.makedirs(path, exist_ok=True)
@@ -345,6 +395,14 @@ def write_case(case: Case, path: str) -> str:
     with open(os.path.join(path, "control"), "w") as f:
         for k, v in case.control.items():
             f.write(f"{k} = {v}\n")
+    if case.adap_elements is not None:
+        # "elno adap refine_level" then the Tensor serialisation (TensorStream.h:95-145): type,
+        # ndim, extents, the storage in index order N + nnod*M
+        nnod = case.nnod
+        with open(os.path.join(path, "adap"), "w") as f:
+            for e, lev, H in zip(case.adap_elements, case.adap_levels, case.adap_hnm):
+                vals = " ".join(repr(float(v)) for v in H.T.ravel())
+                f.write(f"{int(e)} 1 {int(lev)} double 2 {nnod} {nnod} {vals}\n")
     with open(os.path.join(path, "aero"), "w") as f:
         for k, v in case.aero.items():
             f.write(f"{k} = {v}\n")
@@ -376,5 +434,25 @@ def read_case(path: str) -> Case:
     E = int(control["elements"])
     nodes = np.fromfile(os.path.join(path, "binarynodes"), dtype="<f8").reshape(-1, 2 * ndim + 2)[:Nn]
     el = np.fromfile(os.path.join(path, "binaryelements"), dtype="<i4").reshape(-1, nnod + nface)[:E]
-    return Case(os.path.basename(os.path.normpath(path)), ndim, np.ascontiguousarray(nodes),
+    case = Case(os.path.basename(os.path.normpath(path)), ndim, np.ascontiguousarray(nodes),
                 np.ascontiguousarray(el), control, aero)
+    adap = os.path.join(path, "adap")
+    if control.get("adap", "0").strip().lower() in ("1", "true") and os.path.exists(adap):
+        els, levs, hs = [], [], []
+        with open(adap) as f:
+            for line in f:
+                t = line.split()
+                if not t:
+                    continue
+                ni, nj = int(t[5]), int(t[6])
+                vals = np.array([float(v) for v in t[7:7 + ni * nj]])
+                if int(t[1]) == 0:
+                    continue
+                els.append(int(t[0]))
+                levs.append(int(t[2]))
+                hs.append(vals.reshape(nj, ni).T)  # storage N + ni*M -> H[N, M]
+        if els:
+            case.adap_elements = np.array(els, dtype=np.int32)
+            case.adap_levels = np.array(levs, dtype=np.int32)
+            case.adap_hnm = np.array(hs)
+    return case

@@ -586,6 +586,7 @@ struct ElemCtx {
   double dt, dtsq_2, s1, s2, s3, s4;
   int phys3d;
   NodeState* nd[8];
+  const double* H;  // Hnm of an adaptive element (Hnm(N, M) at N + nnod*M) or null
   double* R;    // column-major Ke x Ke
   double* rhs;
   double gz[2], gw[2];
@@ -612,17 +613,30 @@ void node_flux(const ElemCtx& c, const FlowPt& f, NodeState* const* nd, int nn, 
   }
 }
 
+// MeshRefine2D.h:877-900 (adap): Phi_M <- sum_N Phi_N Hnm(N, M), dPxi(M, j) likewise, for
+// the shape functions of an adaptive element before its Jacobian
+void hnm_transform(const double* H, int nnod, int ndim, double* Phi, double dPxi[][3]) {
+  double P[8] = {0, 0, 0, 0, 0, 0, 0, 0}, D[8][3] = {};
+  for (int N = 0; N < nnod; N++)
+    for (int M = 0; M < nnod; M++) {
+      P[M] += Phi[N] * H[N + nnod * M];
+      for (int j = 0; j < ndim; j++) D[M][j] += dPxi[N][j] * H[N + nnod * M];
+    }
+  for (int M = 0; M < nnod; M++) {
+    Phi[M] = P[M];
+    for (int j = 0; j < ndim; j++) dPxi[M][j] = D[M][j];
+  }
+}
+
 // FDVGalerkin.h:157-451 (domain integral at one Gauss point)
 void domain(ElemCtx& c, const double* w, const double* zeta) {
   const int ndim = c.ndim, nnod = c.nnod, neqn = c.neqn;
   double Phi[8], dPxi[8][3], dPhi[8][3], J, jac[3][3];
-  if (ndim == 2) {
-    shape2(zeta, Phi, dPxi);
-    J = jac2(dPxi, c.nd, jac, dPhi);
-  } else {
-    shape3(zeta, Phi, dPxi);
-    J = jac3(dPxi, c.nd, dPhi);
-  }
+  if (ndim == 2) shape2(zeta, Phi, dPxi);
+  else shape3(zeta, Phi, dPxi);
+  if (c.H) hnm_transform(c.H, nnod, ndim, Phi, dPxi);  // FDVGalerkin.h:183-186, 198-201
+  if (ndim == 2) J = jac2(dPxi, c.nd, jac, dPhi);
+  else J = jac3(dPxi, c.nd, dPhi);
   FlowPt f;
   gp_sum(*c.g, ndim, neqn, nnod, c.nd, Phi, dPhi, f);
   tau_calc(ndim, f);
@@ -630,12 +644,21 @@ void domain(ElemCtx& c, const double* w, const double* zeta) {
   double Psi[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double tau = 0;
   if (ndim == 2) {  // FDVGalerkin.h:225-332 streamline-upwind diffusion (2D only)
-    double J_xi = std::pow(jac[0][0], 2) + std::pow(jac[1][0], 2);
-    double J_eta = std::pow(jac[0][1], 2) + std::pow(jac[1][1], 2);
+    // its Jacobian comes from the untransformed shape functions (FDVGalerkin.h:235-239), which
+    // differs from jac for an adaptive element
+    double (*sj)[3] = jac, jp[3][3];
+    if (c.H) {
+      double pph[8], pdx[8][3], pdp[8][3];
+      shape2(zeta, pph, pdx);
+      jac2(pdx, c.nd, jp, pdp);
+      sj = jp;
+    }
+    double J_xi = std::pow(sj[0][0], 2) + std::pow(sj[1][0], 2);
+    double J_eta = std::pow(sj[0][1], 2) + std::pow(sj[1][1], 2);
     double e_xi[2], e_eta[2];
     for (int i = 0; i < 2; i++) {
-      e_xi[i] = 1. / std::pow(J_xi, 0.5) * jac[i][0];
-      e_eta[i] = 1. / std::pow(J_eta, 0.5) * jac[i][1];
+      e_xi[i] = 1. / std::pow(J_xi, 0.5) * sj[i][0];
+      e_eta[i] = 1. / std::pow(J_eta, 0.5) * sj[i][1];
     }
     double v_xi = 0, v_eta = 0, S = 0;
     for (int i = 0; i < 2; i++) v_xi += f.v[i] * e_xi[i];
@@ -926,10 +949,23 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
     phib[1] = 0.25 * (1 + zeta[0]) * (1 - zeta[1]);
     phib[2] = 0.25 * (1 + zeta[0]) * (1 + zeta[1]);
     phib[3] = 0.25 * (1 - zeta[0]) * (1 + zeta[1]);
+    // face node positions; for an adaptive element the rows of Hnm x of the face's nodes
+    // (calc_TF_norm3D.h:25-57: allnode(N) = sum_M Hnm(N, M) x_M)
+    double nodeloc[4][3];
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) nodeloc[j][k] = nd[j]->x[k];
+    if (c.H) {
+      for (int j = 0; j < 4; j++) {
+        double an[3] = {0, 0, 0};
+        for (int M = 0; M < c.nnod; M++)
+          for (int k = 0; k < 3; k++) an[k] += c.H[fn[j] + c.nnod * M] * c.nd[M]->x[k];
+        for (int k = 0; k < 3; k++) nodeloc[j][k] = an[k];
+      }
+    }
     double Lam[3], Mu[3];
     for (int i = 0; i < 3; i++) {
-      Lam[i] = nd[1]->x[i] - nd[0]->x[i];
-      Mu[i] = nd[3]->x[i] - nd[0]->x[i];
+      Lam[i] = nodeloc[1][i] - nodeloc[0][i];
+      Mu[i] = nodeloc[3][i] - nodeloc[0][i];
     }
     for (int j = 0; j < 3; j++) {  // magnitude recomputed after each component
       Lam[j] /= std::sqrt(0 + Lam[0] * Lam[0] + Lam[1] * Lam[1] + Lam[2] * Lam[2]);
@@ -949,7 +985,7 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
     double dxdxi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
     for (int N = 0; N < 4; N++)
       for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 2; j++) dxdxi[i][j] += dpxi[N][j] * nd[N]->x[i];
+        for (int j = 0; j < 2; j++) dxdxi[i][j] += dpxi[N][j] * nodeloc[N][i];
     double tr[2][2] = {{0, 0}, {0, 0}};
     for (int i = 0; i < 2; i++)
       for (int j = 0; j < 2; j++)
@@ -965,6 +1001,12 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
       for (int N = 0; N < 4; N++)
         for (int j = 0; j < 2; j++) dpidx[N][i] += T[j][i] * dpdx[N][j];
       en[i] = enorm[i] * w[0] * w[1] * detjac;
+    }
+    if (c.H) {  // FDVGalerkin.h:488-497, MeshRefine2D.h:904-951 (adap_face): phib only
+      double pt[4] = {0, 0, 0, 0};
+      for (int N = 0; N < 4; N++)
+        for (int M = 0; M < 4; M++) pt[M] += phib[N] * c.H[fn[N] + c.nnod * fn[M]];
+      for (int M = 0; M < 4; M++) phib[M] = pt[M];
     }
   }
   FlowPt f;
@@ -1238,6 +1280,8 @@ void oracle_form(const oracle_mesh* m, const oracle_aero* a, const double* U, do
   double sv[4] = {0, 0, 0, 0};
   for (int e = 0; e < m->n_elements; e++) {
     for (int N = 0; N < nnod; N++) c.nd[N] = &ns[m->conn[(size_t)e * nnod + N]];
+    const int hi = m->hnm_idx ? m->hnm_idx[e] : -1;
+    c.H = (hi >= 0 && m->hnm) ? m->hnm + (size_t)hi * nnod * nnod : nullptr;
     c.R = R + (size_t)e * Ke * Ke;
     c.rhs = rhs + (size_t)e * Ke;
     std::fill(c.R, c.R + (size_t)Ke * Ke, 0.0);

@@ -24,6 +24,11 @@ typedef struct {
   const double* x;   /* [Nn][ndim] */
   const int* conn;   /* [E][nnod]  */
   const int* bc;     /* [E][nface] */
+  /* adaptive (hanging-node) elements (Element.h:39-40, LoadBinary.h:246-260): hnm_idx[e] is
+   * the row of hnm that applies to element e, -1 for a plain element (both may be null);
+   * hnm[k] holds Hnm(N, M) at N + nnod*M */
+  const int* hnm_idx;
+  const double* hnm;
 } oracle_mesh;
 
 typedef struct {

@@ -60,7 +60,8 @@ def lib():
 class _Mesh(C.Structure):
     _fields_ = [("ndim", C.c_int), ("nnod", C.c_int), ("neqn", C.c_int), ("nbnod", C.c_int),
                 ("nface", C.c_int), ("n_nodes", C.c_int), ("n_elements", C.c_int),
-                ("x", C.c_void_p), ("conn", C.c_void_p), ("bc", C.c_void_p)]
+                ("x", C.c_void_p), ("conn", C.c_void_p), ("bc", C.c_void_p),
+                ("hnm_idx", C.c_void_p), ("hnm", C.c_void_p)]
 
 
 class _Aero(C.Structure):
@@ -89,9 +90,15 @@ class Oracle:
         self._x = np.ascontiguousarray(case.nodes[:, :nd], dtype=np.float64)
         self._conn = np.ascontiguousarray(case.conn, dtype=np.int32)
         self._bc = np.ascontiguousarray(case.bc, dtype=np.int32)
+        # adaptive elements: Hnm(N, M) stored at N + nnod*M, as the reference's Tensor
+        adaptive = getattr(case, "adap_elements", None) is not None
+        self._hidx = np.ascontiguousarray(case.hnm_index(), dtype=np.int32) if adaptive else None
+        self._hnm = (np.ascontiguousarray(np.transpose(case.adap_hnm, (0, 2, 1)), dtype=np.float64)
+                     if adaptive else None)
         self.mesh = _Mesh(nd, self.nnod, self.neqn, 2 if nd == 2 else 4, 4 if nd == 2 else 6,
                           case.n_nodes, case.n_elements, _p(self._x).value, _p(self._conn).value,
-                          _p(self._bc).value)
+                          _p(self._bc).value, _p(self._hidx).value if adaptive else None,
+                          _p(self._hnm).value if adaptive else None)
         a = case.aero
         self.aero = _Aero(float(a["gamma"]), float(a["M"]), float(a["Re"]), float(a["Pr"]), float(a["Tinf"]),
                           float(a["Twall"]), int(float(a["Adiabatic"])))

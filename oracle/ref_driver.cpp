@@ -141,6 +141,7 @@ int main(int argc, char** argv) {
   LoadBinaryData load(elements, nodes, path, nnod, neqn, ndim, nbnod);
   load.read_nodes(0, Nn - 1);
   load.read_elements(0, E);
+  if (geti(cm, "adap", 0)) load.read_adap();  // MPIBinaryConfiguration.h:110-113: hanging-node Hnm
   CalcLength<Element*> cl(ndim, nnod);  // main.cpp:120-121
   for_each(elements.begin(), elements.end(), std::ref(cl));
   NavierStokes* NS = (ndim == 2) ? (NavierStokes*)new NavierStokes2D : (NavierStokes*)new NavierStokes3D;

@@ -12,6 +12,7 @@ if ROOT not in sys.path:
 from cfdv_b200 import meshgen as mg  # noqa: E402
 
 SMALL_CASES = ["lid8", "plate20", "ramp4", "cyl4", "duct4"]
+ADAPTIVE_CASES = ["lid8_adap", "plate20_adap", "ramp4_adap", "cyl4_adap"]  # every third element with an Hnm
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
@@ -23,8 +24,13 @@ _cases = {}
 
 
 def get_case(name):
+    """A small synthetic case; "<name>_adap" is the case with every third element adaptive
+    (meshgen.adaptive_demo: hanging-node Hnm matrices)."""
     if name not in _cases:
-        _cases[name] = mg.SMALL[name]()
+        if name.endswith("_adap"):
+            _cases[name] = mg.adaptive_demo(get_case(name[: -len("_adap")]))
+        else:
+            _cases[name] = mg.SMALL[name]()
     return _cases[name]
 
 

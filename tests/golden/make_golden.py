@@ -22,13 +22,25 @@ sys.path.insert(0, ROOT)
 from cfdv_b200 import meshgen as mg  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-STEPS = {"lid8": 3, "plate20": 3, "ramp4": 2, "cyl4": 2, "duct4": 2}
+STEPS = {"lid8": 3, "plate20": 3, "ramp4": 2, "cyl4": 2, "duct4": 2,
+         # the same cases with every third element adaptive (meshgen.adaptive_demo), read by the
+         # reference from its "adap" file (control adap = 1)
+         "lid8_adap": 3, "plate20_adap": 2, "ramp4_adap": 2, "cyl4_adap": 2}
+
+
+def make_case(name):
+    if name.endswith("_adap"):
+        return mg.adaptive_demo(mg.SMALL[name[: -len("_adap")]]())
+    return mg.SMALL[name]()
 
 
 def case_digest(case):
     h = hashlib.sha256()
     h.update(case.nodes.astype("<f8").tobytes())
     h.update(case.elements.astype("<i4").tobytes())
+    if case.adap_elements is not None:
+        h.update(case.adap_elements.astype("<i4").tobytes())
+        h.update(case.adap_hnm.astype("<f8").tobytes())
     return h.hexdigest()
 
 
@@ -43,7 +55,7 @@ def sample_elements(case, k=12):
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     for name, steps in STEPS.items():
-        case = mg.SMALL[name]()
+        case = make_case(name)
         with tempfile.TemporaryDirectory() as d:
             mg.write_case(case, d)
             rec = O.run_reference(d, os.path.join(d, "out.rec"), steps=steps, dump_step=0)
@@ -53,7 +65,9 @@ def main():
         Ke = case.nnod * case.neqn
         R = rec["R_bc"].reshape(case.n_elements, Ke, Ke)
         rhs = rec["rhs_bc"].reshape(case.n_elements, Ke)
-        el = np.arange(case.n_elements) if name == "lid8" else sample_elements(case)
+        el = np.arange(case.n_elements) if name.startswith("lid8") else sample_elements(case)
+        if case.adap_elements is not None:  # add adaptive elements to the sample
+            el = np.union1d(el, case.adap_elements[: 24]).astype(np.int64)
         out["elements"] = el
         out["R_bc"] = R[el]
         out["rhs_bc"] = rhs[el]

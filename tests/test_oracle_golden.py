@@ -3,16 +3,16 @@ itself (tests/golden/*.npz, written by tests/golden/make_golden.py from oracle/_
 import numpy as np
 import pytest
 
-from conftest import SMALL_CASES, get_case, golden, rel_err, elem_rel_err
+from conftest import ADAPTIVE_CASES, SMALL_CASES, get_case, golden, rel_err, elem_rel_err
 from golden.make_golden import case_digest
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ADAPTIVE_CASES)
 def test_case_inputs_match_fixture(name):
     assert str(golden(name)["digest"]) == case_digest(get_case(name))
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ADAPTIVE_CASES)
 def test_setup_matches_reference(name, oracle_lib):
     g, case = golden(name), get_case(name)
     o = oracle_lib.Oracle(case)
@@ -24,7 +24,7 @@ def test_setup_matches_reference(name, oracle_lib):
     assert o.cfl(U, float(case.control["cfl"])) == g["dt@0"][0]
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ADAPTIVE_CASES)
 def test_formation_matches_reference(name, oracle_lib):
     g, case = golden(name), get_case(name)
     o = oracle_lib.Oracle(case)
@@ -35,7 +35,7 @@ def test_formation_matches_reference(name, oracle_lib):
     assert rel_err(rhs[el], g["rhs_bc"]) <= 1e-15
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ADAPTIVE_CASES)
 def test_reference_steps_match(name, oracle_lib):
     g, case = golden(name), get_case(name)
     o = oracle_lib.Oracle(case)
