@@ -142,6 +142,7 @@ FunctionalArgs functional_args(cfdv_ctx* c, double dt) {
   a.n_elements = c->n_elements;
   a.physical_3d_flux = c->phys3d;
   a.U = c->d_U; a.x = c->d_x; a.conn = c->d_conn; a.bc = c->d_bc; a.rowmask = c->d_mask;
+  a.hnm_idx = c->d_hnm_idx; a.hnm = c->d_hnm;
   return a;
 }
 
@@ -243,6 +244,7 @@ int wall_force_device(cfdv_ctx* c, int wall_bc, double* F, double* d_gradU, doub
   a.wall_bc = wall_bc;
   a.elems = c->d_wall_elems;
   a.U = c->d_U; a.x = c->d_x; a.conn = c->d_conn; a.bc = c->d_bc;
+  a.hnm_idx = c->d_hnm_idx; a.hnm = c->d_hnm;
   a.out = c->d_wall_buf;
   a.out_mach = c->d_wall_buf + (size_t)nl * Ke;
   a.out_val = c->d_wall_buf + (size_t)nl * (Ke + 1);

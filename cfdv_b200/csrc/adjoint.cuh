@@ -47,6 +47,8 @@ struct FunctionalArgs {
   const int* conn;          // [E][nnod]
   const int* bc;            // [E][nface]
   const uint64_t* rowmask;  // [E]
+  const int* hnm_idx;       // [E] adaptive elements (as in FormArgs), or null
+  const double* hnm;
   const double* dU;         // the step's solution [Nn][neqn]
   const double* w;          // VJP: adjoint weights [Nn][neqn]
   const double* tU;         // JVP: tangent of U [Nn][neqn]
@@ -66,6 +68,8 @@ struct ForceArgs {
   const double* x;
   const int* conn;
   const int* bc;
+  const int* hnm_idx;       // [E] adaptive elements (as in FormArgs), or null
+  const double* hnm;
   double* out;              // [n_list][Ke] d F / d U_e
   double* out_mach;         // [n_list] d F / d Mach
   double* out_val;          // [n_list] F of the element's wall faces
@@ -206,6 +210,7 @@ template <int NDIM>
 CFDV_HD Dual element_functional(const FunctionalArgs& a, int e, int k) {
   using T = FormTraits<NDIM>;
   constexpr int NNOD = T::NNOD, NEQ = T::NEQ, KE = T::KE, NFACE = T::NFACE, NBN = T::NBN;
+  const double* Hn = (a.hnm_idx && a.hnm_idx[e] >= 0) ? a.hnm + (size_t)a.hnm_idx[e] * NNOD * NNOD : nullptr;
   const bool vjp = a.mode != 1;
   const uint64_t mask = a.rowmask ? a.rowmask[e] : 0ull;
   if (!vjp && ((mask >> k) & 1ull)) return Dual(0.0);
@@ -253,6 +258,7 @@ CFDV_HD Dual element_functional(const FunctionalArgs& a, int e, int k) {
       w *= a.gw[bit];
     }
     shape_fn<NDIM>(z, Phi, dPxi);
+    if (Hn) hnm_shape<NDIM>(Hn, Phi, dPxi);
     const double J = phys_deriv<NDIM>(dPxi, nd, dPhi, jac);
     const double wJ = w * J;
     GpStateT<Dual> f;
@@ -263,7 +269,9 @@ CFDV_HD Dual element_functional(const FunctionalArgs& a, int e, int k) {
     Dual Psi[NNOD];
     if constexpr (NDIM == 2) {
       const double* x4[4] = {nd[0].x, nd[1].x, nd[2].x, nd[3].x};
-      psi_2d<Dual>(jac, x4, f, dPhi, Psi);
+      double pj[3][3];  // the upwind term's Jacobian: of the untransformed shape functions
+      if (Hn) plain_jac_2d(z, x4, pj);
+      psi_2d<Dual>(Hn ? pj : jac, x4, f, dPhi, Psi);
     }
     double wi[3][5], u0[5], u1[3][5], uS[5], m0[5];
     Dual mPsi[5];
@@ -310,9 +318,18 @@ CFDV_HD Dual element_functional(const FunctionalArgs& a, int e, int k) {
       fn[i] = &nd[ln[i]];
       xf[i] = nd[ln[i]].x;
     }
+    double xl[4][3];
+    if (NDIM == 3 && Hn) {  // adaptive element: face geometry from Hnm x
+      const double* xe[8];
+      for (int M = 0; M < 8; M++) xe[M] = nd[M % NNOD].x;
+      hnm_face_nodes_3d(Hn, xe, fc, xl);
+      for (int i = 0; i < NBN; i++) xf[i] = xl[i % 4];
+    }
     for (int qf = 0; qf < T::QF; qf++) {
       double phib[NBN], dpidx[NBN][3], en[3];
       face_point_geom<NDIM>(a.gz, a.gw, xf, qf, phib, dpidx, en);
+      if constexpr (NDIM == 3)
+        if (Hn) hnm_face_phi_3d(Hn, fc, phib);
       GpStateT<Dual> f;
       gp_state_sums<NDIM, NBN>(fn, phib, dpidx, f);
       f.mu = gas_mu(g, f.T);
@@ -349,6 +366,7 @@ template <int NDIM>
 CFDV_HD Dual wall_force_element(const ForceArgs& a, int e, int k) {
   using T = FormTraits<NDIM>;
   constexpr int NNOD = T::NNOD, NEQ = T::NEQ, KE = T::KE, NFACE = T::NFACE;
+  const double* Hn = (a.hnm_idx && a.hnm_idx[e] >= 0) ? a.hnm + (size_t)a.hnm_idx[e] * NNOD * NNOD : nullptr;
   const GasT<Dual> g = dual_gas(a.gas, k == KE ? 1.0 : 0.0);
   NodePrimT<Dual> nd[NNOD];
   for (int N = 0; N < NNOD; N++) {
@@ -386,6 +404,7 @@ CFDV_HD Dual wall_force_element(const ForceArgs& a, int e, int k) {
       }
       double Phi[NNOD], dPxi[NNOD][3], dPhi[NNOD][3], jac[3][3];
       shape_fn<NDIM>(z, Phi, dPxi);
+      if (Hn) hnm_shape<NDIM>(Hn, Phi, dPxi);
       phys_deriv<NDIM>(dPxi, nd, dPhi, jac);
       double n[3] = {0, 0, 0};  // outward normal times the surface element and the weight
       if (NDIM == 2) {
@@ -739,6 +758,7 @@ template <int NDIM>
 CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double* gout) {
   using T = FormTraits<NDIM>;
   constexpr int NNOD = T::NNOD, NEQ = T::NEQ, KE = T::KE, NFACE = T::NFACE, NBN = T::NBN;
+  const double* Hn = (a.hnm_idx && a.hnm_idx[e] >= 0) ? a.hnm + (size_t)a.hnm_idx[e] * NNOD * NNOD : nullptr;
   const GasParams& gp = a.gas;
   const uint64_t mask = a.rowmask ? a.rowmask[e] : 0ull;
   const double dt = a.dt, dtsq_2 = dt * dt / 2.0;
@@ -781,6 +801,7 @@ CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double*
       w *= a.gw[bit];
     }
     shape_fn<NDIM>(z, Phi, dPxi);
+    if (Hn) hnm_shape<NDIM>(Hn, Phi, dPxi);
     const double J = phys_deriv<NDIM>(dPxi, nd, dPhi, jac);
     const double wJ = w * J;
     GpState f;
@@ -789,8 +810,11 @@ CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double*
     f.k = gas_k(gp, f.mu);
     viscous_stress<NDIM>(f);
     double Psi[NNOD];
-    const double* x4[4] = {nd[0].x, nd[1].x, nd[2].x, nd[3].x};
-    if constexpr (NDIM == 2) psi_2d<double>(jac, x4, f, dPhi, Psi);
+    const double* x4[4] = {nd[0].x, nd[1].x, nd[2].x, nd[3 % NNOD].x};
+    double pj[3][3];  // the upwind term's Jacobian: of the untransformed shape functions
+    if (NDIM == 2 && Hn) plain_jac_2d(z, x4, pj);
+    const double (*sj)[3] = (NDIM == 2 && Hn) ? pj : jac;
+    if constexpr (NDIM == 2) psi_2d<double>(sj, x4, f, dPhi, Psi);
     double wi[3][5], u0[5], u1[3][5], uS[5], m0[5], mPsi[5];
     for (int r = 0; r < NEQ; r++) {
       double a0 = 0.0, b0 = 0.0, bs = 0.0, ps = 0.0, a1[3] = {0, 0, 0}, b1[3] = {0, 0, 0};
@@ -829,7 +853,7 @@ CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double*
         for (int r = 0; r < NEQ; r++) t += mPsibar[r] * wgt[N * NEQ + r];
         psibar[N] = t;
       }
-      psi_2d_adj(jac, x4, f, dPhi, psibar, g);
+      psi_2d_adj(sj, x4, f, dPhi, psibar, g);
     }
     stress_adj<NDIM>(f, g);
     gas_adj(gp, f, g);
@@ -849,9 +873,18 @@ CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double*
       fa[i] = &na[ln[i]];
       xf[i] = nd[ln[i]].x;
     }
+    double xl[4][3];
+    if (NDIM == 3 && Hn) {  // adaptive element: face geometry from Hnm x
+      const double* xe[8];
+      for (int M = 0; M < 8; M++) xe[M] = nd[M % NNOD].x;
+      hnm_face_nodes_3d(Hn, xe, fc, xl);
+      for (int i = 0; i < NBN; i++) xf[i] = xl[i % 4];
+    }
     for (int qf = 0; qf < T::QF; qf++) {
       double phib[NBN], dpidx[NBN][3], en[3];
       face_point_geom<NDIM>(a.gz, a.gw, xf, qf, phib, dpidx, en);
+      if constexpr (NDIM == 3)
+        if (Hn) hnm_face_phi_3d(Hn, fc, phib);
       GpState fr;
       gp_state_sums<NDIM, NBN>(fn, phib, dpidx, fr);
       fr.mu = gas_mu(gp, fr.T);

@@ -30,6 +30,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
   dfree(c->d_pm);
+  dfree(c->d_hnm_idx); dfree(c->d_hnm); c->n_adaptive = 0;
   dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
   c->adj_state_cap = 0;
   c->n_wall_elems = 0;
@@ -673,6 +674,33 @@ int cfdv_upload_mesh(cfdv_ctx* c, const cfdv_mesh* mesh) {
   return setup_mesh(c, mesh);
 }
 
+int cfdv_set_adaptive(cfdv_ctx* c, int n, const int* elements, const double* hnm) {
+  if (!c || n < 0 || (n > 0 && (!elements || !hnm))) return CFDV_ERR_ARG;
+  cudaSetDevice(c->dev);
+  CK(cudaStreamSynchronize(c->st));
+  dfree(c->d_hnm_idx);
+  dfree(c->d_hnm);
+  c->n_adaptive = 0;
+  if (n == 0) return CFDV_OK;
+  const size_t nn = (size_t)c->nnod * c->nnod;
+  std::vector<int> idx((size_t)c->n_elements, -1);
+  for (int k = 0; k < n; k++) {
+    const int e = elements[k];
+    if (e < 0 || e >= c->n_elements) return fail(c, CFDV_ERR_ARG, "set_adaptive: element id out of range");
+    if (idx[e] >= 0) return fail(c, CFDV_ERR_ARG, "set_adaptive: element listed twice");
+    idx[e] = k;
+    for (size_t i = 0; i < nn; i++)
+      if (!std::isfinite(hnm[(size_t)k * nn + i])) return fail(c, CFDV_ERR_ARG, "set_adaptive: non-finite Hnm entry");
+  }
+  int rc;
+  if ((rc = dalloc(c, &c->d_hnm_idx, idx.size())) || (rc = dalloc(c, &c->d_hnm, (size_t)n * nn))) return rc;
+  CK(cudaMemcpyAsync(c->d_hnm_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d_hnm, hnm, sizeof(double) * n * nn, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->n_adaptive = n;
+  return CFDV_OK;
+}
+
 void cfdv_destroy(cfdv_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->dev);
@@ -771,6 +799,7 @@ int form_enqueue(cfdv_ctx* c, double dt, const double* dt_dev, int precision) {
   a.n_elements = c->n_elements;
   a.physical_3d_flux = c->phys3d;
   a.U = c->d_U; a.x = c->d_x; a.conn = c->d_conn; a.bc = c->d_bc; a.rowmask = c->d_mask;
+  a.hnm_idx = c->d_hnm_idx; a.hnm = c->d_hnm;
   a.R64 = c->d_R64;
   a.R32 = (precision == CFDV_PREC_MIXED) ? c->d_R32 : nullptr;
   a.rhs = c->d_rhs; a.s_out = c->d_s; a.status = c->d_status;

@@ -89,6 +89,8 @@ struct FormArgs {
   const int* conn;           // [E][nnod]
   const int* bc;             // [E][nface]
   const uint64_t* rowmask;   // [E] Dirichlet rows after ApplyBC
+  const int* hnm_idx;        // [E] row of hnm for an adaptive element, -1 otherwise (or null)
+  const double* hnm;         // [n_adaptive][nnod*nnod] Hnm(N, M) at N + nnod*M
   double* R64;               // [E][Ke*Ke] column-major per element (FP64 output) or null
   float* R32;                // [E][Ke*Ke] (FP32 output) or null
   double* rhs;               // [E][Ke]

@@ -21,6 +21,9 @@ struct cfdv_ctx {
   int* d_conn = nullptr;
   int* d_bc = nullptr;
   uint64_t* d_mask = nullptr;
+  int* d_hnm_idx = nullptr;   // [E] row of d_hnm for an adaptive element, -1 otherwise (null: none)
+  double* d_hnm = nullptr;    // [n_adaptive][nnod*nnod] Hnm(N, M) at N + nnod*M
+  int n_adaptive = 0;
   double* d_cleng = nullptr;
   int* d_csr_ptr = nullptr;
   int* d_csr_idx = nullptr;

@@ -55,6 +55,68 @@ CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
   return (int)((w >> (4 * i)) & 15ull);
 }
 
+// ---- adaptive (hanging-node) elements ---------------------------------------------------
+// An adaptive element carries Hnm (nnod x nnod, Hnm(N, M) at H[N + nnod*M], the reference
+// Tensor's storage).  Its domain shape functions become Phi_M <- sum_N Phi_N Hnm(N, M) and
+// dPxi(M, j) likewise (MeshRefine2D.h:877-900, applied at FDVGalerkin.h:183-186, 198-201)
+// before the Jacobian; the 2D streamline-upwind term keeps the Jacobian of the untransformed
+// shape functions (FDVGalerkin.h:235-239).  A 3D boundary face takes its geometry from the
+// rows of Hnm x at its nodes (calc_TF_norm3D.h:25-57) and transforms its face shape
+// functions with the face's block of Hnm (MeshRefine2D.h:904-951 via FDVGalerkin.h:488-497;
+// the face derivatives stay as computed).  2D faces are unchanged (FDVGalerkin.h:481-484).
+template <int NDIM>
+CFDV_HD CFDV_INLINE void hnm_shape(const double* H, double* Phi, double (*dPxi)[3]) {
+  constexpr int NNOD = (NDIM == 2) ? 4 : 8;
+  double P[NNOD], D[NNOD][3];
+  for (int M = 0; M < NNOD; M++) {
+    P[M] = 0.0;
+    for (int j = 0; j < NDIM; j++) D[M][j] = 0.0;
+  }
+  for (int N = 0; N < NNOD; N++)
+    for (int M = 0; M < NNOD; M++) {
+      const double h = H[N + NNOD * M];
+      P[M] = RN_ADD(P[M], RN_MUL(Phi[N], h));
+      for (int j = 0; j < NDIM; j++) D[M][j] = RN_ADD(D[M][j], RN_MUL(dPxi[N][j], h));
+    }
+  for (int M = 0; M < NNOD; M++) {
+    Phi[M] = P[M];
+    for (int j = 0; j < NDIM; j++) dPxi[M][j] = D[M][j];
+  }
+}
+
+// the 2D isoparametric Jacobian of the untransformed shape functions at z (x4: node x)
+CFDV_HD CFDV_INLINE void plain_jac_2d(const double* z, const double* const* x4, double (*jac)[3]) {
+  double ph[4], dpx[4][3];
+  shape_fn<2>(z, ph, dpx);
+  for (int i = 0; i < 2; i++)
+    for (int k = 0; k < 2; k++) {
+      double j = 0.0;
+      for (int N = 0; N < 4; N++) j = RN_ADD(j, RN_MUL(dpx[N][k], x4[N][i]));
+      jac[i][k] = j;
+    }
+}
+
+// 3D face f of an adaptive element: the face nodes' positions sum_M Hnm(N, M) x_M (xe: the
+// element's node coordinates), face order
+CFDV_HD CFDV_INLINE void hnm_face_nodes_3d(const double* H, const double* const* xe, int f, double (*xl)[3]) {
+  for (int j = 0; j < 4; j++) {
+    const int N = face_node(3, f, j);
+    for (int k = 0; k < 3; k++) {
+      double s = 0.0;
+      for (int M = 0; M < 8; M++) s = RN_ADD(s, RN_MUL(H[N + 8 * M], xe[M][k]));
+      xl[j][k] = s;
+    }
+  }
+}
+
+// 3D face f of an adaptive element: phib_M <- sum_N phib_N Hnm(n_N, n_M) over the face nodes
+CFDV_HD CFDV_INLINE void hnm_face_phi_3d(const double* H, int f, double* phib) {
+  double pt[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int N = 0; N < 4; N++)
+    for (int M = 0; M < 4; M++) pt[M] = RN_ADD(pt[M], RN_MUL(phib[N], H[face_node(3, f, N) + 8 * face_node(3, f, M)]));
+  for (int M = 0; M < 4; M++) phib[M] = pt[M];
+}
+
 // one Gauss point's worth of coefficients
 template <int NDIM>
 struct GpGeom {  // isoparametric map at the Gauss point (dead once the flow state exists)
@@ -62,6 +124,7 @@ struct GpGeom {  // isoparametric map at the Gauss point (dead once the flow sta
   double inv[3][3];  // adjugate (3D)
   double iJ;         // 1 / det
   double dPxi[FormTraits<NDIM>::NNOD][3];
+  double pjac[NDIM == 2 ? 3 : 1][3];  // 2D adaptive element: Jacobian of the plain shape functions
 };
 
 template <int NDIM>
@@ -92,6 +155,7 @@ struct FormShared {
   int faces[T::NFACE];
   int codes[T::NFACE];
   int nfaces;
+  int hnm;  // row of a.hnm for an adaptive element, -1 otherwise
   uint64_t mask;
   double Mn[T::NNOD], Ren[T::NNOD];  // node Mach and Reynolds numbers
   double s[4];                        // s1..s4 of the element
@@ -205,6 +269,7 @@ CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int 
       }
     }
     sh.nfaces = nf;
+    sh.hnm = a.hnm_idx ? a.hnm_idx[e] : -1;
     sh.mask = a.rowmask ? a.rowmask[e] : 0ull;
     sh.dt = a.dt_dev ? *a.dt_dev : a.dt;
     sh.dtsq_2 = a.dt_dev ? sh.dt * sh.dt / 2.0 : a.dtsq_2;
@@ -214,6 +279,8 @@ CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int 
     double z[3];
     gp_point<NDIM>(a, q, z);
     shape_fn<NDIM>(z, sh.slot[q].Phi, sh.slot[q].g.dPxi);
+    const int hi = a.hnm_idx ? a.hnm_idx[e] : -1;
+    if (hi >= 0) hnm_shape<NDIM>(a.hnm + (size_t)hi * T::NNOD * T::NNOD, sh.slot[q].Phi, sh.slot[q].g.dPxi);
   }
 }
 
@@ -225,6 +292,12 @@ CFDV_HD CFDV_INLINE void step_geom_jac(const FormArgs& a, FormShared<NDIM>& sh, 
     const int q = tid / (NDIM * NDIM), i = (tid / NDIM) % NDIM, k = tid % NDIM;
     GpSlot<NDIM>& sl = sh.slot[q];
     sl.g.jac[i][k] = geom_jac_entry<T::NNOD>(sl.g.dPxi, sh.nd, i, k);
+    if (NDIM == 2 && sh.hnm >= 0 && i == 0 && k == 0) {
+      double z[3];
+      gp_point<NDIM>(a, q, z);
+      const double* x4[4] = {sh.nd[0].x, sh.nd[1].x, sh.nd[2].x, sh.nd[3 % T::NNOD].x};
+      plain_jac_2d(z, x4, sl.g.pjac);
+    }
   }
   if (tid >= T::THREADS - 2) {
     const int which = tid - (T::THREADS - 2);
@@ -372,7 +445,7 @@ CFDV_HD CFDV_INLINE void psi_2d(const double (*jac)[3], const double* const* x4,
 
 CFDV_HD CFDV_INLINE void supg_psi_2d(const FormShared<2>& sh, GpSlot<2>& sl) {
   const double* x4[4] = {sh.nd[0].x, sh.nd[1].x, sh.nd[2].x, sh.nd[3].x};
-  psi_2d<double>(sl.g.jac, x4, sl.st, sl.dPhi, sl.Psi);
+  psi_2d<double>(sh.hnm >= 0 ? sl.g.pjac : sl.g.jac, x4, sl.st, sl.dPhi, sl.Psi);
 }
 
 // step 5: viscosity, conductivity, stress; the 2D test function (one thread per Gauss point)
@@ -782,7 +855,17 @@ CFDV_HD CFDV_INLINE void step_face_geom(const FormArgs& a, FormShared<NDIM>& sh,
   const int f = sh.faces[lf];
   const double* xf[NBN];
   for (int i = 0; i < NBN; i++) xf[i] = sh.nd[face_node(NDIM, f, i)].x;
+  double xl[4][3];
+  const double* H = (NDIM == 3 && sh.hnm >= 0) ? a.hnm + (size_t)sh.hnm * 64 : nullptr;
+  if (H) {
+    const double* xe[8];
+    for (int M = 0; M < 8; M++) xe[M] = sh.nd[M % T::NNOD].x;
+    hnm_face_nodes_3d(H, xe, f, xl);
+    for (int i = 0; i < NBN; i++) xf[i] = xl[i % 4];
+  }
   face_point_geom<NDIM>(a.gz, a.gw, xf, qf, sl.Phi, sl.dPhi, sl.en);
+  if constexpr (NDIM == 3)
+    if (H) hnm_face_phi_3d(H, f, sl.Phi);
   for (int m = 0; m < NBN; m++) {
     sl.cM[0][m] = sl.Phi[m];
     for (int j = 0; j < NDIM; j++) sl.cM[1 + j][m] = sl.dPhi[m][j];

@@ -29,7 +29,7 @@ EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error",
            "cfdv_form", "cfdv_set_element_matrices", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
            "cfdv_profile_read", "cfdv_vjp", "cfdv_jvp", "cfdv_element_functional", "cfdv_wall_force",
-           "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static"]
+           "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static", "cfdv_set_adaptive"]
 
 
 class CfdvError(RuntimeError):
@@ -91,6 +91,7 @@ def lib():
         P, I, D = C.c_void_p, C.c_int, C.c_double
         L.cfdv_create.argtypes = [P, P, P]
         L.cfdv_upload_mesh.argtypes = [P, P]
+        L.cfdv_set_adaptive.argtypes = [P, C.c_int, P, P]
         L.cfdv_destroy.argtypes = [P]
         L.cfdv_destroy.restype = None
         L.cfdv_last_error.argtypes = [P]
@@ -157,6 +158,17 @@ class FDVSolver:
                 self.L.cfdv_destroy(self._ctx)
                 self._ctx = C.c_void_p()
             raise CfdvError(rc, msg)
+        if getattr(case, "adap_elements", None) is not None:
+            self.set_adaptive(case.adap_elements, case.adap_hnm)
+
+    def set_adaptive(self, elements, hnm):
+        """Adaptive elements and their hanging-node matrices hnm[k][N, M] (cfdv_set_adaptive);
+        an empty list clears them."""
+        el = np.ascontiguousarray(elements, dtype=np.int32)
+        # Hnm(N, M) stored at N + nnod*M
+        h = np.ascontiguousarray(np.transpose(np.asarray(hnm, dtype=np.float64).reshape(len(el), self.nnod, self.nnod),
+                                              (0, 2, 1)))
+        self._ck(self.L.cfdv_set_adaptive(self._ctx, len(el), _p(el) if len(el) else None, _p(h) if len(el) else None))
 
     def _ck(self, rc):
         if rc:

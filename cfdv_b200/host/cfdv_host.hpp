@@ -71,6 +71,10 @@ struct BinaryCase {
   std::vector<double> records;  // [Nn][2*ndim+2]
   std::vector<double> x;        // [Nn][ndim]
   std::vector<int> conn, bc;
+  // adaptive elements from the "adap" file when control adap is set (LoadBinary.h:246-260):
+  // ids, refine levels, and Hnm(N, M) at [k][N + nnod*M] (the Tensor storage, as written)
+  std::vector<int> adap_el, adap_level;
+  std::vector<double> adap_hnm;
 
   BinaryCase(const std::string& dir, const CaseConfig& cfg) {
     ndim = cfg.ci("ndim", 2);
@@ -91,6 +95,28 @@ struct BinaryCase {
     for (int e = 0; e < n_elements; e++) {
       for (int k = 0; k < nnod; k++) conn[(size_t)e * nnod + k] = el[(size_t)e * (nnod + nface) + k];
       for (int k = 0; k < nface; k++) bc[(size_t)e * nface + k] = el[(size_t)e * (nnod + nface) + nnod + k];
+    }
+    if (cfg.ci("adap", 0)) read_adap(dir + "/adap");
+  }
+  // "elno adap refine_level" then the Tensor serialisation: type, ndim, extents, data
+  // (TensorStream.h:95-145); records with adap = 0 are skipped
+  void read_adap(const std::string& path) {
+    std::ifstream in(path.c_str());
+    if (!in) throw std::runtime_error("cannot open " + path);
+    int e, flag, level, nd;
+    std::string type;
+    while (in >> e >> flag >> level >> type >> nd) {
+      int ext[2] = {1, 1};
+      for (int k = 0; k < nd && k < 2; k++) in >> ext[k];
+      if (nd != 2 || ext[0] != nnod || ext[1] != nnod || e < 0 || e >= n_elements)
+        throw std::runtime_error("adap: bad record for element " + std::to_string(e));
+      std::vector<double> h((size_t)nnod * nnod);
+      for (double& v : h) in >> v;
+      if (!in) throw std::runtime_error("adap: short record for element " + std::to_string(e));
+      if (!flag) continue;
+      adap_el.push_back(e);
+      adap_level.push_back(level);
+      adap_hnm.insert(adap_hnm.end(), h.begin(), h.end());
     }
   }
   static void read_all(const std::string& p, void* dst, size_t bytes) {
@@ -130,6 +156,8 @@ class GpuFDV {
       throw std::runtime_error("cfdv_create: " + msg);
     }
     check(ctx_, cfdv_load_node_records(ctx_, c.records.data(), c.n_nodes), "load_node_records");
+    if (!c.adap_el.empty())
+      check(ctx_, cfdv_set_adaptive(ctx_, (int)c.adap_el.size(), c.adap_el.data(), c.adap_hnm.data()), "set_adaptive");
   }
   ~GpuFDV() { cfdv_destroy(ctx_); }
   GpuFDV(const GpuFDV&) = delete;
@@ -269,6 +297,16 @@ inline void save_case(const std::string& dir, int iter, const BinaryCase& c, con
   };
   write("binarynodes", rec.data(), rec.size() * sizeof(double));
   write("binaryelements", el.data(), el.size() * sizeof(int));
+  if (!c.adap_el.empty()) {  // SaveBinary.h:153-168 (write_adap), at full precision
+    std::ofstream a((out + "/adap").c_str());
+    a << std::setprecision(17);
+    const size_t nn = (size_t)c.nnod * c.nnod;
+    for (size_t k = 0; k < c.adap_el.size(); k++) {
+      a << c.adap_el[k] << " 1 " << c.adap_level[k] << " double 2 " << c.nnod << " " << c.nnod;
+      for (size_t i = 0; i < nn; i++) a << " " << c.adap_hnm[k * nn + i];
+      a << "\n";
+    }
+  }
   auto kv = [&](const std::string& name, std::map<std::string, std::string> m) {
     std::ofstream f((out + "/" + name).c_str());
     for (const auto& it : m) f << it.first << " = " << it.second << "\n";

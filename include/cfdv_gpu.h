@@ -6,6 +6,8 @@
  *   ---------------------------------------------------  ----------------------------------
  *   LoadBinaryData::read_nodes/read_elements             cfdv_create / cfdv_upload_mesh
  *     (Utility/IO/ASCIItoBinary/LoadBinary.h:116-246)      + cfdv_load_node_records
+ *   LoadBinaryData::adap (LoadBinary.h:246-260; the      cfdv_set_adaptive
+ *     hanging-node Hnm of refined elements)
  *   CalcLength (FDV/Function/CalcLength.h:34-66)         inside cfdv_create
  *   ClearElement + NodeUnpack (main.cpp:169-171)         fused into cfdv_cfl / cfdv_form
  *   CFL (FDV/Function/MPI_CFL.h:124-134, main.cpp:179)   cfdv_cfl
@@ -116,6 +118,13 @@ typedef struct {
 int cfdv_create(const cfdv_mesh* mesh, const cfdv_params* params, cfdv_ctx** out);
 /* Replace the mesh (e.g. after host-side refinement); state and matrices are reset. */
 int cfdv_upload_mesh(cfdv_ctx* ctx, const cfdv_mesh* mesh);
+/* Adaptive (hanging-node) elements after a host refinement, replacing the reference's
+ * "adap" file load (LoadBinary.h:246-260 into Element::adap / Element::Hnm, Element.h:39-40):
+ * elements[k] carries hnm[k*nnod*nnod ...], Hnm(N, M) at N + nnod*M (the reference Tensor's
+ * storage).  Formation then transforms the element's shape functions (MeshRefine2D.h:877-952,
+ * FDVGalerkin.h:183-201, 488-497; calc_TF_norm3D.h:25-57).  n = 0 clears the set;
+ * cfdv_upload_mesh clears it too.  Element ids must be distinct and in range. */
+int cfdv_set_adaptive(cfdv_ctx* ctx, int n, const int* elements, const double* hnm);
 void cfdv_destroy(cfdv_ctx* ctx);
 const char* cfdv_last_error(const cfdv_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t) for event timing by the caller. */

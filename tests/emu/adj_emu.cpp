@@ -12,6 +12,14 @@ using namespace cfdv;
 
 // mode 0: out[e*(Ke+2)+k] = d L_e / d(direction k) (k < Ke unknowns, Ke: dt, Ke+1: Mach),
 //         val[e] = L_e;   mode 1: out[e*Ke + row] = d r_e(row) along (tU, t_dt, t_mach)
+// adaptive elements for the following calls (hnm_idx / hnm of the argument structs), or null
+static const int* g_hnm_idx = nullptr;
+static const double* g_hnm = nullptr;
+extern "C" void emu_set_adaptive(const int* hnm_idx, const double* hnm) {
+  g_hnm_idx = hnm_idx;
+  g_hnm = hnm;
+}
+
 extern "C" void emu_functional(int ndim, int n_elements, const double* U, const double* x, const int* conn,
                                const int* bc, const uint64_t* rowmask, double gamma, double M, double Re, double Pr,
                                double Tinf, double Tw, int adiabatic, double dt, int physical_3d_flux, int mode,
@@ -26,6 +34,7 @@ extern "C" void emu_functional(int ndim, int n_elements, const double* U, const 
   a.physical_3d_flux = physical_3d_flux;
   a.mode = mode;
   a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
+  a.hnm_idx = g_hnm_idx; a.hnm = g_hnm;
   a.dU = dU; a.w = w; a.tU = tU; a.t_dt = t_dt; a.t_mach = t_mach;
   const int Ke = (ndim == 2) ? 16 : 40;
   const int nd = mode == 0 ? Ke + 2 : Ke;
@@ -47,6 +56,7 @@ extern "C" void emu_wall_force(int ndim, int n_elements, const double* U, const 
   gauss_legendre(2, a.gz, a.gw);
   a.wall_bc = wall_bc;
   a.U = U; a.x = x; a.conn = conn; a.bc = bc;
+  a.hnm_idx = g_hnm_idx; a.hnm = g_hnm;
   const int Ke = (ndim == 2) ? 16 : 40;
   for (int e = 0; e < n_elements; e++)
     for (int k = 0; k <= Ke; k++) {
@@ -70,6 +80,7 @@ extern "C" void emu_vjp_rev(int ndim, int n_elements, const double* U, const dou
   a.physical_3d_flux = physical_3d_flux;
   a.mode = 0;
   a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
+  a.hnm_idx = g_hnm_idx; a.hnm = g_hnm;
   a.dU = dU; a.w = w;
   const int Ke = (ndim == 2) ? 16 : 40;
   for (int e = 0; e < n_elements; e++) {

@@ -28,6 +28,14 @@ static int run(const FormArgs& a) {
   return bad;
 }
 
+// adaptive elements for the following emu_form calls (FormArgs::hnm_idx / hnm), or null
+static const int* g_hnm_idx = nullptr;
+static const double* g_hnm = nullptr;
+extern "C" void emu_set_adaptive(const int* hnm_idx, const double* hnm) {
+  g_hnm_idx = hnm_idx;
+  g_hnm = hnm;
+}
+
 extern "C" int emu_form(int ndim, int n_elements, const double* U, const double* x, const int* conn, const int* bc,
                         const uint64_t* rowmask, double gamma, double M, double Re, double Pr, double Tinf,
                         double Tw, int adiabatic, double dt, int physical_3d_flux, double* R64, float* R32,
@@ -41,6 +49,7 @@ extern "C" int emu_form(int ndim, int n_elements, const double* U, const double*
   a.n_elements = n_elements;
   a.physical_3d_flux = physical_3d_flux;
   a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
+  a.hnm_idx = g_hnm_idx; a.hnm = g_hnm;
   a.R64 = R64; a.R32 = R32; a.rhs = rhs; a.s_out = s_out;
   return ndim == 2 ? run<2>(a) : run<3>(a);
 }

@@ -29,6 +29,7 @@ def emu():
     L.emu_functional.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, I, P, P, P, D, D, P, P]
     L.emu_wall_force.argtypes = [I, I, P, P, P, P, D, D, D, D, D, D, I, I, P, P]
     L.emu_vjp_rev.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, P, P, P]
+    L.emu_set_adaptive.argtypes = [P, P]
     return L
 
 
@@ -60,6 +61,18 @@ class Setup:
         self.gas = (float(a["gamma"]), float(a["M"]), float(a["Re"]), float(a["Pr"]), float(a["Tinf"]),
                     float(a["Twall"]), int(a["Adiabatic"]))
         self.E, self.Ke = case.n_elements, o.Ke
+        # adaptive elements: Hnm(N, M) at N + nnod*M
+        self.hidx = self.hnm = None
+        if case.adap_elements is not None:
+            self.hidx = np.ascontiguousarray(case.hnm_index(), np.int32)
+            self.hnm = np.ascontiguousarray(np.transpose(case.adap_hnm, (0, 2, 1)), np.float64)
+
+    def arm(self, L):
+        """Point the emulator's adaptive-element arrays at this case's (or clear them)."""
+        if self.hidx is None:
+            L.emu_set_adaptive(None, None)
+        else:
+            L.emu_set_adaptive(_p(self.hidx), _p(self.hnm))
 
     def idx(self, e):
         nodes = self.case.conn[e]
@@ -75,6 +88,7 @@ class Setup:
         out = np.zeros(self.E * nd)
         val = np.zeros(self.E)
         tU = self.du if tU is None else tU
+        self.arm(L)
         L.emu_functional(self.case.ndim, self.E, _p(U), _p(self.x), _p(self.conn), _p(self.bc), _p(self.mask), *g,
                          float(dt), 0, mode, _p(self.du), _p(self.w), _p(tU), float(tdt), float(tM), _p(out),
                          _p(val))
@@ -102,7 +116,7 @@ class Setup:
         return out
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ["lid8_adap", "ramp4_adap"])
 def test_functional_value_matches_oracle_residual(emu, oracle_lib, name):
     s = Setup(oracle_lib, name)
     _, val = s.emu(emu)
@@ -110,7 +124,7 @@ def test_functional_value_matches_oracle_residual(emu, oracle_lib, name):
     assert np.abs(val - ref).max() <= 1e-13 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
+@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4", "plate20_adap", "cyl4_adap"])
 def test_vjp_matches_finite_differences(emu, oracle_lib, name):
     """Every direction of two elements, and dt and Mach, against central differences of the
     oracle's formation (step 1e-7 relative: the FDV parameter s1 jumps at r = 0.01, so a
@@ -140,7 +154,7 @@ def test_vjp_matches_finite_differences(emu, oracle_lib, name):
     assert worst <= 1e-5
 
 
-@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("name", SMALL_CASES + ["lid8_adap", "ramp4_adap", "cyl4_adap"])
 def test_reverse_mode_matches_forward_mode(emu, oracle_lib, name):
     """The one-pass reverse sweep (generated Jacobian reverse + hand-written rest) against the
     per-seed forward-mode functional, every unknown of every element."""
@@ -181,6 +195,7 @@ def _force(emu, s, U, M=None, wall_bc=1):
     Ke = s.Ke
     out = np.zeros(s.E * (Ke + 1))
     val = np.zeros(s.E)
+    s.arm(emu)
     emu.emu_wall_force(s.case.ndim, s.E, _p(U), _p(s.x), _p(s.conn), _p(s.bc), *g, int(wall_bc), _p(out), _p(val))
     return out.reshape(s.E, Ke + 1), val
 

@@ -24,6 +24,7 @@ def emu():
     L = C.CDLL(EMU)
     P, D, I = C.c_void_p, C.c_double, C.c_int
     L.emu_form.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, P, P, P, P]
+    L.emu_set_adaptive.argtypes = [P, P]
     return L
 
 
@@ -63,3 +64,28 @@ def test_emulated_formation_matches_oracle(emu, oracle_lib, name, phys):
     assert rel_err(rhs, ro) <= 1e-13
     assert rel_err(s, o.fdvparam(U)) == 0.0
     assert elem_rel_err(R32.astype(np.float64), Ro) <= 1e-6
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_emulated_adaptive_formation_matches_oracle(emu, oracle_lib, name):
+    """Adaptive (hanging-node) elements: every third element carries an Hnm; the kernel's
+    phases against the oracle restatement (itself pinned to the reference's outputs on the
+    same cases, tests/golden/*_adap.npz)."""
+    from cfdv_b200 import meshgen as mg
+    case = mg.adaptive_demo(get_case(name))
+    o = oracle_lib.Oracle(case)
+    U = o.init_U()
+    dt = o.cfl(U, float(case.control["cfl"]))
+    Ro, ro = o.form(U, dt, apply_bc=True)
+    idx = np.ascontiguousarray(case.hnm_index(), np.int32)
+    hnm = np.ascontiguousarray(np.transpose(case.adap_hnm, (0, 2, 1)), np.float64)  # Hnm(N, M) at N + nnod*M
+    emu.emu_set_adaptive(_p(idx), _p(hnm))
+    try:
+        bad, R, R32, rhs, s = run_emu(emu, case, U, dt, o.rowmask())
+    finally:
+        emu.emu_set_adaptive(None, None)
+    assert bad == 0
+    assert elem_rel_err(R, Ro) <= 1e-13
+    assert rel_err(rhs, ro) <= 1e-13
+    plain = oracle_lib.Oracle(get_case(name)).form(U, dt, apply_bc=True)[0]
+    assert elem_rel_err(R[case.adap_elements], plain[case.adap_elements]) > 1e-6  # the transform acted

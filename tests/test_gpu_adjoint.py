@@ -69,7 +69,7 @@ TOL_VAL = {"lid8": 1e-9}
 TOL_DER = {"lid8": 1e-3}
 
 
-@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4"])
+@pytest.mark.parametrize("name", ["lid8", "plate20", "ramp4", "cyl4", "plate20_adap", "cyl4_adap"])
 def test_functionals_match_cpu_build(gpu, emu, oracle_lib, name):
     s = Setup(oracle_lib, name)
     with gpu.FDVSolver(s.case) as g:

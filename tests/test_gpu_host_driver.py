@@ -16,7 +16,8 @@ DRIVER = os.path.join(ROOT, "cfdv_b200", "cfdv_gpu")
 
 
 @pytest.mark.skipif(not os.path.exists(REF), reason="reference build oracle/_ref not present")
-@pytest.mark.parametrize("name,steps", [("lid8", 5), ("plate20", 3), ("ramp4", 2)])
+@pytest.mark.parametrize("name,steps", [("lid8", 5), ("plate20", 3), ("ramp4", 2), ("lid8_adap", 4),
+                                        ("ramp4_adap", 2)])
 def test_driver_outputs_match_reference(name, steps):
     from cfdv_b200 import meshgen as mg
     case = get_case(name)
