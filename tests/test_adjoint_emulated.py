@@ -69,7 +69,7 @@ class Setup:
 
     def arm(self, L):
         """Point the emulator's adaptive-element arrays at this case's (or clear them)."""
-        if self.hidx is None:
+        if getattr(self, "hidx", None) is None:
             L.emu_set_adaptive(None, None)
         else:
             L.emu_set_adaptive(_p(self.hidx), _p(self.hnm))
