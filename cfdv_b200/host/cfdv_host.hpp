@@ -10,6 +10,7 @@
 //   RmsLog       RMSError.txt            (FDV/Function/MPI_RMSError.h:56-75)
 //   save_case    <iter>/ checkpoints     (MPIBinaryConfiguration.h:148-161, SaveBinary.h)
 //   EnsightSeries EnSight Gold output    (new: the reference's EnsightOut.h:9-13 is a stub)
+//   convert_ascii ASCII case -> binary   (ConvertMain.cpp, AsciiLoad.h: the CONVERT tool)
 #pragma once
 #include <cstdint>
 #include <cstdio>
@@ -76,6 +77,7 @@ struct BinaryCase {
   std::vector<int> adap_el, adap_level;
   std::vector<double> adap_hnm;
 
+  BinaryCase() = default;
   BinaryCase(const std::string& dir, const CaseConfig& cfg) {
     ndim = cfg.ci("ndim", 2);
     nnod = cfg.ci("nnod", ndim == 2 ? 4 : 8);
@@ -264,9 +266,22 @@ inline void tecplot_write(const std::string& path, const BinaryCase& c, const cf
 // control file with iter = <iter>, so that the run resumes from it (main.cpp:177, control
 // "iter").  The reference writes its 3D records with the 2D struct (SaveBinary.h:48-52,
 // 110-116); here both layouts are the ones LoadBinary reads (LoadBinary.h:20-48).
+inline void write_case_dir(const std::string& out, const BinaryCase& c, const std::map<std::string, std::string>& control,
+                           const std::map<std::string, std::string>& aero, const cfdv_params& p,
+                           const std::vector<double>& U);
+
 inline void save_case(const std::string& dir, int iter, const BinaryCase& c, const CaseConfig& cfg,
                       const cfdv_params& p, const std::vector<double>& U) {
   const std::string out = dir + "/" + std::to_string(iter);
+  std::map<std::string, std::string> ctl = cfg.control;
+  ctl["iter"] = std::to_string(iter);
+  write_case_dir(out, c, ctl, cfg.aero, p, U);
+}
+
+// the case directory `out` (created if needed) of mesh c and conserved state U
+inline void write_case_dir(const std::string& out, const BinaryCase& c, const std::map<std::string, std::string>& control,
+                           const std::map<std::string, std::string>& aero, const cfdv_params& p,
+                           const std::vector<double>& U) {
   if (std::system(("mkdir -p '" + out + "'").c_str()) != 0) throw std::runtime_error("cannot create " + out);
   const int nd = c.ndim, ne = nd + 2, rs = 2 * nd + 2;
   const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
@@ -311,14 +326,110 @@ inline void save_case(const std::string& dir, int iter, const BinaryCase& c, con
     std::ofstream f((out + "/" + name).c_str());
     for (const auto& it : m) f << it.first << " = " << it.second << "\n";
   };
-  std::map<std::string, std::string> ctl = cfg.control;
-  ctl["iter"] = std::to_string(iter);
-  kv("control", ctl);
-  kv("aero", cfg.aero);
+  kv("control", control);
+  kv("aero", aero);
   std::ofstream b((out + "/MPIBreakdown").c_str());  // one rank (MPI_Breakdown.h:23-70)
   b << "1\n";
   b << "elemin, elemax, nodemin, nodemax, nedgenode_l, nedgenode_r, NodeIteratorMin, NodeIteratorMax\n";
   b << "0 " << c.n_elements << " 0 " << c.n_nodes - 1 << " 0 0 0 " << c.n_nodes - 1 << "\n";
+}
+
+// ASCII case directory -> binary case directory: the reference's CONVERT (ConvertMain.cpp:20-66:
+// AsciiLoad.h:27-340, then NodeUnpack and SaveBinary's write_nodes / write_elements /
+// write_adap, with a one-rank MPIBreakdown).  src holds control and aero ("key = value"),
+// nodes ("number x[ndim] U[ndim+2]": conserved variables, 1-based numbers), elements
+// ("number node[nnod]", 1-based), faces ("element face bc node[nbnod]": 0-based element, the
+// bc goes to the element's slot `face`, a later line for the same slot wins) and, with
+// control adap, adap (the format LoadBinary reads).  Lines with fewer numbers than their
+// record are skipped, as AsciiLoad does; a node or element that no line defines is an error.
+// Differences from the reference, on purpose: the 3D records are written in LoadBinary's
+// layout (SaveBinary uses the 2D struct for them), and Hnm keeps full precision (AsciiLoad's
+// add_adap re-prints it through to_string).
+inline std::vector<std::vector<double>> read_number_lines(const std::string& path, bool required) {
+  std::vector<std::vector<double>> rows;
+  std::ifstream in(path.c_str());
+  if (!in) {
+    if (required) throw std::runtime_error("cannot open " + path);
+    return rows;
+  }
+  std::string line;
+  while (std::getline(in, line)) {
+    std::vector<double> r;
+    const char* p = line.c_str();
+    char* end;
+    for (;;) {
+      while (*p == ' ' || *p == '\t' || *p == '\r') p++;
+      if (!*p) break;
+      const double v = std::strtod(p, &end);
+      if (end == p) {  // a word (the Tensor type name in adap lines): kept as 0
+        while (*p && *p != ' ' && *p != '\t') p++;
+        r.push_back(0.0);
+        continue;
+      }
+      r.push_back(v);
+      p = end;
+    }
+    if (!r.empty()) rows.push_back(r);
+  }
+  return rows;
+}
+
+inline void convert_ascii(const std::string& src, const std::string& dst) {
+  CaseConfig cfg(src);
+  const cfdv_params p = cfg.params();
+  BinaryCase c;
+  c.ndim = cfg.ci("ndim", 2);
+  c.nnod = cfg.ci("nnod", c.ndim == 2 ? 4 : 8);
+  c.nface = c.ndim == 2 ? 4 : 6;
+  c.n_nodes = cfg.ci("nodes", 0);
+  c.n_elements = cfg.ci("elements", 0);
+  const int nd = c.ndim, ne = nd + 2, nn = c.nnod, nbnod = cfg.ci("nbnod", nd == 2 ? 2 : 4);
+  if (c.n_nodes <= 0 || c.n_elements <= 0) throw std::runtime_error("convert: control needs nodes and elements");
+  c.x.assign((size_t)c.n_nodes * nd, 0.0);
+  std::vector<double> U((size_t)c.n_nodes * ne, 0.0);
+  std::vector<char> seen(c.n_nodes, 0), eseen(c.n_elements, 0);
+  for (const auto& r : read_number_lines(src + "/nodes", true)) {  // AsciiLoad.h:188-236
+    if ((int)r.size() < 2 * nd + 3) continue;
+    const int i = (int)r[0] - 1;
+    if (i < 0 || i >= c.n_nodes) throw std::runtime_error("convert: node number out of range");
+    for (int j = 0; j < nd; j++) c.x[(size_t)i * nd + j] = r[1 + j];
+    for (int j = 0; j < ne; j++) U[(size_t)i * ne + j] = r[1 + nd + j];
+    seen[i] = 1;
+  }
+  c.conn.assign((size_t)c.n_elements * nn, 0);
+  c.bc.assign((size_t)c.n_elements * c.nface, 0);
+  for (const auto& r : read_number_lines(src + "/elements", true)) {  // AsciiLoad.h:239-253
+    if ((int)r.size() < nn + 1) continue;
+    const int i = (int)r[0] - 1;
+    if (i < 0 || i >= c.n_elements) throw std::runtime_error("convert: element number out of range");
+    for (int j = 0; j < nn; j++) {
+      const int n = (int)r[1 + j] - 1;
+      if (n < 0 || n >= c.n_nodes) throw std::runtime_error("convert: element node out of range");
+      c.conn[(size_t)i * nn + j] = n;
+    }
+    eseen[i] = 1;
+  }
+  for (int i = 0; i < c.n_nodes; i++)
+    if (!seen[i]) throw std::runtime_error("convert: node " + std::to_string(i + 1) + " is not defined");
+  for (int i = 0; i < c.n_elements; i++)
+    if (!eseen[i]) throw std::runtime_error("convert: element " + std::to_string(i + 1) + " is not defined");
+  for (const auto& r : read_number_lines(src + "/faces", true)) {  // AsciiLoad.h:256-313, SaveBinary.h:68-71
+    if ((int)r.size() < 3 + nbnod) continue;
+    const int e = (int)r[0], f = (int)r[1];
+    if (e < 0 || e >= c.n_elements || f < 0 || f >= c.nface) throw std::runtime_error("convert: bad face line");
+    c.bc[(size_t)e * c.nface + f] = (int)r[2];
+  }
+  if (cfg.ci("adap", 0))  // AsciiLoad.h:116-158
+    for (const auto& r : read_number_lines(src + "/adap", true)) {
+      if ((int)r.size() < 7 + nn * nn || !(int)r[1]) continue;
+      const int e = (int)r[0];
+      if (e < 0 || e >= c.n_elements) throw std::runtime_error("convert: adap element out of range");
+      c.adap_el.push_back(e);
+      c.adap_level.push_back((int)r[2]);
+      c.adap_hnm.insert(c.adap_hnm.end(), r.begin() + 7, r.begin() + 7 + nn * nn);
+    }
+  c.records.clear();
+  write_case_dir(dst, c, cfg.control, cfg.aero, p, U);
 }
 
 // EnSight Gold ASCII time series (the reference's EnsightOut.h:9-13 is an empty stub): one

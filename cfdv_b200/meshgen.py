@@ -412,6 +412,47 @@ def write_case(case: Case, path: str) -> str:
     return path
 
 
+# local node order of each face (FiniteElement/get_face.h:80-89, 106-164)
+_FACE2 = [[0, 1], [1, 2], [2, 3], [3, 0]]
+_FACE3 = [[3, 2, 1, 0], [0, 1, 5, 4], [1, 2, 6, 5], [2, 3, 7, 6], [3, 0, 4, 7], [6, 7, 4, 5]]
+
+
+def write_ascii_case(case: Case, path: str, U: np.ndarray) -> str:
+    """Write ``case`` as the reference's ASCII case directory (the input of its CONVERT tool,
+    AsciiLoad.h): control, aero, nodes "number x[ndim] U[ndim+2]" with the conserved state U
+    (1-based numbers), elements "number node[nnod]" (1-based), faces "element face bc
+    node[nbnod]" (0-based element, local face nodes) and the adap file if any."""
+    os.makedirs(path, exist_ok=True)
+    nd, ne = case.ndim, case.neqn
+    Ur = np.asarray(U, dtype=np.float64).reshape(case.n_nodes, ne)
+    with open(os.path.join(path, "control"), "w") as f:
+        for k, v in case.control.items():
+            f.write(f"{k} = {v}\n")
+    with open(os.path.join(path, "aero"), "w") as f:
+        for k, v in case.aero.items():
+            f.write(f"{k} = {v}\n")
+    with open(os.path.join(path, "nodes"), "w") as f:
+        for n in range(case.n_nodes):
+            vals = list(case.nodes[n, :nd]) + list(Ur[n])
+            f.write(f"{n + 1} " + " ".join(repr(float(v)) for v in vals) + "\n")
+    with open(os.path.join(path, "elements"), "w") as f:
+        for e in range(case.n_elements):
+            f.write(f"{e + 1} " + " ".join(str(int(v) + 1) for v in case.conn[e]) + "\n")
+    faces = _FACE2 if nd == 2 else _FACE3
+    with open(os.path.join(path, "faces"), "w") as f:
+        for e in range(case.n_elements):
+            for k, code in enumerate(case.bc[e]):
+                if code != 0:
+                    f.write(f"{e} {k} {int(code)} " + " ".join(str(v) for v in faces[k]) + "\n")
+    if case.adap_elements is not None:
+        nnod = case.nnod
+        with open(os.path.join(path, "adap"), "w") as f:
+            for e, lev, H in zip(case.adap_elements, case.adap_levels, case.adap_hnm):
+                f.write(f"{int(e)} 1 {int(lev)} double 2 {nnod} {nnod} " +
+                        " ".join(repr(float(v)) for v in H.T.ravel()) + "\n")
+    return path
+
+
 def _parse_kv(path):
     kv = {}
     with open(path) as f:
