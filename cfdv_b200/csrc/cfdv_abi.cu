@@ -38,6 +38,9 @@ void free_all(cfdv_ctx* c) {
   c->pers_cap = 0;
   if (c->h_pin) cudaFreeHost(c->h_pin);
   c->h_pin = nullptr;
+  if (c->h_hist) cudaFreeHost(c->h_hist);
+  c->h_hist = nullptr;
+  c->h_hist_cap = 0;
   c->m_cap = 0;
   c->formed = false;
   c->have32 = false;
@@ -574,6 +577,19 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   double* hp = c->h_pin + cfdv::ctxi::kPinSolve;
   CK(cudaMemcpyAsync(hp, pi, sizeof(int) * 8, cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(hp + 4, a.result, sizeof(double) * 8, cudaMemcpyDeviceToHost, c->st));
+  // the residual history comes back with the results (est and gfinal are contiguous), so the
+  // report needs no copy after the wait
+  const size_t nh = (size_t)est_cap + gf_cap;
+  if (nh > c->h_hist_cap) {
+    if (c->h_hist) cudaFreeHost(c->h_hist);
+    c->h_hist = nullptr;
+    c->h_hist_cap = 0;
+    CK(cudaMallocHost((void**)&c->h_hist, sizeof(double) * nh));
+    c->h_hist_cap = nh;
+  }
+  CK(cudaMemcpyAsync(c->h_hist, a.est, sizeof(double) * nh, cudaMemcpyDeviceToHost, c->st));
+  L->h_est = c->h_hist;
+  L->h_gfinal = c->h_hist + est_cap;
   L->est = a.est; L->gfinal = a.gfinal; L->est_cap = est_cap; L->gf_cap = gf_cap;
   L->err = a.err; L->fp32 = fp32;
   return CFDV_OK;
@@ -599,11 +615,11 @@ int cfdv::ctxi::solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_repor
     rep->true_rel_res = bnorm > 0.0 ? res[0] / bnorm : 0.0;
     if (rep->est && rep->est_capacity > 0) {
       const int k = std::min(std::min(nest, rep->est_capacity), L.est_cap);
-      if (k > 0) CK(cudaMemcpy(rep->est, L.est, sizeof(double) * k, cudaMemcpyDeviceToHost));
+      if (k > 0) std::memcpy(rep->est, L.h_est, sizeof(double) * k);
     }
     if (rep->gfinal && rep->gfinal_capacity > 0) {
       const int k = std::min(std::min(hi[1], rep->gfinal_capacity), L.gf_cap);
-      if (k > 0) CK(cudaMemcpy(rep->gfinal, L.gfinal, sizeof(double) * k, cudaMemcpyDeviceToHost));
+      if (k > 0) std::memcpy(rep->gfinal, L.h_gfinal, sizeof(double) * k);
     }
   }
   c->mv_launches += (long)res[3];

@@ -53,6 +53,8 @@ struct cfdv_ctx {
   double* d_rms = nullptr;
   int* d_status = nullptr;
   double* h_pin = nullptr;  // pinned host staging
+  double* h_hist = nullptr;  // pinned: the Givens estimates and final |g| of a persistent solve
+  size_t h_hist_cap = 0;
   double* d_pers = nullptr;  // persistent-solve scratch
   size_t pers_cap = 0;
   int* d_pers_int = nullptr;
@@ -129,6 +131,8 @@ constexpr int kPinStep = 4016;   // dt, formation status of a step
 struct SolveLaunch {
   double* est;
   double* gfinal;
+  const double* h_est;  // pinned copies of est and gfinal, filled by the stream
+  const double* h_gfinal;
   int est_cap, gf_cap;
   int* err;   // device error flags of the launch (bit 0 barrier timeout, bit 1 non-finite)
   int fp32;

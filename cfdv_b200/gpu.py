@@ -242,9 +242,18 @@ class FDVSolver:
                      int(engine), int(precond), int(orth))
 
     def _report(self, m, restarts):
-        est = np.zeros(max(m * max(restarts, 1), 1))
-        fin = np.zeros(max(restarts, 1))
-        rep = _Report(0, 0, 0, est.size, _p(est).value, fin.size, _p(fin).value, 0, 0, -1.0)
+        """Report struct and history buffers for (m, restarts), kept between calls (the
+        returned dict copies what it needs)."""
+        key = (m, restarts)
+        cache = self.__dict__.setdefault("_rep_cache", {})
+        if key not in cache:
+            est = np.zeros(max(m * max(restarts, 1), 1))
+            fin = np.zeros(max(restarts, 1))
+            cache[key] = (_Report(0, 0, 0, est.size, _p(est).value, fin.size, _p(fin).value, 0, 0, -1.0), est, fin)
+        rep, est, fin = cache[key]
+        rep.tol = rep.bnorm = 0.0
+        rep.n_est = rep.n_restarts = rep.n_matvec = 0
+        rep.true_rel_res = -1.0
         return rep, est, fin
 
     @staticmethod
