@@ -81,8 +81,8 @@ __device__ __forceinline__ bool grid_sync(Barrier& b) {
     if ((v & 0x7fffffffu) < b.target && !(v & 0x80000000u)) {
       const unsigned long long t0 = now_ns();
       unsigned int polls = 0;
-      do {
-        if (++polls > 16) __nanosleep(32);
+      do {  // one poll in flight per block; a back-off sleep measured 1% slower on the plate solve
+        ++polls;
         asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(b.count) : "memory");
         if ((polls & 255u) == 0 && now_ns() - t0 > kWaitNs) {
           atomicOr(b.count, 0x80000000u);
