@@ -45,8 +45,14 @@ WORKLOADS = {
 }
 
 
+# The timed steps march from the state after the warm-up steps and go back to it every
+# RESTART_EVERY steps (between steps, outside the timed regions): with converged solves at
+# CFL 1 the synthetic plate develops an instability after about 20 steps (the oracle's
+# converged solve shows it too), and a longer --steps run would then time stalled solves.
+RESTART_EVERY = 10
+
 # orthogonalisation of the persistent solve (cfdv_gmres_opts.orth)
-ORTH = {"cgs2": 0, "mgs": 1, "dcgs2": 2}
+ORTH = {"cgs2": 0, "mgs": 1, "dcgs2": 2, "dcgs2-grid": 3}  # dcgs2-grid: grid barriers only
 
 
 def dist_info():
@@ -183,7 +189,11 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
             sampler.start()  # runs across every timed region of the run (both forms, e2e)
         solver.profile(True)
         step_ms, res, mvs = [], [], []
-        for _ in range(steps):
+        snap = solver.get_state()
+        for i in range(steps):
+            if i and i % RESTART_EVERY == 0:
+                torch.cuda.synchronize()
+                solver.set_state(snap)
             with torch.cuda.stream(ext):
                 flush.fill_(1.0)  # evict the previous step's matrices from L2
                 e0 = torch.cuda.Event(enable_timing=True)
@@ -318,7 +328,10 @@ def bench_gpu(args, ws, rank, local):
     barrier()
     solver.profile(True)
     e2e_ms = []
-    for _ in range(args.steps):
+    snap = host.numpy().copy()
+    for i in range(args.steps):
+        if i and i % RESTART_EVERY == 0:
+            host.numpy()[:] = snap
         with torch.cuda.stream(ext):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)

@@ -29,7 +29,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
-  dfree(c->d_pm);
+  dfree(c->d_pm); dfree(c->d_nbr_ptr); dfree(c->d_nbr_idx); c->nbr_blocks = 0;
   dfree(c->d_hnm_idx); dfree(c->d_hnm); c->n_adaptive = 0;
   dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
   c->adj_state_cap = 0;
@@ -189,7 +189,14 @@ int setup_mesh(cfdv_ctx* c, const cfdv_mesh* m) {
     for (int e = 0; e < c->n_elements; e++)
       for (int l = 0; l < c->nnod; l++) idx[fill[m->conn[(size_t)e * c->nnod + l]]++] = e * c->nnod + l;
   }
+  // neighbour sets of the persistent solve's delayed-CGS2 step (2D; none: grid barriers)
+  std::vector<int> nptr, nidx;
+  const int nblk = persistent_blocks();
+  const bool nbr = persistent_neighbour_sets(c->ndim, c->n_nodes, c->n_elements, m->conn, ptr.data(), idx.data(),
+                                             nblk, nptr, nidx);
   const size_t E = c->n_elements, Ke = c->Ke;
+  if (nbr && ((rc = dalloc(c, &c->d_nbr_ptr, nptr.size())) || (rc = dalloc(c, &c->d_nbr_idx, nidx.size()))))
+    return rc;
   if ((rc = dalloc(c, &c->d_x, (size_t)c->n_nodes * c->ndim)) || (rc = dalloc(c, &c->d_conn, E * c->nnod)) ||
       (rc = dalloc(c, &c->d_bc, E * c->nface)) || (rc = dalloc(c, &c->d_mask, E)) ||
       (rc = dalloc(c, &c->d_cleng, E)) || (rc = dalloc(c, &c->d_csr_ptr, (size_t)c->n_nodes + 1)) ||
@@ -210,6 +217,12 @@ int setup_mesh(cfdv_ctx* c, const cfdv_mesh* m) {
   CK(cudaMemcpyAsync(c->d_cleng, cleng.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_csr_ptr, ptr.data(), sizeof(int) * ptr.size(), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(c->d_csr_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, c->st));
+  if (nbr) {
+    CK(cudaMemcpyAsync(c->d_nbr_ptr, nptr.data(), sizeof(int) * nptr.size(), cudaMemcpyHostToDevice, c->st));
+    if (!nidx.empty())
+      CK(cudaMemcpyAsync(c->d_nbr_idx, nidx.data(), sizeof(int) * nidx.size(), cudaMemcpyHostToDevice, c->st));
+    c->nbr_blocks = nblk;
+  }
   CK(cudaMemsetAsync(c->d_U, 0, sizeof(double) * c->n_dof, c->st));
   CK(cudaMemsetAsync(c->d_U0, 0, sizeof(double) * c->n_dof, c->st));
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
@@ -511,7 +524,9 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
     if ((rc = dalloc(c, &c->d_pers, need))) return rc;
     c->pers_cap = need;
   }
-  if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, 8))) return rc;
+  // stop, cycles, err, barrier count | a neighbour-sync flag per block, 32 apart
+  const size_t n_int = 32 + 32 * (size_t)persistent_max_blocks();
+  if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, n_int))) return rc;
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
   if (rhs_vec) {
     if (rhs_vec != c->d_b)
@@ -520,14 +535,14 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
     CK(launch_compose_rhs(ebe_args(c), c->d_rhs, c->d_b, c->d_pa, c->st));
     c->launches++;
   }
-  CK(cudaMemsetAsync(c->d_pers_int, 0, sizeof(int) * 8, c->st));
+  CK(cudaMemsetAsync(c->d_pers_int, 0, sizeof(int) * n_int, c->st));
   PersistentArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n_dof = c->n_dof; a.n_elements = c->n_elements; a.m = m; a.max_restarts = o->restarts;
   a.max_blocks = persistent_max_blocks();
   a.orth = o->orth;
-  if (o->orth == 0 || o->orth == 2) {
-    if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 128))) return rc;
+  if (o->orth == 0 || o->orth == 2 || o->orth == 3) {  // two buffers of 128 partial slots
+    if (!c->d_pm && (rc = dalloc(c, &c->d_pm, (size_t)persistent_max_blocks() * 256))) return rc;
     a.partm = c->d_pm;
   }
   a.rtol = o->rtol;
@@ -558,6 +573,8 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   int* pi = c->d_pers_int;
   a.stop = pi; a.out = pi + 1; a.err = pi + 2;
   a.bar_count = (unsigned int*)(pi + 3);
+  a.nbr_ptr = c->d_nbr_ptr; a.nbr_idx = c->d_nbr_idx; a.nbr_blocks = c->nbr_blocks;
+  a.nbr_flag = (unsigned int*)(pi + 32);
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
   if (c->prof) {
     cudaEventCreate(&ev.first);

@@ -60,7 +60,10 @@ struct cfdv_ctx {
   int* d_pers_int = nullptr;
   double* d_Dinv = nullptr;  // node-block Jacobi inverse [Nn][neqn][neqn]
   double* d_Z = nullptr;     // preconditioned Krylov vector
-  double* d_pm = nullptr;    // CGS2 multi-dot partials [blocks][64]
+  double* d_pm = nullptr;    // (D)CGS2 multi-dot partials, two buffers [128][kRedBlocks]
+  int* d_nbr_ptr = nullptr;  // neighbour sets of the persistent solve (2D), CSR over its blocks
+  int* d_nbr_idx = nullptr;
+  int nbr_blocks = 0;        // grid size they were built for (0: none)
   // adjoint and tangent runs (adjoint.cu)
   std::vector<double> h_records;   // node records of cfdv_load_node_records: the initial state
   double* d_adj_e = nullptr;       // [E][Ke + 3] per-element gradient rows, d/ddt, d/dMach

@@ -41,6 +41,8 @@
 // L1 is not coherent across SMs.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "gmres_persistent.h"
 #include "kernels.h"
 
@@ -92,6 +94,51 @@ __device__ __forceinline__ bool grid_sync(Barrier& b) {
       } while ((v & 0x7fffffffu) < b.target && !(v & 0x80000000u));
     }
     ok = (v & 0x80000000u) ? 0 : 1;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+constexpr int kFlagStride = 32;  // neighbour-sync flags one 128-byte line apart
+
+// Neighbour sync: publish this block's writes (the k-th neighbour sync of the launch sets its
+// flag to k), then wait until every block of its set has reached the same sync.  Lane i of
+// warp 0 polls block nbrs[i] (shared memory, -1: none; sets have at most 32 blocks).  Every
+// block takes the same sequence of syncs, so equal counts mean the same point of the solve.
+// Returns false if a block gave up waiting, here or at a grid barrier (bit 31 of its count).
+__device__ __forceinline__ bool local_sync(Barrier& b, unsigned int* flag, const int* nbrs, unsigned int& phase) {
+  __shared__ int ok;
+  __syncthreads();
+  ++phase;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x, o = nbrs[lane];
+    if (lane == 0)  // release: the block's writes (ordered before by the block barrier) precede it
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag + blockIdx.x * kFlagStride), "r"(phase) : "memory");
+    bool good = true;
+    if (o >= 0) {
+      unsigned int v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag + o * kFlagStride) : "memory");
+      if (v < phase) {
+        const unsigned long long t0 = now_ns();
+        unsigned int polls = 0;
+        do {
+          asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag + o * kFlagStride) : "memory");
+          if ((++polls & 255u) == 0) {
+            unsigned int cnt;
+            asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(cnt) : "l"(b.count) : "memory");
+            if (cnt & 0x80000000u) { good = false; break; }
+            if (now_ns() - t0 > kWaitNs) {
+              atomicOr(b.count, 0x80000000u);
+              atomicOr(b.err, 1);
+              good = false;
+              break;
+            }
+          }
+        } while (v < phase);
+      }
+    }
+    good = __all_sync(0xffffffffu, good);
+    if (lane == 0) ok = good ? 1 : 0;
   }
   __syncthreads();
   return ok != 0;
@@ -320,7 +367,25 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* V = a.V;
   double* W = a.W;
   const bool cgs = a.orth == 0 && m + 2 <= kMaxBasis && a.partm != nullptr;
-  const bool dcgs = a.orth == 2 && m + 2 <= kMaxBasis && a.partm != nullptr;
+  const bool dcgs = (a.orth == 2 || a.orth == 3) && m + 2 <= kMaxBasis && a.partm != nullptr;
+  // DCGS2 step: neighbour syncs where only neighbours' data is read (the gathers of the element
+  // and node passes); the one reduction per step stays a grid barrier
+  const bool local = a.orth == 2 && a.nbr_ptr != nullptr && a.nbr_blocks == nb;
+  __shared__ int s_nbr[2][32];  // this block's two neighbour sets, one block per lane (-1: none)
+  if (local && tid < 64) {
+    const int row = (tid >> 5) * (nb + 1) + bid, p0 = __ldg(a.nbr_ptr + row) + lane;
+    s_nbr[tid >> 5][lane] = p0 < __ldg(a.nbr_ptr + row + 1) ? __ldg(a.nbr_idx + p0) : -1;
+  }  // visible after the first grid barrier
+  unsigned int lphase = 0;
+  auto sync_x = [&]() -> bool {  // x of the next element pass written by the blocks owning its nodes
+    return local ? local_sync(bar, a.nbr_flag, s_nbr[0], lphase) : grid_sync(bar);
+  };
+  auto sync_y = [&]() -> bool {  // element products at this block's nodes written by their owners
+    return local ? local_sync(bar, a.nbr_flag, s_nbr[1], lphase) : grid_sync(bar);
+  };
+  // dot partials: DCGS2 alternates two buffers by step parity, so a block running ahead writes
+  // step j+1's partials while others still read step j's (the grid barrier of step j+1 bounds it)
+  double* pm = a.partm;
 
   // own-slice accessors: basis entry i, w
   auto vld = [&](int i, int dl) -> double {
@@ -389,7 +454,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
         double acc = 0.0;
         for (int dl = lane; dl < ns; dl += 32) acc += vi[dl] * sW[dl];
         acc = xor_sum(acc);
-        if (lane == 0) a.partm[(size_t)i * kPartLd + bid] = acc;
+        if (lane == 0) pm[(size_t)i * kPartLd + bid] = acc;
       }
     } else {  // streaming: each thread its own unknowns, four projections per load batch
       for (int i0 = 0; i0 < nt; i0 += 4) {
@@ -411,7 +476,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       for (int i = tid; i < nt; i += kThreads) {
         double t = 0.0;
         for (int k = 0; k < kWarps; k++) t += red[k][i];
-        a.partm[(size_t)i * kPartLd + bid] = t;
+        pm[(size_t)i * kPartLd + bid] = t;
       }
     }
   };
@@ -420,7 +485,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     for (int i = wid; i < nt; i += kWarps) {
       double acc = 0.0;
 #pragma unroll 4
-      for (int b = lane; b < nb; b += 32) acc += __ldcg(a.partm + (size_t)i * kPartLd + b);
+      for (int b = lane; b < nb; b += 32) acc += __ldcg(pm + (size_t)i * kPartLd + b);
       acc = xor_sum(acc);
       if (lane == 0) hs[i] = acc;
     }
@@ -456,7 +521,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
         double acc = 0.0;
         for (int dl = lane; dl < ns; dl += 32) acc += x[dl] * yv[dl];
         acc = xor_sum(acc);
-        if (lane == 0) a.partm[(size_t)sl * kPartLd + bid] = acc;
+        if (lane == 0) pm[(size_t)sl * kPartLd + bid] = acc;
       }
     } else {  // streaming: each thread its own unknowns, four basis vectors per load batch
       for (int i0 = 0; i0 < j; i0 += 4) {
@@ -508,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       for (int sl = tid; sl < nt; sl += kThreads) {
         double t = 0.0;
         for (int k = 0; k < kWarps; k++) t += red[k][sl];
-        a.partm[(size_t)sl * kPartLd + bid] = t;
+        pm[(size_t)sl * kPartLd + bid] = t;
       }
     }
   };
@@ -651,8 +716,9 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
       double tpend = 0.0;
       bool done = false;
       for (int j = 0; j < m && !done; j++) {
+        pm = a.partm + (size_t)(j & 1) * kSlots * kPartLd;
         elem_pass_op(a.Dinv ? a.Z : V + (size_t)j * n);  // A P u~_j
-        if (!grid_sync(bar)) return;
+        if (!sync_y()) return;
         node_pass(sizeof(TR) == 4, 0, nullptr);
         mv++;
         dots_d(j, true);
@@ -710,10 +776,11 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
         tpend = sigma / nu;
         if (a.Dinv) precond_slice(j + 1);
         k = j + 1;
-        if (!grid_sync(bar)) return;
+        if (!sync_x()) return;
       }
       if (!done && k == m) {
         // the cycle ran to m: complete the last column from u~_m's coefficients
+        pm = a.partm + (size_t)(m & 1) * kSlots * kPartLd;
         dots_d(m, false);
         if (!grid_sync(bar)) return;
         reduce_parts(m + 1, hs1);
@@ -877,7 +944,7 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int blocks = sms < a.max_blocks ? sms : a.max_blocks;
   const int pn = (a.n_dof / NEQ + blocks - 1) / blocks, S = pn * NEQ;
-  const bool cgs = (a.orth == 0 || a.orth == 2) && a.m + 2 <= kMaxBasis && a.partm != nullptr;
+  const bool cgs = (a.orth == 0 || a.orth == 2 || a.orth == 3) && a.m + 2 <= kMaxBasis && a.partm != nullptr;
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, true>);
   if (e != cudaSuccess) return e;
@@ -903,5 +970,50 @@ cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a,
 }
 
 int persistent_max_blocks() { return kRedBlocks; }
+
+int persistent_blocks() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  return sms < kRedBlocks ? sms : kRedBlocks;
+}
+
+// Ownership as in the kernel: block b owns nodes [b pn, (b+1) pn), pn = ceil(n_nodes / nb)
+// (gmres_persistent_kernel), and in 2D elements [b per, (b+1) per), per = ceil(E / nb)
+// (ElemChunks with U > 1).
+bool persistent_neighbour_sets(int ndim, int n_nodes, int n_elements, const int* conn, const int* csr_ptr,
+                               const int* csr_idx, int blocks, std::vector<int>& ptr, std::vector<int>& idx) {
+  constexpr int kMaxSet = 32;  // one polling lane each
+  if (ndim != 2 || blocks <= 0 || n_nodes <= 0 || n_elements <= 0) return false;
+  constexpr int nnod = 4;
+  const int nb = blocks, pn = (n_nodes + nb - 1) / nb, per = (n_elements + nb - 1) / nb;
+  ptr.assign(2 * (nb + 1), 0);
+  idx.clear();
+  std::vector<int> seen(nb, -1);
+  auto add = [&](int b, int o) {
+    if (o != b && seen[o] != b) {
+      seen[o] = b;
+      idx.push_back(o);
+    }
+  };
+  for (int b = 0; b < nb; b++) {  // blocks owning the nodes of b's elements
+    ptr[b] = (int)idx.size();
+    const int e0 = std::min(n_elements, b * per), e1 = std::min(n_elements, e0 + per);
+    for (int e = e0; e < e1; e++)
+      for (int l = 0; l < nnod; l++) add(b, conn[(size_t)e * nnod + l] / pn);
+    if ((int)idx.size() - ptr[b] > kMaxSet) return false;
+  }
+  ptr[nb] = (int)idx.size();
+  std::fill(seen.begin(), seen.end(), -1);
+  for (int b = 0; b < nb; b++) {  // blocks owning the elements at b's nodes
+    ptr[nb + 1 + b] = (int)idx.size();
+    const int n0 = std::min(n_nodes, b * pn), n1 = std::min(n_nodes, n0 + pn);
+    for (int nd = n0; nd < n1; nd++)
+      for (int p = csr_ptr[nd]; p < csr_ptr[nd + 1]; p++) add(b, (csr_idx[p] / nnod) / per);
+    if ((int)idx.size() - ptr[nb + 1 + b] > kMaxSet) return false;
+  }
+  ptr[2 * nb + 1] = (int)idx.size();
+  return true;
+}
 
 }  // namespace cfdv

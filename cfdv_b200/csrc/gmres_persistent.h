@@ -2,11 +2,13 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace cfdv {
 
 struct PersistentArgs {
   int n_dof, n_elements, m, max_restarts, max_blocks;
-  int orth;                    // 0: classical Gram-Schmidt twice (CGS2), 1: modified Gram-Schmidt
+  int orth;                    // 0: CGS2, 1: MGS, 2: delayed CGS2, 3: delayed CGS2 with grid barriers only
   double* partm;               // CGS2 multi-dot partials [gridDim.x][m+1]
   double rtol;                 // stop when ||b - A du|| < rtol ||b|| (true residual, FP64 matrices)
   const int* conn;
@@ -40,7 +42,21 @@ struct PersistentArgs {
                                // [7] the stopping threshold rtol ||b||
   unsigned int* bar_count;     // grid barrier arrivals, zero before launch
   int* err;                    // bit 0: barrier timeout, bit 1: non-finite residual
+  // Neighbour sets of the delayed-CGS2 step (2D, orth 2), CSR over the blocks: rows [0, nb] list
+  // the blocks owning nodes of a block's elements, rows [nb + 1, 2 nb + 1] the blocks owning
+  // elements at a block's nodes.  Null, or built for another grid size: grid barriers only.
+  const int* nbr_ptr;
+  const int* nbr_idx;
+  int nbr_blocks;
+  unsigned int* nbr_flag;      // per block (32 apart): neighbour syncs passed, zero before launch
 };
+
+// The neighbour sets above for `blocks` blocks (the kernel's node and element ownership);
+// false when they do not apply (3D, whose element waves interleave over the grid) or when a
+// set has more than 32 blocks.
+bool persistent_neighbour_sets(int ndim, int n_nodes, int n_elements, const int* conn, const int* csr_ptr,
+                               const int* csr_idx, int blocks, std::vector<int>& ptr, std::vector<int>& idx);
+int persistent_blocks();
 
 cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st);
 int persistent_max_blocks();

@@ -94,8 +94,10 @@ typedef struct {
                         barriers per Arnoldi step; m <= 62), 1 = modified Gram-Schmidt as the
                         reference's Arnoldi (MPI_GMRES.h:164-181; j+3 barriers per step j),
                         2 = delayed CGS2: the second projection of a step's vector is taken in
-                        the next step's single reduction (3 grid barriers and two passes over
-                        the basis per step; m <= 62) */
+                        the next step's single reduction (two passes over the basis and 3
+                        synchronisations per step; m <= 62; in 2D the two around the product
+                        wait only for the blocks owning neighbouring nodes and elements),
+                        3 = delayed CGS2 with grid barriers at all 3 (bitwise equal to 2) */
 } cfdv_gmres_opts;
 
 typedef struct {

@@ -1,7 +1,8 @@
 """Edge cases of the persistent GMRES solve (engine 0): Krylov dimensions at and beyond the
 delayed-CGS2 limit (m + 2 <= 64 partial slots; larger m runs MGS in the same kernel), a zero
-right-hand side (||b|| = 0 computed inside the kernel: du = 0, nothing iterated), and zero
-restarts (only the final residual)."""
+right-hand side (||b|| = 0 computed inside the kernel: du = 0, nothing iterated), zero
+restarts (only the final residual), and the 2D neighbour syncs of the delayed-CGS2 step
+against grid barriers."""
 import numpy as np
 import pytest
 
@@ -59,3 +60,33 @@ def test_zero_restarts_reports_the_initial_residual(gpu):
         du = s.du()
     assert not du.any()
     assert rep["true_rel_res"] == pytest.approx(1.0, rel=1e-12)  # r = b - A 0
+
+
+@pytest.mark.parametrize("name", ["lid8", "lid32", "plate20", "lid8_adap", "plate200x100"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("precond", [True, False])
+def test_neighbour_syncs_match_grid_barriers(gpu, name, prec, precond):
+    """orth 2 replaces two of the three grid barriers of a 2D delayed-CGS2 step by waits on the
+    blocks owning neighbouring nodes and elements; orth 3 keeps grid barriers.  The arithmetic
+    and its order are the same, so the solves agree bit for bit, and repeated runs with the
+    neighbour syncs do too.  lid8 has fewer elements than blocks (empty blocks and sets)."""
+    if name == "plate200x100":
+        from cfdv_b200 import meshgen as mg
+        case = mg.plate(200, 100)
+    else:
+        case = get_case(name)
+    p = gpu.PREC_MIXED if prec == "mixed" else gpu.PREC_FP64
+    runs = []
+    with gpu.FDVSolver(case) as s:
+        s.load_node_records()
+        s.form(s.cfl(float(case.control["cfl"])), precision=gpu.PREC_MIXED)
+        for orth in (3, 2, 2):
+            r = s.gmres(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=p, engine=0,
+                        precond=precond, orth=orth)
+            runs.append((r, s.du()))
+    (r3, d3), (r2, d2), (r2b, d2b) = runs
+    assert r3["true_rel_res"] < 1e-8
+    for r, d in ((r2, d2), (r2b, d2b)):
+        assert np.array_equal(d, d3)
+        assert np.array_equal(r["est"], r3["est"])
+        assert r["restarts"] == r3["restarts"] and r["true_rel_res"] == r3["true_rel_res"]
