@@ -183,6 +183,8 @@ int setup_mesh(cfdv_ctx* c, const cfdv_mesh* m) {
   // node -> (element, local node) CSR, entries in element order
   std::vector<int> ptr(c->n_nodes + 1, 0), idx((size_t)c->n_elements * c->nnod);
   for (size_t k = 0; k < idx.size(); k++) ptr[m->conn[k] + 1]++;
+  c->max_valence = 0;
+  for (int n = 0; n < c->n_nodes; n++) c->max_valence = std::max(c->max_valence, ptr[n + 1]);
   for (int n = 0; n < c->n_nodes; n++) ptr[n + 1] += ptr[n];
   {
     std::vector<int> fill(ptr.begin(), ptr.end() - 1);
@@ -575,6 +577,7 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   a.bar_count = (unsigned int*)(pi + 3);
   a.nbr_ptr = c->d_nbr_ptr; a.nbr_idx = c->d_nbr_idx; a.nbr_blocks = c->nbr_blocks;
   a.nbr_flag = (unsigned int*)(pi + 32);
+  a.max_valence = c->max_valence;
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
   if (c->prof) {
     cudaEventCreate(&ev.first);

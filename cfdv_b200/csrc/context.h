@@ -64,6 +64,7 @@ struct cfdv_ctx {
   int* d_nbr_ptr = nullptr;  // neighbour sets of the persistent solve (2D), CSR over its blocks
   int* d_nbr_idx = nullptr;
   int nbr_blocks = 0;        // grid size they were built for (0: none)
+  int max_valence = 0;       // most (element, local node) entries of a node
   // adjoint and tangent runs (adjoint.cu)
   std::vector<double> h_records;   // node records of cfdv_load_node_records: the initial state
   double* d_adj_e = nullptr;       // [E][Ke + 3] per-element gradient rows, d/ddt, d/dMach

@@ -53,6 +53,7 @@ namespace {
 constexpr int kThreads = 1024;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxBasis = 64;         // CGS2 / DCGS2: m + 2 <= kMaxBasis
+constexpr int kMaxValence = 8;        // node-pass offsets cached for nodes with at most 8 entries
 constexpr int kSlots = 128;           // partial slots of one reduction (DCGS2: 2j + 3)
 constexpr int kPartLd = kRedBlocks;   // partm[i * kPartLd + block]
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s: far above any barrier wait
@@ -363,6 +364,9 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* rest = pend + (m + 1);
   double* sV = rest;                          // resident: (m+1) x S own-slice basis
   double* sW = rest + (size_t)(m + 1) * S;    // resident: own slice of w
+  // resident, with room: per own node its entry count and the offsets (into Y) of its entries
+  int* ncnt = reinterpret_cast<int*>(rest + (size_t)(m + 2) * S);
+  int* noff = ncnt + pn;
   double (*red)[kSlots] = reinterpret_cast<double (*)[kSlots]>(rest);  // streaming: per-warp dots
   double* V = a.V;
   double* W = a.W;
@@ -420,11 +424,19 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     for (int dl = tid; dl < ns; dl += kThreads) {
       const int d = lo + dl, nd = d / NEQ, k = d % NEQ;
       double s = 0.0;
-      const int p1 = __ldg(a.csr_ptr + nd + 1);
-      for (int p = __ldg(a.csr_ptr + nd); p < p1; p++) {
-        const int v = __ldg(a.csr_idx + p);
-        const size_t yi = (size_t)(v / NNOD) * KE + (v % NNOD) * NEQ + k;
-        s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
+      if (RES && a.node_cache) {  // the same entries in the same order, offsets from shared memory
+        const int il = dl / NEQ, cnt = ncnt[il];
+        for (int q = 0; q < cnt; q++) {
+          const size_t yi = (size_t)noff[il * kMaxValence + q] + k;
+          s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
+        }
+      } else {
+        const int p1 = __ldg(a.csr_ptr + nd + 1);
+        for (int p = __ldg(a.csr_ptr + nd); p < p1; p++) {
+          const int v = __ldg(a.csr_idx + p);
+          const size_t yi = (size_t)(v / NNOD) * KE + (v % NNOD) * NEQ + k;
+          s += fp32 ? (double)__ldcg(a.Y32 + yi) : __ldcg(a.Y64 + yi);
+        }
       }
       const double val = mode ? a.b[d] - s : s;
       wst(dl, val);
@@ -630,6 +642,15 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     }
     __syncthreads();
   };
+  if (RES && a.node_cache)  // visible after the first grid barrier
+    for (int il = tid; il < ns / NEQ; il += kThreads) {
+      const int nd = lo / NEQ + il, p0 = __ldg(a.csr_ptr + nd), cnt = __ldg(a.csr_ptr + nd + 1) - p0;
+      ncnt[il] = cnt;
+      for (int q = 0; q < cnt; q++) {
+        const int v = __ldg(a.csr_idx + p0 + q);
+        noff[il * kMaxValence + q] = (v / NNOD) * KE + (v % NNOD) * NEQ;
+      }
+    }
   // ||b|| over the own unknowns, then the stopping threshold rtol ||b|| (the same bits in
   // every block)
   {
@@ -922,7 +943,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
 namespace {
 
 template <int KE, int NEQ, int NNOD, typename TR, bool RES>
-cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, cudaStream_t st) {
+cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, int node_cache, cudaStream_t st) {
   auto* k = gmres_persistent_kernel<KE, NEQ, NNOD, TR, RES>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_bytes);
   if (e != cudaSuccess) return e;
@@ -931,6 +952,7 @@ cudaError_t launch_cfg(const PersistentArgs& a, int blocks, size_t dyn_bytes, cu
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   PersistentArgs args = a;
+  args.node_cache = node_cache;
   void* params[] = {&args};
   return cudaLaunchCooperativeKernel((void*)k, dim3(blocks), dim3(kThreads), params, dyn_bytes, st);
 }
@@ -949,13 +971,17 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
   cudaError_t e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, true>);
   if (e != cudaSuccess) return e;
   const size_t res_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, true);
+  // the node pass's offsets: an entry count and kMaxValence offsets per own node
+  const size_t cache_bytes = (sizeof(int) * (size_t)pn * (kMaxValence + 1) + 7) / 8 * 8;
+  if (cgs && a.max_valence <= kMaxValence && fa.sharedSizeBytes + res_bytes + cache_bytes <= (size_t)optin)
+    return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes + cache_bytes, 1, st);
   if (cgs && fa.sharedSizeBytes + res_bytes <= (size_t)optin)
-    return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes, st);
+    return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes, 0, st);
   e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, false>);
   if (e != cudaSuccess) return e;
   const size_t str_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, false);
   if (fa.sharedSizeBytes + str_bytes > (size_t)optin) return cudaErrorInvalidValue;  // m too large
-  return launch_cfg<KE, NEQ, NNOD, TR, false>(a, blocks, str_bytes, st);
+  return launch_cfg<KE, NEQ, NNOD, TR, false>(a, blocks, str_bytes, 0, st);
 }
 
 cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {

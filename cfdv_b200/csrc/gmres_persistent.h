@@ -49,6 +49,8 @@ struct PersistentArgs {
   const int* nbr_idx;
   int nbr_blocks;
   unsigned int* nbr_flag;      // per block (32 apart): neighbour syncs passed, zero before launch
+  int max_valence;             // most (element, local node) entries of a node in the CSR
+  int node_cache;              // set at launch: the node pass's gather offsets kept in shared memory
 };
 
 // The neighbour sets above for `blocks` blocks (the kernel's node and element ownership);
