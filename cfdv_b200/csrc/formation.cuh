@@ -24,6 +24,10 @@
 
 namespace cfdv {
 
+#ifndef CFDV_FORM3D_BLOCKS
+#define CFDV_FORM3D_BLOCKS 5  // 3D formation blocks per SM the register allocation is sized for
+#endif
+
 template <int NDIM>
 struct FormTraits {
   static constexpr int NNOD = (NDIM == 2) ? 4 : 8;
@@ -42,7 +46,7 @@ struct FormTraits {
   // coefficient rows per Gauss point for the column node M: Phi_M, dPhi_M,j (j < NDIM) and,
   // in 2D, S_M = sum_j dPhi_M,j for the upwind term
   static constexpr int NCOEF = 1 + NDIM + (NDIM == 2 ? 1 : 0);
-  static constexpr int MIN_BLOCKS = (NDIM == 2) ? 12 : 5;  // resident blocks per SM (register cap)
+  static constexpr int MIN_BLOCKS = (NDIM == 2) ? 12 : CFDV_FORM3D_BLOCKS;  // resident blocks per SM (register cap)
 };
 
 // hex8 faces (FiniteElement/get_face.h:106-164), quad4 edges (get_face.h:80-89)
