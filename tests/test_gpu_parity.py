@@ -3,8 +3,8 @@
 Tolerances: element matrices, rhs and the EBE product agree with the FP64 oracle to
 <= 1e-12 relative (per element max-norm); the reference-mode solve, whose break
 decisions and Givens arithmetic run on the host exactly as in the reference, matches
-the per-step GMRES history and conserved fields to <= 1e-10 relative (north-star
-bar); the textbook solver reaches its 1e-8 true residual in FP64 and in mixed
+the per-step GMRES history and conserved fields to <= 1e-10 relative (the parity bar
+for the plain FP64 form); the textbook solver reaches its 1e-8 true residual in FP64 and in mixed
 precision, the mixed field within 1e-6 of FP64."""
 import numpy as np
 import pytest
