@@ -493,13 +493,22 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
     }
   };
   // hs[i] = sum over the blocks of partm[i][b], i < nt, in the same order in every block
+  // (two slots per warp at once, so up to 64 slots cost one round trip to L2)
   auto reduce_parts = [&](int nt, double* hs) {
-    for (int i = wid; i < nt; i += kWarps) {
-      double acc = 0.0;
+    for (int i = wid; i < nt; i += 2 * kWarps) {
+      const int i2 = i + kWarps;
+      double acc = 0.0, acc2 = 0.0;
 #pragma unroll 4
-      for (int b = lane; b < nb; b += 32) acc += __ldcg(pm + (size_t)i * kPartLd + b);
+      for (int b = lane; b < nb; b += 32) {
+        acc += __ldcg(pm + (size_t)i * kPartLd + b);
+        if (i2 < nt) acc2 += __ldcg(pm + (size_t)i2 * kPartLd + b);
+      }
       acc = xor_sum(acc);
-      if (lane == 0) hs[i] = acc;
+      acc2 = xor_sum(acc2);
+      if (lane == 0) {
+        hs[i] = acc;
+        if (i2 < nt) hs[i2] = acc2;
+      }
     }
     __syncthreads();
   };
