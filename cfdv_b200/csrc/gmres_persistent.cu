@@ -1013,42 +1013,5 @@ int persistent_blocks() {
   return sms < kRedBlocks ? sms : kRedBlocks;
 }
 
-// Ownership as in the kernel: block b owns nodes [b pn, (b+1) pn), pn = ceil(n_nodes / nb)
-// (gmres_persistent_kernel), and in 2D elements [b per, (b+1) per), per = ceil(E / nb)
-// (ElemChunks with U > 1).
-bool persistent_neighbour_sets(int ndim, int n_nodes, int n_elements, const int* conn, const int* csr_ptr,
-                               const int* csr_idx, int blocks, std::vector<int>& ptr, std::vector<int>& idx) {
-  constexpr int kMaxSet = 32;  // one polling lane each
-  if (ndim != 2 || blocks <= 0 || n_nodes <= 0 || n_elements <= 0) return false;
-  constexpr int nnod = 4;
-  const int nb = blocks, pn = (n_nodes + nb - 1) / nb, per = (n_elements + nb - 1) / nb;
-  ptr.assign(2 * (nb + 1), 0);
-  idx.clear();
-  std::vector<int> seen(nb, -1);
-  auto add = [&](int b, int o) {
-    if (o != b && seen[o] != b) {
-      seen[o] = b;
-      idx.push_back(o);
-    }
-  };
-  for (int b = 0; b < nb; b++) {  // blocks owning the nodes of b's elements
-    ptr[b] = (int)idx.size();
-    const int e0 = std::min(n_elements, b * per), e1 = std::min(n_elements, e0 + per);
-    for (int e = e0; e < e1; e++)
-      for (int l = 0; l < nnod; l++) add(b, conn[(size_t)e * nnod + l] / pn);
-    if ((int)idx.size() - ptr[b] > kMaxSet) return false;
-  }
-  ptr[nb] = (int)idx.size();
-  std::fill(seen.begin(), seen.end(), -1);
-  for (int b = 0; b < nb; b++) {  // blocks owning the elements at b's nodes
-    ptr[nb + 1 + b] = (int)idx.size();
-    const int n0 = std::min(n_nodes, b * pn), n1 = std::min(n_nodes, n0 + pn);
-    for (int nd = n0; nd < n1; nd++)
-      for (int p = csr_ptr[nd]; p < csr_ptr[nd + 1]; p++) add(b, (csr_idx[p] / nnod) / per);
-    if ((int)idx.size() - ptr[nb + 1 + b] > kMaxSet) return false;
-  }
-  ptr[2 * nb + 1] = (int)idx.size();
-  return true;
-}
 
 }  // namespace cfdv

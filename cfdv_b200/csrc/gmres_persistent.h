@@ -4,6 +4,8 @@
 
 #include <vector>
 
+#include "neighbour_sets.h"
+
 namespace cfdv {
 
 struct PersistentArgs {
@@ -53,11 +55,6 @@ struct PersistentArgs {
   int node_cache;              // set at launch: the node pass's gather offsets kept in shared memory
 };
 
-// The neighbour sets above for `blocks` blocks (the kernel's node and element ownership);
-// false when they do not apply (3D, whose element waves interleave over the grid) or when a
-// set has more than 32 blocks.
-bool persistent_neighbour_sets(int ndim, int n_nodes, int n_elements, const int* conn, const int* csr_ptr,
-                               const int* csr_idx, int blocks, std::vector<int>& ptr, std::vector<int>& idx);
 int persistent_blocks();
 
 cudaError_t launch_gmres_persistent(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st);
