@@ -935,14 +935,25 @@ int cfdv_rms(cfdv_ctx* c, double* rms) {
 }
 
 int cfdv_step(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, double* dt) {
+  return cfdv_step_host(c, cfl, o, rep, dt, nullptr, nullptr);
+}
+
+int cfdv_step_host(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, double* dt,
+                   const double* U_in, double* U_out) {
   if (!c || !o) return CFDV_ERR_ARG;
   int rc;
   if (o->mode == CFDV_GMRES_REFERENCE || o->engine == 1) {  // host-driven solvers
+    if (U_in && (rc = cfdv_set_state(c, U_in, (size_t)c->n_dof))) return rc;
     double d;
-    if ((rc = cfdv_cfl(c, cfl, &d))) return rc;
-    if ((rc = cfdv_form(c, d, o->precision))) return rc;
-    if ((rc = cfdv_gmres(c, o, rep))) return rc;
-    if ((rc = cfdv_update(c))) return rc;
+    rc = cfdv_cfl(c, cfl, &d);
+    if (!rc) rc = cfdv_form(c, d, o->precision);
+    if (!rc) rc = cfdv_gmres(c, o, rep);
+    if (!rc) rc = cfdv_update(c);
+    if (U_out) {
+      const int rc2 = cfdv_get_state(c, U_out, nullptr, (size_t)c->n_dof);
+      if (!rc) rc = rc2;
+    }
+    if (rc) return rc;
     if (dt) *dt = d;
     return CFDV_OK;
   }
@@ -952,6 +963,7 @@ int cfdv_step(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres_repo
   if (o->m <= 0 || o->restarts < 0) return fail(c, CFDV_ERR_ARG, "gmres: m > 0, restarts >= 0");
   cudaSetDevice(c->dev);
   if (rep) { rep->n_est = 0; rep->n_restarts = 0; rep->n_matvec = 0; rep->true_rel_res = -1.0; }
+  if (U_in) CK(cudaMemcpyAsync(c->d_U, U_in, sizeof(double) * c->n_dof, cudaMemcpyHostToDevice, c->st));
   double* d_dt = c->d_sc + 2;
   CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, kRedBlocks, d_dt,
                 c->st));
@@ -964,6 +976,7 @@ int cfdv_step(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres_repo
   double* hs = c->h_pin + cfdv::ctxi::kPinStep;
   CK(cudaMemcpyAsync(hs, d_dt, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(hs + 1, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  if (U_out) CK(cudaMemcpyAsync(U_out, c->d_U, sizeof(double) * c->n_dof, cudaMemcpyDeviceToHost, c->st));
   rc = cfdv::ctxi::solve_finish(c, L, rep);  // waits for the stream
   const double d = hs[0];
   int status;

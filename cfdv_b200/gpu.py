@@ -29,7 +29,8 @@ EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error",
            "cfdv_form", "cfdv_set_element_matrices", "cfdv_gmres", "cfdv_update", "cfdv_rms", "cfdv_step", "cfdv_get_fdv_params",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
            "cfdv_profile_read", "cfdv_vjp", "cfdv_jvp", "cfdv_element_functional", "cfdv_wall_force",
-           "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static", "cfdv_set_adaptive"]
+           "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static", "cfdv_set_adaptive",
+           "cfdv_step_host"]
 
 
 class CfdvError(RuntimeError):
@@ -108,6 +109,7 @@ def lib():
         L.cfdv_update.argtypes = [P]
         L.cfdv_rms.argtypes = [P, P]
         L.cfdv_step.argtypes = [P, D, P, P, P]
+        L.cfdv_step_host.argtypes = [P, D, P, P, P, P, P]
         L.cfdv_get_fdv_params.argtypes = [P, P]
         L.cfdv_get_element_matrices.argtypes = [P, P, P]
         L.cfdv_get_rhs_vector.argtypes = [P, P]
@@ -283,6 +285,22 @@ class FDVSolver:
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))
+        out = self._unpack(rep, est, fin)
+        out["dt"] = dt.value
+        return out
+
+    def step_host(self, cfl, U_in, U_out, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
+                  true_residual=False, engine=0, precond=True, orth=2):
+        """step() with the state passed in and out as host float64 arrays (None: not copied);
+        one host synchronisation for copies and step together."""
+        for a in (U_in, U_out):
+            if a is not None:
+                assert a.dtype == np.float64 and a.size == self.n_dof and a.flags.c_contiguous
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
+        rep, est, fin = self._report(m, restarts)
+        dt = C.c_double()
+        self._ck(self.L.cfdv_step_host(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt),
+                                       None if U_in is None else _p(U_in), None if U_out is None else _p(U_out)))
         out = self._unpack(rep, est, fin)
         out["dt"] = dt.value
         return out

@@ -160,6 +160,13 @@ int cfdv_update(cfdv_ctx* ctx);
 int cfdv_rms(cfdv_ctx* ctx, double* rms);
 /* cfdv_cfl + cfdv_form + cfdv_gmres + cfdv_update in the driver's order (main.cpp:179-197). */
 int cfdv_step(cfdv_ctx* ctx, double cfl, const cfdv_gmres_opts* opts, cfdv_gmres_report* report, double* dt);
+/* cfdv_step with the state in host memory: U_in [n_nodes*neqn] (null: keep the device state) is
+ * copied in before the step and the state after it (unchanged when the step failed) is copied to
+ * U_out (null: none), all on the context's stream with the step's single wait.  The same as
+ * cfdv_set_state + cfdv_step + cfdv_get_state, one host synchronisation instead of three: a
+ * driver that keeps its nodes' state on the host, as main.cpp:169-198 does, calls this. */
+int cfdv_step_host(cfdv_ctx* ctx, double cfl, const cfdv_gmres_opts* opts, cfdv_gmres_report* report, double* dt,
+                   const double* U_in, double* U_out);
 
 /* ---- inspection (tests, output) --------------------------------------------- */
 /* s1..s4 per element [n_elements][4] from the last cfdv_form (Tecplot cell data). */

@@ -90,3 +90,24 @@ def test_neighbour_syncs_match_grid_barriers(gpu, name, prec, precond):
         assert np.array_equal(d, d3)
         assert np.array_equal(r["est"], r3["est"])
         assert r["restarts"] == r3["restarts"] and r["true_rel_res"] == r3["true_rel_res"]
+
+
+@pytest.mark.parametrize("name", ["plate20", "ramp4"])
+@pytest.mark.parametrize("engine", [0, 1])
+def test_step_host_equals_set_step_get(gpu, name, engine):
+    """cfdv_step_host (state in and out as host arrays, one wait) gives the same state, dt and
+    residual history as cfdv_set_state + cfdv_step + cfdv_get_state."""
+    case = get_case(name)
+    kw = dict(mode=gpu.GMRES_CORRECT, m=30, restarts=80, rtol=1e-8, precision=gpu.PREC_MIXED, engine=engine)
+    with gpu.FDVSolver(case) as s:
+        s.load_node_records()
+        U0 = s.get_state()
+        s.set_state(U0)
+        r1 = s.step(float(case.control["cfl"]), **kw)
+        U1 = s.get_state()
+        s.set_state(np.zeros_like(U0))  # overwritten by the step's own upload
+        U2 = np.empty_like(U0)
+        r2 = s.step_host(float(case.control["cfl"]), U0, U2, **kw)
+        U3 = s.get_state()
+    assert np.array_equal(U1, U2) and np.array_equal(U2, U3)
+    assert r1["dt"] == r2["dt"] and np.array_equal(r1["est"], r2["est"])
