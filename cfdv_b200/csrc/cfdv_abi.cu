@@ -29,7 +29,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
-  dfree(c->d_pm); dfree(c->d_nbr_ptr); dfree(c->d_nbr_idx); c->nbr_blocks = 0;
+  dfree(c->d_pm); dfree(c->d_cfl_count); dfree(c->d_nbr_ptr); dfree(c->d_nbr_idx); c->nbr_blocks = 0;
   dfree(c->d_hnm_idx); dfree(c->d_hnm); c->n_adaptive = 0;
   dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
   c->adj_state_cap = 0;
@@ -209,7 +209,7 @@ int setup_mesh(cfdv_ctx* c, const cfdv_mesh* m) {
       (rc = dalloc(c, &c->d_Y32, E * Ke)) || (rc = dalloc(c, &c->d_W, (size_t)c->n_dof)) ||
       (rc = dalloc(c, &c->d_b, (size_t)c->n_dof)) || (rc = dalloc(c, &c->d_pa, (size_t)kRedBlocks * 10)) ||
       (rc = dalloc(c, &c->d_pb, (size_t)kRedBlocks * 10)) || (rc = dalloc(c, &c->d_sc, 16)) ||
-      (rc = dalloc(c, &c->d_status, 1)) || (rc = dalloc(c, &c->d_rms, 16)))
+      (rc = dalloc(c, &c->d_status, 1)) || (rc = dalloc(c, &c->d_rms, 16)) || (rc = dalloc(c, &c->d_cfl_count, 1)))
     return rc;
   CK(cudaMallocHost((void**)&c->h_pin, 4096 * sizeof(double)));
   CK(cudaMemcpyAsync(c->d_x, m->x, sizeof(double) * c->n_nodes * c->ndim, cudaMemcpyHostToDevice, c->st));
@@ -229,6 +229,7 @@ int setup_mesh(cfdv_ctx* c, const cfdv_mesh* m) {
   CK(cudaMemsetAsync(c->d_U0, 0, sizeof(double) * c->n_dof, c->st));
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
   CK(cudaMemsetAsync(c->d_status, 0, sizeof(int), c->st));
+  CK(cudaMemsetAsync(c->d_cfl_count, 0, sizeof(unsigned int), c->st));
   CK(cudaStreamSynchronize(c->st));
   return CFDV_OK;
 }
@@ -805,9 +806,9 @@ int cfdv_state_device_ptr(cfdv_ctx* c, double** U) {
 int cfdv_cfl(cfdv_ctx* c, double cfl, double* dt) {
   if (!c || !dt) return CFDV_ERR_ARG;
   cudaSetDevice(c->dev);
-  CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, kRedBlocks,
-                c->d_sc + 2, c->st));
-  c->launches += 2;
+  CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, c->d_cfl_count,
+                kRedBlocks, c->d_sc + 2, c->st));
+  c->launches++;
   CK(cudaMemcpyAsync(c->h_pin, c->d_sc + 2, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   *dt = c->h_pin[0];
@@ -965,9 +966,9 @@ int cfdv_step_host(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres
   if (rep) { rep->n_est = 0; rep->n_restarts = 0; rep->n_matvec = 0; rep->true_rel_res = -1.0; }
   if (U_in) CK(cudaMemcpyAsync(c->d_U, U_in, sizeof(double) * c->n_dof, cudaMemcpyHostToDevice, c->st));
   double* d_dt = c->d_sc + 2;
-  CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, kRedBlocks, d_dt,
-                c->st));
-  c->launches += 2;
+  CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, c->d_cfl_count,
+                kRedBlocks, d_dt, c->st));
+  c->launches++;
   if ((rc = form_enqueue(c, 0.0, d_dt, o->precision))) return rc;
   cfdv::ctxi::SolveLaunch L;
   if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L))) return rc;

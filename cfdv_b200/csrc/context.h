@@ -52,6 +52,7 @@ struct cfdv_ctx {
   double* d_y = nullptr;
   double* d_rms = nullptr;
   int* d_status = nullptr;
+  unsigned int* d_cfl_count = nullptr;  // blocks of the CFL kernel done (the last one resets it)
   double* h_pin = nullptr;  // pinned host staging
   double* h_hist = nullptr;  // pinned: the Givens estimates and final |g| of a persistent solve
   size_t h_hist_cap = 0;

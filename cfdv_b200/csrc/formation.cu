@@ -39,7 +39,8 @@ cudaError_t launch_form(int ndim, const FormArgs& a, cudaStream_t st) {
 // ---- CFL (MPI_CFL.h:124-171): dt = cfl * min_e min_nodes cleng_e / (|v| + sqrt(1.4 cgas T))
 template <int NDIM>
 __global__ void cfl_partial_kernel(const double* __restrict__ U, const int* __restrict__ conn,
-                                   const double* __restrict__ cleng, int E, GasParams g, double* partial) {
+                                   const double* __restrict__ cleng, int E, GasParams g, double* partial,
+                                   unsigned int* count, double cfl, double* dt_out) {
   constexpr int NNOD = (NDIM == 2) ? 4 : 8, NEQ = NDIM + 2;
   double best = 1000.0;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
@@ -52,23 +53,31 @@ __global__ void cfl_partial_kernel(const double* __restrict__ U, const int* __re
     best = fmin(best, dxele);
   }
   best = block_reduce_min(best);
-  if (threadIdx.x == 0) partial[blockIdx.x] = best;
-}
-
-// final min over the block partials and dt = cfl * min (dt stays unset when no element
-// has a finite signal speed, as in the reference where dx_dv starts at 1000)
-__global__ void cfl_final_kernel(const double* partial, int nb, double cfl, double* dt_out) {
-  double best = 1000.0;
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) best = fmin(best, partial[i]);
-  best = block_reduce_min(best);
-  if (threadIdx.x == 0) dt_out[0] = (best < 1000.0) ? cfl * best : 0.0;
+  // the last block to finish takes the min over the block partials: dt = cfl * min (dt stays
+  // unset when no element has a finite signal speed, as in the reference where dx_dv starts
+  // at 1000); a min does not depend on the order, and the last block resets the count
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = best;
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double all = 1000.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) all = fmin(all, __ldcg(partial + i));
+  all = block_reduce_min(all);
+  if (threadIdx.x == 0) {
+    dt_out[0] = (all < 1000.0) ? cfl * all : 0.0;
+    *count = 0u;
+  }
 }
 
 cudaError_t launch_cfl(int ndim, const double* U, const int* conn, const double* cleng, int E, const GasParams& g,
-                       double cfl, double* partial, int nb, double* dt_out, cudaStream_t st) {
-  if (ndim == 2) cfl_partial_kernel<2><<<nb, 256, 0, st>>>(U, conn, cleng, E, g, partial);
-  else cfl_partial_kernel<3><<<nb, 256, 0, st>>>(U, conn, cleng, E, g, partial);
-  cfl_final_kernel<<<1, 256, 0, st>>>(partial, nb, cfl, dt_out);
+                       double cfl, double* partial, unsigned int* count, int nb, double* dt_out, cudaStream_t st) {
+  if (ndim == 2) cfl_partial_kernel<2><<<nb, 256, 0, st>>>(U, conn, cleng, E, g, partial, count, cfl, dt_out);
+  else cfl_partial_kernel<3><<<nb, 256, 0, st>>>(U, conn, cleng, E, g, partial, count, cfl, dt_out);
   return cudaGetLastError();
 }
 

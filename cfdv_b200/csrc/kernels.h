@@ -71,7 +71,7 @@ __device__ __forceinline__ double reduce_partials(const double* __restrict__ p, 
 struct FormArgs;
 cudaError_t launch_form(int ndim, const FormArgs& a, cudaStream_t st);
 cudaError_t launch_cfl(int ndim, const double* U, const int* conn, const double* cleng, int E, const GasParams& g,
-                       double cfl, double* partial, int nb, double* dt_out, cudaStream_t st);
+                       double cfl, double* partial, unsigned int* count, int nb, double* dt_out, cudaStream_t st);
 
 // EBE product y = sum_e P_e^T R_e P_e x (optionally transposed), element pass + node pass.
 struct EbeArgs {
