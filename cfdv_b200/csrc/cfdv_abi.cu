@@ -430,11 +430,13 @@ int gmres_reference(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* re
 }
 
 // node-block Jacobi inverse from the FP64 element matrices (one pass over them)
-int build_block_jacobi(cfdv_ctx* c) {
+// (with rhs: b = gather(rhs) assembled by the same launch)
+int build_block_jacobi(cfdv_ctx* c, const double* rhs = nullptr, double* b = nullptr) {
   int rc;
   if (!c->d_Dinv && (rc = dalloc(c, &c->d_Dinv, (size_t)c->n_nodes * c->neqn * c->neqn))) return rc;
   if (!c->d_Z && (rc = dalloc(c, &c->d_Z, (size_t)c->n_dof))) return rc;
-  CK(launch_block_jacobi(c->ndim, c->d_csr_ptr, c->d_csr_idx, c->d_R64, c->n_nodes, c->d_Dinv, c->d_status, c->st));
+  CK(launch_block_jacobi(c->ndim, c->d_csr_ptr, c->d_csr_idx, c->d_R64, c->n_nodes, c->d_Dinv, c->d_status, rhs, b,
+                         c->st));
   c->launches++;
   return CFDV_OK;
 }
@@ -531,10 +533,12 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   const size_t n_int = 32 + 32 * (size_t)persistent_max_blocks();
   if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, n_int))) return rc;
   CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
+  // b from the element rhs: assembled by the block-Jacobi launch when there is one
+  const bool fuse_b = !rhs_vec && !transpose && o->precond;
   if (rhs_vec) {
     if (rhs_vec != c->d_b)
       CK(cudaMemcpyAsync(c->d_b, rhs_vec, sizeof(double) * c->n_dof, cudaMemcpyDeviceToDevice, c->st));
-  } else {
+  } else if (!fuse_b) {
     CK(launch_compose_rhs(ebe_args(c), c->d_rhs, c->d_b, c->d_pa, c->st));
     c->launches++;
   }
@@ -560,7 +564,7 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
     c->launches += r32 ? 2 : 1;
   }
   if (o->precond) {
-    if ((rc = build_block_jacobi(c))) {
+    if ((rc = fuse_b ? build_block_jacobi(c, c->d_rhs, c->d_b) : build_block_jacobi(c))) {
       if (transpose) launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st);
       return rc;
     }

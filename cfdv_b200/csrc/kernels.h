@@ -110,7 +110,7 @@ cudaError_t launch_to_float(const double* in, float* out, size_t n, cudaStream_t
 cudaError_t launch_transpose_blocks(int ke, double* R64, float* R32, int E, cudaStream_t st);
 // node-block Jacobi: Dinv_n = (sum of the node's diagonal element blocks)^-1, FP64
 cudaError_t launch_block_jacobi(int ndim, const int* ptr, const int* idx, const double* R, int n_nodes, double* Dinv,
-                                int* status, cudaStream_t st);
+                                int* status, const double* rhs, double* b, cudaStream_t st);
 // z = Dinv v
 cudaError_t launch_block_apply(int ndim, const double* Dinv, const double* v, double* z, int n_nodes, cudaStream_t st);
 // du += Dinv (V y)

@@ -276,11 +276,23 @@ cudaError_t launch_rms_partial(const double* U, const double* U0, int n_nodes, i
 // neqn x neqn block at that local node; Dinv_n by Gauss-Jordan with partial pivoting in FP64.
 namespace cfdv {
 
+// With rhs, the node also assembles b = gather(rhs) over the same list, in the list's order as
+// the node pass does (so the same bits), saving that pass its own launch.
 template <int NEQ, int NNOD>
 __global__ void block_jacobi_kernel(const int* __restrict__ ptr, const int* __restrict__ idx,
-                                    const double* __restrict__ R, int n_nodes, double* Dinv, int* status) {
+                                    const double* __restrict__ R, int n_nodes, double* Dinv, int* status,
+                                    const double* __restrict__ rhs, double* b) {
   constexpr int KE = NEQ * NNOD;
   for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_nodes; n += gridDim.x * blockDim.x) {
+    if (rhs)
+      for (int k = 0; k < NEQ; k++) {
+        double s = 0.0;
+        for (int p = ptr[n]; p < ptr[n + 1]; p++) {
+          const int v = idx[p];
+          s += rhs[(size_t)(v / NNOD) * KE + (v % NNOD) * NEQ + k];
+        }
+        b[(size_t)n * NEQ + k] = s;
+      }
     double A[NEQ][2 * NEQ];
 #pragma unroll
     for (int r = 0; r < NEQ; r++)
@@ -373,9 +385,9 @@ __global__ void combine_precond_kernel(double* du, const double* __restrict__ V,
 }
 
 cudaError_t launch_block_jacobi(int ndim, const int* ptr, const int* idx, const double* R, int n_nodes, double* Dinv,
-                                int* status, cudaStream_t st) {
-  if (ndim == 2) block_jacobi_kernel<4, 4><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status);
-  else block_jacobi_kernel<5, 8><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status);
+                                int* status, const double* rhs, double* b, cudaStream_t st) {
+  if (ndim == 2) block_jacobi_kernel<4, 4><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status, rhs, b);
+  else block_jacobi_kernel<5, 8><<<kRedBlocks, 128, 0, st>>>(ptr, idx, R, n_nodes, Dinv, status, rhs, b);
   return cudaGetLastError();
 }
 
