@@ -4,7 +4,7 @@
 //
 // One step of the textbook path is  dt = CFL(U),  A(U, dt) dU = b(U, dt),  U' = U + dU,
 // with A, b the assembled element matrices and rhs after ApplyBC (FDVGalerkin.h:121-154,
-// ApplyBC.h:131-250).  With dU held fixed, the element residual r_e = rhs_e - R_e dU_e
+// ApplyBC.h:14-133).  With dU held fixed, the element residual r_e = rhs_e - R_e dU_e
 // carries every dependence of the step on U, dt and the Mach number; its derivatives are
 // evaluated here by forward-mode dual numbers through the same templated physics the
 // formation kernel runs (fdv_physics.cuh, formation.cuh), so they are the derivatives of

@@ -47,7 +47,7 @@ void free_all(cfdv_ctx* c) {
 }
 
 // Dirichlet flags per DOF from the faces (LoadBinary.h:264-318) and the per-element
-// row mask that ApplyBC (ApplyBC.h:131-250) zeroes: rows of face nodes whose DOF is
+// row mask that ApplyBC (ApplyBC.h:14-133) zeroes: rows of face nodes whose DOF is
 // flagged, except energy on bc 1 faces of an isothermal wall (its handler is empty).
 void build_bc_masks(const cfdv_mesh* m, int adiabatic, std::vector<uint64_t>& mask) {
   const int ndim = m->ndim, nnod = ndim == 2 ? 4 : 8, neqn = ndim + 2, nface = ndim == 2 ? 4 : 6;
@@ -973,9 +973,19 @@ int cfdv_step_host(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres
   CK(launch_cfl(c->ndim, c->d_U, c->d_conn, c->d_cleng, c->n_elements, c->gas, cfl, c->d_pa, c->d_cfl_count,
                 kRedBlocks, d_dt, c->st));
   c->launches++;
-  if ((rc = form_enqueue(c, 0.0, d_dt, o->precision))) return rc;
+  // a failure before the update is enqueued leaves the state as it was: hand it back in U_out
+  // as the host-driven branch does
+  auto unchanged_out = [&](int code) {
+    if (U_out) {
+      if (cudaMemcpyAsync(U_out, c->d_U, sizeof(double) * c->n_dof, cudaMemcpyDeviceToHost, c->st) == cudaSuccess)
+        cudaStreamSynchronize(c->st);
+      cudaGetLastError();
+    }
+    return code;
+  };
+  if ((rc = form_enqueue(c, 0.0, d_dt, o->precision))) return unchanged_out(rc);
   cfdv::ctxi::SolveLaunch L;
-  if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L))) return rc;
+  if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L))) return unchanged_out(rc);
   CK(launch_state_update_guarded(c->d_U, c->d_U0, c->d_du, c->n_dof, L.err, c->d_status, d_dt, c->st));
   c->launches++;
   double* hs = c->h_pin + cfdv::ctxi::kPinStep;
@@ -1010,6 +1020,25 @@ int cfdv_get_element_matrices(cfdv_ctx* c, double* R, double* rhs) {
   const size_t E = c->n_elements, Ke = c->Ke;
   if (R) CK(cudaMemcpyAsync(R, c->d_R64, sizeof(double) * E * Ke * Ke, cudaMemcpyDeviceToHost, c->st));
   if (rhs) CK(cudaMemcpyAsync(rhs, c->d_rhs, sizeof(double) * E * Ke, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CFDV_OK;
+}
+
+int cfdv_get_element_subset(cfdv_ctx* c, int n, const int* ids, double* R, double* rhs, double* s) {
+  if (!c || n < 0 || (n > 0 && !ids)) return CFDV_ERR_ARG;
+  if (!c->formed) return fail(c, CFDV_ERR_STATE, "element matrices before form");
+  for (int k = 0; k < n; k++)
+    if (ids[k] < 0 || ids[k] >= c->n_elements) return fail(c, CFDV_ERR_ARG, "element subset: id out of range");
+  cudaSetDevice(c->dev);
+  const size_t Ke = c->Ke;
+  // one copy per element and array: meant for a few hundred elements at most
+  for (int k = 0; k < n; k++) {
+    const size_t e = (size_t)ids[k];
+    if (R) CK(cudaMemcpyAsync(R + k * Ke * Ke, c->d_R64 + e * Ke * Ke, sizeof(double) * Ke * Ke,
+                              cudaMemcpyDeviceToHost, c->st));
+    if (rhs) CK(cudaMemcpyAsync(rhs + k * Ke, c->d_rhs + e * Ke, sizeof(double) * Ke, cudaMemcpyDeviceToHost, c->st));
+    if (s) CK(cudaMemcpyAsync(s + 4 * k, c->d_s + 4 * e, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+  }
   CK(cudaStreamSynchronize(c->st));
   return CFDV_OK;
 }

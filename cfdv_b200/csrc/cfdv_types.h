@@ -13,7 +13,7 @@
 
 namespace cfdv {
 
-// Nondimensional gas model of the reference (Thermo::set, FDV/Thermo.h:158-169).  The
+// Nondimensional gas model of the reference (Thermo::set, FDV/Thermo.h:22-33).  The
 // Mach-number-dependent constants Cv, cgas and cmach have the scalar type S, so that the
 // adjoint kernels can differentiate through them (GasT<Dual>); the step uses GasT<double>.
 template <class S>

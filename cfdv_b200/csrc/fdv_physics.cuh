@@ -2,9 +2,9 @@
 // Gauss-point flow state, viscous stress, flux Jacobians and fluxes.
 //
 // Formulas follow the CFDV reference (paths relative to its src/):
-//   gas model            FDV/Thermo.h:148-211
-//   shape functions      FiniteElement/TestFunctions2D.h:173-256, TestFunctions3D.h:7-123
-//   Gauss-point state    FDV/FDVGalerkin.h:761-797, FDV/tau.h:105-133
+//   gas model            FDV/Thermo.h:8-86
+//   shape functions      FiniteElement/TestFunctions2D.h:7-102, TestFunctions3D.h:7-123
+//   Gauss-point state    FDV/FDVGalerkin.h:761-797, FDV/tau.h:14-42
 //   a = dF/dU            FDV/NavierStokes2D.h:59-97,  FDV/NavierStokes3D.h:74-189
 //   b = dG/dU            FDV/NavierStokes2D.h:100-158, FDV/NavierStokes3D.h:193-343
 //   c = dG/dU_,j         FDV/NavierStokes2D.h:163-222, FDV/NavierStokes3D.h:347-477
@@ -40,7 +40,7 @@ CFDV_HD CFDV_INLINE S gas_k(const GasT<S>& g, S mu) {
   return mu / ((g.gamma - 1.0) * (g.cmach * g.cmach) * g.Pr);
 }
 
-// primitive state of a node (NodeUnpack.h:185-205); coordinates are plain doubles
+// primitive state of a node (NodeUnpack.h:9-29); coordinates are plain doubles
 template <class S>
 struct NodePrimT {
   S U[5];
@@ -69,8 +69,8 @@ CFDV_HD CFDV_INLINE void node_unpack(const GasT<S>& g, const S* U, const double*
   n.p = RN_MUL(RN_MUL(n.rho, g.gamma - 1.0), e);
 }
 
-// CFL length of one node of an element (MPI_CFL.h:124-171): cleng / (|v| + sqrt(1.4 cgas T))
-// with T from NodeUnpack (NodeUnpack.h:191-203) clipped at 1e-9; the reference uses 1.4, not
+// CFL length of one node of an element (MPI_CFL.h:7-56): cleng / (|v| + sqrt(1.4 cgas T))
+// with T from NodeUnpack (NodeUnpack.h:24-28) clipped at 1e-9; the reference uses 1.4, not
 // gamma.  Returns false (no candidate) where the signal speed is not above 1e-9.
 template <int NDIM, class S>
 CFDV_HD CFDV_INLINE bool cfl_node_len(const S* u, double cleng, const GasT<S>& g, S* dxn) {

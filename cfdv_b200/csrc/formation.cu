@@ -36,7 +36,7 @@ cudaError_t launch_form(int ndim, const FormArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// ---- CFL (MPI_CFL.h:124-171): dt = cfl * min_e min_nodes cleng_e / (|v| + sqrt(1.4 cgas T))
+// ---- CFL (MPI_CFL.h:7-56): dt = cfl * min_e min_nodes cleng_e / (|v| + sqrt(1.4 cgas T))
 template <int NDIM>
 __global__ void cfl_partial_kernel(const double* __restrict__ U, const int* __restrict__ conn,
                                    const double* __restrict__ cleng, int E, GasParams g, double* partial,

@@ -1,8 +1,8 @@
 // FDV element formation as the phases of one thread block ("CTA") per element.
 //
 // Per element the CTA computes what the reference builds in FDVGalerkin::operator()
-// (FDV/FDVGalerkin.h:121-154) followed by ApplyBC (FDV/Function/ApplyBC.h:131-250):
-//   load      node unpack (NodeUnpack.h:185-205), boundary face list
+// (FDV/FDVGalerkin.h:121-154) followed by ApplyBC (FDV/Function/ApplyBC.h:14-133):
+//   load      node unpack (NodeUnpack.h:9-29), boundary face list
 //   domain    one thread per Gauss point: FDVParam (FDVParam.h:15-111), shape functions,
 //             Gauss-point state, stress, SUPG/discontinuity-capturing test function
 //             (FDVGalerkin.h:225-387), flux Jacobians and the rhs flux terms
@@ -13,7 +13,7 @@
 //             wJ dPhi_Ni dPhi_Mj (C = h_ij); X_i = dt (s1 a_i + s3 b_i) = -g_i = nd_i
 //             (FDVGalerkin.h:405-451)
 //   faces     same three phases per boundary face with 0 != bc < 100
-//             (FDVGalerkin.h:455-533, 643-756; TFNorm2D TestFunctions1D.h:207-216,
+//             (FDVGalerkin.h:455-533, 643-756; TFNorm2D TestFunctions1D.h:73-82,
 //             TFNorm3D calc_TF_norm3D.h:9-167, eval1dboundary.h, eval2dboundary.h)
 //   write     ApplyBC through the precomputed Dirichlet row mask, then a coalesced
 //             store of R (column-major, FP64 or FP32) and rhs.
@@ -64,9 +64,9 @@ CFDV_HD CFDV_INLINE int face_node(int ndim, int f, int i) {
 // Tensor's storage).  Its domain shape functions become Phi_M <- sum_N Phi_N Hnm(N, M) and
 // dPxi(M, j) likewise (MeshRefine2D.h:877-900, applied at FDVGalerkin.h:183-186, 198-201)
 // before the Jacobian; the 2D streamline-upwind term keeps the Jacobian of the untransformed
-// shape functions (FDVGalerkin.h:235-239).  A 3D boundary face takes its geometry from the
-// rows of Hnm x at its nodes (calc_TF_norm3D.h:25-57) and transforms its face shape
-// functions with the face's block of Hnm (MeshRefine2D.h:904-951 via FDVGalerkin.h:488-497;
+// shape functions (FDVGalerkin.h:237-240).  A 3D boundary face takes its geometry from the
+// rows of Hnm x at its nodes (calc_TF_norm3D.h:25-66) and transforms its face shape
+// functions with the face's block of Hnm (MeshRefine2D.h:904-951 via FDVGalerkin.h:489-497;
 // the face derivatives stay as computed).  2D faces are unchanged (FDVGalerkin.h:481-484).
 template <int NDIM>
 CFDV_HD CFDV_INLINE void hnm_shape(const double* H, double* Phi, double (*dPxi)[3]) {
@@ -252,7 +252,7 @@ CFDV_HD CFDV_INLINE double gp_point(const FormArgs& a, int q, double* z) {
   return w;
 }
 
-// step 0: node unpack (NodeUnpack.h:185-205) with the node's Mach and Reynolds numbers,
+// step 0: node unpack (NodeUnpack.h:9-29) with the node's Mach and Reynolds numbers,
 // boundary face list, shape functions
 template <int NDIM>
 CFDV_HD CFDV_INLINE void step_load(const FormArgs& a, FormShared<NDIM>& sh, int e, int tid) {
@@ -789,7 +789,7 @@ CFDV_HD CFDV_INLINE void edit_face_state_2d(int code, GpStateT<S>& f, const doub
 }
 
 // Face shape functions phib, derivatives along the face dpidx and the weighted normal en
-// at face Gauss point qf (2D TestFunctions1D.h:141-216, 3D calc_TF_norm3D.h:9-167); xf
+// at face Gauss point qf (2D TestFunctions1D.h:7-82, 3D calc_TF_norm3D.h:9-167); xf
 // holds the coordinates of the face's NBN nodes in face order.
 template <int NDIM>
 CFDV_HD CFDV_INLINE void face_point_geom(const double* gz, const double* gw, const double* const* xf, int qf,
@@ -798,7 +798,7 @@ CFDV_HD CFDV_INLINE void face_point_geom(const double* gz, const double* gw, con
   for (int i = 0; i < NBN; i++)
     for (int j = 0; j < 3; j++) dpidx[i][j] = 0.0;
   en[2] = 0.0;
-  if (NDIM == 2) {  // TestFunctions1D.h:141-216
+  if (NDIM == 2) {  // TestFunctions1D.h:7-82
     const double z = gz[qf], w = gw[qf];
     phib[0] = 0.5 * (1 - z);
     phib[1] = 0.5 * (1 + z);

@@ -29,34 +29,53 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
 std::atomic<double*> g_scratch[kMaxDevices];  // static storage: starts as nullptr
 
-// device address of the scratch array on the current device `dev`
-int scratch_on_device(int dev, double** out) {
-  double* p = g_scratch[dev].load(std::memory_order_acquire);
-  if (!p) {
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    p = g_scratch[dev].load(std::memory_order_relaxed);
-    if (!p) {
-      void* addr = nullptr;
-      if (cudaGetSymbolAddress(&addr, cfdv_static_elem_products) != cudaSuccess || !addr) {
-        cudaGetLastError();
-        return CFDV_ERR_CUDA;
-      }
-      p = static_cast<double*>(addr);
-      g_scratch[dev].store(p, std::memory_order_release);
-    }
-  }
-  *out = p;
-  return CFDV_OK;
-}
-
-// the GPU can only use memory the CUDA runtime knows: reject plain host memory
-bool device_reachable(const void* p) {
+// is `p` device memory of device `dev` (the runtime's view)?
+bool on_device(const void* p, int dev) {
   cudaPointerAttributes at;
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged || at.type == cudaMemoryTypeHost;
+  return at.type == cudaMemoryTypeDevice && at.device == dev;
+}
+
+// device address of the scratch array on the current device `dev`.  The address found at
+// the first call is kept; a later call checks that it still names memory of this device
+// (a cudaDeviceReset unloads the library's module and the array moves when it is loaded
+// again) and looks it up again when it does not.
+int scratch_on_device(int dev, double** out) {
+  double* p = g_scratch[dev].load(std::memory_order_acquire);
+  if (p && on_device(p, dev)) {
+    *out = p;
+    return CFDV_OK;
+  }
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  p = g_scratch[dev].load(std::memory_order_relaxed);
+  if (!p || !on_device(p, dev)) {
+    void* addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, cfdv_static_elem_products) != cudaSuccess || !addr) {
+      cudaGetLastError();
+      return CFDV_ERR_CUDA;
+    }
+    p = static_cast<double*>(addr);
+    g_scratch[dev].store(p, std::memory_order_release);
+  }
+  *out = p;
+  return CFDV_OK;
+}
+
+// The kernels run on device `dev`: accept its own device memory and managed memory, and
+// reject everything else -- pageable host memory, pinned host memory (reachable over the
+// bus, but not what this entry point promises to read) and another GPU's memory, whose
+// loads would fault instead of returning an error here.
+bool device_reachable(const void* p, int dev) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (at.type == cudaMemoryTypeManaged) return true;
+  return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
 }  // namespace
@@ -80,7 +99,7 @@ extern "C" int cfdv_ebe_matvec_static(int ndim, int n_nodes, int n_elements, con
   if (dev < 0 || dev >= kMaxDevices) return CFDV_ERR_ARG;
   const void* ptrs[] = {conn, node_ptr, node_idx, R, x, y};
   for (const void* p : ptrs)
-    if (!device_reachable(p)) return CFDV_ERR_ARG;
+    if (!device_reachable(p, dev)) return CFDV_ERR_ARG;
   double* scratch = nullptr;
   if (int rc = scratch_on_device(dev, &scratch)) return rc;
 

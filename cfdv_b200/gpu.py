@@ -30,7 +30,7 @@ EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
            "cfdv_profile_read", "cfdv_vjp", "cfdv_jvp", "cfdv_element_functional", "cfdv_wall_force",
            "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static", "cfdv_set_adaptive",
-           "cfdv_step_host"]
+           "cfdv_step_host", "cfdv_get_element_subset"]
 
 
 class CfdvError(RuntimeError):
@@ -112,6 +112,7 @@ def lib():
         L.cfdv_step_host.argtypes = [P, D, P, P, P, P, P]
         L.cfdv_get_fdv_params.argtypes = [P, P]
         L.cfdv_get_element_matrices.argtypes = [P, P, P]
+        L.cfdv_get_element_subset.argtypes = [P, I, P, P, P, P]
         L.cfdv_get_rhs_vector.argtypes = [P, P]
         L.cfdv_get_du.argtypes = [P, P]
         L.cfdv_matvec.argtypes = [P, P, P, I, I]
@@ -316,6 +317,16 @@ class FDVSolver:
         rhs = np.zeros((self.n_elements, self.Ke))
         self._ck(self.L.cfdv_get_element_matrices(self._ctx, _p(R), _p(rhs)))
         return R, rhs
+
+    def element_subset(self, ids):
+        """(R [n, Ke, Ke] column-major per element as element_matrices(), rhs [n, Ke],
+        s1..s4 [n, 4]) of the listed elements, copied alone."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        R = np.zeros((ids.size, self.Ke, self.Ke))
+        rhs = np.zeros((ids.size, self.Ke))
+        s = np.zeros((ids.size, 4))
+        self._ck(self.L.cfdv_get_element_subset(self._ctx, ids.size, _p(ids), _p(R), _p(rhs), _p(s)))
+        return R, rhs, s
 
     def rhs_vector(self):
         b = np.zeros(self.n_dof)

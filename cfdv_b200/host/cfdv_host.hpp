@@ -72,7 +72,7 @@ struct BinaryCase {
   std::vector<double> records;  // [Nn][2*ndim+2]
   std::vector<double> x;        // [Nn][ndim]
   std::vector<int> conn, bc;
-  // adaptive elements from the "adap" file when control adap is set (LoadBinary.h:246-260):
+  // adaptive elements from the "adap" file when control adap is set (LoadBinary.h:247-261):
   // ids, refine levels, and Hnm(N, M) at [k][N + nnod*M] (the Tensor storage, as written)
   std::vector<int> adap_el, adap_level;
   std::vector<double> adap_hnm;
@@ -205,7 +205,7 @@ inline void tecplot_write(const std::string& path, const BinaryCase& c, const cf
   const int nd = c.ndim, ne = nd + 2, Nn = c.n_nodes;
   const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
   std::vector<double> rho(Nn), T(Nn), pr(Nn), v((size_t)Nn * nd);
-  for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:185-205
+  for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:9-29
     const double* u = &U[(size_t)n * ne];
     rho[n] = u[0];
     double vsqr = 0;
@@ -286,7 +286,7 @@ inline void write_case_dir(const std::string& out, const BinaryCase& c, const st
   const int nd = c.ndim, ne = nd + 2, rs = 2 * nd + 2;
   const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
   std::vector<double> rec((size_t)c.n_nodes * rs);
-  for (int n = 0; n < c.n_nodes; n++) {  // NodeUnpack.h:185-205
+  for (int n = 0; n < c.n_nodes; n++) {  // NodeUnpack.h:9-29
     const double* u = &U[(size_t)n * ne];
     double* r = &rec[(size_t)n * rs];
     for (int k = 0; k < nd; k++) r[k] = c.x[(size_t)n * nd + k];
@@ -460,7 +460,7 @@ class EnsightSeries {
     const int nd = c_.ndim, ne = nd + 2, Nn = c_.n_nodes, step = (int)times_.size();
     const double Cv = 1. / p.gamma / (p.gamma - 1.0) / (p.mach * p.mach);
     std::vector<double> rho(Nn), T(Nn), pr(Nn), v((size_t)Nn * 3, 0.0);
-    for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:185-205
+    for (int n = 0; n < Nn; n++) {  // NodeUnpack.h:9-29
       const double* u = &U[(size_t)n * ne];
       rho[n] = u[0];
       double vsqr = 0;

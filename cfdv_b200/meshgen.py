@@ -40,7 +40,7 @@ class Case:
     control: dict = field(default_factory=dict)
     aero: dict = field(default_factory=dict)
     # adaptive (hanging-node) elements: ids, refine levels and Hnm[N, M] (nnod x nnod), as the
-    # reference's "adap" file holds them (LoadBinary.h:246-260, Element.h:39-40)
+    # reference's "adap" file holds them (LoadBinary.h:247-261, Element.h:39-40)
     adap_elements: np.ndarray | None = None
     adap_levels: np.ndarray | None = None
     adap_hnm: np.ndarray | None = None

@@ -6,14 +6,14 @@
  *   ---------------------------------------------------  ----------------------------------
  *   LoadBinaryData::read_nodes/read_elements             cfdv_create / cfdv_upload_mesh
  *     (Utility/IO/ASCIItoBinary/LoadBinary.h:116-246)      + cfdv_load_node_records
- *   LoadBinaryData::adap (LoadBinary.h:246-260; the      cfdv_set_adaptive
+ *   LoadBinaryData::adap (LoadBinary.h:247-261; the      cfdv_set_adaptive
  *     hanging-node Hnm of refined elements)
  *   CalcLength (FDV/Function/CalcLength.h:34-66)         inside cfdv_create
  *   ClearElement + NodeUnpack (main.cpp:169-171)         fused into cfdv_cfl / cfdv_form
- *   CFL (FDV/Function/MPI_CFL.h:124-134, main.cpp:179)   cfdv_cfl
+ *   CFL (FDV/Function/MPI_CFL.h:7-56, main.cpp:179)   cfdv_cfl
  *   FDVGalerkin over elements (main.cpp:185-186,         cfdv_form
  *     FDV/FDVGalerkin.h:121-154) + ApplyBC (main.cpp:194,
- *     FDV/Function/ApplyBC.h:131-250)
+ *     FDV/Function/ApplyBC.h:14-133)
  *   GMRESbase::iterate (Utility/Solvers/GMRESbase.h:16,  cfdv_gmres
  *     MPI_GMRES.h:125-220)
  *   GMRESbase::update (GMRESbase.h:21, MPI_GMRES.h:224)  cfdv_update
@@ -64,7 +64,7 @@ typedef struct {
   const int* bc;   /* [n_elements][nface] */
 } cfdv_mesh;
 
-/* aero + control parameters (MPIBinaryConfiguration.h:29-69, Thermo.h:158-169) */
+/* aero + control parameters (MPIBinaryConfiguration.h:29-69, Thermo.h:22-33) */
 typedef struct {
   double gamma, mach, reynolds, prandtl, tinf, twall;
   int adiabatic;
@@ -77,7 +77,9 @@ typedef enum { CFDV_GMRES_REFERENCE = 0, CFDV_GMRES_CORRECT = 1 } cfdv_gmres_mod
 typedef struct {
   int mode;       /* cfdv_gmres_mode: REFERENCE reproduces MPI_GMRES::iterate (restart count,
                      tol = ||b||*1e-9 inner break, rotate_and_check, back substitution);
-                     CORRECT is restarted GMRES(m), MGS + Givens, to rtol */
+                     CORRECT is restarted GMRES(m) to rtol with Givens QR and textbook back
+                     substitution; its Gram-Schmidt is `orth` below with engine 0 (the host
+                     driver and the Python binding pass 2, delayed CGS2), MGS with engine 1 */
   int m;          /* Krylov dimension (control "gmresiter") */
   int restarts;   /* REFERENCE: restart count (control "gmresrestart"); CORRECT: maximum */
   double rtol;    /* CORRECT: stop when ||b - A du|| / ||b|| < rtol */
@@ -121,10 +123,10 @@ int cfdv_create(const cfdv_mesh* mesh, const cfdv_params* params, cfdv_ctx** out
 /* Replace the mesh (e.g. after host-side refinement); state and matrices are reset. */
 int cfdv_upload_mesh(cfdv_ctx* ctx, const cfdv_mesh* mesh);
 /* Adaptive (hanging-node) elements after a host refinement, replacing the reference's
- * "adap" file load (LoadBinary.h:246-260 into Element::adap / Element::Hnm, Element.h:39-40):
+ * "adap" file load (LoadBinary.h:247-261 into Element::adap / Element::Hnm, Element.h:39-40):
  * elements[k] carries hnm[k*nnod*nnod ...], Hnm(N, M) at N + nnod*M (the reference Tensor's
  * storage).  Formation then transforms the element's shape functions (MeshRefine2D.h:877-952,
- * FDVGalerkin.h:183-201, 488-497; calc_TF_norm3D.h:25-57).  n = 0 clears the set;
+ * FDVGalerkin.h:183-201, 488-497; calc_TF_norm3D.h:25-66).  n = 0 clears the set;
  * cfdv_upload_mesh clears it too.  Element ids must be distinct and in range. */
 int cfdv_set_adaptive(cfdv_ctx* ctx, int n, const int* elements, const double* hnm);
 void cfdv_destroy(cfdv_ctx* ctx);
@@ -143,7 +145,7 @@ int cfdv_get_state(cfdv_ctx* ctx, double* U, double* U0, size_t n);
 int cfdv_state_device_ptr(cfdv_ctx* ctx, double** U);
 
 /* ---- the step --------------------------------------------------------------- */
-/* dt = cfl * min_e min_nodes cleng/(|v| + sqrt(1.4 cgas T)) (MPI_CFL.h:124-171). */
+/* dt = cfl * min_e min_nodes cleng/(|v| + sqrt(1.4 cgas T)) (MPI_CFL.h:7-56). */
 int cfdv_cfl(cfdv_ctx* ctx, double cfl, double* dt);
 /* Element LHS/RHS at time step dt with ApplyBC; precision MIXED also keeps FP32
  * copies of the matrices for the FP32 products. */
@@ -173,6 +175,10 @@ int cfdv_step_host(cfdv_ctx* ctx, double cfl, const cfdv_gmres_opts* opts, cfdv_
 int cfdv_get_fdv_params(cfdv_ctx* ctx, double* s);
 /* Element matrices [E][Ke*Ke] (FP64) and rhs [E][Ke] from the last cfdv_form. */
 int cfdv_get_element_matrices(cfdv_ctx* ctx, double* R, double* rhs);
+/* The same for the n elements ids[0..n): R [n][Ke*Ke], rhs [n][Ke] and s1..s4 [n][4] (any
+ * may be NULL), without copying the whole mesh's matrices -- the reference's elements[e]->R,
+ * ->rhs and FDVParam (Element.h:33-34, FDVParam.h:15-111) for a sample of e. */
+int cfdv_get_element_subset(cfdv_ctx* ctx, int n, const int* ids, double* R, double* rhs, double* s);
 /* Assembled rhs b [n_nodes*neqn] (MPI_GMRES::compose_rhs, MPI_GMRES.h:369-438). */
 int cfdv_get_rhs_vector(cfdv_ctx* ctx, double* b);
 /* dU of the last solve [n_nodes*neqn]. */
@@ -267,7 +273,9 @@ int cfdv_tangent(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, double dmach, con
  *
  * y = A x (transpose = 1: A^T x) for element matrices R [n_elements][Ke*Ke] (column-
  * major per element, as above), computed by the same element and node passes as
- * cfdv_matvec.  Every pointer is DEVICE memory owned by the caller:
+ * cfdv_matvec.  Every pointer is memory of the CURRENT device (cudaMalloc'd or from the
+ * caller's pool) or managed memory, owned by the caller; host memory (pageable or pinned)
+ * and another GPU's memory are rejected with CFDV_ERR_ARG before any GPU work:
  *   conn     [n_elements][nnod] node ids (nnod 4 in 2D, 8 in 3D), as in cfdv_mesh
  *   node_ptr [n_nodes+1], node_idx [n_elements*nnod]: for node n, the entries
  *            node_idx[node_ptr[n] .. node_ptr[n+1]) are e*nnod + l for every element e
@@ -279,7 +287,9 @@ int cfdv_tangent(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, double dmach, con
  * CFDV_STATIC_SCRATCH_DOUBLES (2D quads: 131072 elements, 3D hexes: 52428); a larger
  * mesh returns CFDV_ERR_TOO_LARGE before any GPU work.  The call allocates nothing.
  * The first call on a device looks up the array's device address (with that device
- * current) and keeps it; make that first call before any stream capture begins.  The
+ * current) and keeps it; make that first call before any stream capture begins.  After a
+ * cudaDeviceReset the kept address no longer names device memory, and the next call looks
+ * it up again: that call, too, belongs outside a capture.  The
  * work is queued on `stream` (a cudaStream_t; NULL = the default stream) and the call
  * returns without waiting for it.  All calls share the one array, which keeps the last
  * call's contents: calls whose work overlaps on a GPU (different streams, or different

@@ -14,7 +14,7 @@
 
 namespace {
 
-// Thermo.h:148-211 (nondimensional gas model)
+// Thermo.h:8-86 (nondimensional gas model)
 struct Gas {
   double gamma, gamm1, gm1d2, gamm3, gm3d2, Pr, csuth, Cv, cgas, cmach, creyn, Twall;
   bool adiabatic;
@@ -33,14 +33,14 @@ struct Gas {
     Twall = a->twall;
     adiabatic = a->adiabatic != 0;
   }
-  double mu(double T) const {  // Thermo.h:189-206
+  double mu(double T) const {  // Thermo.h:53-70
     if (T < 1.0E-12) return 1.0;
     return ((1 + csuth) / (T + csuth)) * T * std::sqrt(T);
   }
-  double k(double mu) const { return mu / ((gamma - 1.0) * (cmach * cmach) * Pr); }  // Thermo.h:208-211
+  double k(double mu) const { return mu / ((gamma - 1.0) * (cmach * cmach) * Pr); }  // Thermo.h:72-75
 };
 
-// NodeUnpack.h:185-205: primitives from the conserved vector
+// NodeUnpack.h:9-29: primitives from the conserved vector
 struct NodeState {
   double x[3], U[5], v[3];
   double rho, E, e, T, p;
@@ -95,7 +95,7 @@ void gauss(int N, double* zeta, double* w) {
 }
 
 // ---- shape functions ------------------------------------------------------
-// TestFunctions2D.h:173-198
+// TestFunctions2D.h:7-43
 void shape2(const double* z, double* Phi, double dPxi[][3]) {
   Phi[0] = 0.25 * (1 - z[0]) * (1 - z[1]);
   Phi[1] = 0.25 * (1 + z[0]) * (1 - z[1]);
@@ -134,7 +134,7 @@ void shape3(const double* z, double* Phi, double dPxi[][3]) {
   }
 }
 
-// TestFunctions2D.h:212-256 (jacobian, dtestfunctiondx)
+// TestFunctions2D.h:46-90 (jacobian, dtestfunctiondx)
 double jac2(const double dPxi[][3], NodeState* const* nd, double jac[3][3], double dPhi[][3]) {
   for (int i = 0; i < 2; i++)
     for (int j = 0; j < 2; j++) jac[i][j] = 0;
@@ -176,7 +176,7 @@ double jac3(const double dPxi[][3], NodeState* const* nd, double dPhi[][3]) {
   return J;
 }
 
-// ---- Gauss-point flow state (Flow.h, FDVGalerkin.h:761-797, tau.h:105-133) ---
+// ---- Gauss-point flow state (Flow.h, FDVGalerkin.h:761-797, tau.h:14-42) ---
 struct FlowPt {
   double E, T, v[3], x[3], U[5], dU[5][3], dV[3][3], dT[3], k, mu, tau[3][3];
 };
@@ -202,7 +202,7 @@ void gp_sum(const Gas& g, int ndim, int neqn, int nn, NodeState* const* nd, cons
   f.k = g.k(f.mu);
 }
 
-void tau_calc(int ndim, FlowPt& f) {  // tau.h:105-133
+void tau_calc(int ndim, FlowPt& f) {  // tau.h:14-42
   double vkk = 0;
   for (int k = 0; k < ndim; k++) vkk += f.dV[k][k];
   for (int i = 0; i < ndim; i++)
@@ -644,7 +644,7 @@ void domain(ElemCtx& c, const double* w, const double* zeta) {
   double Psi[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double tau = 0;
   if (ndim == 2) {  // FDVGalerkin.h:225-332 streamline-upwind diffusion (2D only)
-    // its Jacobian comes from the untransformed shape functions (FDVGalerkin.h:235-239), which
+    // its Jacobian comes from the untransformed shape functions (FDVGalerkin.h:237-240), which
     // differs from jac for an adaptive element
     double (*sj)[3] = jac, jp[3][3];
     if (c.H) {
@@ -928,7 +928,7 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
   for (int i = 0; i < nb; i++) nd[i] = c.nd[fn[i]];
   double phib[4], en[3], dpidx[4][3];
   std::memset(dpidx, 0, sizeof(dpidx));
-  if (ndim == 2) {  // TestFunctions1D.h:141-216
+  if (ndim == 2) {  // TestFunctions1D.h:7-82
     phib[0] = 0.5 * (1 - zeta[0]);
     phib[1] = 0.5 * (1 + zeta[0]);
     double dxds = 0, dyds = 0;
@@ -950,7 +950,7 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
     phib[2] = 0.25 * (1 + zeta[0]) * (1 + zeta[1]);
     phib[3] = 0.25 * (1 - zeta[0]) * (1 + zeta[1]);
     // face node positions; for an adaptive element the rows of Hnm x of the face's nodes
-    // (calc_TF_norm3D.h:25-57: allnode(N) = sum_M Hnm(N, M) x_M)
+    // (calc_TF_norm3D.h:25-66: allnode(N) = sum_M Hnm(N, M) x_M)
     double nodeloc[4][3];
     for (int j = 0; j < 4; j++)
       for (int k = 0; k < 3; k++) nodeloc[j][k] = nd[j]->x[k];
@@ -1002,7 +1002,7 @@ void boundary_face(ElemCtx& c, const double* w, const double* zeta, int code, co
         for (int j = 0; j < 2; j++) dpidx[N][i] += T[j][i] * dpdx[N][j];
       en[i] = enorm[i] * w[0] * w[1] * detjac;
     }
-    if (c.H) {  // FDVGalerkin.h:488-497, MeshRefine2D.h:904-951 (adap_face): phib only
+    if (c.H) {  // FDVGalerkin.h:489-497, MeshRefine2D.h:904-951 (adap_face): phib only
       double pt[4] = {0, 0, 0, 0};
       for (int N = 0; N < 4; N++)
         for (int M = 0; M < 4; M++) pt[M] += phib[N] * c.H[fn[N] + c.nnod * fn[M]];
@@ -1153,7 +1153,7 @@ void oracle_bc_rowmask(const oracle_mesh* m, const oracle_aero* a, const uint8_t
         const uint8_t* d = dir + (size_t)m->conn[(size_t)e * m->nnod + ja] * neqn;
         for (int je = 0; je < neqn; je++) {
           if (!d[je]) continue;
-          if (bc == 1 && je == neqn - 1 && !a->adiabatic) continue;  // ApplyBC.h:158 (isothermal wall body is empty)
+          if (bc == 1 && je == neqn - 1 && !a->adiabatic) continue;  // ApplyBC.h:41-63 (the isothermal-wall branch is commented out)
           mk |= 1ull << (neqn * ja + je);
         }
       }
@@ -1314,7 +1314,7 @@ void oracle_form(const oracle_mesh* m, const oracle_aero* a, const double* U, do
             if (bc[f] != 0 && bc[f] < 100) boundary_face(c, w, z, bc[f], kFace3[f]);
         }
     }
-    if (apply_bc) {  // ApplyBC.h:131-250: Dirichlet rows zeroed, diagonal 0.5, rhs 0
+    if (apply_bc) {  // ApplyBC.h:14-133: Dirichlet rows zeroed, diagonal 0.5, rhs 0
       uint64_t mk = mask[e];
       for (int I = 0; I < Ke; I++) {
         if (!((mk >> I) & 1ull)) continue;

@@ -24,7 +24,7 @@ typedef struct {
   const double* x;   /* [Nn][ndim] */
   const int* conn;   /* [E][nnod]  */
   const int* bc;     /* [E][nface] */
-  /* adaptive (hanging-node) elements (Element.h:39-40, LoadBinary.h:246-260): hnm_idx[e] is
+  /* adaptive (hanging-node) elements (Element.h:39-40, LoadBinary.h:247-261): hnm_idx[e] is
    * the row of hnm that applies to element e, -1 for a plain element (both may be null);
    * hnm[k] holds Hnm(N, M) at N + nnod*M */
   const int* hnm_idx;
@@ -38,13 +38,13 @@ typedef struct {
 
 /* node Dirichlet flags per DOF, set by the faces (LoadBinary.h:264-318) */
 void oracle_dirichlet(const oracle_mesh* m, const oracle_aero* a, uint8_t* dir /*[Nn*neqn]*/);
-/* per-element Dirichlet row mask after ApplyBC (ApplyBC.h:131-250); bit i = local DOF i */
+/* per-element Dirichlet row mask after ApplyBC (ApplyBC.h:14-133); bit i = local DOF i */
 void oracle_bc_rowmask(const oracle_mesh* m, const oracle_aero* a, const uint8_t* dir, uint64_t* mask /*[E]*/);
 /* conserved U from the binary node records {x, rho, v, T} (LoadBinary.h:179-196) */
 void oracle_init_U(const oracle_mesh* m, const oracle_aero* a, const double* prim, double* U);
 /* element characteristic length (CalcLength.h:34-110) */
 void oracle_cleng(const oracle_mesh* m, double* cleng);
-/* dt from the CFL condition (MPI_CFL.h:124-171); returns dt */
+/* dt from the CFL condition (MPI_CFL.h:7-56); returns dt */
 double oracle_cfl(const oracle_mesh* m, const oracle_aero* a, const double* cleng, const double* U, double cfl);
 /* FDV parameters s1..s4 per element (FDVParam.h:15-111), [E][4] */
 void oracle_fdvparam(const oracle_mesh* m, const oracle_aero* a, const double* U, double* s);

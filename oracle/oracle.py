@@ -20,11 +20,15 @@ REF_BIN = os.path.join(HERE, "_ref", "cfdv_ref")
 _lib = None
 
 
+# The reference checkout: CFDV_REFERENCE_SRC, else a "reference" tree beside this repository.
+REF_SRC_DEFAULT = os.path.normpath(os.path.join(HERE, "..", "..", "reference", "src"))
+
+
 def build(quiet: bool = True) -> None:
     """Compile the restatement (and the reference build when its sources are present)."""
     subprocess.run(["make", "-C", HERE, "port"], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
-    ref_src = os.environ.get("CFDV_REFERENCE_SRC", "/root/reference/src")
+    ref_src = os.environ.get("CFDV_REFERENCE_SRC", REF_SRC_DEFAULT)
     if os.path.isdir(ref_src):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={ref_src}"], check=True,
                        stdout=subprocess.DEVNULL if quiet else None)
@@ -228,8 +232,10 @@ def read_records(path: str) -> dict:
 
 
 def run_reference(case_dir: str, out_path: str, steps: int = 1, dump_step: int = -1,
-                  gmresiter: int | None = None, restart: int | None = None) -> dict:
-    """Run the reference build on a case directory and return its records."""
+                  gmresiter: int | None = None, restart: int | None = None, extra=(),
+                  timeout: float = 3600) -> dict:
+    """Run the reference build on a case directory and return its records; `extra` holds
+    further driver options (ref_driver.cpp: --elements FILE, --form-subset, --tecplot)."""
     if not os.path.exists(REF_BIN):
         raise FileNotFoundError(f"reference build missing: {REF_BIN}")
     cmd = [REF_BIN, case_dir, out_path, "--steps", str(steps), "--dump-step", str(dump_step), "--quiet"]
@@ -237,6 +243,7 @@ def run_reference(case_dir: str, out_path: str, steps: int = 1, dump_step: int =
         cmd += ["--gmresiter", str(gmresiter)]
     if restart:
         cmd += ["--restart", str(restart)]
-    # the reference stops at std::cin.get() on mesh errors (e.g. calc_TF_norm3D.h:143); give it no input
-    subprocess.run(cmd, check=True, stdin=subprocess.DEVNULL, timeout=3600)
+    cmd += list(extra)
+    # the reference stops at std::cin.get() on mesh errors (calc_TF_norm3D.h:137-144); give it no input
+    subprocess.run(cmd, check=True, stdin=subprocess.DEVNULL, timeout=timeout)
     return read_records(out_path)

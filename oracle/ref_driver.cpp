@@ -20,6 +20,13 @@
 //
 // Usage: cfdv_ref <case_dir> <out_file> [--steps N] [--dump-step K]
 //                 [--gmresiter M] [--restart R] [--quiet] [--tecplot]
+//                 [--elements FILE] [--form-subset]
+// --elements FILE (int32 element ids) limits the step-K dumps of R and rhs to those
+// elements, in the file's order; with --form-subset, step K forms (FDVGalerkin, ApplyBC)
+// only those elements, writes the dumps and stops before the solve: on a mesh of 10^5-10^6
+// hex8 elements this samples the reference's formation without forming every element.
+// The element functor depends only on the element and its nodes, so a subset's matrices
+// are those a full pass would give.
 // --tecplot writes the reference's outputs into the working directory: tecplot_<iter>.plt
 // (MPI_TecplotOut.h) at every iteration divisible by 100, as main.cpp:183 does, and the
 // RMSError.txt line of every step (MPI_RMSError.h), as main.cpp:198 does.
@@ -108,7 +115,8 @@ int main(int argc, char** argv) {
   std::string path = argv[1];
   std::string out = argv[2];
   int nsteps = 1, dump_step = -1, m_override = -1, r_override = -1;
-  bool quiet = false, tecplot = false;
+  bool quiet = false, tecplot = false, form_subset = false;
+  std::string elements_file;
   for (int i = 3; i < argc; i++) {
     std::string a = argv[i];
     if (a == "--steps" && i + 1 < argc) nsteps = atoi(argv[++i]);
@@ -117,6 +125,8 @@ int main(int argc, char** argv) {
     else if (a == "--restart" && i + 1 < argc) r_override = atoi(argv[++i]);
     else if (a == "--quiet") quiet = true;
     else if (a == "--tecplot") tecplot = true;
+    else if (a == "--elements" && i + 1 < argc) elements_file = argv[++i];
+    else if (a == "--form-subset") form_subset = true;
   }
 
   auto cm = parse_kv(path + "/control");
@@ -165,6 +175,25 @@ int main(int argc, char** argv) {
     rf.puti("dirichlet", dir);
   }
 
+  // the elements whose matrices a dump writes (all, or the --elements list)
+  std::vector<int> dump_el;
+  if (!elements_file.empty()) {
+    FILE* ef = fopen(elements_file.c_str(), "rb");
+    if (!ef) { perror("open elements"); return 1; }
+    int id;
+    while (fread(&id, 4, 1, ef) == 1) {
+      if (id < 0 || id >= E) { fprintf(stderr, "element id %d out of range\n", id); return 1; }
+      dump_el.push_back(id);
+    }
+    fclose(ef);
+  } else {
+    for (int e = 0; e < E; e++) dump_el.push_back(e);
+  }
+  if (form_subset && elements_file.empty()) { fprintf(stderr, "--form-subset needs --elements\n"); return 2; }
+  rf.puti("dump_elements", dump_el);
+  std::vector<Element*> subset;
+  for (int e : dump_el) subset.push_back(elements[e]);
+
   const int Ke = nnod * neqn;
   double t = 0, dt = 0, t_form = 0, t_gmres = 0;
   std::cout.precision(17);
@@ -180,29 +209,34 @@ int main(int argc, char** argv) {
       std::cout.rdbuf(saved);
     }
     auto t0 = std::chrono::steady_clock::now();
+    const bool sub_only = form_subset && iter == dump_step;
+    std::vector<Element*>& formed = sub_only ? subset : elements;
     FDVGalerkin<Element*> fdv(nnod, neqn, ndim, nbnod, dt, NS);  // main.cpp:185-186
-    for_each(elements.begin(), elements.end(), std::ref(fdv));
+    for_each(formed.begin(), formed.end(), std::ref(fdv));
+    const size_t D = dump_el.size();
     if (iter == dump_step) {
-      std::vector<double> R((size_t)E * Ke * Ke), rhs((size_t)E * Ke), s(4 * (size_t)E);
-      for (int e = 0; e < E; e++) {
+      std::vector<double> R(D * Ke * Ke), rhs(D * Ke), s(4 * D);
+      for (size_t k = 0; k < D; k++) {
+        Element* el = elements[dump_el[k]];
         for (int j = 0; j < Ke; j++)
-          for (int i = 0; i < Ke; i++) R[(size_t)e * Ke * Ke + (size_t)j * Ke + i] = elements[e]->R(i, j);
-        for (int i = 0; i < Ke; i++) rhs[(size_t)e * Ke + i] = elements[e]->rhs(i);
+          for (int i = 0; i < Ke; i++) R[k * Ke * Ke + (size_t)j * Ke + i] = el->R(i, j);
+        for (int i = 0; i < Ke; i++) rhs[k * Ke + i] = el->rhs(i);
         FDVParam<Element*> fp;
-        fp(elements[e], s[4 * e + 0], s[4 * e + 1], s[4 * e + 2], s[4 * e + 3]);
+        fp(el, s[4 * k + 0], s[4 * k + 1], s[4 * k + 2], s[4 * k + 3]);
       }
       rf.putd("R_form", R);  // column-major per element: R(i,j) at j*Ke+i
       rf.putd("rhs_form", rhs);
       rf.putd("s1234", s);
     }
-    for_each(elements.begin(), elements.end(), ApplyBC<Element*>(neqn, nnod, ndim, nbnod));  // main.cpp:194
+    for_each(formed.begin(), formed.end(), ApplyBC<Element*>(neqn, nnod, ndim, nbnod));  // main.cpp:194
     auto t1 = std::chrono::steady_clock::now();
     if (iter == dump_step) {
-      std::vector<double> R((size_t)E * Ke * Ke), rhs((size_t)E * Ke);
-      for (int e = 0; e < E; e++) {
+      std::vector<double> R(D * Ke * Ke), rhs(D * Ke);
+      for (size_t k = 0; k < D; k++) {
+        Element* el = elements[dump_el[k]];
         for (int j = 0; j < Ke; j++)
-          for (int i = 0; i < Ke; i++) R[(size_t)e * Ke * Ke + (size_t)j * Ke + i] = elements[e]->R(i, j);
-        for (int i = 0; i < Ke; i++) rhs[(size_t)e * Ke + i] = elements[e]->rhs(i);
+          for (int i = 0; i < Ke; i++) R[k * Ke * Ke + (size_t)j * Ke + i] = el->R(i, j);
+        for (int i = 0; i < Ke; i++) rhs[k * Ke + i] = el->rhs(i);
       }
       rf.putd("R_bc", R);
       rf.putd("rhs_bc", rhs);
@@ -211,6 +245,10 @@ int main(int argc, char** argv) {
         for (int k = 0; k < neqn; k++) Ucur.push_back(n->U(k));
       rf.putd("U_dump", Ucur);
       rf.putd("dt_dump", {dt});
+      if (sub_only) {
+        rf.putd("form_time", {std::chrono::duration<double>(t1 - t0).count()});
+        break;
+      }
     }
 
     // GMRES prints its tolerance, per-iteration Givens estimates and g(m) on

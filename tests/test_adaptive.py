@@ -1,4 +1,4 @@
-"""Adaptive (hanging-node) cases on the CPU: the reference's "adap" file (LoadBinary.h:246-260,
+"""Adaptive (hanging-node) cases on the CPU: the reference's "adap" file (LoadBinary.h:247-261,
 TensorStream.h:95-145) written and read back by cfdv_b200.meshgen, the identity Hnm in the
 oracle, and, where the reference build is present, the oracle against the reference run on
 an adaptive case directly (the committed fixtures tests/golden/*_adap.npz hold the same

@@ -81,7 +81,7 @@ def test_ensight_series(emit, oracle_lib, name):
     if nd == 2:
         assert np.all(xyz[:, 2] == 0.0)
     assert np.array_equal(conn, case.elements[:, : 4 if nd == 2 else 8] + 1)
-    # NodeUnpack of U (NodeUnpack.h:185-205)
+    # NodeUnpack of U (NodeUnpack.h:9-29)
     Ur = U.reshape(nn, nd + 2)
     rho = Ur[:, 0]
     v = Ur[:, 1:nd + 1] / rho[:, None]

@@ -1,5 +1,5 @@
 """Adaptive (hanging-node) elements on the device (cfdv_set_adaptive; the reference's adap
-file, LoadBinary.h:246-260, and the Hnm transforms of MeshRefine2D.h:877-952): argument
+file, LoadBinary.h:247-261, and the Hnm transforms of MeshRefine2D.h:877-952): argument
 checks, the identity Hnm, steps of the textbook solve against the oracle, and the discrete
 adjoint against the tangent-linear run on an adaptive mesh.  Formation and the reference
 GMRES history against the reference's own outputs are in test_gpu_parity.py."""

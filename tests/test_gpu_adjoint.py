@@ -166,7 +166,7 @@ def test_adjoint_matches_gpu_finite_differences(gpu, adj):
 def test_per_node_gradient_matches_unit_tangents(gpu, adj):
     """Single wall nodes are checked against tangent runs along unit directions, not against
     differences: the wall starts at rest at one temperature, so the CFL minimum
-    (MPI_CFL.h:124-171) is attained at many wall nodes at once, and moving one node's
+    (MPI_CFL.h:7-56) is attained at many wall nodes at once, and moving one node's
     temperature breaks the tie on one side only (dt = cfl * min is not differentiable
     there).  Both the adjoint and the tangent give the whole dt sensitivity to the first
     arg-min node in element order."""

@@ -9,7 +9,7 @@ check it against cfdv_matvec (a context's product, same tolerance as the other E
 tests) on consecutive calls, and that it rejects meshes larger than its fixed scratch.
 
 The file name sorts last, so a run that stops at the first failure has already run every
-other test when it gets here; the GPU test also passes when this file runs on its own."""
+other test when it gets here; the GPU tests also pass when this file runs on its own."""
 import ctypes as C
 
 import numpy as np
@@ -117,3 +117,44 @@ def test_static_matvec_matches_context_matvec(name):
     for g, w in zip(got, want):
         assert np.all(np.isfinite(g))
         assert rel_err(g, w) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_static_matvec_rejects_host_memory_and_leaves_y_alone():
+    """Host memory (pageable or pinned) in place of a device buffer is CFDV_ERR_ARG, and a
+    mesh above the scratch limit is CFDV_ERR_TOO_LARGE: both before any GPU work, so the
+    caller's y keeps what it held."""
+    import torch
+
+    case = get_case("lid8")
+    n_dof = case.n_nodes * 4
+    ptr, idx = node_csr(case.conn, case.n_nodes)
+    dev = torch.device("cuda:0")
+
+    def to_dev(a, dtype):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=dtype).ravel()).to(dev)
+
+    conn_d, ptr_d, idx_d = to_dev(case.conn, np.int32), to_dev(ptr, np.int32), to_dev(idx, np.int32)
+    R_d = torch.zeros(case.n_elements * 256, dtype=torch.float64, device=dev)
+    x_d = torch.ones(n_dof, dtype=torch.float64, device=dev)
+    y_d = torch.full((n_dof,), float("nan"), dtype=torch.float64, device=dev)
+    x_pageable = np.ones(n_dof)
+    x_pinned = torch.ones(n_dof, dtype=torch.float64).pin_memory()
+    L = G.lib()
+
+    def call(n_el, x_ptr, R_ptr=None):
+        return L.cfdv_ebe_matvec_static(2, case.n_nodes, n_el, conn_d.data_ptr(), ptr_d.data_ptr(), idx_d.data_ptr(),
+                                        R_ptr or R_d.data_ptr(), x_ptr, y_d.data_ptr(), 0, None)
+
+    torch.cuda.synchronize()
+    assert call(case.n_elements, x_pageable.ctypes.data) == ERR_ARG
+    assert call(case.n_elements, x_pinned.data_ptr()) == ERR_ARG
+    R_host = np.zeros(case.n_elements * 256)
+    assert call(case.n_elements, x_d.data_ptr(), R_host.ctypes.data) == ERR_ARG
+    assert call(MAX_DOUBLES // 16 + 1, x_d.data_ptr()) == ERR_TOO_LARGE
+    torch.cuda.synchronize()
+    assert torch.isnan(y_d).all()
+    # a valid call after the rejected ones works (zero matrices: y = 0)
+    assert call(case.n_elements, x_d.data_ptr()) == 0
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(y_d).item() == 0
