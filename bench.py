@@ -31,18 +31,45 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "FDV steps/s & EBE matvec GB/s: mixed vs FP64 on 1 B200 at equal residual"
+# Each workload states where it departs from the configuration it stands for.
 WORKLOADS = {
     "plate": dict(desc="2D supersonic flat plate 200x100 quad4, M=3, Re=1e4, GMRES(30) to 1e-8",
-                  make=lambda mg: mg.plate(200, 100), m=30, cfl=1.0),
+                  make=lambda mg: mg.plate(200, 100), m=30, cfl=1.0,
+                  deviations=["initial state: uniform freestream with the seeded 1e-3 Gaussian density noise, except "
+                              "over the plate, which starts from a tanh boundary-layer profile (u = tanh(y/0.005), "
+                              "Crocco-Busemann T): with an exact linear solve the impulsive start drives the density "
+                              "negative in the first step",
+                              "CFL 1.0 (the configuration names none)",
+                              "timed steps return to the post-warm-up state every 10 steps, outside the timed "
+                              "regions: with converged solves the plate becomes unstable near t = 0.015 (step ~16), "
+                              "on the oracle's CPU solve too, so the 2000-step run is not reached"]),
     "lid": dict(desc="2D lid-driven cavity 32x32 quad4, M=0.1, Re=100, GMRES(20) to 1e-8",
-                make=lambda mg: mg.lid(32), m=20, cfl=0.5),
+                make=lambda mg: mg.lid(32), m=20, cfl=0.5,
+                deviations=["a few timed steps of the 200; the full 200-step run is a GPU parity test "
+                            "(reference-mode solver against the oracle)"]),
     "ramp": dict(desc="3D compression ramp 128x64x32 hex8, M=2.5, Re=1e5, GMRES(50) to 1e-8",
-                 make=lambda mg: mg.ramp(128, 64, 32), m=50, cfl=0.25),
+                 make=lambda mg: mg.ramp(128, 64, 32), m=50, cfl=0.25,
+                 deviations=["3 timed steps of the 500", "CFL 0.25 (the configuration names none)"]),
     "ramp64": dict(desc="3D compression ramp 64x32x32 hex8 (profiling size), M=2.5, Re=1e5, GMRES(50) to 1e-8",
-                   make=lambda mg: mg.ramp(64, 32, 32), m=50, cfl=0.25),
+                   make=lambda mg: mg.ramp(64, 32, 32), m=50, cfl=0.25, deviations=["profiling size"]),
     "duct": dict(desc="3D duct 200x100x50 hex8 (1,000,000 elements, jittered), M=0.8, Re=5e4, GMRES(40) to 1e-8",
-                 make=lambda mg: mg.duct(200, 100, 50), m=40, cfl=0.5),
+                 make=lambda mg: mg.duct(200, 100, 50), m=40, cfl=0.5,
+                 deviations=["3 timed steps of the 100", "stored element matrices (FP64 and FP32); the "
+                             "on-the-fly recomputation is measured separately"]),
 }
+ADJOINT_DEVIATIONS = ["span: 16 node layers with symmetry planes (bc 2), not periodic by connectivity (elements take "
+                      "their geometry from absolute coordinates, so a wrapped layer would be inverted)"]
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 # The timed steps march from the state after the warm-up steps and go back to it every
@@ -50,6 +77,10 @@ WORKLOADS = {
 # CFL 1 the synthetic plate develops an instability after about 20 steps (the oracle's
 # converged solve shows it too), and a longer --steps run would then time stalled solves.
 RESTART_EVERY = 10
+
+# CPU-baseline sample of the reference build per workload: (timed steps, warm-up steps), about
+# 15-20 s of one core
+CPU_SAMPLE = {"plate": (20, 5), "lid": (40, 5), "ramp": (1, 0), "duct": (1, 0)}
 
 # orthogonalisation of the persistent solve (cfdv_gmres_opts.orth)
 ORTH = {"cgs2": 0, "mgs": 1, "dcgs2": 2, "dcgs2-grid": 3}  # dcgs2-grid: grid barriers only
@@ -241,28 +272,91 @@ def solve_roofline(r, peak, peak_kind, label, traffic=None):
             "avg_launch_us": 1e3 * st["solve_ms"] / st["solves"]}
 
 
+class MemPeak:
+    """Device memory in use (total - free, every process on the GPU), sampled every 50 ms."""
+
+    def __init__(self):
+        import torch
+        self.torch, self.peak, self.run = torch, 0, True
+        self.t = threading.Thread(target=self._loop, daemon=True)
+        self.t.start()
+
+    def _loop(self):
+        while self.run:
+            free, total = self.torch.cuda.mem_get_info()
+            self.peak = max(self.peak, total - free)
+            time.sleep(0.05)
+
+    def stop(self):
+        self.run = False
+        self.t.join()
+        return self.peak
+
+
 def measure_adjoint(args, ws, max_over_ranks):
     """Discrete adjoint on the O-grid cylinder: forward run with checkpoints, reverse sweep;
     device time of each phase from the library's own CUDA events."""
     from cfdv_b200 import gpu as G, meshgen as mg
     case = mg.cylinder(96, 128, 16)
     s = G.FDVSolver(case)
+    k = args.adj_every
     out = {"workload": f"3D cylinder O-grid 96x128x16 hex8 ({case.n_elements} elements), M=0.3, Re=150, isothermal "
                        "wall; J = mean_n wall x-force; gradient w.r.t. Mach, wall temperature and each wall-node "
                        "temperature", "elements": case.n_elements, "steps": args.adj_steps,
-           "checkpoint_every": 2, "gmres": "GMRES(40) to 1e-8 (forward, tangent and adjoint solves)"}
+           "checkpoint_every": k, "gmres": "GMRES(40) to 1e-8 (forward, tangent and adjoint solves)",
+           "deviations": ADJOINT_DEVIATIONS + ([] if (args.adj_steps, k) == (1000, 50) else
+                                              [f"{args.adj_steps} steps with checkpoints every {k} (the configuration: "
+                                               "1000 steps, every 50)"])}
     for name, prec in (("fp64", G.PREC_FP64), ("mixed", G.PREC_MIXED)):
         s.load_node_records()
         s.adjoint(2, 0.5, checkpoint_every=1, m=40, rtol=1e-8, precision=prec)  # warm-up
         s.load_node_records()
-        r = s.adjoint(args.adj_steps, 0.5, checkpoint_every=2, m=40, rtol=1e-8, precision=prec)
+        mem = MemPeak()
+        r = s.adjoint(args.adj_steps, 0.5, checkpoint_every=k, m=40, rtol=1e-8, precision=prec)
+        peak_bytes = mem.stop()
         f, b = max_over_ranks(r["forward_ms"]), max_over_ranks(r["backward_ms"])
         out[name] = {"forward_ms_per_step": f / args.adj_steps, "backward_ms_per_step": b / args.adj_steps,
                      "backward_over_forward": b / f, "forward_matvecs": r["forward_matvecs"],
                      "adjoint_matvecs": r["adjoint_matvecs"], "J": r["J"], "dJ_dmach": r["dJ_dmach"],
-                     "dJ_dtwall": r["dJ_dtwall"], "wall_nodes": int(len(r["wall_nodes"]))}
+                     "dJ_dtwall": r["dJ_dtwall"], "wall_nodes": int(len(r["wall_nodes"])),
+                     "device_memory_peak_gb": peak_bytes / 1e9}
     s.close()
     return out
+
+
+def matvec_roofline(r, peak, peak_kind, label):
+    """The whole EBE product (element pass + node pass: gather, multiply, scatter) of the
+    host-driven step's products: E*Ke^2*s_R + DOF*(8 + 8) bytes each over their device time."""
+    e = r["ebe"]
+    if e.get("matvec_ms", 0) <= 0 or e["launches"] == 0:
+        return None
+    achieved = e["matvec_bytes"] / (e["matvec_ms"] / 1e3) / 1e9
+    return {"kernel": label, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_launch": e["matvec_bytes"] / e["launches"],
+            "launches": e["launches"], "avg_us": 1e3 * e["matvec_ms"] / e["launches"]}
+
+
+def summarize(sec, name, steps, warmup, peak, peak_kind, tile=None):
+    """One more workload beside the headline: both forms, their ratio and rooflines."""
+    s_m, s_f = sec["mixed"], sec["fp64"]
+    return {
+        "workload": sec["desc"], "elements": sec["case"].n_elements,
+        "dof": sec["case"].n_nodes * sec["case"].neqn, "steps": steps, "warmup": warmup,
+        "deviations": WORKLOADS[name]["deviations"],
+        "mixed": {"value": s_m["steps_per_s"], "ms_per_step": s_m["ms_per_step"],
+                  "true_rel_res_max": s_m["true_rel_res_max"], "matvecs_per_step": s_m["matvecs_per_step"],
+                  "form_ms": s_m["form_ms"], "solve_ms": s_m["solve_ms"]},
+        "fp64": {"value": s_f["steps_per_s"], "ms_per_step": s_f["ms_per_step"],
+                 "true_rel_res_max": s_f["true_rel_res_max"], "matvecs_per_step": s_f["matvecs_per_step"],
+                 "form_ms": s_f["form_ms"], "solve_ms": s_f["solve_ms"]},
+        "mixed_over_fp64": s_m["steps_per_s"] / s_f["steps_per_s"],
+        "roofline": solve_roofline(s_m, peak, peak_kind, "gmres_persistent_kernel, mixed (" + name + ")", tile),
+        "roofline_ebe": ebe_roofline(s_m, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + name + ")"),
+        "roofline_ebe_fp64": ebe_roofline(s_f, peak, peak_kind, "ebe_elem_kernel, FP64 matrices (" + name + ")"),
+        "roofline_matvec": matvec_roofline(s_m, peak, peak_kind, "EBE product, element + node pass, FP32 matrices"),
+        "roofline_matvec_fp64": matvec_roofline(s_f, peak, peak_kind,
+                                                "EBE product, element + node pass, FP64 matrices"),
+    }
 
 
 def ebe_roofline(r, peak, peak_kind, label, traffic=None):
@@ -378,7 +472,8 @@ def bench_gpu(args, ws, rank, local):
         "config": {"workload": head["desc"], "elements": case.n_elements, "dof": n,
                    "gmres": f"restarted GMRES({m}), {args.orth.upper()}, right node-block Jacobi, to true relative "
                             f"residual {rtol:g}",
-                   "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}"},
+                   "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}",
+                   "deviations": WORKLOADS[args.workload]["deviations"]},
         "fp64": {"value": fp64["steps_per_s"], "ms_per_step": fp64["ms_per_step"],
                  "true_rel_res_max": fp64["true_rel_res_max"], "matvecs_per_step": fp64["matvecs_per_step"],
                  "form_ms": fp64["form_ms"], "solve_ms": fp64["solve_ms"]},
@@ -394,47 +489,43 @@ def bench_gpu(args, ws, rank, local):
         "roofline_ebe": ebe_roofline(mixed, peak, peak_kind, "ebe_elem_kernel, FP32 matrices (" + args.workload + ")"),
         "roofline_ebe_fp64": ebe_roofline(fp64, peak, peak_kind,
                                           "ebe_elem_kernel, FP64 matrices (" + args.workload + ")"),
+        "roofline_matvec": matvec_roofline(mixed, peak, peak_kind, "EBE product, element + node pass, FP32 matrices"),
+        "roofline_matvec_fp64": matvec_roofline(fp64, peak, peak_kind,
+                                                "EBE product, element + node pass, FP64 matrices"),
         "e2e": {"value": ws * args.steps / e2e_s, "unit": "FDV steps/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clocks,
     }
     del head
+    tiles = {}
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tiles = json.load(f)
     if args.secondary in WORKLOADS and args.secondary != args.workload:
         sec = measure_workload(args, args.secondary, 3, 3, flush, ws, barrier, max_over_ranks)
         sec["solver"].close()
-        s_m, s_f = sec["mixed"], sec["fp64"]
-        stile = None
-        if os.path.exists(tfile):
-            with open(tfile) as f:
-                stile = json.load(f).get(args.secondary)
-        line["secondary"] = {
-            "workload": sec["desc"], "elements": sec["case"].n_elements,
-            "dof": sec["case"].n_nodes * sec["case"].neqn, "steps": 3, "warmup": 3,
-            "mixed": {"value": s_m["steps_per_s"], "ms_per_step": s_m["ms_per_step"],
-                      "true_rel_res_max": s_m["true_rel_res_max"], "matvecs_per_step": s_m["matvecs_per_step"],
-                      "form_ms": s_m["form_ms"], "solve_ms": s_m["solve_ms"]},
-            "fp64": {"value": s_f["steps_per_s"], "ms_per_step": s_f["ms_per_step"],
-                     "true_rel_res_max": s_f["true_rel_res_max"], "matvecs_per_step": s_f["matvecs_per_step"],
-                     "form_ms": s_f["form_ms"], "solve_ms": s_f["solve_ms"]},
-            "mixed_over_fp64": s_m["steps_per_s"] / s_f["steps_per_s"],
-            "roofline": solve_roofline(s_m, peak, peak_kind, "gmres_persistent_kernel, mixed (" + args.secondary + ")",
-                                       stile),
-            "roofline_ebe": ebe_roofline(s_m, peak, peak_kind,
-                                         "ebe_elem_kernel, FP32 matrices (" + args.secondary + ")"),
-            "roofline_ebe_fp64": ebe_roofline(s_f, peak, peak_kind,
-                                              "ebe_elem_kernel, FP64 matrices (" + args.secondary + ")"),
-        }
+        line["secondary"] = summarize(sec, args.secondary, 3, 3, peak, peak_kind, tiles.get(args.secondary))
+        del sec
+    for name in [w for w in args.extra.split(",") if w in WORKLOADS and w not in (args.workload, args.secondary)]:
+        k, w = (10, 3) if name == "lid" else (3, 3)
+        ex = measure_workload(args, name, k, w, flush, ws, barrier, max_over_ranks)
+        ex["solver"].close()
+        line[name] = summarize(ex, name, k, w, peak, peak_kind, tiles.get(name))
+        del ex
     if args.adj_steps > 0:
         line["adjoint"] = measure_adjoint(args, ws, max_over_ranks)
     if rank == 0:
         if not args.no_cpu_baseline:
-            k = 2
+            # the same sample as the reference arm's default: warm-up steps, then timed steps
+            k, w = CPU_SAMPLE.get(args.workload, (2, 1))
             from cfdv_b200 import meshgen as mg
-            times = run_reference_cpu(WORKLOADS[args.workload]["make"](mg), k, 0)
+            times = run_reference_cpu(WORKLOADS[args.workload]["make"](mg), k, w)
             line["cpu_baseline"] = {"value": k / sum(times), "unit": "FDV steps/s", "cores": 1, "kind": "reference",
-                                    "sample": f"{k} steps of the same case through oracle/_ref/cfdv_ref (reference "
-                                              f"sources, reference GMRES({m}) x1 restart: not equal residual)"}
+                                    "cpu": cpu_model(),
+                                    "sample": f"{k} timed steps after {w} warm-up steps of the same case through "
+                                              f"oracle/_ref/cfdv_ref (reference sources, 1 core, the reference's "
+                                              f"GMRES({m}) with one restart: not equal residual)"}
         print(json.dumps(line))
     if ws > 1:
         import torch.distributed as dist
@@ -455,7 +546,7 @@ def bench_reference(args, ws, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": W["desc"], "elements": case.n_elements, "dof": case.n_nodes * case.neqn,
                    "gmres": f"reference MPI_GMRES({W['m']}), 1 restart (its own stopping rule)"},
-        "cpu_baseline": {"value": v, "unit": "FDV steps/s", "cores": 1, "kind": "reference",
+        "cpu_baseline": {"value": v, "unit": "FDV steps/s", "cores": 1, "kind": "reference", "cpu": cpu_model(),
                          "sample": f"{args.steps} timed steps after {args.warmup} warm-up steps of the full case"},
         "e2e": {"value": v, "unit": "FDV steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -474,6 +565,9 @@ def main():
                                                                          "(profiling runs)")
     ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('none' to skip)")
     ap.add_argument("--adj-steps", type=int, default=4, help="steps of the adjoint leg on the cylinder (0 to skip)")
+    ap.add_argument("--adj-every", type=int, default=2, help="checkpoint spacing of the adjoint leg")
+    ap.add_argument("--extra", default="lid,duct", help="further workloads reported beside the headline "
+                                                         "(comma-separated; 'none' to skip)")
     ap.add_argument("--orth", default="dcgs2", choices=sorted(ORTH), help="Gram-Schmidt of the persistent GMRES solve")
     args = ap.parse_args()
     ws, rank, local = dist_info()

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -272,6 +273,7 @@ int matvec(cfdv_ctx* c, int fp32, const double* x, double* out, int mode, const 
     const double sr = fp32 ? 4.0 : 8.0;
     c->mv_bytes += (double)c->n_elements * c->Ke * c->Ke * sr + (double)c->n_dof * 8.0 +
                    (double)c->n_elements * c->Ke * sr;
+    c->mv_full_bytes += (double)c->n_elements * c->Ke * c->Ke * sr + (double)c->n_dof * 16.0;
   }
   if (rep) rep->n_matvec++;
   return CFDV_OK;
@@ -583,6 +585,13 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   a.nbr_ptr = c->d_nbr_ptr; a.nbr_idx = c->d_nbr_idx; a.nbr_blocks = c->nbr_blocks;
   a.nbr_flag = (unsigned int*)(pi + 32);
   a.max_valence = c->max_valence;
+  // 3D element pass through the shared-memory ring (default); CFDV_ELEM_RING=0 selects the
+  // direct-load pass (same products bit for bit), for comparison
+  static const int ring_env = [] {
+    const char* v = std::getenv("CFDV_ELEM_RING");
+    return (v && v[0] == '0') ? 0 : 1;
+  }();
+  a.ring = ring_env;
   std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
   if (c->prof) {
     cudaEventCreate(&ev.first);
@@ -1089,6 +1098,7 @@ int cfdv_profile(cfdv_ctx* c, int enable) {
   c->ev_used = 0;
   c->mv_launches = 0;
   c->mv_bytes = 0;
+  c->mv_full_bytes = 0;
   c->solve_bytes = 0;
   c->launches = 0;
   c->prof = enable != 0;
@@ -1101,9 +1111,11 @@ int cfdv_profile_read(cfdv_ctx* c, cfdv_kernel_stats* out) {
   CK(cudaStreamSynchronize(c->st));
   std::memset(out, 0, sizeof(*out));
   for (size_t i = 0; i + 3 <= c->ev_used; i += 3) {
-    float ms = 0;
+    float ms = 0, ms_all = 0;
     CK(cudaEventElapsedTime(&ms, c->ev_pool[i], c->ev_pool[i + 1]));
+    CK(cudaEventElapsedTime(&ms_all, c->ev_pool[i], c->ev_pool[i + 2]));
     out->total_ms += ms;
+    out->matvec_ms += ms_all;
     out->launches++;
   }
   for (auto& e : c->ev_form) {
@@ -1119,6 +1131,7 @@ int cfdv_profile_read(cfdv_ctx* c, cfdv_kernel_stats* out) {
     out->solves++;
   }
   out->bytes = c->mv_bytes;
+  out->matvec_bytes = c->mv_full_bytes;
   out->solve_bytes = c->solve_bytes;
   out->kernel_launches = c->launches;
   return CFDV_OK;

@@ -84,6 +84,7 @@ struct cfdv_ctx {
   long mv_launches = 0;
   long launches = 0;    // kernels launched since the last cfdv_profile()
   double mv_bytes = 0;  // algorithmic bytes of the timed element passes
+  double mv_full_bytes = 0;  // ... and of the whole products (element + node pass)
   double solve_bytes = 0;  // algorithmic bytes of the timed single-launch solves
   std::string err;
 };

@@ -174,6 +174,177 @@ __device__ __forceinline__ double sum_partials(const double* p, int n) {
   return block_sum(v);
 }
 
+// ---- 3D element pass through a shared-memory ring ---------------------------------------
+// The element matrices are one contiguous stream per block (its elements form one range), so a
+// ring of kRingStages stages in shared memory is filled by bulk copies (cp.async.bulk, no
+// tensor map, this GPU's memory only) that one producer thread issues, each completing on the
+// stage's `full` mbarrier.  The other warps form kRingStages groups; group g consumes the stages
+// of slot g: a warp takes whole elements (lane l owns rows l and l + 32), gathers x_e while the
+// stage's copy is in flight, waits for `full`, forms its rows from shared memory and stores
+// them, and arrives on the slot's `empty` mbarrier, which the producer waits for before
+// refilling the slot.  No block barrier stands between stages.  Each row sums over j in
+// increasing order, as the direct pass does, so the products are bitwise the same.
+constexpr int kRingStages = 3;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// wait for the phase of `parity` to complete, at most kWaitNs, and give up early when another
+// block has set the launch's failure bit; false: the launch is failing (bit set here if not yet)
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, const Barrier& b) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (unsigned polls = 1;; polls++) {
+    if (mbar_test(bar, parity)) return true;
+    if ((polls & 63u) == 0) {
+      unsigned cnt;
+      asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(cnt) : "l"(b.count) : "memory");
+      if (cnt & 0x80000000u) return false;
+      if (now_ns() - t0 > kWaitNs) {
+        atomicOr(b.count, 0x80000000u);
+        atomicOr(b.err, 1);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, unsigned bytes, unsigned long long* bar,
+                                               unsigned long long policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+      : "memory");
+}
+
+// consumer warps (all but warp 0) of slot g
+__host__ __device__ constexpr int ring_members(int g) { return (kWarps - 1 - g + kRingStages - 1) / kRingStages; }
+
+// dynamic shared memory of the ring: the stages, then per-warp x_e buffers (KE doubles a warp),
+// then the 2 kRingStages mbarriers
+constexpr size_t ring_xbuf_offset(size_t stage_bytes) { return (size_t)kRingStages * stage_bytes; }
+constexpr size_t ring_bar_offset(size_t stage_bytes) { return ring_xbuf_offset(stage_bytes) + (size_t)kWarps * 40 * 8; }
+constexpr size_t ring_total_bytes(size_t stage_bytes) { return ring_bar_offset(stage_bytes) + 64; }
+
+// the ring's pieces in dynamic shared memory (stage_bytes: the launch's stage size)
+struct RingView {
+  unsigned char* buf;
+  unsigned long long* full;
+  unsigned long long* empty;
+  __device__ __forceinline__ explicit RingView(unsigned stage_bytes) {
+    extern __shared__ __align__(16) double dyn[];
+    buf = reinterpret_cast<unsigned char*>(dyn);
+    full = reinterpret_cast<unsigned long long*>(buf + ring_bar_offset(stage_bytes));
+    empty = full + kRingStages;
+  }
+};
+
+// one thread: barriers of every slot (full: the producer's arrival + the copy's bytes; empty:
+// one arrival per consumer warp of the slot), made visible to the bulk-copy unit
+__device__ __forceinline__ void ring_init(unsigned stage_bytes) {
+  if (threadIdx.x == 0) {
+    const RingView rv(stage_bytes);
+    for (int sl = 0; sl < kRingStages; sl++) {
+      mbar_init(rv.full + sl, 1);
+      mbar_init(rv.empty + sl, ring_members(sl));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+}
+
+// ring_t: stages of this launch so far (every thread keeps the same count)
+template <int KE, int NEQ, int NNOD, typename TM>
+__device__ __noinline__ void elem_pass_ring(const TM* __restrict__ R, const int* __restrict__ conn, const double* x,
+                                               TM* Y, int E, unsigned stage_bytes, unsigned& ring_t,
+                                               const Barrier& bar) {
+  constexpr unsigned EB = KE * KE * sizeof(TM);
+  const RingView rv(stage_bytes);
+  const int per = (E + gridDim.x - 1) / gridDim.x;
+  const int e0 = min(E, (int)blockIdx.x * per), e1 = min(E, e0 + per);
+  const int SE = (int)(stage_bytes / EB);
+  const int T = (e1 - e0 + SE - 1) / SE;
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (wid == 0) {
+    if (lane == 0) {
+      unsigned long long policy;  // L2 evict-first for the streamed matrices
+      asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+      int issued = 0;
+      for (int t = 0; t < T; t++) {
+        const unsigned tt = ring_t + t, sl = tt % kRingStages, k = tt / kRingStages;
+        if (k >= 1 && !mbar_wait(rv.empty + sl, (k - 1) & 1u, bar)) break;
+        const int es = e0 + t * SE, ne = min(SE, e1 - es);
+        const unsigned bytes = (unsigned)ne * EB;
+        mbar_expect_tx(rv.full + sl, bytes);
+        bulk_to_shared(rv.buf + (size_t)sl * stage_bytes, R + (size_t)es * KE * KE, bytes, rv.full + sl, policy);
+        issued = t + 1;
+      }
+      // copies still in flight land before the pass ends (the consumers wait for them too;
+      // this covers a pass that is being abandoned)
+      for (int t = max(0, issued - kRingStages); t < issued; t++) {
+        const unsigned tt = ring_t + t;
+        mbar_wait(rv.full + tt % kRingStages, (tt / kRingStages) & 1u, bar);
+      }
+    }
+  } else {
+    const int c = wid - 1, g = c % kRingStages, q = c / kRingStages, members = ring_members(g);
+    TM* xw = reinterpret_cast<TM*>(rv.buf + ring_xbuf_offset(stage_bytes)) + wid * KE;  // this warp's x_e
+    for (int t = 0; t < T; t++) {
+      const unsigned tt = ring_t + t, sl = tt % kRingStages, k = tt / kRingStages;
+      if ((int)sl != g) continue;
+      const int es = e0 + t * SE, ne = min(SE, e1 - es);
+      bool first = true;
+      for (int le = q; le < ne; le += members) {
+        const int e = es + le;
+        // x_e: rows lane and lane + 32
+        const TM xa = (TM)__ldcg(x + (size_t)__ldg(conn + (size_t)e * NNOD + lane / NEQ) * NEQ + lane % NEQ);
+        TM xb = 0;
+        if (lane + 32 < KE)
+          xb = (TM)__ldcg(x + (size_t)__ldg(conn + (size_t)e * NNOD + (lane + 32) / NEQ) * NEQ + (lane + 32) % NEQ);
+        xw[lane] = xa;
+        if (lane + 32 < KE) xw[lane + 32] = xb;
+        __syncwarp();
+        if (first) {
+          if (!mbar_wait(rv.full + sl, k & 1u, bar)) return;
+          first = false;
+        }
+        const TM* Rs = reinterpret_cast<const TM*>(rv.buf + (size_t)sl * stage_bytes) + (size_t)le * KE * KE;
+        TM acc0 = 0, acc1 = 0;
+#pragma unroll 8
+        for (int j = 0; j < KE; j++) {
+          const TM xj = xw[j];
+          acc0 += Rs[j * KE + lane] * xj;
+          if (lane + 32 < KE) acc1 += Rs[j * KE + lane + 32] * xj;
+        }
+        Y[(size_t)e * KE + lane] = acc0;
+        if (lane + 32 < KE) Y[(size_t)e * KE + lane + 32] = acc1;
+        __syncwarp();  // xw is rewritten for the next element
+      }
+      if (first && !mbar_wait(rv.full + sl, k & 1u, bar)) return;  // no element of this stage: keep phases in step
+      __syncwarp();
+      if (lane == 0) mbar_arrive(rv.empty + sl);
+    }
+  }
+  ring_t += T;
+}
+
 // Element pass Y_e = R_e x_e, thread (le, i) owning row i of element le.
 // 2D (L2-resident, latency-bound): the block's warps form groups of G = lcm(Ke, 32) / 32
 // warps (one warp, two elements) that each take U = 3 waves of their elements at once from
@@ -332,8 +503,9 @@ constexpr size_t tile_doubles() {
 // then either the resident basis and w ((m+1)*S + S, S = unknowns per block) or the
 // per-warp dot partials of the streaming passes (kWarps * kSlots).
 template <int KE>
-size_t persistent_dyn_doubles(int m, int S, bool resident) {
-  const size_t base = tile_doubles<KE>() + (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2 + (size_t)(m + 1) * (m + 1);
+size_t persistent_dyn_doubles(int m, int S, bool resident, size_t ring_stage_bytes = 0) {
+  const size_t front = ring_stage_bytes ? ring_total_bytes(ring_stage_bytes) / sizeof(double) : tile_doubles<KE>();
+  const size_t base = front + (size_t)5 * m + 2 + (size_t)m * (m + 1) / 2 + (size_t)(m + 1) * (m + 1);
   return base + (resident ? (size_t)(m + 2) * S : (size_t)kWarps * kSlots);
 }
 
@@ -350,10 +522,14 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* tile64 = dyn;
   TR* tileR = reinterpret_cast<TR*>(dyn);
   auto* first = reinterpret_cast<int (*)[kThreads]>(dyn + (size_t)ElemGroups<KE>::TILES);
-  elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
+  // 3D: element matrices streamed through the shared-memory ring in place of the tiles
+  const bool use_ring = KE == 40 && !RES && a.ring_stage_bytes > 0;
+  unsigned ring_t = 0;
+  if (use_ring) ring_init(a.ring_stage_bytes);  // visible after the first grid barrier
+  else elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
   __shared__ double hs1[kSlots], hs2[kMaxBasis], sc[4];
   __shared__ int s_stop;
-  double* g = dyn + tile_doubles<KE>();  // Givens right-hand side
+  double* g = dyn + (use_ring ? ring_total_bytes(a.ring_stage_bytes) / sizeof(double) : tile_doubles<KE>());  // Givens right-hand side
   double* cs = g + (m + 1);    // rotations
   double* sn = cs + m;
   double* col = sn + m;        // Hessenberg column being rotated
@@ -410,11 +586,15 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   };
 
   auto elem_pass64 = [&](const double* x) {
-    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
+    if (use_ring) elem_pass_ring<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, a.ring_stage_bytes, ring_t, bar);
+    else elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
     if (sizeof(TR) == 8) elem_pass64(x);
+    else if (use_ring)
+      elem_pass_ring<KE, NEQ, NNOD, TR>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, a.ring_stage_bytes,
+                                        ring_t, bar);
     else elem_pass<KE, NEQ, NNOD, TR>((const TR*)a.R32, a.conn, x, (TR*)a.Y32, a.n_elements, first, tileR);
   };
   // node pass over the own unknowns: w = gather(Y) (mode 0) or b - gather(Y) (mode 1);
@@ -988,9 +1168,24 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
     return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes, 0, st);
   e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, false>);
   if (e != cudaSuccess) return e;
+  if (KE == 40 && a.ring) {
+    // 3D: the largest ring stage (a multiple of one FP64 element matrix, at most 4 of them) that
+    // fits beside the rest; stages hold 4 FP64 or 8 FP32 element matrices at m <= 50
+    constexpr size_t kElem64 = (size_t)KE * KE * sizeof(double);
+    for (size_t se = 4; se >= 1; se--) {
+      const size_t ring_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, false, se * kElem64);
+      if (fa.sharedSizeBytes + ring_bytes <= (size_t)optin) {
+        PersistentArgs ar = a;
+        ar.ring_stage_bytes = (int)(se * kElem64);
+        return launch_cfg<KE, NEQ, NNOD, TR, false>(ar, blocks, ring_bytes, 0, st);
+      }
+    }
+  }
   const size_t str_bytes = sizeof(double) * persistent_dyn_doubles<KE>(a.m, S, false);
   if (fa.sharedSizeBytes + str_bytes > (size_t)optin) return cudaErrorInvalidValue;  // m too large
-  return launch_cfg<KE, NEQ, NNOD, TR, false>(a, blocks, str_bytes, 0, st);
+  PersistentArgs ad = a;
+  ad.ring_stage_bytes = 0;
+  return launch_cfg<KE, NEQ, NNOD, TR, false>(ad, blocks, str_bytes, 0, st);
 }
 
 cudaError_t launch_dim(int ndim, int fp32, const PersistentArgs& a, cudaStream_t st) {

@@ -53,6 +53,9 @@ struct PersistentArgs {
   unsigned int* nbr_flag;      // per block (32 apart): neighbour syncs passed, zero before launch
   int max_valence;             // most (element, local node) entries of a node in the CSR
   int node_cache;              // set at launch: the node pass's gather offsets kept in shared memory
+  int ring;                    // 3D: 1 = stream the element matrices through the shared-memory ring
+                               // (bulk copies under mbarriers), 0 = direct loads in waves
+  int ring_stage_bytes;        // set at launch: bytes of one ring stage (0: direct loads)
 };
 
 int persistent_blocks();

@@ -64,7 +64,8 @@ class _Report(C.Structure):
 class _Stats(C.Structure):
     _fields_ = [("launches", C.c_long), ("total_ms", C.c_double), ("bytes", C.c_double),
                 ("form_launches", C.c_long), ("form_ms", C.c_double), ("kernel_launches", C.c_long),
-                ("solves", C.c_long), ("solve_ms", C.c_double), ("solve_bytes", C.c_double)]
+                ("solves", C.c_long), ("solve_ms", C.c_double), ("solve_bytes", C.c_double),
+                ("matvec_ms", C.c_double), ("matvec_bytes", C.c_double)]
 
 
 class _AdjOpts(C.Structure):
@@ -353,7 +354,7 @@ class FDVSolver:
         return {"launches": s.launches, "total_ms": s.total_ms, "bytes": s.bytes,
                 "form_launches": s.form_launches, "form_ms": s.form_ms,
                 "kernel_launches": s.kernel_launches, "solves": s.solves, "solve_ms": s.solve_ms,
-                "solve_bytes": s.solve_bytes}
+                "solve_bytes": s.solve_bytes, "matvec_ms": s.matvec_ms, "matvec_bytes": s.matvec_bytes}
 
     # -- discrete adjoint and tangent --
     def vjp(self, mu, du):

@@ -198,6 +198,10 @@ typedef struct {
   double solve_ms;
   double solve_bytes;   /* algorithmic bytes of those solves: per product E*Ke^2*s_R + 2*DOF*8,
                            per Arnoldi step (j+2) DOF vectors, per cycle (k+2) DOF vectors */
+  double matvec_ms;     /* the whole EBE products of the `launches` above (element pass and node
+                           pass, gather-multiply-scatter), summed device time */
+  double matvec_bytes;  /* their algorithmic bytes: E*Ke^2*s_R + DOF*(8 + 8) each (matrices once,
+                           x read, y written) */
 } cfdv_kernel_stats;
 int cfdv_profile(cfdv_ctx* ctx, int enable);
 int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);

@@ -32,6 +32,10 @@ def build(quiet: bool = True) -> None:
     if os.path.isdir(ref_src):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={ref_src}"], check=True,
                        stdout=subprocess.DEVNULL if quiet else None)
+        # the reference loop with the B200 plug-ins, once the CUDA library is built
+        if os.path.exists(os.path.join(HERE, "..", "cfdv_b200", "libcfdv_gpu.so")):
+            subprocess.run(["make", "-C", HERE, "ref-gpu", f"REF={ref_src}"], check=True,
+                           stdout=subprocess.DEVNULL if quiet else None)
 
 
 def lib():

@@ -27,6 +27,13 @@
 // hex8 elements this samples the reference's formation without forming every element.
 // The element functor depends only on the element and its nodes, so a subset's matrices
 // are those a full pass would give.
+// Built with -DCFDV_GPU_PLUGIN (oracle/Makefile target ref-gpu, _ref/cfdv_ref_gpu, linked
+// against libcfdv_gpu.so) the same loop can run the B200 plug-ins of
+// cfdv_b200/host/cfdv_reference_plugin.hpp in place of the reference's classes:
+//   --gpu-solver   CudaGMRES : GMRESbase instead of MPI_GMRES (main.cpp:196-197)
+//   --gpu-form     GpuFormation instead of the FDVGalerkin and ApplyBC passes (main.cpp:185-194)
+// so that everything else -- load, CalcLength, ClearElement, NodeUnpack, CFL, RMS, the record
+// file -- is the reference's own code path.
 // --tecplot writes the reference's outputs into the working directory: tecplot_<iter>.plt
 // (MPI_TecplotOut.h) at every iteration divisible by 100, as main.cpp:183 does, and the
 // RMSError.txt line of every step (MPI_RMSError.h), as main.cpp:198 does.
@@ -57,6 +64,11 @@
 #include "Utility/Solvers/MPI_GMRES.h"
 #include "Utility/IO/ASCIItoBinary/LoadBinary.h"
 #include "Utility/IO/MPI_TecplotOut.h"
+#ifdef CFDV_GPU_PLUGIN
+#include <memory>
+
+#include "cfdv_reference_plugin.hpp"
+#endif
 
 namespace {
 
@@ -115,7 +127,7 @@ int main(int argc, char** argv) {
   std::string path = argv[1];
   std::string out = argv[2];
   int nsteps = 1, dump_step = -1, m_override = -1, r_override = -1;
-  bool quiet = false, tecplot = false, form_subset = false;
+  bool quiet = false, tecplot = false, form_subset = false, gpu_solver = false, gpu_form = false;
   std::string elements_file;
   for (int i = 3; i < argc; i++) {
     std::string a = argv[i];
@@ -127,7 +139,15 @@ int main(int argc, char** argv) {
     else if (a == "--tecplot") tecplot = true;
     else if (a == "--elements" && i + 1 < argc) elements_file = argv[++i];
     else if (a == "--form-subset") form_subset = true;
+    else if (a == "--gpu-solver") gpu_solver = true;
+    else if (a == "--gpu-form") gpu_form = true;
   }
+#ifndef CFDV_GPU_PLUGIN
+  if (gpu_solver || gpu_form) {
+    fprintf(stderr, "--gpu-solver / --gpu-form need the build with CFDV_GPU_PLUGIN (cfdv_ref_gpu)\n");
+    return 2;
+  }
+#endif
 
   auto cm = parse_kv(path + "/control");
   auto am = parse_kv(path + "/aero");
@@ -157,6 +177,23 @@ int main(int argc, char** argv) {
   NavierStokes* NS = (ndim == 2) ? (NavierStokes*)new NavierStokes2D : (NavierStokes*)new NavierStokes3D;
   MPI_GMRES gmres(restart, m, Nn * neqn, neqn, nnod, ndim, 1, 0, 0);  // MPIBinaryConfiguration.h:123
   std::cout.rdbuf(saved);
+  GMRESbase* solver = &gmres;
+#ifdef CFDV_GPU_PLUGIN
+  std::unique_ptr<cfdv_plugin::Context> gctx;
+  std::unique_ptr<CudaGMRES> cuda_gmres;
+  std::unique_ptr<cfdv_plugin::GpuFormation> gpu_formation;
+  if (gpu_solver || gpu_form) {
+    cfdv_params gp{getd(am, "gamma", 1.4), getd(am, "M", 1.0),        getd(am, "Re", 1.0),
+                   getd(am, "Pr", 0.72),   getd(am, "Tinf", 216.6666), getd(am, "Twall", 1.0),
+                   geti(am, "Adiabatic", 1) != 0 ? 1 : 0, 0};
+    gctx.reset(new cfdv_plugin::Context(elements, nodes, ndim, nnod, neqn, gp));
+    if (gpu_solver) {
+      cuda_gmres.reset(new CudaGMRES(*gctx, restart, m));
+      solver = cuda_gmres.get();
+    }
+    if (gpu_form) gpu_formation.reset(new cfdv_plugin::GpuFormation(*gctx));
+  }
+#endif
 
   RecordFile rf;
   rf.f = fopen(out.c_str(), "wb");
@@ -211,9 +248,17 @@ int main(int argc, char** argv) {
     auto t0 = std::chrono::steady_clock::now();
     const bool sub_only = form_subset && iter == dump_step;
     std::vector<Element*>& formed = sub_only ? subset : elements;
+    const size_t D = dump_el.size();
+#ifdef CFDV_GPU_PLUGIN
+    if (gpu_formation) {
+      // the device forms and applies the Dirichlet rows in one pass: R and rhs come back to the
+      // elements only when the host needs them (a dump, or the reference's own solver)
+      (*gpu_formation)(elements, nodes, dt, iter == dump_step || !cuda_gmres);
+    } else
+#endif
+    {
     FDVGalerkin<Element*> fdv(nnod, neqn, ndim, nbnod, dt, NS);  // main.cpp:185-186
     for_each(formed.begin(), formed.end(), std::ref(fdv));
-    const size_t D = dump_el.size();
     if (iter == dump_step) {
       std::vector<double> R(D * Ke * Ke), rhs(D * Ke), s(4 * D);
       for (size_t k = 0; k < D; k++) {
@@ -229,6 +274,7 @@ int main(int argc, char** argv) {
       rf.putd("s1234", s);
     }
     for_each(formed.begin(), formed.end(), ApplyBC<Element*>(neqn, nnod, ndim, nbnod));  // main.cpp:194
+    }
     auto t1 = std::chrono::steady_clock::now();
     if (iter == dump_step) {
       std::vector<double> R(D * Ke * Ke), rhs(D * Ke);
@@ -256,8 +302,8 @@ int main(int argc, char** argv) {
     std::ostringstream cap;
     cap.precision(17);
     std::cout.rdbuf(cap.rdbuf());
-    gmres.iterate(elements);  // main.cpp:196
-    gmres.update(nodes);      // main.cpp:197
+    solver->iterate(elements);  // main.cpp:196
+    solver->update(nodes);      // main.cpp:197
     std::cout.rdbuf(saved);
     auto t2 = std::chrono::steady_clock::now();
     t_form += std::chrono::duration<double>(t1 - t0).count();

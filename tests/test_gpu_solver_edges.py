@@ -111,3 +111,44 @@ def test_step_host_equals_set_step_get(gpu, name, engine):
         U3 = s.get_state()
     assert np.array_equal(U1, U2) and np.array_equal(U2, U3)
     assert r1["dt"] == r2["dt"] and np.array_equal(r1["est"], r2["est"])
+
+
+_RING_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
+from conftest import get_case
+from cfdv_b200 import gpu as G
+out = {}
+for name in ("ramp4", "cyl4", "duct4", "ramp4_adap"):
+    case = get_case(name)
+    with G.FDVSolver(case) as s:
+        s.load_node_records()
+        s.form(s.cfl(float(case.control["cfl"])), precision=G.PREC_MIXED)
+        for prec in (G.PREC_FP64, G.PREC_MIXED):
+            for m in (30, 62):
+                r = s.gmres(mode=G.GMRES_CORRECT, m=m, restarts=40, rtol=1e-10, precision=prec, engine=0)
+                out[f"{name}_{prec}_{m}"] = s.du()
+                out[f"{name}_{prec}_{m}_est"] = r["est"]
+np.savez(sys.argv[2], **out)
+"""
+
+
+def test_3d_element_ring_matches_direct_pass_bitwise(tmp_path):
+    """The 3D element pass of the persistent solve streams the element matrices through a
+    shared-memory ring of bulk copies; CFDV_ELEM_RING=0 selects the pass that loads them
+    directly.  Each row sums in the same order in both, so whole solves (FP64 and mixed, the
+    ring's largest stage at m = 30 and a smaller one at m = 62) agree bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+
+    res = {}
+    for ring in ("1", "0"):
+        out = str(tmp_path / f"ring{ring}.npz")
+        env = dict(os.environ, CFDV_ELEM_RING=ring)
+        subprocess.run([sys.executable, "-c", _RING_CHILD, ROOT, out], check=True, env=env, timeout=600)
+        res[ring] = dict(np.load(out))
+    assert res["1"].keys() == res["0"].keys()
+    for k in res["1"]:
+        assert np.array_equal(res["1"][k], res["0"][k]), k
