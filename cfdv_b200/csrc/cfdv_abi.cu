@@ -28,6 +28,7 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_csr_ptr); dfree(c->d_csr_idx);
   dfree(c->d_U); dfree(c->d_U0); dfree(c->d_du);
   dfree(c->d_R64); dfree(c->d_R32); dfree(c->d_rhs); dfree(c->d_s); dfree(c->d_Y64); dfree(c->d_Y32);
+  dfree(c->d_marks);
   dfree(c->d_V); dfree(c->d_W); dfree(c->d_b); dfree(c->d_pa); dfree(c->d_pb); dfree(c->d_H); dfree(c->d_sc);
   dfree(c->d_y); dfree(c->d_rms); dfree(c->d_status); dfree(c->d_pers); dfree(c->d_pers_int); dfree(c->d_Dinv); dfree(c->d_Z);
   dfree(c->d_pm); dfree(c->d_cfl_count); dfree(c->d_nbr_ptr); dfree(c->d_nbr_idx); c->nbr_blocks = 0;
@@ -1030,6 +1031,26 @@ int cfdv_get_element_matrices(cfdv_ctx* c, double* R, double* rhs) {
   if (R) CK(cudaMemcpyAsync(R, c->d_R64, sizeof(double) * E * Ke * Ke, cudaMemcpyDeviceToHost, c->st));
   if (rhs) CK(cudaMemcpyAsync(rhs, c->d_rhs, sizeof(double) * E * Ke, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return CFDV_OK;
+}
+
+int cfdv_refine_marks(cfdv_ctx* c, double threshold, int* elements, int capacity, int* n) {
+  if (!c || !n || capacity < 0 || (capacity > 0 && !elements)) return CFDV_ERR_ARG;
+  cudaSetDevice(c->dev);
+  int rc;
+  if (!c->d_marks && (rc = dalloc(c, &c->d_marks, (size_t)c->n_elements))) return rc;
+  CK(launch_refine_marks(c->ndim, c->d_U, c->d_x, c->d_conn, c->n_elements, c->gas, threshold, c->d_marks, c->st));
+  c->launches++;
+  std::vector<unsigned char> flags((size_t)c->n_elements);
+  CK(cudaMemcpyAsync(flags.data(), c->d_marks, flags.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  int k = 0;
+  for (int e = 0; e < c->n_elements; e++)
+    if (flags[(size_t)e]) {
+      if (k < capacity) elements[k] = e;
+      k++;
+    }
+  *n = k;
   return CFDV_OK;
 }
 

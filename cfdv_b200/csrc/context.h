@@ -36,6 +36,7 @@ struct cfdv_ctx {
   float* d_R32 = nullptr;
   double* d_rhs = nullptr;
   double* d_s = nullptr;
+  unsigned char* d_marks = nullptr;  // [E] refinement marks (cfdv_refine_marks)
   double* d_Y64 = nullptr;
   float* d_Y32 = nullptr;
   bool formed = false, have32 = false;

@@ -36,6 +36,35 @@ cudaError_t launch_form(int ndim, const FormArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// ---- refinement marks (RefineListAdaptive.h:25-36): FDVParam's s1 from the element's node
+// Mach numbers, by the same node unpack and s1 arithmetic as the formation's FDV parameters
+template <int NDIM>
+__global__ void refine_mark_kernel(const double* __restrict__ U, const double* __restrict__ x,
+                                   const int* __restrict__ conn, int E, GasParams g, double threshold,
+                                   unsigned char* marks) {
+  constexpr int NNOD = (NDIM == 2) ? 4 : 8, NEQ = NDIM + 2;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+    double Mn[NNOD], Ren[NNOD], s[2];
+    for (int i = 0; i < NNOD; i++) {
+      const int n = conn[(size_t)e * NNOD + i];
+      NodePrim nd;
+      node_unpack<NDIM>(g, U + (size_t)n * NEQ, x + (size_t)n * NDIM, nd);
+      node_mach_re<NDIM>(g, nd, &Mn[i], &Ren[i]);
+    }
+    fdv_pair<NNOD>(Mn, 0, s);
+    marks[e] = s[0] > threshold ? 1 : 0;
+  }
+}
+
+cudaError_t launch_refine_marks(int ndim, const double* U, const double* x, const int* conn, int E, const GasParams& g,
+                                double threshold, unsigned char* marks, cudaStream_t st) {
+  if (E <= 0) return cudaSuccess;
+  const int grid = (E + 255) / 256;
+  if (ndim == 2) refine_mark_kernel<2><<<grid, 256, 0, st>>>(U, x, conn, E, g, threshold, marks);
+  else refine_mark_kernel<3><<<grid, 256, 0, st>>>(U, x, conn, E, g, threshold, marks);
+  return cudaGetLastError();
+}
+
 // ---- CFL (MPI_CFL.h:7-56): dt = cfl * min_e min_nodes cleng_e / (|v| + sqrt(1.4 cgas T))
 template <int NDIM>
 __global__ void cfl_partial_kernel(const double* __restrict__ U, const int* __restrict__ conn,

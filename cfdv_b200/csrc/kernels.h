@@ -70,6 +70,9 @@ __device__ __forceinline__ double reduce_partials(const double* __restrict__ p, 
 // ---- launchers ---------------------------------------------------------------
 struct FormArgs;
 cudaError_t launch_form(int ndim, const FormArgs& a, cudaStream_t st);
+// FDVParam's s1 > threshold per element from the node states U (refinement marks, 1 byte each)
+cudaError_t launch_refine_marks(int ndim, const double* U, const double* x, const int* conn, int E, const GasParams& g,
+                                double threshold, unsigned char* marks, cudaStream_t st);
 cudaError_t launch_cfl(int ndim, const double* U, const int* conn, const double* cleng, int E, const GasParams& g,
                        double cfl, double* partial, unsigned int* count, int nb, double* dt_out, cudaStream_t st);
 

@@ -30,7 +30,7 @@ EXPORTS = ["cfdv_create", "cfdv_upload_mesh", "cfdv_destroy", "cfdv_last_error",
            "cfdv_get_element_matrices", "cfdv_get_rhs_vector", "cfdv_get_du", "cfdv_matvec", "cfdv_profile",
            "cfdv_profile_read", "cfdv_vjp", "cfdv_jvp", "cfdv_element_functional", "cfdv_wall_force",
            "cfdv_wall_nodes", "cfdv_adjoint", "cfdv_tangent", "cfdv_ebe_matvec_static", "cfdv_set_adaptive",
-           "cfdv_step_host", "cfdv_get_element_subset"]
+           "cfdv_step_host", "cfdv_get_element_subset", "cfdv_refine_marks"]
 
 
 class CfdvError(RuntimeError):
@@ -114,6 +114,7 @@ def lib():
         L.cfdv_get_fdv_params.argtypes = [P, P]
         L.cfdv_get_element_matrices.argtypes = [P, P, P]
         L.cfdv_get_element_subset.argtypes = [P, I, P, P, P, P]
+        L.cfdv_refine_marks.argtypes = [P, D, P, I, P]
         L.cfdv_get_rhs_vector.argtypes = [P, P]
         L.cfdv_get_du.argtypes = [P, P]
         L.cfdv_matvec.argtypes = [P, P, P, I, I]
@@ -328,6 +329,33 @@ class FDVSolver:
         s = np.zeros((ids.size, 4))
         self._ck(self.L.cfdv_get_element_subset(self._ctx, ids.size, _p(ids), _p(R), _p(rhs), _p(s)))
         return R, rhs, s
+
+    def refine_marks(self, threshold=0.8):
+        """Element ids with s1 > threshold at the current state (the reference's refinement
+        criterion), ascending."""
+        n = C.c_int()
+        self._ck(self.L.cfdv_refine_marks(self._ctx, float(threshold), None, 0, C.byref(n)))
+        ids = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._ck(self.L.cfdv_refine_marks(self._ctx, float(threshold), _p(ids), ids.size, C.byref(n)))
+        return ids[: n.value].copy()
+
+    def upload_case(self, case):
+        """Replace the mesh by `case`'s (a refined mesh from the host): cfdv_upload_mesh, then
+        the adaptive elements of `case` if it has any (cfdv_set_adaptive).  The state and the
+        matrices are reset; load node records or set the state next."""
+        ndim = case.ndim
+        assert ndim == self.ndim
+        self._x = np.ascontiguousarray(case.nodes[:, :ndim], dtype=np.float64)
+        self._conn = np.ascontiguousarray(case.conn, dtype=np.int32)
+        self._bc = np.ascontiguousarray(case.bc, dtype=np.int32)
+        mesh = _Mesh(ndim, case.n_nodes, case.n_elements, _p(self._x).value, _p(self._conn).value, _p(self._bc).value)
+        self._ck(self.L.cfdv_upload_mesh(self._ctx, C.byref(mesh)))
+        self.case = case
+        self.n_nodes, self.n_elements = case.n_nodes, case.n_elements
+        self.n_dof = self.n_nodes * self.neqn
+        self.__dict__.pop("_rep_cache", None)
+        if getattr(case, "adap_elements", None) is not None:
+            self.set_adaptive(case.adap_elements, case.adap_hnm)
 
     def rhs_vector(self):
         b = np.zeros(self.n_dof)

@@ -175,6 +175,13 @@ int cfdv_step_host(cfdv_ctx* ctx, double cfl, const cfdv_gmres_opts* opts, cfdv_
 int cfdv_get_fdv_params(cfdv_ctx* ctx, double* s);
 /* Element matrices [E][Ke*Ke] (FP64) and rhs [E][Ke] from the last cfdv_form. */
 int cfdv_get_element_matrices(cfdv_ctx* ctx, double* R, double* rhs);
+/* The elements the reference's adaptive refinement marks at the current state: FDVParam's s1
+ * of the element above `threshold` (0.8 in the reference, RefineListAdaptive.h:25-36),
+ * computed on the device from U; ascending element ids, min(*n, capacity) of them written to
+ * elements, *n = how many.  The dependency closure and the refinement itself stay on the host
+ * (AdaptiveRefineList, MeshRefine2D); the refined mesh comes back through cfdv_upload_mesh,
+ * cfdv_load_node_records (or cfdv_set_state) and cfdv_set_adaptive. */
+int cfdv_refine_marks(cfdv_ctx* ctx, double threshold, int* elements, int capacity, int* n);
 /* The same for the n elements ids[0..n): R [n][Ke*Ke], rhs [n][Ke] and s1..s4 [n][4] (any
  * may be NULL), without copying the whole mesh's matrices -- the reference's elements[e]->R,
  * ->rhs and FDVParam (Element.h:33-34, FDVParam.h:15-111) for a sample of e. */

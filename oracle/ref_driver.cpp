@@ -34,6 +34,11 @@
 //   --gpu-form     GpuFormation instead of the FDVGalerkin and ApplyBC passes (main.cpp:185-194)
 // so that everything else -- load, CalcLength, ClearElement, NodeUnpack, CFL, RMS, the record
 // file -- is the reference's own code path.
+// --refine runs, after the steps, the reference's mesh-refinement branch (main.cpp:139-148:
+// NodeUnpack, NodeCheck, AdaptiveRefineList -- elements with FDVParam s1 > 0.8
+// (RefineListAdaptive.h:25-36) and their dependencies -- then MeshRefine2D) and records the
+// marked elements and the refined case as Save would write it: node records {x, rho, v, T},
+// element node ids and face codes, and the adaptive elements with refine level and Hnm.
 // --tecplot writes the reference's outputs into the working directory: tecplot_<iter>.plt
 // (MPI_TecplotOut.h) at every iteration divisible by 100, as main.cpp:183 does, and the
 // RMSError.txt line of every step (MPI_RMSError.h), as main.cpp:198 does.
@@ -64,6 +69,9 @@
 #include "Utility/Solvers/MPI_GMRES.h"
 #include "Utility/IO/ASCIItoBinary/LoadBinary.h"
 #include "Utility/IO/MPI_TecplotOut.h"
+#include "FDV/Function/NodeCheck.h"
+#include "adap/RefineListAdaptive.h"
+#include "adap/MeshRefine2D.h"
 #ifdef CFDV_GPU_PLUGIN
 #include <memory>
 
@@ -127,7 +135,7 @@ int main(int argc, char** argv) {
   std::string path = argv[1];
   std::string out = argv[2];
   int nsteps = 1, dump_step = -1, m_override = -1, r_override = -1;
-  bool quiet = false, tecplot = false, form_subset = false, gpu_solver = false, gpu_form = false;
+  bool quiet = false, tecplot = false, form_subset = false, gpu_solver = false, gpu_form = false, refine = false;
   std::string elements_file;
   for (int i = 3; i < argc; i++) {
     std::string a = argv[i];
@@ -141,6 +149,7 @@ int main(int argc, char** argv) {
     else if (a == "--form-subset") form_subset = true;
     else if (a == "--gpu-solver") gpu_solver = true;
     else if (a == "--gpu-form") gpu_form = true;
+    else if (a == "--refine") refine = true;
   }
 #ifndef CFDV_GPU_PLUGIN
   if (gpu_solver || gpu_form) {
@@ -346,6 +355,60 @@ int main(int argc, char** argv) {
     rf.putd("steptime" + sfx, {std::chrono::duration<double>(t2 - t_step0).count()});
     t += dt;
     if (!quiet) fprintf(stderr, "step %d dt %.6e gfinal %.3e\n", iter, dt, fin.empty() ? -1.0 : fin.back());
+  }
+  if (refine) {  // main.cpp:139-148 (the refinement prints its progress: kept off stdout)
+    const int nface = geti(cm, "nface", ndim == 2 ? 4 : 6);
+    std::cout.rdbuf(sink.rdbuf());
+    for_each(nodes.begin(), nodes.end(), NodeUnpack<Node*>());
+    for_each(nodes.begin(), nodes.end(), NodeCheck<Node*>());
+    std::vector<int> marks;  // the criterion of RefineListAdaptive.h:25-36 before its dependency closure
+    {
+      FDVParam<Element*> fp;
+      double s1, s2, s3, s4;
+      for (size_t e = 0; e < elements.size(); e++) {
+        fp(elements[e], s1, s2, s3, s4);
+        if (s1 > 0.8) marks.push_back((int)e);
+      }
+    }
+    std::vector<int> elelist, refine_level;
+    AdaptiveRefineList<Element, Node>(elelist, refine_level, elements, nodes, nnod, nface);
+    MeshRefine2D<Element, Node>(elements, nodes, elelist, refine_level, ndim, neqn, nnod, nsteps, nface);
+    for_each(nodes.begin(), nodes.end(), NodeUnpack<Node*>());
+    for_each(nodes.begin(), nodes.end(), NodeCheck<Node*>());
+    std::cout.rdbuf(saved);
+    rf.puti("refine_marks", marks);
+    rf.puti("refine_elelist", elelist);
+    std::vector<double> rec;
+    std::vector<int> num;
+    for (Node* n : nodes) {  // the binarynodes record (LoadBinary.h:156-205)
+      for (int i = 0; i < ndim; i++) rec.push_back(n->x(i));
+      rec.push_back(n->rho);
+      for (int i = 0; i < ndim; i++) rec.push_back(n->v(i));
+      rec.push_back(n->T);
+      num.push_back((int)n->number);
+    }
+    rf.putd("refined_nodes", rec);
+    rf.puti("refined_node_numbers", num);
+    std::vector<int> conn, bcs, adap, level;
+    std::vector<double> hnm;
+    for (size_t e = 0; e < elements.size(); e++) {
+      Element* el = elements[e];
+      for (int k = 0; k < nnod; k++) conn.push_back((int)el->node[k]->number);
+      std::vector<int> b(nface, 0);
+      for (Face* f : el->face) b[f->face] = f->bc;
+      bcs.insert(bcs.end(), b.begin(), b.end());
+      if (el->adap) {
+        adap.push_back((int)e);
+        level.push_back(el->refine_level);
+        for (int M = 0; M < nnod; M++)
+          for (int N = 0; N < nnod; N++) hnm.push_back(el->Hnm(N, M));  // Hnm(N, M) at N + nnod*M
+      }
+    }
+    rf.puti("refined_conn", conn);
+    rf.puti("refined_bc", bcs);
+    rf.puti("refined_adap", adap);
+    rf.puti("refined_levels", level);
+    rf.putd("refined_hnm", hnm);
   }
   rf.putd("timing", {t_form / std::max(nsteps, 1), t_gmres / std::max(nsteps, 1)});
   fclose(rf.f);

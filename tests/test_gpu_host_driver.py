@@ -1,6 +1,8 @@
 """The C++ host driver (cfdv_b200/cfdv_gpu, the reference's time loop over the C ABI)
-writes the same output files as the reference: tecplot_0.plt byte for byte, and the
-RMSError.txt lines (iteration, per-field RMS change) to the printed precision."""
+writes the same output files as the reference: tecplot_0.plt byte for byte, tecplot_100.plt
+(after 100 steps of the reference-mode solver, with the cell-centred s1..s4 of that step)
+token by token to the printed precision, and the RMSError.txt lines (iteration, per-field
+RMS change) to the printed precision."""
 import os
 import subprocess
 import tempfile
@@ -39,6 +41,45 @@ def test_driver_outputs_match_reference(name, steps):
         assert a[0] == b[0]
         # 6 significant digits are printed; allow one unit in the last place
         np.testing.assert_allclose(np.array(a[1:], float), np.array(b[1:], float), rtol=2e-5, atol=1e-12)
+
+
+def _tokens(path):
+    return open(path).read().replace(",", " , ").replace("=", " = ").split()
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference build oracle/_ref not present")
+@pytest.mark.parametrize("name", ["lid8", "plate20"])
+def test_driver_tecplot_after_100_steps_matches_reference(name):
+    """tecplot_100.plt: the state after 100 reference-mode steps, its time in the title and the
+    s1..s4 of step 100 (MPI_TecplotOut.h:186-373, written at main.cpp:183 after NodeUnpack and
+    CFL).  The reference prints 6 significant digits; every number must agree to one unit in
+    the last printed place, every other token exactly."""
+    from cfdv_b200 import meshgen as mg
+    case = get_case(name)
+    with tempfile.TemporaryDirectory() as d:
+        cdir = os.path.join(d, "case")
+        mg.write_case(case, cdir)
+        rdir, gdir = os.path.join(d, "ref"), os.path.join(d, "gpu")
+        os.makedirs(rdir)
+        os.makedirs(gdir)
+        subprocess.run([REF, cdir, os.path.join(d, "r.rec"), "--steps", "101", "--tecplot", "--quiet"],
+                       cwd=rdir, check=True, stdin=subprocess.DEVNULL)
+        subprocess.run([DRIVER, cdir, "--steps", "101", "--out", gdir, "--save-every", "0"], check=True,
+                       capture_output=True)
+        ref = _tokens(os.path.join(rdir, "tecplot_100.plt"))
+        got = _tokens(os.path.join(gdir, "tecplot_100.plt"))
+    assert len(ref) == len(got)
+    nums_r, nums_g = [], []
+    for a, b in zip(got, ref):
+        try:
+            fb = float(b.strip('"'))
+        except ValueError:
+            assert a == b
+            continue
+        nums_r.append(fb)
+        nums_g.append(float(a.strip('"')))
+    assert len(nums_r) > 100
+    np.testing.assert_allclose(np.array(nums_g), np.array(nums_r), rtol=2e-5, atol=1e-12)
 
 
 @pytest.mark.parametrize("name", ["lid8", "ramp4"])
