@@ -426,8 +426,9 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
       const bool act = lact && e < E;
       TM* tb = tiles + (size_t)buf * EPW * KE;
       if (act) {
-        const int f = e0 == (int)blockIdx.x * EPW ? first[0][threadIdx.x]
-                                                  : __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ;
+        const int f = (first && e0 == (int)blockIdx.x * EPW)
+                          ? first[0][threadIdx.x]
+                          : __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ;
         tb[le * KE + i] = (TM)__ldcg(x + f);
       }
       __syncthreads();  // the other buffer was last read before the previous barrier
@@ -522,11 +523,15 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* tile64 = dyn;
   TR* tileR = reinterpret_cast<TR*>(dyn);
   auto* first = reinterpret_cast<int (*)[kThreads]>(dyn + (size_t)ElemGroups<KE>::TILES);
-  // 3D: element matrices streamed through the shared-memory ring in place of the tiles
-  const bool use_ring = KE == 40 && !RES && a.ring_stage_bytes > 0;
+  // 3D, FP32 products: those element matrices streamed through the shared-memory ring; the FP64
+  // restart residuals of that kernel use the direct pass, with its tiles at the start of the ring
+  // area (idle then: every ring pass has consumed its last stage before the grid barrier that
+  // ends it) and without the cached first-chunk offsets
+  const bool use_ring = KE == 40 && !RES && sizeof(TR) == 4 && a.ring_stage_bytes > 0;
   unsigned ring_t = 0;
   if (use_ring) ring_init(a.ring_stage_bytes);  // visible after the first grid barrier
   else elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
+  const int (*first_or_null)[kThreads] = use_ring ? nullptr : first;
   __shared__ double hs1[kSlots], hs2[kMaxBasis], sc[4];
   __shared__ int s_stop;
   double* g = dyn + (use_ring ? ring_total_bytes(a.ring_stage_bytes) / sizeof(double) : tile_doubles<KE>());  // Givens right-hand side
@@ -586,8 +591,7 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   };
 
   auto elem_pass64 = [&](const double* x) {
-    if (use_ring) elem_pass_ring<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, a.ring_stage_bytes, ring_t, bar);
-    else elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
+    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first_or_null, tile64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {
@@ -628,6 +632,18 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   auto precond_slice = [&](int i) {
     __syncthreads();  // v_i of the whole node is written
     for (int dl = tid; dl < ns; dl += kThreads) {
+      const int d = lo + dl, nd = d / NEQ, r = d % NEQ, base = dl - r;
+      const double* D = a.Dinv + (size_t)nd * NEQ * NEQ;
+      double t = 0.0;
+#pragma unroll
+      for (int s = 0; s < NEQ; s++) t += D[r * NEQ + s] * vld(i, base + s);
+      a.Z[d] = t;
+    }
+  };
+  // the same by the first nthr threads (a multiple of 32), synchronised by named barrier 15
+  auto precond_slice_part = [&](int i, int nthr) {
+    asm volatile("bar.sync 15, %0;" ::"r"(nthr) : "memory");  // v_i of the whole node is written
+    for (int dl = tid; dl < ns; dl += nthr) {
       const int d = lo + dl, nd = d / NEQ, r = d % NEQ, base = dl - r;
       const double* D = a.Dinv + (size_t)nd * NEQ * NEQ;
       double t = 0.0;
@@ -781,6 +797,22 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   // DCGS2 pass B over the own unknowns, with c = hs1[0..j), p = hs1[j..2j) ++ pj:
   //   q_j = (u~_j - Q_j c) / nu  (final, into slot j),  u = w - Q_j p[0..j) - pj q_j,
   //   slot j+1 = u / sigma (sigma > 0), or u kept in w (sigma = 0); returns the share of ||u||^2
+  // pass B by the first nthr threads of the block (the resident path's overlapped step)
+  auto pass_b_part = [&](int j, double nu, double pj, double sigma, int nthr) {
+    for (int dl = tid; dl < ns; dl += nthr) {
+      double su = 0.0, sw = 0.0;
+#pragma unroll 4
+      for (int i = 0; i < j; i++) {
+        const double q = vld(i, dl);
+        su += hs1[i] * q;
+        sw += hs1[j + i] * q;
+      }
+      const double qj = (vld(j, dl) - su) / nu;
+      const double u = wld(dl) - sw - pj * qj;
+      vst(j, dl, qj);
+      vst(j + 1, dl, u / sigma);
+    }
+  };
   auto pass_b = [&](int j, double nu, double pj, double sigma) -> double {
     double acc = 0.0;
     for (int dl = tid; dl < ns; dl += kThreads) {
@@ -936,6 +968,48 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
         reduce_parts(2 * j + 3, hs1);
         dcgs_scalars(j, true);
         const double nu = sc[0], pj = sc[1], s2 = sc[2], w2 = sc[3];
+        if (RES && s2 > kPythMin * w2) {  // the same decision in every block; then sigma > 0
+          // Resident basis (latency-bound): the last warp completes column j-1, rotates it (the
+          // stopping test) and forms the pending column j, while the other warps run pass B and
+          // the preconditioner; the two parts share no data.  When the test stops the cycle,
+          // pass B has written slots j and j+1 only, which the update (slots < j) does not read.
+          const double sigma = sqrt(s2);
+          if (wid == kWarps - 1) {
+            if (j == 0) {
+              if (lane == 0) g[0] = beta * nu;  // r = beta u~_0 = beta nu q_0
+            } else {
+              for (int r = lane; r <= j; r += 32) {
+                const double h = r < j ? pend[r] + tpend * hs1[r] : tpend * nu;
+                col[r] = h;
+                Hf[(size_t)(j - 1) * (m + 1) + r] = h;
+              }
+              __syncwarp();
+              givens(j - 1, tpend * nu);
+              __syncwarp();
+            }
+            for (int r = lane; r <= j; r += 32) {
+              double hc = 0.0;
+              for (int cj = r > 0 ? r - 1 : 0; cj < j; cj++) hc += Hf[(size_t)cj * (m + 1) + r] * hs1[cj];
+              pend[r] = ((r < j ? hs1[j + r] : pj) - hc) / nu;
+            }
+          } else {
+            pass_b_part(j, nu, pj, sigma, kThreads - 32);
+            if (a.Dinv) precond_slice_part(j + 1, kThreads - 32);
+          }
+          __syncthreads();
+          if (j > 0) {
+            total_est++;
+            if (s_stop) {
+              k = j;
+              break;
+            }
+          }
+          passes += j + 2;
+          tpend = sigma / nu;
+          k = j + 1;
+          if (!sync_x()) return;
+          continue;
+        }
         if (j == 0) {
           if (tid == 0) g[0] = beta * nu;  // r = beta u~_0 = beta nu q_0
         } else {  // complete column j-1 and rotate it
@@ -1168,7 +1242,7 @@ cudaError_t launch_one(const PersistentArgs& a, cudaStream_t st) {
     return launch_cfg<KE, NEQ, NNOD, TR, true>(a, blocks, res_bytes, 0, st);
   e = cudaFuncGetAttributes(&fa, gmres_persistent_kernel<KE, NEQ, NNOD, TR, false>);
   if (e != cudaSuccess) return e;
-  if (KE == 40 && a.ring) {
+  if (KE == 40 && a.ring && sizeof(TR) == 4) {
     // 3D: the largest ring stage (a multiple of one FP64 element matrix, at most 4 of them) that
     // fits beside the rest; stages hold 4 FP64 or 8 FP32 element matrices at m <= 50
     constexpr size_t kElem64 = (size_t)KE * KE * sizeof(double);

@@ -113,13 +113,13 @@ def test_step_host_equals_set_step_get(gpu, name, engine):
     assert r1["dt"] == r2["dt"] and np.array_equal(r1["est"], r2["est"])
 
 
-_RING_CHILD = r"""
+_PASS_CHILD = r"""
 import sys, numpy as np
 sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
 from conftest import get_case
 from cfdv_b200 import gpu as G
 out = {}
-for name in ("ramp4", "cyl4", "duct4", "ramp4_adap"):
+for name in sys.argv[3].split(","):
     case = get_case(name)
     with G.FDVSolver(case) as s:
         s.load_node_records()
@@ -129,26 +129,37 @@ for name in ("ramp4", "cyl4", "duct4", "ramp4_adap"):
                 r = s.gmres(mode=G.GMRES_CORRECT, m=m, restarts=40, rtol=1e-10, precision=prec, engine=0)
                 out[f"{name}_{prec}_{m}"] = s.du()
                 out[f"{name}_{prec}_{m}_est"] = r["est"]
+        # whole steps (formation and solve again each step)
+        for k in range(3):
+            r = s.step(float(case.control["cfl"]), mode=G.GMRES_CORRECT, m=30, restarts=40, rtol=1e-8,
+                       precision=G.PREC_MIXED)
+        out[f"{name}_steps"] = s.get_state()
 np.savez(sys.argv[2], **out)
 """
 
 
-def test_3d_element_ring_matches_direct_pass_bitwise(tmp_path):
-    """The 3D element pass of the persistent solve streams the element matrices through a
-    shared-memory ring of bulk copies; CFDV_ELEM_RING=0 selects the pass that loads them
-    directly.  Each row sums in the same order in both, so whole solves (FP64 and mixed, the
-    ring's largest stage at m = 30 and a smaller one at m = 62) agree bit for bit."""
+def _runs_agree_bitwise(tmp_path, var, names):
     import os
     import subprocess
     import sys
     from conftest import ROOT
 
     res = {}
-    for ring in ("1", "0"):
-        out = str(tmp_path / f"ring{ring}.npz")
-        env = dict(os.environ, CFDV_ELEM_RING=ring)
-        subprocess.run([sys.executable, "-c", _RING_CHILD, ROOT, out], check=True, env=env, timeout=600)
-        res[ring] = dict(np.load(out))
+    for flag in ("1", "0"):
+        out = str(tmp_path / f"{var}{flag}.npz")
+        env = dict(os.environ, **{var: flag})
+        subprocess.run([sys.executable, "-c", _PASS_CHILD, ROOT, out, ",".join(names)], check=True, env=env,
+                       timeout=600)
+        res[flag] = dict(np.load(out))
     assert res["1"].keys() == res["0"].keys()
     for k in res["1"]:
         assert np.array_equal(res["1"][k], res["0"][k]), k
+
+
+def test_3d_element_ring_matches_direct_pass_bitwise(tmp_path):
+    """The 3D element pass of the persistent solve streams the FP32 element matrices (the mixed
+    form's Arnoldi products) through a shared-memory ring of bulk copies; CFDV_ELEM_RING=0
+    selects the pass that loads them directly.  Each row sums in the same order in both, so
+    whole solves (mixed, with the FP64 solves beside them, the ring's largest stage at m = 30
+    and a smaller one at m = 62) and whole steps agree bit for bit."""
+    _runs_agree_bitwise(tmp_path, "CFDV_ELEM_RING", ["ramp4", "cyl4", "duct4", "ramp4_adap"])
