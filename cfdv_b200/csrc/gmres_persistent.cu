@@ -426,9 +426,8 @@ __device__ __forceinline__ void elem_pass(const TM* __restrict__ R, const int* _
       const bool act = lact && e < E;
       TM* tb = tiles + (size_t)buf * EPW * KE;
       if (act) {
-        const int f = (first && e0 == (int)blockIdx.x * EPW)
-                          ? first[0][threadIdx.x]
-                          : __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ;
+        const int f = e0 == (int)blockIdx.x * EPW ? first[0][threadIdx.x]
+                                                  : __ldg(conn + (size_t)e * NNOD + i / NEQ) * NEQ + i % NEQ;
         tb[le * KE + i] = (TM)__ldcg(x + f);
       }
       __syncthreads();  // the other buffer was last read before the previous barrier
@@ -523,15 +522,13 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   double* tile64 = dyn;
   TR* tileR = reinterpret_cast<TR*>(dyn);
   auto* first = reinterpret_cast<int (*)[kThreads]>(dyn + (size_t)ElemGroups<KE>::TILES);
-  // 3D, FP32 products: those element matrices streamed through the shared-memory ring; the FP64
-  // restart residuals of that kernel use the direct pass, with its tiles at the start of the ring
-  // area (idle then: every ring pass has consumed its last stage before the grid barrier that
-  // ends it) and without the cached first-chunk offsets
+  // 3D with FP32 products (the mixed form): every element pass of the launch, the FP64 restart
+  // residuals included, streams its matrices through the shared-memory ring.  The FP64 form keeps
+  // the direct pass: measured, the ring made its whole solve slower (see the element pass notes).
   const bool use_ring = KE == 40 && !RES && sizeof(TR) == 4 && a.ring_stage_bytes > 0;
   unsigned ring_t = 0;
   if (use_ring) ring_init(a.ring_stage_bytes);  // visible after the first grid barrier
   else elem_first<KE, NEQ, NNOD>(a.conn, a.n_elements, first);  // each thread reads its own entries
-  const int (*first_or_null)[kThreads] = use_ring ? nullptr : first;
   __shared__ double hs1[kSlots], hs2[kMaxBasis], sc[4];
   __shared__ int s_stop;
   double* g = dyn + (use_ring ? ring_total_bytes(a.ring_stage_bytes) / sizeof(double) : tile_doubles<KE>());  // Givens right-hand side
@@ -591,7 +588,8 @@ __global__ void __launch_bounds__(kThreads, 1) gmres_persistent_kernel(Persisten
   };
 
   auto elem_pass64 = [&](const double* x) {
-    elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first_or_null, tile64);
+    if (use_ring) elem_pass_ring<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, a.ring_stage_bytes, ring_t, bar);
+    else elem_pass<KE, NEQ, NNOD, double>(a.R64, a.conn, x, a.Y64, a.n_elements, first, tile64);
   };
   // FP64 matrices, or FP32 matrices with FP32 accumulation
   auto elem_pass_op = [&](const double* x) {

@@ -157,9 +157,9 @@ def _runs_agree_bitwise(tmp_path, var, names):
 
 
 def test_3d_element_ring_matches_direct_pass_bitwise(tmp_path):
-    """The 3D element pass of the persistent solve streams the FP32 element matrices (the mixed
-    form's Arnoldi products) through a shared-memory ring of bulk copies; CFDV_ELEM_RING=0
-    selects the pass that loads them directly.  Each row sums in the same order in both, so
-    whole solves (mixed, with the FP64 solves beside them, the ring's largest stage at m = 30
-    and a smaller one at m = 62) and whole steps agree bit for bit."""
+    """In 3D the mixed form's persistent solve streams the element matrices of every element pass
+    (its FP32 products and FP64 restart residuals) through a shared-memory ring of bulk copies;
+    CFDV_ELEM_RING=0 selects the pass that loads them directly.  Each row sums in the same order
+    in both, so whole solves (mixed, with the FP64 solves beside them, the ring's largest stage
+    at m = 30 and a smaller one at m = 62) and whole steps agree bit for bit."""
     _runs_agree_bitwise(tmp_path, "CFDV_ELEM_RING", ["ramp4", "cyl4", "duct4", "ramp4_adap"])
