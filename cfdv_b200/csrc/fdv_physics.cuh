@@ -393,6 +393,7 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
   const S mu = f.mu, E = f.E;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const S rho = f.U[0], denom = 1. / (rho * rho), TERM1 = f.k * denom / th.Cv;
+  const S irho = 1. / rho;  // one division: the entries below multiply by it
   const S u = f.v[0], v = f.v[1], w = f.v[2], uu = u * u, vv = v * v, ww = w * w, q2 = uu + vv + ww;
   const S drdx = f.dU[0][0], dldx = f.dU[1][0], dmdx = f.dU[2][0], dndx = f.dU[3][0], dedx = f.dU[4][0];
   const S drdy = f.dU[0][1], dldy = f.dU[1][1], dmdy = f.dU[2][1], dndy = f.dU[3][1], dedy = f.dU[4][1];
@@ -426,9 +427,9 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
     JA(blk, 0, 4, 0) = u * b010 + v * b020 + w * b030 +
         (denom * (l * t[0][0] + mv * t[0][1] + n * t[0][2]) -
         TERM1 * (-dedx + (2. * E - 3. * q2) * drdx + 2. * (u * dldx + v * dmdx + w * dndx)));
-    JA(blk, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] / rho - TERM1 * (2. * u * drdx - dldx));
-    JA(blk, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] / rho - TERM1 * (-dmdx + 2. * v * drdx));
-    JA(blk, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] / rho - TERM1 * (2 * w * drdx - dndx));
+    JA(blk, 0, 4, 1) = u * b011 + v * b021 + w * b031 + (-t[0][0] * irho - TERM1 * (2. * u * drdx - dldx));
+    JA(blk, 0, 4, 2) = u * b012 + v * b022 + w * 0.0 + (-t[0][1] * irho - TERM1 * (-dmdx + 2. * v * drdx));
+    JA(blk, 0, 4, 3) = u * b013 + v * 0.0 + w * b033 + (-t[0][2] * irho - TERM1 * (2 * w * drdx - dndx));
     JA(blk, 0, 4, 4) = TERM1 * drdx;
   } else if (i == 1) {
     JA(blk, 0, 1, 0) = b020;
@@ -444,9 +445,9 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
     JA(blk, 0, 4, 0) = u * b020 + v * b120 + w * b130 +
         (denom * (l * t[1][0] + mv * t[1][1] + n * t[1][2]) -
         TERM1 * (-dedy + (2. * E - 3. * q2) * drdy + 2. * (u * dldy + v * dmdy + w * dndy)));
-    JA(blk, 0, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] / rho - TERM1 * (-dldy + 2. * u * drdy));
-    JA(blk, 0, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] / rho - TERM1 * (2. * v * drdy - dmdy));
-    JA(blk, 0, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] / rho - TERM1 * (2. * w * drdy - dndy));
+    JA(blk, 0, 4, 1) = u * b021 + v * b121 + w * 0.0 + (-t[1][0] * irho - TERM1 * (-dldy + 2. * u * drdy));
+    JA(blk, 0, 4, 2) = u * b022 + v * b122 + w * b132 + (-t[1][1] * irho - TERM1 * (2. * v * drdy - dmdy));
+    JA(blk, 0, 4, 3) = u * 0.0 + v * b123 + w * b133 + (-t[1][2] * irho - TERM1 * (2. * w * drdy - dndy));
     JA(blk, 0, 4, 4) = TERM1 * drdy;
   } else {
     JA(blk, 0, 1, 0) = b030;
@@ -462,9 +463,9 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
     JA(blk, 0, 4, 0) = u * b030 + v * b130 + w * b230 +
         (denom * (l * t[2][0] + mv * t[2][1] + n * t[2][2]) -
         TERM1 * (-dedz + (2. * E - 3. * q2) * drdz + 2. * (u * dldz + v * dmdz + w * dndz)));
-    JA(blk, 0, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] / rho - TERM1 * (2. * u * drdz - dldz));
-    JA(blk, 0, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] / rho - TERM1 * (2. * v * drdz - dmdz));
-    JA(blk, 0, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] / rho - TERM1 * (2. * w * drdz - dndz));
+    JA(blk, 0, 4, 1) = u * b031 + v * 0.0 + w * b231 + (-t[2][0] * irho - TERM1 * (2. * u * drdz - dldz));
+    JA(blk, 0, 4, 2) = u * 0.0 + v * b132 + w * b232 + (-t[2][1] * irho - TERM1 * (2. * v * drdz - dmdz));
+    JA(blk, 0, 4, 3) = u * b033 + v * b133 + w * b233 + (-t[2][2] * irho - TERM1 * (2. * w * drdz - dndz));
     JA(blk, 0, 4, 4) = TERM1 * drdz;
   }
   const S reinv = 1.0 / th.creyn;
@@ -477,90 +478,91 @@ CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const S mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const S rho = f.U[0], denom = 1. / (rho * rho);
+  const S irho = 1. / rho;  // one division: the entries below multiply by it
   const S l = f.U[1], mv = f.U[2], n = f.U[3], re = f.U[4];
   const S ll = l * l, mm = mv * mv, nn = n * n, hkocv = f.k / th.Cv, TERM1 = f.k / th.Cv * denom;
-  const S q = (-re + (ll + mm + nn) / rho);
+  const S q = (-re + (ll + mm + nn) * irho);
   if (i == 0) {
     const S d10[3] = {mu_R * l * denom, mu * mv * denom, mu * n * denom};    // JC(0,0,1..3,0)
     JC(blk, 0, 0, 1, 0) = mu_R * l * denom;
-    JC(blk, 0, 0, 1, 1) = (-mu_R / rho);
+    JC(blk, 0, 0, 1, 1) = (-mu_R * irho);
     JC(blk, 0, 0, 2, 0) = mu * mv * denom;
-    JC(blk, 0, 0, 2, 2) = (-mu / rho);
+    JC(blk, 0, 0, 2, 2) = (-mu * irho);
     JC(blk, 0, 0, 3, 0) = mu * n * denom;
-    JC(blk, 0, 0, 3, 3) = (-mu / rho);
-    JC(blk, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) / rho - TERM1 * q;
-    JC(blk, 0, 0, 4, 1) = (l / rho) * (-mu_R / rho) + TERM1 * l;
-    JC(blk, 0, 0, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-    JC(blk, 0, 0, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-    JC(blk, 0, 0, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 0, 3, 3) = (-mu * irho);
+    JC(blk, 0, 0, 4, 0) = (l * d10[0] + mv * d10[1] + n * d10[2]) * irho - TERM1 * q;
+    JC(blk, 0, 0, 4, 1) = (l * irho) * (-mu_R * irho) + TERM1 * l;
+    JC(blk, 0, 0, 4, 2) = (mv * irho) * (-mu * irho) + TERM1 * mv;
+    JC(blk, 0, 0, 4, 3) = (n * irho) * (-mu * irho) + TERM1 * n;
+    JC(blk, 0, 0, 4, 4) = (-hkocv * irho);
     JC(blk, 0, 1, 1, 0) = lambda * mv * denom;
-    JC(blk, 0, 1, 1, 2) = (-lambda / rho);
+    JC(blk, 0, 1, 1, 2) = (-lambda * irho);
     JC(blk, 0, 1, 2, 0) = mu * l * denom;
-    JC(blk, 0, 1, 2, 1) = (-mu / rho);
-    JC(blk, 0, 1, 4, 0) = (l / rho) * (lambda * mv * denom) + (mv / rho) * (mu * l * denom);
-    JC(blk, 0, 1, 4, 1) = (mv / rho) * (-mu / rho);
-    JC(blk, 0, 1, 4, 2) = (l / rho) * (-lambda / rho);
+    JC(blk, 0, 1, 2, 1) = (-mu * irho);
+    JC(blk, 0, 1, 4, 0) = (l * irho) * (lambda * mv * denom) + (mv * irho) * (mu * l * denom);
+    JC(blk, 0, 1, 4, 1) = (mv * irho) * (-mu * irho);
+    JC(blk, 0, 1, 4, 2) = (l * irho) * (-lambda * irho);
     JC(blk, 0, 2, 1, 0) = lambda * n * denom;
-    JC(blk, 0, 2, 1, 3) = (-lambda / rho);
+    JC(blk, 0, 2, 1, 3) = (-lambda * irho);
     JC(blk, 0, 2, 3, 0) = mu * l * denom;
-    JC(blk, 0, 2, 3, 1) = (-mu / rho);
-    JC(blk, 0, 2, 4, 0) = (l / rho) * (lambda * n * denom) + (n / rho) * (mu * l * denom);
-    JC(blk, 0, 2, 4, 1) = (n / rho) * (-mu / rho);
-    JC(blk, 0, 2, 4, 3) = (l / rho) * (-lambda / rho);
+    JC(blk, 0, 2, 3, 1) = (-mu * irho);
+    JC(blk, 0, 2, 4, 0) = (l * irho) * (lambda * n * denom) + (n * irho) * (mu * l * denom);
+    JC(blk, 0, 2, 4, 1) = (n * irho) * (-mu * irho);
+    JC(blk, 0, 2, 4, 3) = (l * irho) * (-lambda * irho);
   } else if (i == 1) {
     const S e10 = mu * l * denom, e20 = mu_R * mv * denom, e30 = mu * n * denom;  // JC(1,1,1..3,0)
     JC(blk, 0, 1, 1, 0) = e10;
-    JC(blk, 0, 1, 1, 1) = (-mu / rho);
+    JC(blk, 0, 1, 1, 1) = (-mu * irho);
     JC(blk, 0, 1, 2, 0) = e20;
-    JC(blk, 0, 1, 2, 2) = (-mu_R / rho);
+    JC(blk, 0, 1, 2, 2) = (-mu_R * irho);
     JC(blk, 0, 1, 3, 0) = e30;
-    JC(blk, 0, 1, 3, 3) = (-mu / rho);
-    JC(blk, 0, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) / rho - TERM1 * q;
-    JC(blk, 0, 1, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-    JC(blk, 0, 1, 4, 2) = (mv / rho) * (-mu_R / rho) + TERM1 * mv;
-    JC(blk, 0, 1, 4, 3) = (n / rho) * (-mu / rho) + TERM1 * n;
-    JC(blk, 0, 1, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 1, 3, 3) = (-mu * irho);
+    JC(blk, 0, 1, 4, 0) = (l * e10 + mv * e20 + n * e30) * irho - TERM1 * q;
+    JC(blk, 0, 1, 4, 1) = (l * irho) * (-mu * irho) + TERM1 * l;
+    JC(blk, 0, 1, 4, 2) = (mv * irho) * (-mu_R * irho) + TERM1 * mv;
+    JC(blk, 0, 1, 4, 3) = (n * irho) * (-mu * irho) + TERM1 * n;
+    JC(blk, 0, 1, 4, 4) = (-hkocv * irho);
     JC(blk, 0, 0, 1, 0) = mu * mv * denom;
-    JC(blk, 0, 0, 1, 2) = (-mu / rho);
+    JC(blk, 0, 0, 1, 2) = (-mu * irho);
     JC(blk, 0, 0, 2, 0) = lambda * l * denom;
-    JC(blk, 0, 0, 2, 1) = (-lambda / rho);
-    JC(blk, 0, 0, 4, 0) = (l / rho) * (mu * mv * denom) + (mv / rho) * (lambda * l * denom);
-    JC(blk, 0, 0, 4, 1) = (mv / rho) * (-lambda / rho);
-    JC(blk, 0, 0, 4, 2) = (l / rho) * (-mu / rho);
+    JC(blk, 0, 0, 2, 1) = (-lambda * irho);
+    JC(blk, 0, 0, 4, 0) = (l * irho) * (mu * mv * denom) + (mv * irho) * (lambda * l * denom);
+    JC(blk, 0, 0, 4, 1) = (mv * irho) * (-lambda * irho);
+    JC(blk, 0, 0, 4, 2) = (l * irho) * (-mu * irho);
     JC(blk, 0, 2, 2, 0) = lambda * n * denom;
-    JC(blk, 0, 2, 2, 3) = (-lambda / rho);
+    JC(blk, 0, 2, 2, 3) = (-lambda * irho);
     JC(blk, 0, 2, 3, 0) = mu * mv * denom;
-    JC(blk, 0, 2, 3, 2) = (-mu / rho);
-    JC(blk, 0, 2, 4, 0) = (mv / rho) * (lambda * n * denom) + (n / rho) * (mu * mv * denom);
-    JC(blk, 0, 2, 4, 2) = (n / rho) * (-mu / rho);
-    JC(blk, 0, 2, 4, 3) = (mv / rho) * (-lambda / rho);
+    JC(blk, 0, 2, 3, 2) = (-mu * irho);
+    JC(blk, 0, 2, 4, 0) = (mv * irho) * (lambda * n * denom) + (n * irho) * (mu * mv * denom);
+    JC(blk, 0, 2, 4, 2) = (n * irho) * (-mu * irho);
+    JC(blk, 0, 2, 4, 3) = (mv * irho) * (-lambda * irho);
   } else {
     const S f10 = mu * l * denom, f20 = mu * mv * denom, f30 = mu_R * n * denom;  // JC(2,2,1..3,0)
     JC(blk, 0, 2, 1, 0) = f10;
-    JC(blk, 0, 2, 1, 1) = (-mu / rho);
+    JC(blk, 0, 2, 1, 1) = (-mu * irho);
     JC(blk, 0, 2, 2, 0) = f20;
-    JC(blk, 0, 2, 2, 2) = (-mu / rho);
+    JC(blk, 0, 2, 2, 2) = (-mu * irho);
     JC(blk, 0, 2, 3, 0) = f30;
-    JC(blk, 0, 2, 3, 3) = (-mu_R / rho);
-    JC(blk, 0, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) / rho - TERM1 * q;
-    JC(blk, 0, 2, 4, 1) = (l / rho) * (-mu / rho) + TERM1 * l;
-    JC(blk, 0, 2, 4, 2) = (mv / rho) * (-mu / rho) + TERM1 * mv;
-    JC(blk, 0, 2, 4, 3) = (n / rho) * (-mu_R / rho) + TERM1 * n;
-    JC(blk, 0, 2, 4, 4) = (-hkocv / rho);
+    JC(blk, 0, 2, 3, 3) = (-mu_R * irho);
+    JC(blk, 0, 2, 4, 0) = (l * f10 + mv * f20 + n * f30) * irho - TERM1 * q;
+    JC(blk, 0, 2, 4, 1) = (l * irho) * (-mu * irho) + TERM1 * l;
+    JC(blk, 0, 2, 4, 2) = (mv * irho) * (-mu * irho) + TERM1 * mv;
+    JC(blk, 0, 2, 4, 3) = (n * irho) * (-mu_R * irho) + TERM1 * n;
+    JC(blk, 0, 2, 4, 4) = (-hkocv * irho);
     JC(blk, 0, 0, 1, 0) = mu * n * denom;
-    JC(blk, 0, 0, 1, 3) = (-mu / rho);
+    JC(blk, 0, 0, 1, 3) = (-mu * irho);
     JC(blk, 0, 0, 3, 0) = lambda * l * denom;
-    JC(blk, 0, 0, 3, 1) = (-lambda / rho);
-    JC(blk, 0, 0, 4, 0) = (l / rho) * (mu * n * denom) + (n / rho) * (lambda * l * denom);
-    JC(blk, 0, 0, 4, 1) = (n / rho) * (-lambda / rho);
-    JC(blk, 0, 0, 4, 3) = (l / rho) * (-mu / rho);
+    JC(blk, 0, 0, 3, 1) = (-lambda * irho);
+    JC(blk, 0, 0, 4, 0) = (l * irho) * (mu * n * denom) + (n * irho) * (lambda * l * denom);
+    JC(blk, 0, 0, 4, 1) = (n * irho) * (-lambda * irho);
+    JC(blk, 0, 0, 4, 3) = (l * irho) * (-mu * irho);
     JC(blk, 0, 1, 2, 0) = mu * n * denom;
-    JC(blk, 0, 1, 2, 3) = (-mu / rho);
+    JC(blk, 0, 1, 2, 3) = (-mu * irho);
     JC(blk, 0, 1, 3, 0) = lambda * mv * denom;
-    JC(blk, 0, 1, 3, 2) = (-lambda / rho);
-    JC(blk, 0, 1, 4, 0) = (mv / rho) * (mu * n * denom) + (n / rho) * (lambda * mv * denom);
-    JC(blk, 0, 1, 4, 2) = (n / rho) * (-lambda / rho);
-    JC(blk, 0, 1, 4, 3) = (mv / rho) * (-mu / rho);
+    JC(blk, 0, 1, 3, 2) = (-lambda * irho);
+    JC(blk, 0, 1, 4, 0) = (mv * irho) * (mu * n * denom) + (n * irho) * (lambda * mv * denom);
+    JC(blk, 0, 1, 4, 2) = (n * irho) * (-lambda * irho);
+    JC(blk, 0, 1, 4, 3) = (mv * irho) * (-mu * irho);
   }
   const S reinv = 1.0 / th.creyn;
   for (int k = 0; k < 75; k++) blk[k] *= reinv;
