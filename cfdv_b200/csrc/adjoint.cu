@@ -10,6 +10,7 @@
 
 #include "context.h"
 #include "adjoint.cuh"
+#include "adjoint_warp.cuh"
 #include "kernels.h"
 
 using namespace cfdv;
@@ -48,6 +49,22 @@ __global__ void __launch_bounds__(64) vjp_rev_kernel(FunctionalArgs a) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= a.n_elements) return;
   element_vjp_rev<NDIM>(a, e, a.out + (size_t)e * KE);
+}
+
+// the collectives of warp_vjp: the warp's lanes
+struct WarpLanes {
+  __device__ __forceinline__ void sync() const { __syncwarp(); }
+  __device__ __forceinline__ double sum(double v, int m) const { return v + __shfl_xor_sync(0xffffffffu, v, m); }
+  __device__ __forceinline__ bool any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
+};
+
+// reverse mode, one lane per Gauss point: d L_e / d U_e, d dt, d Mach (and L_e) of the
+// warp's 4 (hex8) or 8 (quad4) elements
+template <int NDIM>
+__global__ void __launch_bounds__(32) vjp_warp_kernel(FunctionalArgs a) {
+  __shared__ WarpVjpShared<NDIM> sh;
+  WarpLanes L;
+  warp_vjp<NDIM>(a, sh, (int)blockIdx.x * WarpVjp<NDIM>::EPW, (int)threadIdx.x, L);
 }
 
 template <int NDIM>
@@ -163,21 +180,17 @@ int vjp_device(cfdv_ctx* c, double dt, const double* d_w, const double* d_du, do
   if (rc) return rc;
   const size_t E = c->n_elements, Ke = c->Ke;
   FunctionalArgs a = functional_args(c, dt);
-  a.mode = 2;  // forward mode for dt and the Mach number
   a.dU = d_du;
   a.w = d_w;
   a.out = c->d_adj_e;
   a.out_dt = c->d_adj_e + E * Ke;
   a.out_mach = c->d_adj_e + E * (Ke + 1);
   a.out_val = d_val;
-  CK(launch_functional(c, a));
-  {  // reverse mode for the element's unknowns
-    const int grid = (int)((E + 63) / 64);
-    if (c->ndim == 2) vjp_rev_kernel<2><<<grid, 64, 0, c->st>>>(a);
-    else vjp_rev_kernel<3><<<grid, 64, 0, c->st>>>(a);
-    c->launches++;
-    CK(cudaGetLastError());
-  }
+  // reverse mode, one lane per Gauss point: the element's unknowns, dt and the Mach number
+  if (c->ndim == 2) vjp_warp_kernel<2><<<(unsigned)((E + 7) / 8), 32, 0, c->st>>>(a);
+  else vjp_warp_kernel<3><<<(unsigned)((E + 3) / 4), 32, 0, c->st>>>(a);
+  c->launches++;
+  CK(cudaGetLastError());
   CK(launch_compose_rhs(ebe_of(c), a.out, d_g, c->d_pa, c->st));
   c->launches++;
   rc = CFDV_OK;

@@ -515,20 +515,22 @@ CFDV_HD CFDV_INLINE void gp_zero(GpState& g) {
   }
 }
 
-template <int NDIM>
-CFDV_HD CFDV_INLINE void jac_a_adj(const GasParams& th, const GpState& f, const double* W, GpState& g) {
-  if constexpr (NDIM == 2) jac_a_adj_2d(th, f, W, g);
-  else jac_a_adj_3d(th, f, W, g);
+template <int NDIM, class WA>
+CFDV_HD CFDV_INLINE void jac_a_adj(const GasParams& th, const GpState& f, const WA& W, GpState& g, double& gCv) {
+  if constexpr (NDIM == 2) jac_a_adj_2d(th, f, W, g, gCv);
+  else jac_a_adj_3d(th, f, W, g, gCv);
 }
-template <int NDIM>
-CFDV_HD CFDV_INLINE void jac_b_rows_adj(const GasParams& th, const GpState& f, int i, const double* W, GpState& g) {
-  if constexpr (NDIM == 2) jac_b_rows_adj_2d(th, f, i, W, g);
-  else jac_b_rows_adj_3d(th, f, i, W, g);
+template <int NDIM, class WA>
+CFDV_HD CFDV_INLINE void jac_b_rows_adj(const GasParams& th, const GpState& f, int i, const WA& W, GpState& g,
+                                        double& gCv) {
+  if constexpr (NDIM == 2) jac_b_rows_adj_2d(th, f, i, W, g, gCv);
+  else jac_b_rows_adj_3d(th, f, i, W, g, gCv);
 }
-template <int NDIM>
-CFDV_HD CFDV_INLINE void jac_c_rows_adj(const GasParams& th, const GpState& f, int i, const double* W, GpState& g) {
-  if constexpr (NDIM == 2) jac_c_rows_adj_2d(th, f, i, W, g);
-  else jac_c_rows_adj_3d(th, f, i, W, g);
+template <int NDIM, class WA>
+CFDV_HD CFDV_INLINE void jac_c_rows_adj(const GasParams& th, const GpState& f, int i, const WA& W, GpState& g,
+                                        double& gCv) {
+  if constexpr (NDIM == 2) jac_c_rows_adj_2d(th, f, i, W, g, gCv);
+  else jac_c_rows_adj_3d(th, f, i, W, g, gCv);
 }
 
 // Reverse of pass_terms for seed `omega` (the pass weight): adjoints of the Gauss-point
@@ -620,14 +622,15 @@ CFDV_HD void pass_terms_adj(const GasParams& gp, const GpState& f, const NodePri
       for (int c = 0; c < NEQ; c++)
         W[i * 25 + r * 5 + c] = wi[i][r] * abar_b[c] + va1_b[r] * u1[i][c] + Sa_b * wi[i][r] * u0[c] +
                                 (with_psi ? vaS_b[r] * uS[c] : 0.0);
-  jac_a_adj<NDIM>(gp, f, W, g);
+  double gCv = 0.0;  // the Mach number's dependence stays with the forward-mode threads here
+  jac_a_adj<NDIM>(gp, f, W, g, gCv);
   for (int i = 0; i < NDIM; i++) {
     for (int k = 0; k < 25; k++) W[k] = 0.0;
     for (int r = 0; r < NEQ; r++)
       for (int c = 0; c < NEQ; c++)
         W[r * 5 + c] = wi[i][r] * abar_b[c] + vb1_b[r] * u1[i][c] + Sb_b * wi[i][r] * u0[c] +
                        (with_psi ? vbS_b[r] * uS[c] : 0.0);
-    jac_b_rows_adj<NDIM>(gp, f, i, W, g);
+    jac_b_rows_adj<NDIM>(gp, f, i, W, g, gCv);
   }
   {
     double Wc[75];
@@ -636,7 +639,7 @@ CFDV_HD void pass_terms_adj(const GasParams& gp, const GpState& f, const NodePri
       for (int j = 0; j < NDIM; j++)
         for (int r = 0; r < NEQ; r++)
           for (int c = 0; c < NEQ; c++) Wc[j * 25 + r * 5 + c] = Gam_b * wi[i][r] * u1[j][c];
-      jac_c_rows_adj<NDIM>(gp, f, i, Wc, g);
+      jac_c_rows_adj<NDIM>(gp, f, i, Wc, g, gCv);
     }
   }
   // fluxes: FG_b(i, r) = F(node b) + G(tau, k, dT, node b's velocity)

@@ -3,7 +3,8 @@
 Reads the Jacobian functions of fdv_physics.cuh (jac_a_2d/3d, jac_b_rows_2d/3d,
 jac_c_rows_2d/3d), evaluates their straight-line bodies symbolically with sympy for every
 direction i, and emits, for each function, the gradient of sum_entries W_entry * entry with
-respect to the Gauss-point state it reads (E, U, dU, v, mu, k, tau).  The weights W are the
+respect to the Gauss-point state it reads (E, U, dU, v, mu, k, tau) and to the gas constant Cv
+(through which the Mach number enters).  The weights W are the
 adjoint of the entries in the element functional (adjoint.cuh); the generated code is the
 reverse sweep of the same formulas, with common subexpressions shared (sympy cse).
 
@@ -217,18 +218,24 @@ def emit(fname, out_name, ndim, per_row, src):
             total += w * e
         used = [n for _, n in STATE if it.sym[n] in total.free_symbols]
         grads = [sp.diff(total, it.sym[n]) for n in used]
+        names = [gname(n) for n in used]
+        cv = it.gas["Cv"]
+        if cv in total.free_symbols:  # the Mach number enters the Jacobians through Cv
+            grads.append(sp.diff(total, cv))
+            names.append("gCv")
         reps, red = sp.cse(grads, symbols=sp.numbered_symbols("t"), optimizations="basic")
         body = []
         for s_, e in reps:
             body.append(f"    const double {s_} = {ccode(e)};")
-        for n, e in zip(used, red):
-            body.append(f"    {gname(n)} += {ccode(e)};")
+        for n, e in zip(names, red):
+            body.append(f"    {n} += {ccode(e)};")
         cond = "" if i is None else f"  if (i == {i}) {{\n"
         lines.append(cond + "\n".join(body) + ("\n  }" if i is not None else ""))
     sig_i = ", int i" if per_row else ""
-    return (f"// reverse of {fname}: g += d/d(state) of sum_idx W[idx] * entry[idx]\n"
-            f"CFDV_HD inline void {out_name}(const GasParams& th, const GpState& f{sig_i}, const double* W, "
-            f"GpState& g) {{\n" + "\n".join(lines) + "\n}\n")
+    return (f"// reverse of {fname}: g += d/d(state) of sum_idx W[idx] * entry[idx], gCv += d/dCv of it\n"
+            f"template <class WA>\n"
+            f"CFDV_HD CFDV_INLINE void {out_name}(const GasParams& th, const GpState& f{sig_i}, const WA& W, "
+            f"GpState& g, double& gCv) {{\n" + "\n".join(lines) + "\n  (void)gCv;\n}\n")
 
 
 def gname(n):
@@ -275,7 +282,9 @@ def main():
     parts = [
         "// GENERATED by gen_jac_adjoint.py from fdv_physics.cuh -- do not edit.",
         "// Reverse-mode derivatives of the flux Jacobians: for weights W on the entries (the",
-        "// adjoint of the entries in the element functional), g += d/d(state) sum W * entry.",
+        "// adjoint of the entries in the element functional), g += d/d(state) sum W * entry and",
+        "// gCv += d/dCv sum W * entry.  W is any type with operator[](int): an array, or an",
+        "// accessor that forms each weight where the code reads it.",
         "#pragma once",
         '#include "fdv_physics.cuh"',
         "",

@@ -19,16 +19,17 @@ CSRC = os.path.join(ROOT, "cfdv_b200", "csrc")
 @pytest.fixture(scope="module")
 def emu():
     src = os.path.join(ROOT, "tests", "emu", "adj_emu.cpp")
-    deps = [src] + [os.path.join(CSRC, f) for f in ("adjoint.cuh", "dual.cuh", "formation.cuh", "fdv_physics.cuh",
-                                                     "cfdv_types.h", "jac_adjoint.cuh")]
+    deps = [src] + [os.path.join(CSRC, f) for f in ("adjoint.cuh", "adjoint_warp.cuh", "dual.cuh", "formation.cuh",
+                                                     "fdv_physics.cuh", "cfdv_types.h", "jac_adjoint.cuh")]
     if not os.path.exists(EMU) or os.path.getmtime(EMU) < max(os.path.getmtime(f) for f in deps):
-        subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wno-unknown-pragmas", src, "-o", EMU],
-                       check=True)
+        subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-pthread", "-Wno-unknown-pragmas", src, "-o",
+                        EMU], check=True)
     L = C.CDLL(EMU)
     P, D, I = C.c_void_p, C.c_double, C.c_int
     L.emu_functional.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, I, P, P, P, D, D, P, P]
     L.emu_wall_force.argtypes = [I, I, P, P, P, P, D, D, D, D, D, D, I, I, P, P]
     L.emu_vjp_rev.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, P, P, P]
+    L.emu_vjp_warp.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, P, P, P, P, P, P]
     L.emu_set_adaptive.argtypes = [P, P]
     return L
 
@@ -165,6 +166,29 @@ def test_reverse_mode_matches_forward_mode(emu, oracle_lib, name):
                     _p(s.du), _p(s.w), _p(out))
     ref = g[:, : s.Ke]
     assert np.abs(out.reshape(s.E, s.Ke) - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", SMALL_CASES + ["lid8_adap", "ramp4_adap", "cyl4_adap"])
+def test_warp_reverse_sweep_matches_forward_mode(emu, oracle_lib, name):
+    """The warp reverse sweep (one lane per Gauss point, 32 lanes run here as fibers) against the
+    per-seed forward-mode functional: every unknown of every element, d/d dt, d/d Mach and
+    the value L_e."""
+    s = Setup(oracle_lib, name)
+    g, val = s.emu(emu)
+    s.arm(emu)
+    out = np.zeros(s.E * s.Ke)
+    odt, om, ov = np.zeros(s.E), np.zeros(s.E), np.zeros(s.E)
+    emu.emu_vjp_warp(s.case.ndim, s.E, _p(s.U), _p(s.x), _p(s.conn), _p(s.bc), _p(s.mask), *s.gas, float(s.dt), 0,
+                     _p(s.du), _p(s.w), _p(out), _p(odt), _p(om), _p(ov))
+    ref = g[:, : s.Ke]
+    assert np.abs(out.reshape(s.E, s.Ke) - ref).max() <= 1e-13 * np.abs(ref).max()
+    for got, want in ((odt, g[:, s.Ke]), (ov, val)):
+        assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+    # d L_e / d Mach sums terms that cancel: Cv and T both scale with M^-2, so the Cv terms of
+    # the Jacobians, the node temperatures and k(M) nearly balance.  On cyl4 one element's
+    # terms add up to 18.8 in magnitude for a derivative of 3.8e-8, so both evaluations carry
+    # ~1e-16 * 18.8 of rounding; the bound is relative to the largest derivative.
+    assert np.abs(om - g[:, s.Ke + 1]).max() <= 1e-11 * np.abs(g[:, s.Ke + 1]).max()
 
 
 @pytest.mark.parametrize("name", SMALL_CASES)
