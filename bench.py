@@ -319,6 +319,7 @@ def measure_adjoint(args, ws, max_over_ranks):
                      "backward_over_forward": b / f, "forward_matvecs": r["forward_matvecs"],
                      "adjoint_matvecs": r["adjoint_matvecs"], "J": r["J"], "dJ_dmach": r["dJ_dmach"],
                      "dJ_dtwall": r["dJ_dtwall"], "wall_nodes": int(len(r["wall_nodes"])),
+                     "kept_matrix_sets": r["kept_matrix_sets"], "reverse_forms": r["reverse_forms"],
                      "device_memory_peak_gb": peak_bytes / 1e9}
     s.close()
     return out

@@ -35,6 +35,10 @@ void free_all(cfdv_ctx* c) {
   dfree(c->d_hnm_idx); dfree(c->d_hnm); c->n_adaptive = 0;
   dfree(c->d_adj_e); dfree(c->d_adj_v); dfree(c->d_adj_states); dfree(c->d_wall_elems); dfree(c->d_wall_buf);
   c->adj_state_cap = 0;
+  for (auto& p : c->adj_pool64) dfree(p);
+  for (auto& p : c->adj_pool32) dfree(p);
+  c->adj_pool64.clear();
+  c->adj_pool32.clear();
   c->n_wall_elems = 0;
   c->wall_bc_cached = -1 << 30;
   c->pers_cap = 0;

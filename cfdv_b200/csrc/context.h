@@ -73,6 +73,9 @@ struct cfdv_ctx {
   double* d_adj_v = nullptr;       // 4 DOF vectors
   double* d_adj_states = nullptr;  // checkpoints and one segment of states
   size_t adj_state_cap = 0;
+  // element-matrix sets of a segment's recomputed steps, kept for their reverse steps
+  std::vector<double*> adj_pool64;
+  std::vector<float*> adj_pool32;
   int* d_wall_elems = nullptr;     // elements with a face of the wall code
   double* d_wall_buf = nullptr;
   int n_wall_elems = 0, wall_bc_cached = -1 << 30;

@@ -77,7 +77,7 @@ class _AdjResult(C.Structure):
     _fields_ = [("J", C.c_double), ("dJ_dmach", C.c_double), ("dJ_dtwall", C.c_double), ("n_wall_nodes", C.c_int),
                 ("wall_capacity", C.c_int), ("wall_nodes", C.c_void_p), ("dJ_dtnode", C.c_void_p),
                 ("forward_ms", C.c_double), ("backward_ms", C.c_double), ("forward_matvecs", C.c_int),
-                ("adjoint_matvecs", C.c_int)]
+                ("adjoint_matvecs", C.c_int), ("kept_matrix_sets", C.c_int), ("reverse_forms", C.c_int)]
 
 
 _lib = None
@@ -435,11 +435,12 @@ class FDVSolver:
         nw = len(self.wall_nodes(wall_bc))
         ids = np.zeros(max(nw, 1), dtype=np.int32)
         gT = np.zeros(max(nw, 1))
-        r = _AdjResult(0, 0, 0, 0, nw, _p(ids).value, _p(gT).value, 0, 0, 0, 0)
+        r = _AdjResult(0, 0, 0, 0, nw, _p(ids).value, _p(gT).value, 0, 0, 0, 0, 0, 0)
         self._ck(self.L.cfdv_adjoint(self._ctx, C.byref(o), C.byref(r)))
         return {"J": r.J, "dJ_dmach": r.dJ_dmach, "dJ_dtwall": r.dJ_dtwall, "wall_nodes": ids[:nw].copy(),
                 "dJ_dtnode": gT[:nw].copy(), "forward_ms": r.forward_ms, "backward_ms": r.backward_ms,
-                "forward_matvecs": r.forward_matvecs, "adjoint_matvecs": r.adjoint_matvecs}
+                "forward_matvecs": r.forward_matvecs, "adjoint_matvecs": r.adjoint_matvecs,
+                "kept_matrix_sets": r.kept_matrix_sets, "reverse_forms": r.reverse_forms}
 
     def tangent(self, n_steps, cfl, dmach=0.0, dT_wall=None, m=30, restarts=200, rtol=1e-10, precision=PREC_FP64,
                 wall_bc=1):

@@ -230,8 +230,10 @@ int cfdv_profile_read(cfdv_ctx* ctx, cfdv_kernel_stats* out);
 typedef struct {
   int n_steps;          /* N steps from the records of cfdv_load_node_records */
   int checkpoint_every; /* k: the forward run keeps U every k steps; the backward sweep
-                           recomputes each segment's states from its checkpoint and
-                           re-forms the element matrices instead of storing them */
+                           recomputes each segment's states from its checkpoint.  The
+                           element matrices of the recomputed steps stay on the device for
+                           their reverse steps, as many sets as fit beside a reserve of
+                           free memory; the other reverse steps form theirs again */
   double cfl;
   int m, restarts;      /* GMRES(m), at most `restarts` cycles, CORRECT mode, node-block */
   double rtol;          /* Jacobi; forward, tangent and adjoint solves to this rtol */
@@ -251,6 +253,8 @@ typedef struct {
   double backward_ms;   /* device time of the backward sweep, recomputation included */
   int forward_matvecs;  /* EBE products of all forward solves (recomputation included) */
   int adjoint_matvecs;  /* EBE products of the transposed solves */
+  int kept_matrix_sets; /* element-matrix sets of recomputed steps kept per segment */
+  int reverse_forms;    /* formations run by reverse steps (the others reused kept sets) */
 } cfdv_adjoint_result;
 
 /* Vector-Jacobian product of the element residuals at the current U and the dt of the

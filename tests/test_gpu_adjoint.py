@@ -224,6 +224,12 @@ def test_checkpoint_spacing_and_mixed_precision(gpu, adj):
         rN = s.adjoint(N_STEPS, CFL, checkpoint_every=N_STEPS, m=M_GMRES, rtol=RTOL)
         s.load_node_records()
         rm = s.adjoint(N_STEPS, CFL, checkpoint_every=3, m=M_GMRES, rtol=1e-10, precision=gpu.PREC_MIXED)
+    # the recomputed steps' element matrices stay on the device for their reverse steps: only
+    # the last step of each segment forms again (k = 1 recomputes nothing)
+    assert (adj["kept_matrix_sets"], adj["reverse_forms"]) == (1, 3)
+    assert (r1["kept_matrix_sets"], r1["reverse_forms"]) == (0, N_STEPS)
+    assert (rN["kept_matrix_sets"], rN["reverse_forms"]) == (N_STEPS - 1, 1)
+    assert (rm["kept_matrix_sets"], rm["reverse_forms"]) == (2, 2)
     for r in (r1, rN):
         assert r["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-13)
         assert np.abs(r["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-13 * np.abs(adj["dJ_dtnode"]).max()
