@@ -42,29 +42,36 @@ __global__ void __launch_bounds__(128) functional_kernel(FunctionalArgs a) {
   }
 }
 
-// reverse mode: the gradient over the element's Ke unknowns, one thread per element
-template <int NDIM>
-__global__ void __launch_bounds__(64) vjp_rev_kernel(FunctionalArgs a) {
-  constexpr int KE = FormTraits<NDIM>::KE;
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= a.n_elements) return;
-  element_vjp_rev<NDIM>(a, e, a.out + (size_t)e * KE);
-}
-
-// the collectives of warp_vjp: the warp's lanes
+// the collectives of warp_vjp: the warp's lanes; task_sync is the block's barrier
 struct WarpLanes {
   __device__ __forceinline__ void sync() const { __syncwarp(); }
   __device__ __forceinline__ double sum(double v, int m) const { return v + __shfl_xor_sync(0xffffffffu, v, m); }
   __device__ __forceinline__ bool any(bool p) const { return __any_sync(0xffffffffu, p) != 0; }
+  __device__ __forceinline__ void task_sync() const { __syncthreads(); }
 };
 
-// reverse mode, one lane per Gauss point: d L_e / d U_e, d dt, d Mach (and L_e) of the
-// warp's 4 (hex8) or 8 (quad4) elements
+// reverse mode, one lane per Gauss point: d L_e / d U_e, d dt, d Mach (and L_e); each of the
+// block's kVjpWarps warps takes 4 (hex8) or 8 (quad4) elements, its shared state in dynamic
+// shared memory
+constexpr int kVjpWarps = 5;
 template <int NDIM>
-__global__ void __launch_bounds__(32) vjp_warp_kernel(FunctionalArgs a) {
-  __shared__ WarpVjpShared<NDIM> sh;
+__global__ void __launch_bounds__(32 * kVjpWarps, 1) vjp_warp_kernel(FunctionalArgs a) {
+  extern __shared__ __align__(16) unsigned char vjp_smem[];
+  const int w = (int)threadIdx.x / 32;
+  WarpVjpShared<NDIM>& sh = reinterpret_cast<WarpVjpShared<NDIM>*>(vjp_smem)[w];
   WarpLanes L;
-  warp_vjp<NDIM>(a, sh, (int)blockIdx.x * WarpVjp<NDIM>::EPW, (int)threadIdx.x, L);
+  warp_vjp<NDIM>(a, sh, ((int)blockIdx.x * kVjpWarps + w) * WarpVjp<NDIM>::EPW, (int)threadIdx.x % 32, L);
+}
+
+template <int NDIM>
+cudaError_t launch_vjp_warp(const FunctionalArgs& a, cudaStream_t st) {
+  const size_t smem = sizeof(WarpVjpShared<NDIM>) * kVjpWarps;
+  static const cudaError_t attr =
+      cudaFuncSetAttribute(vjp_warp_kernel<NDIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (attr != cudaSuccess) return attr;
+  const int per_block = WarpVjp<NDIM>::EPW * kVjpWarps;
+  vjp_warp_kernel<NDIM><<<(unsigned)((a.n_elements + per_block - 1) / per_block), 32 * kVjpWarps, smem, st>>>(a);
+  return cudaGetLastError();
 }
 
 template <int NDIM>
@@ -187,10 +194,8 @@ int vjp_device(cfdv_ctx* c, double dt, const double* d_w, const double* d_du, do
   a.out_mach = c->d_adj_e + E * (Ke + 1);
   a.out_val = d_val;
   // reverse mode, one lane per Gauss point: the element's unknowns, dt and the Mach number
-  if (c->ndim == 2) vjp_warp_kernel<2><<<(unsigned)((E + 7) / 8), 32, 0, c->st>>>(a);
-  else vjp_warp_kernel<3><<<(unsigned)((E + 3) / 4), 32, 0, c->st>>>(a);
+  CK(c->ndim == 2 ? launch_vjp_warp<2>(a, c->st) : launch_vjp_warp<3>(a, c->st));
   c->launches++;
-  CK(cudaGetLastError());
   CK(launch_compose_rhs(ebe_of(c), a.out, d_g, c->d_pa, c->st));
   c->launches++;
   rc = CFDV_OK;
@@ -527,6 +532,43 @@ int cfdv_tangent(cfdv_ctx* c, const cfdv_adjoint_opts* o, double dmach, const do
   return CFDV_OK;
 }
 
+// Grow the context's pool of element-matrix sets (FP64, and FP32 for the mixed form) toward
+// `want`, while a set fits beside a reserve of free device memory (2 GiB or 5% of the
+// device, the larger).  Returns the number of usable sets.
+static int grow_matrix_pool(cfdv_ctx* c, int want, bool mixed) {
+  const size_t mat = (size_t)c->n_elements * c->Ke * c->Ke;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+  const size_t reserve = std::max((size_t)2 << 30, total_b / 20);
+  int usable = 0;
+  for (int i = 0; i < want; i++) {
+    const bool have64 = i < (int)c->adj_pool64.size();
+    const bool have32 = !mixed || (i < (int)c->adj_pool32.size() && c->adj_pool32[i]);
+    const size_t need = (have64 ? 0 : sizeof(double) * mat) + (have32 ? 0 : sizeof(float) * mat);
+    if (need) {
+      if (free_b < need + reserve) break;
+      if (!have64) {
+        double* p = nullptr;
+        if (cudaMalloc(&p, sizeof(double) * mat) != cudaSuccess) break;
+        c->adj_pool64.push_back(p);
+      }
+      if (!have32) {
+        float* p = nullptr;
+        if (cudaMalloc(&p, sizeof(float) * mat) != cudaSuccess) break;
+        if (i < (int)c->adj_pool32.size()) c->adj_pool32[i] = p;
+        else {
+          c->adj_pool32.resize(i + 1, nullptr);
+          c->adj_pool32[i] = p;
+        }
+      }
+      free_b -= need;
+    }
+    usable++;
+  }
+  cudaGetLastError();  // a refused allocation only ends the growth
+  return usable;
+}
+
 int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* res) {
   if (!c || !res) return CFDV_ERR_ARG;
   int rc = check_opts(c, o);
@@ -552,6 +594,27 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
   double* gF = c->d_adj_v + 2 * n;
   double* du = c->d_adj_v + 3 * n;
   const cfdv_gmres_opts so = solve_opts(o);
+  // The last P recomputed steps of a segment form into kept sets of the pool; their reverse
+  // steps solve with those matrices instead of forming again.  The context's own buffers
+  // are restored on every exit.
+  const bool mixed = o->precision == CFDV_PREC_MIXED;
+  if (mixed && !c->d_R32 && (rc = dalloc(c, &c->d_R32, (size_t)c->n_elements * c->Ke * c->Ke))) return rc;
+  const int P = grow_matrix_pool(c, std::min(k, N) - 1, mixed);
+  struct OwnMatrices {
+    cfdv_ctx* c;
+    double* r64;
+    float* r32;
+    void use(int slot, bool mixed) {
+      c->d_R64 = c->adj_pool64[slot];
+      c->d_R32 = mixed ? c->adj_pool32[slot] : r32;
+    }
+    void restore() {
+      c->d_R64 = r64;
+      c->d_R32 = r32;
+    }
+    ~OwnMatrices() { restore(); }
+  } own{c, c->d_R64, c->d_R32};
+  int reverse_forms = 0;
   cudaEvent_t ev[3];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   struct Guard {
@@ -592,9 +655,13 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
     // recompute U_{n0} .. U_{n1-1} from the checkpoint; U_{n1} is the next checkpoint or U_N
     CK(cudaMemcpyAsync(c->d_U, ckpt + (size_t)s * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
     CK(cudaMemcpyAsync(seg, c->d_U, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+    const int first_kept = n1 - 1 - P;  // recomputed steps from here on keep their matrices
     for (int step = n0; step < n1 - 1; step++) {
       rep.n_matvec = 0;
-      if ((rc = cfdv_step(c, o->cfl, &so, &rep, nullptr))) return rc;
+      if (step >= first_kept) own.use(step - first_kept, mixed);
+      rc = cfdv_step(c, o->cfl, &so, &rep, nullptr);
+      own.restore();
+      if (rc) return rc;
       fwd_mv += rep.n_matvec;
       CK(cudaMemcpyAsync(seg + (size_t)(step - n0 + 1) * n, c->d_U, sizeof(double) * n, cudaMemcpyDeviceToDevice,
                          c->st));
@@ -608,10 +675,21 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
       c->launches++;
       double dt;
       if ((rc = cfdv_cfl(c, o->cfl, &dt))) return rc;
-      if ((rc = cfdv_form(c, dt, o->precision))) return rc;
+      if (step < n1 - 1 && step >= first_kept) {  // the recompute formed this step's matrices
+        own.use(step - first_kept, mixed);
+        c->formed = true;
+        c->have32 = mixed;
+        c->dt_formed = dt;
+      } else {
+        if ((rc = cfdv_form(c, dt, o->precision))) return rc;
+        reverse_forms++;
+      }
       // mu = A^-T lambda
       rep.n_matvec = 0;
-      if ((rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, 1))) return rc;
+      rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, 1);
+      if (c->d_R64 != own.r64) c->formed = false;  // the context's own buffers hold older matrices
+      own.restore();
+      if (rc) return rc;
       adj_mv += rep.n_matvec;
       double g_dt, g_m;
       if ((rc = vjp_device(c, dt, c->d_du, du, g, &g_dt, &g_m, nullptr))) return rc;
@@ -667,6 +745,8 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
   res->backward_ms = ms2;
   res->forward_matvecs = fwd_mv;
   res->adjoint_matvecs = adj_mv;
+  res->kept_matrix_sets = P;
+  res->reverse_forms = reverse_forms;
   // leave the context at the end of the forward run
   CK(cudaMemcpyAsync(c->d_U, UN, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));

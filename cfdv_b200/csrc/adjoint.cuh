@@ -442,42 +442,17 @@ CFDV_HD Dual wall_force_element(const ForceArgs& a, int e, int k) {
 }
 
 
-// ==== reverse mode: the element's gradient over its Ke unknowns in one pass ==========
-// The forward-mode functional above costs one evaluation per seed.  element_vjp_rev
+// ==== pieces of the reverse sweep (adjoint_warp.cuh) ====================================
+// The forward-mode functional above costs one evaluation per seed.  The reverse sweep
 // evaluates L_e once in FP64 and sweeps back through it: the flux Jacobians by the
 // generated reverse code (jac_adjoint.cuh), the rest by hand, and four small pieces (the
 // SUPG test function, the boundary-state edits, the FDV parameters, node unpack) by dual
-// numbers over their few inputs.  Derivatives with respect to dt and the Mach number stay
-// with the forward-mode threads.
+// numbers over their few inputs.
 
 // adjoint of a node's primitives (fields of NodePrim)
 struct PrimAdj {
   double U[5], v[3], rho, E, T, p;
 };
-
-// nodal adjoints from the adjoint g of the Gauss-point state sums
-template <int NDIM, int NN>
-CFDV_HD CFDV_INLINE void gp_state_sums_adj(const double* Phi, const double (*dPhi)[3], const GpState& g,
-                                           PrimAdj* const* nb) {
-  constexpr int NEQ = NDIM + 2;
-  for (int N = 0; N < NN; N++) {
-    PrimAdj& b = *nb[N];
-    b.E += Phi[N] * g.E;
-    double t = Phi[N] * g.T;
-    for (int c = 0; c < NDIM; c++) t += dPhi[N][c] * g.dT[c];
-    b.T += t;
-    for (int q = 0; q < NEQ; q++) {
-      double u = Phi[N] * g.U[q];
-      for (int c = 0; c < NDIM; c++) u += dPhi[N][c] * g.dU[q][c];
-      b.U[q] += u;
-    }
-    for (int i = 0; i < NDIM; i++) {
-      double v = Phi[N] * g.v[i];
-      for (int c = 0; c < NDIM; c++) v += dPhi[N][c] * g.dV[i][c];
-      b.v[i] += v;
-    }
-  }
-}
 
 // tau = mu (dV + dV^T) - 2/3 mu div v I: adjoint into mu and dV
 template <int NDIM>
@@ -531,155 +506,6 @@ CFDV_HD CFDV_INLINE void jac_c_rows_adj(const GasParams& th, const GpState& f, i
                                         double& gCv) {
   if constexpr (NDIM == 2) jac_c_rows_adj_2d(th, f, i, W, g, gCv);
   else jac_c_rows_adj_3d(th, f, i, W, g, gCv);
-}
-
-// Reverse of pass_terms for seed `omega` (the pass weight): adjoints of the Gauss-point
-// state into g, of the pass nodes' primitives into nb, of s1..s4 into sbar, and of the
-// 2D test function into psibar (per pass node).  Same notation as pass_terms.
-template <int NDIM, int NN>
-CFDV_HD void pass_terms_adj(const GasParams& gp, const GpState& f, const NodePrim* const* nd, const double* Phi,
-                            const double (*dPhi)[3], double dt, double dtsq_2, const double* s,
-                            const double (*wi)[5], const double* u0, const double (*u1)[5], const double* uS,
-                            const double* mPsi, bool with_psi, bool withF, double sgn, double omega, GpState& g,
-                            PrimAdj* const* nb, double* sbar, double* mPsibar) {
-  constexpr int NEQ = NDIM + 2;
-  // primal of the contraction vectors
-  double abar[5] = {0, 0, 0, 0, 0}, va1[5] = {0, 0, 0, 0, 0}, vb1[5] = {0, 0, 0, 0, 0};
-  double vaS[5] = {0, 0, 0, 0, 0}, vbS[5] = {0, 0, 0, 0, 0};
-  double Sa = 0.0, Sb = 0.0, Gam = 0.0;
-  double J[NDIM * 25];
-  jac_a<NDIM>(gp, f, J);
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < NEQ; r++)
-      for (int c = 0; c < NEQ; c++) {
-        const double av = J[i * 25 + r * 5 + c];
-        abar[c] += wi[i][r] * av;
-        va1[r] += av * u1[i][c];
-        Sa += wi[i][r] * (av * u0[c]);
-        if (with_psi) vaS[r] += av * uS[c];
-      }
-  for (int i = 0; i < NDIM; i++) {
-    jac_b_rows<NDIM>(gp, f, i, J);
-    for (int r = 0; r < NEQ; r++)
-      for (int c = 0; c < NEQ; c++) {
-        const double bv = J[r * 5 + c];
-        abar[c] += wi[i][r] * bv;
-        vb1[r] += bv * u1[i][c];
-        Sb += wi[i][r] * (bv * u0[c]);
-        if (with_psi) vbS[r] += bv * uS[c];
-      }
-  }
-  {
-    double C[75];
-    for (int i = 0; i < NDIM; i++) {
-      jac_c_rows<NDIM>(gp, f, i, C);
-      for (int j = 0; j < NDIM; j++)
-        for (int r = 0; r < NEQ; r++) {
-          double t = 0.0;
-          for (int c = 0; c < NEQ; c++) t += C[j * 25 + r * 5 + c] * u1[j][c];
-          Gam += wi[i][r] * t;
-        }
-    }
-  }
-  double divF[5] = {0, 0, 0, 0, 0};
-  for (int b = 0; b < NN; b++)
-    for (int i = 0; i < NDIM; i++)
-      for (int r = 0; r < NEQ; r++) divF[r] += dPhi[b][i] * node_flux_entry<NDIM>(f, *nd[b], gp.creyn, withF, i, r);
-  // scalar adjoints
-  const double Fterm_b = omega * sgn * dt;
-  double abar_b[5], beta_b[5], divF_b[5], va1_b[5], vb1_b[5], vaS_b[5], vbS_b[5];
-  double beta[5];
-  for (int r = 0; r < NEQ; r++) beta[r] = s[1] * va1[r] + s[3] * vb1[r];
-  double ad = 0.0, ab = 0.0, pa = 0.0, pb = 0.0, ava = 0.0, avb = 0.0;
-  for (int r = 0; r < NEQ; r++) {
-    abar_b[r] = -omega * sgn * dtsq_2 * (divF[r] + beta[r]);
-    beta_b[r] = -omega * sgn * dtsq_2 * abar[r];
-    divF_b[r] = -omega * sgn * dtsq_2 * abar[r];
-    va1_b[r] = beta_b[r] * s[1];
-    vb1_b[r] = beta_b[r] * s[3];
-    vaS_b[r] = with_psi ? -omega * dt * mPsi[r] * s[0] : 0.0;
-    vbS_b[r] = with_psi ? -omega * dt * mPsi[r] * s[2] : 0.0;
-    if (with_psi) mPsibar[r] += -omega * dt * (s[0] * vaS[r] + s[2] * vbS[r]);
-    ad += abar[r] * divF[r];
-    ab += abar[r] * beta[r];
-    ava += abar[r] * va1[r];
-    avb += abar[r] * vb1[r];
-    pa += mPsi[r] * vaS[r];
-    pb += mPsi[r] * vbS[r];
-  }
-  (void)ad;
-  (void)ab;
-  const double Sa_b = omega * sgn * dt * s[0], Sb_b = omega * sgn * dt * s[2], Gam_b = omega * sgn * dt * s[2];
-  sbar[0] += omega * (sgn * dt * Sa - (with_psi ? dt * pa : 0.0));
-  sbar[1] += -omega * sgn * dtsq_2 * ava;
-  sbar[2] += omega * (sgn * dt * Sb + sgn * dt * Gam - (with_psi ? dt * pb : 0.0));
-  sbar[3] += -omega * sgn * dtsq_2 * avb;
-  // entry weights and the Jacobian reverse
-  double W[NDIM * 25];
-  for (int k = 0; k < NDIM * 25; k++) W[k] = 0.0;
-  for (int i = 0; i < NDIM; i++)
-    for (int r = 0; r < NEQ; r++)
-      for (int c = 0; c < NEQ; c++)
-        W[i * 25 + r * 5 + c] = wi[i][r] * abar_b[c] + va1_b[r] * u1[i][c] + Sa_b * wi[i][r] * u0[c] +
-                                (with_psi ? vaS_b[r] * uS[c] : 0.0);
-  double gCv = 0.0;  // the Mach number's dependence stays with the forward-mode threads here
-  jac_a_adj<NDIM>(gp, f, W, g, gCv);
-  for (int i = 0; i < NDIM; i++) {
-    for (int k = 0; k < 25; k++) W[k] = 0.0;
-    for (int r = 0; r < NEQ; r++)
-      for (int c = 0; c < NEQ; c++)
-        W[r * 5 + c] = wi[i][r] * abar_b[c] + vb1_b[r] * u1[i][c] + Sb_b * wi[i][r] * u0[c] +
-                       (with_psi ? vbS_b[r] * uS[c] : 0.0);
-    jac_b_rows_adj<NDIM>(gp, f, i, W, g, gCv);
-  }
-  {
-    double Wc[75];
-    for (int i = 0; i < NDIM; i++) {
-      for (int k = 0; k < 75; k++) Wc[k] = 0.0;
-      for (int j = 0; j < NDIM; j++)
-        for (int r = 0; r < NEQ; r++)
-          for (int c = 0; c < NEQ; c++) Wc[j * 25 + r * 5 + c] = Gam_b * wi[i][r] * u1[j][c];
-      jac_c_rows_adj<NDIM>(gp, f, i, Wc, g, gCv);
-    }
-  }
-  // fluxes: FG_b(i, r) = F(node b) + G(tau, k, dT, node b's velocity)
-  const double reinv = 1.0 / gp.creyn;
-  for (int b = 0; b < NN; b++) {
-    const NodePrim& n = *nd[b];
-    PrimAdj& na = *nb[b];
-    for (int i = 0; i < NDIM; i++)
-      for (int r = 0; r < NEQ; r++) {
-        const double fb = Fterm_b * Phi[b] * wi[i][r] + divF_b[r] * dPhi[b][i];
-        if (r >= 1 && r <= NDIM) {
-          g.tau[i][r - 1] -= fb * reinv;
-        } else if (r == NDIM + 1) {
-          for (int j = 0; j < NDIM; j++) {
-            g.tau[i][j] -= fb * n.v[j] * reinv;
-            na.v[j] -= fb * f.tau[i][j] * reinv;
-          }
-          g.k -= fb * f.dT[i] * reinv;
-          g.dT[i] -= fb * f.k * reinv;
-        }
-        if (withF) {  // the node's convective flux, by dual numbers over its U and p
-          for (int q = 0; q <= NEQ; q++) {
-            NodePrimT<Dual> nd2;
-            for (int c = 0; c < NEQ; c++) nd2.U[c] = Dual(n.U[c], q == c ? 1.0 : 0.0);
-            for (int c = 0; c < 3; c++) { nd2.x[c] = n.x[c]; nd2.v[c] = n.v[c]; }
-            nd2.rho = n.rho; nd2.E = n.E; nd2.T = n.T;
-            nd2.p = Dual(n.p, q == NEQ ? 1.0 : 0.0);
-            GpStateT<Dual> f0;
-            f0.k = 0.0; f0.mu = 0.0;
-            for (int a2 = 0; a2 < 3; a2++) {
-              f0.dT[a2] = 0.0;
-              for (int b2 = 0; b2 < 3; b2++) f0.tau[a2][b2] = 0.0;
-            }
-            const double dF = node_flux_entry<NDIM>(f0, nd2, gp.creyn, true, i, r).d;
-            if (q < NEQ) na.U[q] += fb * dF;
-            else na.p += fb * dF;
-          }
-        }
-      }
-  }
 }
 
 // the 2D test function's adjoint into the state (dual numbers over v, dV, rho, mu)
@@ -752,206 +578,6 @@ CFDV_HD void face_edit_adj(int code, const GpState& fraw, const double* x0, cons
     else if ((o -= NDIM * NDIM) < NDIM) graw.dT[o] += d;
     else if ((o -= NDIM) < NEQ * NDIM) graw.dU[o / NDIM][o % NDIM] += d;
     else graw.mu += d;
-  }
-}
-
-// d L_e / d U_e for the element's Ke unknowns (weights and dU as in the VJP mode of
-// element_functional; dt and the Mach number held fixed)
-template <int NDIM>
-CFDV_HD CFDV_INLINE void element_vjp_rev(const FunctionalArgs& a, int e, double* gout) {
-  using T = FormTraits<NDIM>;
-  constexpr int NNOD = T::NNOD, NEQ = T::NEQ, KE = T::KE, NFACE = T::NFACE, NBN = T::NBN;
-  const double* Hn = (a.hnm_idx && a.hnm_idx[e] >= 0) ? a.hnm + (size_t)a.hnm_idx[e] * NNOD * NNOD : nullptr;
-  const GasParams& gp = a.gas;
-  const uint64_t mask = a.rowmask ? a.rowmask[e] : 0ull;
-  const double dt = a.dt, dtsq_2 = dt * dt / 2.0;
-  NodePrim nd[NNOD];
-  PrimAdj na[NNOD];
-  double wgt[KE], du[KE], Mn[NNOD], Ren[NNOD], s[4], sbar[4] = {0, 0, 0, 0};
-  double Uloc[NNOD][NEQ];
-  for (int N = 0; N < NNOD; N++) {
-    const int n = a.conn[(size_t)e * NNOD + N];
-    for (int c = 0; c < NEQ; c++) {
-      const size_t gi = (size_t)n * NEQ + c;
-      const int row = N * NEQ + c;
-      Uloc[N][c] = a.U[gi];
-      wgt[row] = ((mask >> row) & 1ull) ? 0.0 : a.w[gi];
-      du[row] = a.dU[gi];
-    }
-    node_unpack<NDIM>(gp, Uloc[N], a.x + (size_t)n * NDIM, nd[N]);
-    node_mach_re<NDIM>(gp, nd[N], &Mn[N], &Ren[N]);
-    PrimAdj& z = na[N];
-    z.rho = z.E = z.T = z.p = 0.0;
-    for (int c = 0; c < 5; c++) z.U[c] = 0.0;
-    for (int c = 0; c < 3; c++) z.v[c] = 0.0;
-  }
-  fdv_pair<NNOD>(Mn, 0, s);
-  fdv_pair<NNOD>(Ren, 1, s);
-  const bool withF = (NDIM == 2) || a.physical_3d_flux;
-  const NodePrim* all[NNOD];
-  PrimAdj* alla[NNOD];
-  for (int N = 0; N < NNOD; N++) {
-    all[N] = &nd[N];
-    alla[N] = &na[N];
-  }
-  // ---- domain Gauss points ----
-  for (int q = 0; q < T::Q; q++) {
-    double z[3], Phi[NNOD], dPxi[NNOD][3], dPhi[NNOD][3], jac[3][3];
-    double w = 1.0;
-    for (int d = 0; d < NDIM; d++) {
-      const int bit = (q >> (NDIM - 1 - d)) & 1;
-      z[d] = a.gz[bit];
-      w *= a.gw[bit];
-    }
-    shape_fn<NDIM>(z, Phi, dPxi);
-    if (Hn) hnm_shape<NDIM>(Hn, Phi, dPxi);
-    const double J = phys_deriv<NDIM>(dPxi, nd, dPhi, jac);
-    const double wJ = w * J;
-    GpState f;
-    gp_state_sums<NDIM, NNOD>(all, Phi, dPhi, f);
-    f.mu = gas_mu(gp, f.T);
-    f.k = gas_k(gp, f.mu);
-    viscous_stress<NDIM>(f);
-    double Psi[NNOD];
-    const double* x4[4] = {nd[0].x, nd[1].x, nd[2].x, nd[3 % NNOD].x};
-    double pj[3][3];  // the upwind term's Jacobian: of the untransformed shape functions
-    if (NDIM == 2 && Hn) plain_jac_2d(z, x4, pj);
-    const double (*sj)[3] = (NDIM == 2 && Hn) ? pj : jac;
-    if constexpr (NDIM == 2) psi_2d<double>(sj, x4, f, dPhi, Psi);
-    double wi[3][5], u0[5], u1[3][5], uS[5], m0[5], mPsi[5];
-    for (int r = 0; r < NEQ; r++) {
-      double a0 = 0.0, b0 = 0.0, bs = 0.0, ps = 0.0, a1[3] = {0, 0, 0}, b1[3] = {0, 0, 0};
-      for (int N = 0; N < NNOD; N++) {
-        const double wv = wgt[N * NEQ + r], dv = du[N * NEQ + r];
-        double sd = 0.0;
-        for (int j = 0; j < NDIM; j++) sd += dPhi[N][j];
-        a0 += Phi[N] * wv;
-        b0 += Phi[N] * dv;
-        bs += sd * dv;
-        if (NDIM == 2) ps += Psi[N] * wv;
-        for (int i = 0; i < NDIM; i++) {
-          a1[i] += dPhi[N][i] * wv;
-          b1[i] += dPhi[N][i] * dv;
-        }
-      }
-      m0[r] = a0;
-      u0[r] = b0;
-      uS[r] = bs;
-      mPsi[r] = ps;
-      for (int i = 0; i < NDIM; i++) {
-        wi[i][r] = a1[i];
-        u1[i][r] = b1[i];
-      }
-    }
-    (void)m0;
-    GpState g;
-    gp_zero(g);
-    double mPsibar[5] = {0, 0, 0, 0, 0};
-    pass_terms_adj<NDIM, NNOD>(gp, f, all, Phi, dPhi, dt, dtsq_2, s, wi, u0, u1, uS, mPsi, NDIM == 2, withF, 1.0,
-                               wJ, g, alla, sbar, mPsibar);
-    if constexpr (NDIM == 2) {
-      double psibar[4];
-      for (int N = 0; N < 4; N++) {
-        double t = 0.0;
-        for (int r = 0; r < NEQ; r++) t += mPsibar[r] * wgt[N * NEQ + r];
-        psibar[N] = t;
-      }
-      psi_2d_adj(sj, x4, f, dPhi, psibar, g);
-    }
-    stress_adj<NDIM>(f, g);
-    gas_adj(gp, f, g);
-    gp_state_sums_adj<NDIM, NNOD>(Phi, dPhi, g, alla);
-  }
-  // ---- boundary faces ----
-  for (int fc = 0; fc < NFACE; fc++) {
-    const int code = a.bc[(size_t)e * NFACE + fc];
-    if (code == 0 || code >= 100) continue;
-    const NodePrim* fn[NBN];
-    PrimAdj* fa[NBN];
-    const double* xf[NBN];
-    int ln[NBN];
-    for (int i = 0; i < NBN; i++) {
-      ln[i] = face_node(NDIM, fc, i);
-      fn[i] = &nd[ln[i]];
-      fa[i] = &na[ln[i]];
-      xf[i] = nd[ln[i]].x;
-    }
-    double xl[4][3];
-    if (NDIM == 3 && Hn) {  // adaptive element: face geometry from Hnm x
-      const double* xe[8];
-      for (int M = 0; M < 8; M++) xe[M] = nd[M % NNOD].x;
-      hnm_face_nodes_3d(Hn, xe, fc, xl);
-      for (int i = 0; i < NBN; i++) xf[i] = xl[i % 4];
-    }
-    for (int qf = 0; qf < T::QF; qf++) {
-      double phib[NBN], dpidx[NBN][3], en[3];
-      face_point_geom<NDIM>(a.gz, a.gw, xf, qf, phib, dpidx, en);
-      if constexpr (NDIM == 3)
-        if (Hn) hnm_face_phi_3d(Hn, fc, phib);
-      GpState fr;
-      gp_state_sums<NDIM, NBN>(fn, phib, dpidx, fr);
-      fr.mu = gas_mu(gp, fr.T);
-      fr.k = gas_k(gp, fr.mu);
-      for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) fr.tau[i][j] = 0.0;
-      GpState f = fr;
-      if constexpr (NDIM == 2) edit_face_state_2d(code, f, xf[0], xf[1], en);
-      else edit_face_state_3d(code, f, en, gp.adiabatic);
-      double wi[3][5], u0[5], u1[3][5];
-      for (int r = 0; r < NEQ; r++) {
-        double m0 = 0.0, b0 = 0.0, b1[3] = {0, 0, 0};
-        for (int m = 0; m < NBN; m++) {
-          const double wv = wgt[ln[m] * NEQ + r], dv = du[ln[m] * NEQ + r];
-          m0 += phib[m] * wv;
-          b0 += phib[m] * dv;
-          for (int j = 0; j < NDIM; j++) b1[j] += dpidx[m][j] * dv;
-        }
-        u0[r] = b0;
-        for (int i = 0; i < NDIM; i++) {
-          wi[i][r] = en[i] * m0;
-          u1[i][r] = b1[i];
-        }
-      }
-      GpState g, graw;
-      gp_zero(g);
-      gp_zero(graw);
-      double unused[5] = {0, 0, 0, 0, 0};
-      pass_terms_adj<NDIM, NBN>(gp, f, fn, phib, dpidx, dt, dtsq_2, s, wi, u0, u1, nullptr, unused, false, withF,
-                                -1.0, 1.0, g, fa, sbar, unused);
-      face_edit_adj<NDIM>(code, fr, xf[0], xf[1], en, gp.adiabatic, g, graw);
-      gas_adj(gp, fr, graw);
-      gp_state_sums_adj<NDIM, NBN>(phib, dpidx, graw, fa);
-    }
-  }
-  // ---- FDV parameters: s1..s4 from the nodes' Mach and Reynolds numbers ----
-  double Mb[NNOD], Rb[NNOD];
-  for (int N = 0; N < NNOD; N++) {
-    Dual vm[NNOD], vr[NNOD], sd[4];
-    for (int k = 0; k < NNOD; k++) {
-      vm[k] = Dual(Mn[k], k == N ? 1.0 : 0.0);
-      vr[k] = Dual(Ren[k], k == N ? 1.0 : 0.0);
-    }
-    fdv_pair<NNOD>(vm, 0, sd);
-    fdv_pair<NNOD>(vr, 1, sd);
-    Mb[N] = sbar[0] * sd[0].d + sbar[1] * sd[1].d;
-    Rb[N] = sbar[2] * sd[2].d + sbar[3] * sd[3].d;
-  }
-  // ---- node primitives -> U (node unpack and the node Mach / Reynolds numbers) ----
-  const GasT<Dual> gd = dual_gas(gp, 0.0);
-  for (int N = 0; N < NNOD; N++) {
-    const PrimAdj& z = na[N];
-    for (int c = 0; c < NEQ; c++) {
-      Dual u[NEQ];
-      for (int k = 0; k < NEQ; k++) u[k] = Dual(Uloc[N][k], k == c ? 1.0 : 0.0);
-      NodePrimT<Dual> p;
-      node_unpack<NDIM>(gd, u, nd[N].x, p);
-      Dual M, R;
-      node_mach_re<NDIM>(gd, p, &M, &R);
-      double d = z.rho * p.rho.d + z.E * p.E.d + z.T * p.T.d + z.p * p.p.d + Mb[N] * M.d + Rb[N] * R.d;
-      for (int k = 0; k < NEQ; k++) d += z.U[k] * p.U[k].d;
-      for (int k = 0; k < NDIM; k++) d += z.v[k] * p.v[k].d;
-      gout[N * NEQ + c] = d;
-    }
   }
 }
 

@@ -1,9 +1,9 @@
 // Reverse sweep of the element functional, one lane per Gauss point (the kernel is in
 // adjoint.cu; tests/emu/adj_emu.cpp runs the same code on the CPU with one fiber per lane).
 //
-// element_vjp_rev (adjoint.cuh) sweeps a whole element in one thread and keeps the element's
-// tape in that thread's local memory.  Here a warp takes EPW = 32 / Q elements (4 hex8, 8
-// quad4) and each lane one Gauss point of one element:
+// A sweep of a whole element by one thread would keep the element's tape in that thread's
+// local memory.  Here a warp takes EPW = 32 / Q elements (4 hex8, 8 quad4) and each lane one
+// Gauss point of one element:
 //   lane = j * Q + q: element slot j of the warp, Gauss point q (and node q: Q == NNOD).
 // Every lane runs the same code on its own point, so the warp never diverges on the
 // Jacobian kind or direction.  Per pass (the domain points, then each boundary face's points)
@@ -26,7 +26,9 @@
 //
 // Lanes is the warp's collectives, called by every lane at the same points: sync() (a barrier
 // with shared-memory ordering), sum(v, m) = v + the value of lane (lane ^ m) for m < Q (the
-// element's lanes), and any(p) (p of some lane of the warp).
+// element's lanes), any(p) (p of some lane of the warp), and task_sync() at each Jacobian
+// task of the domain pass, where every warp of the block meets (a barrier of the block, or
+// nothing), so that the block's warps run one task's code at a time.
 #pragma once
 #include "adjoint.cuh"
 
@@ -272,11 +274,12 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
   double abar[5] = {0, 0, 0, 0, 0}, va1[5] = {0, 0, 0, 0, 0}, vb1[5] = {0, 0, 0, 0, 0};
   double vaS[5] = {0, 0, 0, 0, 0}, vbS[5] = {0, 0, 0, 0, 0}, divF[5] = {0, 0, 0, 0, 0};
   double Sa = 0.0, Sb = 0.0, Gam = 0.0, Fterm = 0.0;
-  if (on) {
-    // one Jacobian at a time (the task is the same in every lane): only one Jacobian's
-    // temporaries are live at once
+  // one Jacobian at a time, the same task in every lane (and, through task_sync in the
+  // domain pass, in every warp of the block): one Jacobian's code and temporaries at once
 #pragma unroll 1
-    for (int t = 0; t < 1 + 2 * NDIM; t++) {
+  for (int t = 0; t < 1 + 2 * NDIM; t++) {
+    if (!FACE) L.task_sync();
+    if (on) {
       switch (t) {
         case 0: fwd_a<NDIM, PSI>(gp, P, abar, va1, Sa, vaS); break;
         case 1: fwd_b_rows<NDIM, 0, PSI>(gp, P, abar, vb1, Sb, vbS); break;
@@ -291,6 +294,8 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
           break;
       }
     }
+  }
+  if (on) {
     for (int b = 0; b < NN; b++) {
       const NodePrim& nb = El.nd[pass_elem_node<NDIM, FACE>(fc, b)];
 #pragma unroll
@@ -365,10 +370,13 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
         g.dT[i] -= fb * P.f.k * reinv;
       }
     }
-    // the Jacobians
-    double gCv = 0.0;
+  }
+  // the Jacobians
+  double gCv = 0.0;
 #pragma unroll 1
-    for (int t = 0; t < 1 + 2 * NDIM; t++) {
+  for (int t = 0; t < 1 + 2 * NDIM; t++) {
+    if (!FACE) L.task_sync();
+    if (on) {
       switch (t) {
         case 0: jac_a_adj<NDIM>(gp, P.f, WeightsAB<NDIM, PSI, 0>{P, abar_b, va1_b, vaS_b, Sa_b}, g, gCv); break;
         case 1:
@@ -388,6 +396,8 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
           break;
       }
     }
+  }
+  if (on) {
     acc.dmach += gCv * (-2.0 * gp.Cv / gp.cmach);  // d Cv / d M = -2 Cv / M
     // stress, gas law, test function; or the boundary edits
     if constexpr (!FACE) {
@@ -477,7 +487,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
 
 // The elements e0 .. e0 + EPW - 1 (those below n_elements): d L_e / d U_e into a.out, and
 // d L_e / d dt, d L_e / d Mach, L_e into a.out_dt, a.out_mach, a.out_val when set.  Every
-// lane of the warp calls it; the functional is that of element_functional.
+// lane of the warp calls it; the functional is that of element_functional (adjoint.cuh).
 template <int NDIM, class Lanes>
 CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& sh, int e0, int lane, Lanes& L) {
   using V = WarpVjp<NDIM>;

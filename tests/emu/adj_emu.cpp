@@ -72,29 +72,6 @@ extern "C" void emu_wall_force(int ndim, int n_elements, const double* U, const 
     }
 }
 
-// reverse-mode gradient rows: out[e*Ke + k] = d L_e / d U_e[k]
-extern "C" void emu_vjp_rev(int ndim, int n_elements, const double* U, const double* x, const int* conn,
-                            const int* bc, const uint64_t* rowmask, double gamma, double M, double Re, double Pr,
-                            double Tinf, double Tw, int adiabatic, double dt, int physical_3d_flux, const double* dU,
-                            const double* w, double* out) {
-  FunctionalArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.gas = make_gas(gamma, M, Re, Pr, Tinf, Tw, adiabatic);
-  a.dt = dt;
-  gauss_legendre(2, a.gz, a.gw);
-  a.n_elements = n_elements;
-  a.physical_3d_flux = physical_3d_flux;
-  a.mode = 0;
-  a.U = U; a.x = x; a.conn = conn; a.bc = bc; a.rowmask = rowmask;
-  a.hnm_idx = g_hnm_idx; a.hnm = g_hnm;
-  a.dU = dU; a.w = w;
-  const int Ke = (ndim == 2) ? 16 : 40;
-  for (int e = 0; e < n_elements; e++) {
-    if (ndim == 2) element_vjp_rev<2>(a, e, out + (size_t)e * Ke);
-    else element_vjp_rev<3>(a, e, out + (size_t)e * Ke);
-  }
-}
-
 // ---- the warp reverse sweep (one lane per Gauss point), one fiber per lane --------------------------------
 // The 32 lanes run as fibers (ucontext) on the calling thread.  At a collective each lane
 // switches to the next one; lane 31 switches back to lane 0, by which time every lane has
@@ -128,6 +105,7 @@ struct EmuLanes {
     w->next(lane);
     return v + o;
   }
+  void task_sync() {}  // one warp: nothing to meet
   bool any(bool p) {
     w->xch[lane] = p ? 1.0 : 0.0;
     w->next(lane);
