@@ -44,18 +44,25 @@ struct WarpVjp {
   static_assert(Q == NNOD, "lane q owns Gauss point q and node q");
 };
 
+// the upwind test function of a 2D domain point (nothing in 3D)
+template <int NDIM>
+struct WarpVjpSupg {
+  double uS[5], mPsi[5], Psi[4];
+  double sj[3][3];  // the upwind term's Jacobian
+};
+template <>
+struct WarpVjpSupg<3> {};
+
 // one lane's Gauss point
 template <int NDIM>
-struct WarpVjpPointData {
+struct WarpVjpPointData : WarpVjpSupg<NDIM> {
   static constexpr int NNOD = FormTraits<NDIM>::NNOD;
-  static constexpr int S2 = (NDIM == 2) ? 5 : 1, N2 = (NDIM == 2) ? NNOD : 1, J2 = (NDIM == 2) ? 3 : 1;
   GpState f;  // state at the point (edited on a face)
   double Phi[NNOD], dPhi[NNOD][3];
-  double wi[NDIM][5], u0[5], u1[NDIM][5], m0[5];  // row weights and interpolated dU
-  double en[3];                                   // face: weighted normal
-  double omega;                                   // w J (domain) or 1 (face)
-  double uS[S2], mPsi[S2], Psi[N2];               // SUPG (2D domain)
-  double sj[J2][3];                               // the upwind term's Jacobian (2D)
+  double wi[NDIM][5], u0[5], u1[NDIM][5];  // row weights and interpolated dU
+  double mterm;                            // sum_r m0(r) u0(r): the mass term of L_e
+  double en[3];                            // face: weighted normal
+  double omega;                            // w J (domain) or 1 (face)
 };
 // padded to an odd number of doubles, so that the 32 lanes reading one field of their own
 // slots hit distinct banks
@@ -68,8 +75,10 @@ template <int NDIM>
 struct WarpVjpElem {
   using T = FormTraits<NDIM>;
   NodePrim nd[T::NNOD];
+  PrimAdj na[T::NNOD];  // node adjoints: lane q alone writes na[q]
   double wgt[T::KE], du[T::KE];
   double Mn[T::NNOD], Ren[T::NNOD];
+  double s[4];  // s1..s4
 };
 
 template <int NDIM>
@@ -99,7 +108,7 @@ CFDV_HD CFDV_INLINE void fwd_b_rows(const GasParams& gp, const WarpVjpPoint<NDIM
       abar[c] += P.wi[I][r] * bv;
       vb1[r] += bv * P.u1[I][c];
       Sb += P.wi[I][r] * (bv * P.u0[c]);
-      if (PSI) vbS[r] += bv * P.uS[c];
+      if constexpr (PSI) vbS[r] += bv * P.uS[c];
     }
 }
 
@@ -137,7 +146,7 @@ CFDV_HD CFDV_INLINE void fwd_a(const GasParams& gp, const WarpVjpPoint<NDIM>& P,
         abar[c] += P.wi[i][r] * av;
         va1[r] += av * P.u1[i][c];
         Sa += P.wi[i][r] * (av * P.u0[c]);
-        if (PSI) vaS[r] += av * P.uS[c];
+        if constexpr (PSI) vaS[r] += av * P.uS[c];
       }
 }
 
@@ -154,7 +163,7 @@ struct WeightsAB {
   CFDV_HD CFDV_INLINE double operator[](int idx) const {
     const int i = I0 + idx / 25, r = (idx / 5) % 5, c = idx % 5;
     double w = P.wi[i][r] * xbar_b[c] + v1_b[r] * P.u1[i][c] + S_b * P.wi[i][r] * P.u0[c];
-    if (PSI) w += vS_b[r] * P.uS[c];
+    if constexpr (PSI) w += vS_b[r] * P.uS[c];
     return w;
   }
 };
@@ -253,21 +262,53 @@ CFDV_HD CFDV_INLINE void warp_state_sum(const WarpVjpElem<NDIM>& El, int fc, War
   *dst = acc;
 }
 
+// sums over the pass nodes of the point's shape functions, weighted by the node velocity:
+// SP = sum_b Phi_b, SD_i = sum_b dPhi_b,i, PV_j = sum_b Phi_b v_b,j, DV_ij = sum_b dPhi_b,i v_b,j
+template <int NDIM>
+CFDV_HD CFDV_INLINE void pass_node_sums(const WarpVjpElem<NDIM>& El, const WarpVjpPoint<NDIM>& P, bool face, int fc,
+                                        double& SP, double* SD, double* PV, double (*DV)[NDIM]) {
+  const int NN = face ? FormTraits<NDIM>::NBN : FormTraits<NDIM>::NNOD;
+  SP = 0.0;
+#pragma unroll
+  for (int i = 0; i < NDIM; i++) {
+    SD[i] = PV[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) DV[i][j] = 0.0;
+  }
+  for (int b = 0; b < NN; b++) {
+    const NodePrim& nb = El.nd[face ? face_node(NDIM, fc, b) : b];
+    const double ph = P.Phi[b];
+    SP += ph;
+#pragma unroll
+    for (int j = 0; j < NDIM; j++) PV[j] += ph * nb.v[j];
+#pragma unroll
+    for (int i = 0; i < NDIM; i++) {
+      const double d = P.dPhi[b][i];
+      SD[i] += d;
+#pragma unroll
+      for (int j = 0; j < NDIM; j++) DV[i][j] += d * nb.v[j];
+    }
+  }
+}
+
 // ---- one pass: the domain points, or the points of boundary face fc ----------------------
 // On entry the lane's point (P; on a face also the state before the edits, fr) is formed
 // when `on` (the lane has a point in this pass); `pass` tells whether the lane's element
 // takes part (it then owns node q in the scatter).  The pass's node adjoints are added into
-// na, the adjoint of the lane's node q.
-template <int NDIM, bool FACE, class Lanes>
+// na, the adjoint of the lane's node q.  Domain and face passes run the same code (one copy
+// of the Jacobians' reverse in the kernel); a 2D face point has uS = mPsi = 0, which drops
+// the upwind terms.
+template <int NDIM, class Lanes>
 CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpElem<NDIM>& El, const WarpVjpPoint<NDIM>& P,
-                                       const GpState& fr, const double* s, bool on, bool pass, int q, int fc,
-                                       int code, Lanes& L, WarpVjpAcc& acc, PrimAdj& na) {
+                                       const GpState& fr, const double* s, bool face, bool on, bool pass, int q,
+                                       int fc, int code, Lanes& L, WarpVjpAcc& acc, PrimAdj& na) {
   using V = WarpVjp<NDIM>;
-  constexpr int NEQ = V::NEQ, NN = FACE ? V::NBN : V::NNOD;
-  constexpr bool PSI = (NDIM == 2) && !FACE;
+  constexpr int NEQ = V::NEQ;
+  constexpr bool PSI = NDIM == 2;
+  const int NN = face ? V::NBN : V::NNOD;
   const GasParams& gp = a.gas;
   const bool withF = (NDIM == 2) || a.physical_3d_flux;
-  const double dt = a.dt, dtsq_2 = dt * dt / 2.0, sgn = FACE ? -1.0 : 1.0;
+  const double dt = a.dt, dtsq_2 = dt * dt / 2.0, sgn = face ? -1.0 : 1.0;
   const double reinv = 1.0 / gp.creyn;
 
   // 1. forward: the Jacobians contracted with the row weights, the flux sums
@@ -278,7 +319,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
   // domain pass, in every warp of the block): one Jacobian's code and temporaries at once
 #pragma unroll 1
   for (int t = 0; t < 1 + 2 * NDIM; t++) {
-    if (!FACE) L.task_sync();
+    if (!face) L.task_sync();
     if (on) {
       switch (t) {
         case 0: fwd_a<NDIM, PSI>(gp, P, abar, va1, Sa, vaS); break;
@@ -296,16 +337,40 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
     }
   }
   if (on) {
-    for (int b = 0; b < NN; b++) {
-      const NodePrim& nb = El.nd[pass_elem_node<NDIM, FACE>(fc, b)];
+    // the viscous flux G(i, r) is the same at every pass node for r = 1..ndim and linear in the
+    // node velocity for the energy row, so its sums over the nodes need only
+    // SP = sum_b Phi_b, SD_i = sum_b dPhi_b,i, PV_j = sum_b Phi_b v_b,j, DV_ij = sum_b dPhi_b,i v_b,j
+    double SP, SD[NDIM], PV[NDIM], DV[NDIM][NDIM];
+    pass_node_sums<NDIM>(El, P, face, fc, SP, SD, PV, DV);
 #pragma unroll
-      for (int i = 0; i < NDIM; i++)
+    for (int i = 0; i < NDIM; i++) {
 #pragma unroll
-        for (int r = 0; r < NEQ; r++) {
-          const double fg = node_flux_entry<NDIM>(P.f, nb, gp.creyn, withF, i, r);
-          Fterm += (P.Phi[b] * P.wi[i][r]) * fg;
-          divF[r] += P.dPhi[b][i] * fg;
-        }
+      for (int r = 1; r <= NDIM; r++) {
+        const double G = -P.f.tau[i][r - 1] * reinv;
+        Fterm += (SP * P.wi[i][r]) * G;
+        divF[r] += SD[i] * G;
+      }
+      double tp = 0.0, td = 0.0;
+#pragma unroll
+      for (int j = 0; j < NDIM; j++) {
+        tp -= P.f.tau[i][j] * PV[j];
+        td -= P.f.tau[i][j] * DV[i][j];
+      }
+      Fterm += P.wi[i][NDIM + 1] * ((tp - P.f.k * P.f.dT[i] * SP) * reinv);
+      divF[NDIM + 1] += (td - P.f.k * P.f.dT[i] * SD[i]) * reinv;
+    }
+    if (withF) {  // the nodes' convective fluxes
+      for (int b = 0; b < NN; b++) {
+        const NodePrim& nb = El.nd[face ? face_node(NDIM, fc, b) : b];
+#pragma unroll
+        for (int i = 0; i < NDIM; i++)
+#pragma unroll
+          for (int r = 0; r < NEQ; r++) {
+            const double F = node_conv_flux_entry<NDIM>(nb, i, r);
+            Fterm += (P.Phi[b] * P.wi[i][r]) * F;
+            divF[r] += P.dPhi[b][i] * F;
+          }
+      }
     }
   }
   // 2. scalar adjoints
@@ -321,7 +386,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
     divF_b[r] = -om * sgn * dtsq_2 * abar[r];  // also the adjoint of beta
     va1_b[r] = divF_b[r] * s[1];
     vb1_b[r] = divF_b[r] * s[3];
-    if (PSI) {
+    if constexpr (PSI) {
       const double mp = on ? P.mPsi[r] : 0.0;
       vaS_b[r] = -om * dt * mp * s[0];
       vbS_b[r] = -om * dt * mp * s[2];
@@ -342,9 +407,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
     acc.sbar[2] += om * (sgn * dt * Sb + sgn * dt * Gam - (PSI ? dt * pb : 0.0));
     acc.sbar[3] += -om * sgn * dtsq_2 * avb;
     acc.ddt += om * (sgn * (Fterm - dt * ad) + sgn * (s[0] * Sa + s[2] * Sb) + sgn * s[2] * Gam - sgn * dt * ab - pterm);
-    double mterm = 0.0;
-    if (!FACE)
-      for (int r = 0; r < NEQ; r++) mterm += P.m0[r] * P.u0[r];
+    const double mterm = face ? 0.0 : P.mterm;
     acc.val += om * (sgn * (dt * Fterm - dtsq_2 * ad) - mterm + sgn * dt * (s[0] * Sa + s[2] * Sb) -
                      sgn * (-(dt * s[2]) * Gam + dtsq_2 * ab) - dt * pterm);
   }
@@ -353,29 +416,26 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
   GpState g;
   gp_zero(g);
   if (on) {
-    // flux sums: the Gauss-point part (the node part is scattered below)
-    for (int b = 0; b < NN; b++) {
-      const NodePrim& nb = El.nd[pass_elem_node<NDIM, FACE>(fc, b)];
+    // flux sums: the Gauss-point part (the node part is scattered below), over the same sums
+    double SP, SD[NDIM], PV[NDIM], DV[NDIM][NDIM];
+    pass_node_sums<NDIM>(El, P, face, fc, SP, SD, PV, DV);
 #pragma unroll
-      for (int i = 0; i < NDIM; i++) {
+    for (int i = 0; i < NDIM; i++) {
 #pragma unroll
-        for (int r = 1; r <= NDIM; r++) {
-          const double fb = Fterm_b * P.Phi[b] * P.wi[i][r] + divF_b[r] * P.dPhi[b][i];
-          g.tau[i][r - 1] -= fb * reinv;
-        }
-        const double fb = Fterm_b * P.Phi[b] * P.wi[i][NDIM + 1] + divF_b[NDIM + 1] * P.dPhi[b][i];
+      for (int r = 1; r <= NDIM; r++) g.tau[i][r - 1] -= (Fterm_b * P.wi[i][r] * SP + divF_b[r] * SD[i]) * reinv;
+      const double aw = Fterm_b * P.wi[i][NDIM + 1], ad_ = divF_b[NDIM + 1];
 #pragma unroll
-        for (int j = 0; j < NDIM; j++) g.tau[i][j] -= fb * nb.v[j] * reinv;
-        g.k -= fb * P.f.dT[i] * reinv;
-        g.dT[i] -= fb * P.f.k * reinv;
-      }
+      for (int j = 0; j < NDIM; j++) g.tau[i][j] -= (aw * PV[j] + ad_ * DV[i][j]) * reinv;
+      const double fbs = aw * SP + ad_ * SD[i];
+      g.k -= fbs * P.f.dT[i] * reinv;
+      g.dT[i] -= fbs * P.f.k * reinv;
     }
   }
   // the Jacobians
   double gCv = 0.0;
 #pragma unroll 1
   for (int t = 0; t < 1 + 2 * NDIM; t++) {
-    if (!FACE) L.task_sync();
+    if (!face) L.task_sync();
     if (on) {
       switch (t) {
         case 0: jac_a_adj<NDIM>(gp, P.f, WeightsAB<NDIM, PSI, 0>{P, abar_b, va1_b, vaS_b, Sa_b}, g, gCv); break;
@@ -400,7 +460,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
   if (on) {
     acc.dmach += gCv * (-2.0 * gp.Cv / gp.cmach);  // d Cv / d M = -2 Cv / M
     // stress, gas law, test function; or the boundary edits
-    if constexpr (!FACE) {
+    if (!face) {
       if constexpr (NDIM == 2) {
         double psibar[4];
         for (int N = 0; N < 4; N++) {
@@ -426,7 +486,7 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
   }
   // 4. scatter to the pass nodes: state sums and the node part of the flux sums
   for (int b = 0; b < NN; b++) {
-    const int node = pass_elem_node<NDIM, FACE>(fc, b);
+    const int node = face ? face_node(NDIM, fc, b) : b;
     double cE = 0.0, cT = 0.0, cU[5] = {0, 0, 0, 0, 0}, cv[3] = {0, 0, 0}, cp = 0.0;
     if (on) {
       const double Phi = P.Phi[b];
@@ -502,6 +562,10 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
     const int n = a.conn[(size_t)e * NNOD + q];
     node_unpack<NDIM>(gp, a.U + (size_t)n * NEQ, a.x + (size_t)n * NDIM, El.nd[q]);
     node_mach_re<NDIM>(gp, El.nd[q], &El.Mn[q], &El.Ren[q]);
+    PrimAdj& z = El.na[q];
+    z.rho = z.E = z.T = z.p = 0.0;
+    for (int c = 0; c < 5; c++) z.U[c] = 0.0;
+    for (int c = 0; c < 3; c++) z.v[c] = 0.0;
     const uint64_t mask = a.rowmask ? a.rowmask[e] : 0ull;
     for (int t = q; t < KE; t += Q) {
       const size_t gi = (size_t)a.conn[(size_t)e * NNOD + t / NEQ] * NEQ + t % NEQ;
@@ -512,10 +576,8 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
   L.sync();
   const int hi = (valid && a.hnm_idx) ? a.hnm_idx[e] : -1;
   const double* Hn = (hi >= 0) ? a.hnm + (size_t)hi * NNOD * NNOD : nullptr;
-  double s[4] = {0, 0, 0, 0};
+  if (valid && q < 2) fdv_pair<NNOD>(q ? El.Ren : El.Mn, q, El.s);  // s1, s2 | s3, s4
   if (valid) {
-    fdv_pair<NNOD>(El.Mn, 0, s);
-    fdv_pair<NNOD>(El.Ren, 1, s);
     // ---- domain point q: geometry, state, row weights, stress (2D: the test function) ----
     double z[3], dPxi[NNOD][3], jac[3][3];
     double w = 1.0;
@@ -529,6 +591,7 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
     const double J = phys_deriv<NDIM>(dPxi, El.nd, P.dPhi, jac);
     P.omega = w * J;
     for (int v = 0; v < V::NSUM; v++) warp_state_sum<NDIM, false>(El, 0, P, v);
+    double mterm = 0.0;
     for (int r = 0; r < NEQ; r++) {
       double a0 = 0.0, b0 = 0.0, bs = 0.0, a1[3] = {0, 0, 0}, b1[3] = {0, 0, 0};
       for (int N = 0; N < NNOD; N++) {
@@ -545,7 +608,7 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
           b1[i] += P.dPhi[N][i] * dv;
         }
       }
-      P.m0[r] = a0;
+      mterm += a0 * b0;
       P.u0[r] = b0;
       if constexpr (NDIM == 2) P.uS[r] = bs;
 #pragma unroll
@@ -554,6 +617,7 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
         P.u1[i][r] = b1[i];
       }
     }
+    P.mterm = mterm;
     P.f.mu = gas_mu(gp, P.f.T);
     P.f.k = gas_k(gp, P.f.mu);
     viscous_stress<NDIM>(P.f);
@@ -576,19 +640,19 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
   WarpVjpAcc acc;
   for (int i = 0; i < 4; i++) acc.sbar[i] = 0.0;
   acc.ddt = acc.dmach = acc.val = 0.0;
-  PrimAdj na;  // adjoint of node q's primitives
-  na.rho = na.E = na.T = na.p = 0.0;
-  for (int c = 0; c < 5; c++) na.U[c] = 0.0;
-  for (int c = 0; c < 3; c++) na.v[c] = 0.0;
-  warp_vjp_pass<NDIM, false>(a, El, P, P.f, s, valid, valid, q, 0, 0, L, acc, na);
-  // ---- boundary faces with 0 != bc < 100 (FDVGalerkin.h:455-533) ----
-  for (int fc = 0; fc < V::NFACE; fc++) {
-    const int code = valid ? a.bc[(size_t)e * V::NFACE + fc] : 0;
-    const bool face = code != 0 && code < 100;
-    if (!L.any(face)) continue;
-    const bool on = face && q < QF;
-    GpState& fr = sh.pt[lane + (q < QF ? QF : 0)].f;  // the slot of an idle point of the element
-    if (on) {
+  PrimAdj& na = El.na[q];  // adjoint of node q's primitives
+  const double* s = El.s;
+  L.sync();  // s1..s4 of every element
+  // ---- the passes: the domain (pass -1), then each boundary face with 0 != bc < 100
+  //      (FDVGalerkin.h:455-533); one call site, so the kernel holds one copy of the pass ----
+  for (int fc = -1; fc < V::NFACE; fc++) {
+    const bool face = fc >= 0;
+    const int code = (face && valid) ? a.bc[(size_t)e * V::NFACE + fc] : 0;
+    const bool pass = face ? (code != 0 && code < 100) : valid;
+    if (face && !L.any(pass)) continue;
+    const bool on = pass && (!face || q < QF);
+    GpState& fr = sh.pt[lane + (q < QF ? QF : 0)].f;  // face: the slot of an idle point of the element
+    if (face && on) {
       const double* xf[NBN];
       for (int i = 0; i < NBN; i++) xf[i] = El.nd[face_node(NDIM, fc, i)].x;
       double xl[4][3];
@@ -599,8 +663,11 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
         for (int i = 0; i < NBN; i++) xf[i] = xl[i % 4];
       }
       face_point_geom<NDIM>(a.gz, a.gw, xf, q, P.Phi, P.dPhi, P.en);
-      if constexpr (NDIM == 3)
+      if constexpr (NDIM == 3) {
         if (Hn) hnm_face_phi_3d(Hn, fc, P.Phi);
+      } else {
+        for (int r = 0; r < 5; r++) P.uS[r] = P.mPsi[r] = 0.0;  // no upwind term on a face
+      }
       P.omega = 1.0;
       for (int v = 0; v < V::NSUM; v++) warp_state_sum<NDIM, true>(El, fc, P, v);
       for (int r = 0; r < NEQ; r++) {
@@ -631,7 +698,7 @@ CFDV_HD CFDV_INLINE void warp_vjp(const FunctionalArgs& a, WarpVjpShared<NDIM>& 
       else
         edit_face_state_3d(code, P.f, P.en, gp.adiabatic);
     }
-    warp_vjp_pass<NDIM, true>(a, El, P, fr, s, on, face, q, fc, code, L, acc, na);
+    warp_vjp_pass<NDIM>(a, El, P, face ? fr : P.f, s, face, on, pass, q, face ? fc : 0, code, L, acc, na);
   }
   // ---- FDV parameters: s1..s4 from the nodes' Mach and Reynolds numbers ----
 #pragma unroll

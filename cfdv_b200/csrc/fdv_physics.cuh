@@ -584,6 +584,33 @@ CFDV_HD CFDV_INLINE void jac_c_rows(const GasT<S>& th, const GpStateT<S>& f, int
   else jac_c_rows_3d(th, f, i, m);
 }
 
+// Convective flux of one node, entry (i, r): F(i,r) from the node's U and p alone.
+template <int NDIM, class S>
+CFDV_HD CFDV_INLINE S node_conv_flux_entry(const NodePrimT<S>& n, int i, int r) {
+  S F = 0.0;
+  if (NDIM == 2) {
+    const S rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
+    const S li = (i == 0) ? l : m;
+    if (r == 0) F = li;
+    else if (r == 1) F = (i == 0) ? p + l * l / rho : (l * m) / rho;
+    else if (r == 2) F = (i == 0) ? (l * m) / rho : p + m * m / rho;
+    else F = (p + e) * (li / rho);
+  } else {
+    const S rho = n.U[0], p = n.p;
+    const S vi = n.U[1 + i] / n.U[0];
+    if (r == 0) {
+      F = rho * vi;
+    } else if (r <= 3) {
+      const S vj = n.U[r] / n.U[0];
+      F = rho * vi * vj + (i == r - 1 ? p : 0.0);
+    } else {
+      const S E = n.U[4] / n.U[0];
+      F = (rho * E + p) * vi;
+    }
+  }
+  return F;
+}
+
 // Convective + viscous flux of one node, entry (i, r): F(i,r) + G(i,r).  F is the node's own
 // flux; G uses the Gauss-point stress, dT and k with the node velocity.  with_F = 0 drops F
 // (the 3D reference evaluates the empty base-class flux).  r may be a run-time index:
@@ -601,29 +628,7 @@ CFDV_HD CFDV_INLINE S node_flux_entry(const GpStateT<S>& f, const NodePrimT<S>& 
     for (int j = 1; j < NDIM; j++) s = s - f.tau[i][j] * n.v[j];
     G = (s - f.k * f.dT[i]) * reinv;
   }
-  S F = 0.0;
-  if (with_F) {
-    if (NDIM == 2) {
-      const S rho = n.U[0], l = n.U[1], m = n.U[2], e = n.U[3], p = n.p;
-      const S li = (i == 0) ? l : m;
-      if (r == 0) F = li;
-      else if (r == 1) F = (i == 0) ? p + l * l / rho : (l * m) / rho;
-      else if (r == 2) F = (i == 0) ? (l * m) / rho : p + m * m / rho;
-      else F = (p + e) * (li / rho);
-    } else {
-      const S rho = n.U[0], p = n.p;
-      const S vi = n.U[1 + i] / n.U[0];
-      if (r == 0) {
-        F = rho * vi;
-      } else if (r <= 3) {
-        const S vj = n.U[r] / n.U[0];
-        F = rho * vi * vj + (i == r - 1 ? p : 0.0);
-      } else {
-        const S E = n.U[4] / n.U[0];
-        F = (rho * E + p) * vi;
-      }
-    }
-  }
+  const S F = with_F ? node_conv_flux_entry<NDIM>(n, i, r) : S(0.0);
   return F + G;
 }
 
