@@ -684,10 +684,10 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
         if ((rc = cfdv_form(c, dt, o->precision))) return rc;
         reverse_forms++;
       }
-      // mu = A^-T lambda
+      // mu = A^-T lambda; no later step reads these matrices, so their blocks stay transposed
       rep.n_matvec = 0;
-      rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, 1);
-      if (c->d_R64 != own.r64) c->formed = false;  // the context's own buffers hold older matrices
+      rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, cfdv::ctxi::kTransposeKeep);
+      c->formed = false;  // the context's own buffers hold transposed or older matrices
       own.restore();
       if (rc) return rc;
       adj_mv += rep.n_matvec;

@@ -572,7 +572,7 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   }
   if (o->precond) {
     if ((rc = fuse_b ? build_block_jacobi(c, c->d_rhs, c->d_b) : build_block_jacobi(c))) {
-      if (transpose) launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st);
+      if (transpose == 1) launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st);
       return rc;
     }
     a.Dinv = c->d_Dinv;
@@ -609,7 +609,7 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
     c->ev_solve.push_back(ev);
   }
   c->launches++;
-  if (transpose) {
+  if (transpose == 1) {  // restore the blocks (kTransposeKeep leaves them transposed)
     CK(launch_transpose_blocks(c->Ke, c->d_R64, r32, c->n_elements, c->st));
     c->launches += r32 ? 2 : 1;
   }

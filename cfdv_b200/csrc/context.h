@@ -129,7 +129,10 @@ inline void dfree(T*& p) {
 // internal steps of the solver (cfdv_abi.cu)
 // Restarted GMRES(m) in CORRECT mode as one persistent launch; the right-hand side is the
 // assembled element rhs (rhs_vec == nullptr) or the device vector rhs_vec; transpose = 1
-// solves A^T x = rhs.  The solution is left in c->d_du.
+// solves A^T x = rhs and restores the element blocks afterwards, kTransposeKeep solves
+// A^T x = rhs and leaves them transposed (the caller re-forms before the next use).  The
+// solution is left in c->d_du.
+constexpr int kTransposeKeep = 2;
 int solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
                  int transpose);
 
