@@ -25,6 +25,9 @@ extern "C" void emu_set_adaptive(const int* hnm_idx, const double* hnm) {
   g_hnm_idx = hnm_idx;
   g_hnm = hnm;
 }
+// elements emu_functional evaluates (mask[e] != 0), or null for all; the others get zeros
+static const unsigned char* g_elem_mask = nullptr;
+extern "C" void emu_set_element_mask(const unsigned char* mask) { g_elem_mask = mask; }
 
 extern "C" void emu_functional(int ndim, int n_elements, const double* U, const double* x, const int* conn,
                                const int* bc, const uint64_t* rowmask, double gamma, double M, double Re, double Pr,
@@ -46,6 +49,11 @@ extern "C" void emu_functional(int ndim, int n_elements, const double* U, const 
   const int nd = mode == 0 ? Ke + 2 : Ke;
   for (int e = 0; e < n_elements; e++)
     for (int k = 0; k < nd; k++) {
+      if (g_elem_mask && !g_elem_mask[e]) {
+        out[(size_t)e * nd + k] = 0.0;
+        if (k == 0 && val) val[e] = 0.0;
+        continue;
+      }
       const Dual L = (ndim == 2) ? element_functional<2>(a, e, k) : element_functional<3>(a, e, k);
       out[(size_t)e * nd + k] = L.d;
       if (k == 0 && val) val[e] = L.v;

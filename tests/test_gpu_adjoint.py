@@ -49,6 +49,8 @@ def _load_emu():
     P, D, I = C.c_void_p, C.c_double, C.c_int
     L.emu_functional.argtypes = [I, I, P, P, P, P, P, D, D, D, D, D, D, I, D, I, I, P, P, P, D, D, P, P]
     L.emu_wall_force.argtypes = [I, I, P, P, P, P, D, D, D, D, D, D, I, I, P, P]
+    L.emu_set_element_mask.argtypes = [P]
+    L.emu_set_adaptive.argtypes = [P, P]
     return L
 
 
@@ -239,3 +241,66 @@ def test_checkpoint_spacing_and_mixed_precision(gpu, adj):
     assert rm["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-6)
     assert rm["dJ_dtwall"] == pytest.approx(adj["dJ_dtwall"], rel=1e-6)
     assert np.abs(rm["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-4 * np.abs(adj["dJ_dtnode"]).max()
+
+
+def test_vjp_full_size_cylinder_sampled(gpu, emu, oracle_lib):
+    """The reverse sweep on the full cylinder 96x128x16 (184,320 hex8, the adjoint leg's mesh)
+    after two FP64 steps: adjoint weights on the nodes of sampled elements only (interior, and
+    the first and last element with each pattern of boundary codes: wall, far field, symmetry
+    planes), so that exactly the elements touching those nodes contribute.  The GPU's assembled
+    gradient, d/d dt and d/d M against the forward-mode functional of the CPU build over those
+    elements."""
+    from cfdv_b200 import meshgen as mg
+    case = mg.FULL["cylinder"]()
+    o = oracle_lib.Oracle(case)
+    E, nnod, neqn, Ke = case.n_elements, 8, 5, 40
+    conn = np.ascontiguousarray(case.conn, np.int32)
+    bc = np.ascontiguousarray(case.bc, np.int32)
+    rng = np.random.default_rng(20261204)
+    pick = set(rng.choice(E, 6, replace=False).tolist())
+    pats = {}
+    for e, row in enumerate(map(tuple, bc)):
+        if any(row):
+            pats.setdefault(row, []).append(e)
+    for es in pats.values():
+        pick.update((es[0], es[-1]))
+    nodes = np.unique(conn[sorted(pick)].ravel())
+    w = np.zeros(case.n_nodes * neqn)
+    for q in range(neqn):
+        w[nodes * neqn + q] = rng.standard_normal(len(nodes))
+    du = rng.standard_normal(case.n_nodes * neqn) * 1e-3
+    cfl = float(case.control["cfl"])
+    with gpu.FDVSolver(case) as s:
+        s.set_state(o.init_U())
+        for _ in range(2):
+            s.step(cfl, mode=gpu.GMRES_CORRECT, m=40, restarts=20, rtol=1e-10)
+        U = s.get_state()
+        dt = s.cfl(cfl)
+        s.form(dt)
+        gU, gdt, gm = s.vjp(w, du)
+    touched = np.isin(conn, nodes).any(axis=1)
+    mask = np.ascontiguousarray(touched.astype(np.uint8))
+    x = np.ascontiguousarray(case.nodes[:, :3])
+    rm = o.rowmask()
+    a = case.aero
+    gas = (float(a["gamma"]), float(a["M"]), float(a["Re"]), float(a["Pr"]), float(a["Tinf"]), float(a["Twall"]),
+           int(a["Adiabatic"]))
+    out = np.zeros(E * (Ke + 2))
+    val = np.zeros(E)
+    emu.emu_set_adaptive(None, None)
+    emu.emu_set_element_mask(_p(mask))
+    try:
+        emu.emu_functional(3, E, _p(U), _p(x), _p(conn), _p(bc), _p(rm), *gas, float(dt), 0, 0, _p(du), _p(w),
+                           _p(du), 0.0, 0.0, _p(out), _p(val))
+    finally:
+        emu.emu_set_element_mask(None)
+    rows = out.reshape(E, Ke + 2)
+    ref = np.zeros(case.n_nodes * neqn)
+    for e in np.nonzero(touched)[0]:
+        ix = (conn[e][:, None] * neqn + np.arange(neqn)[None, :]).ravel()
+        np.add.at(ref, ix, rows[e, :Ke])
+    assert touched.sum() >= 6 * 8 and len(pats) >= 3
+    assert np.abs(gU - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert gdt == pytest.approx(rows[:, Ke].sum(), rel=1e-10)
+    # the Mach derivative sums terms that nearly cancel (Cv and T both scale with M^-2)
+    assert gm == pytest.approx(rows[:, Ke + 1].sum(), rel=1e-8, abs=1e-11 * np.abs(rows[:, Ke + 1]).max())
