@@ -53,9 +53,18 @@ struct WarpVjpSupg {
 template <>
 struct WarpVjpSupg<3> {};
 
+// 3D: the scalar adjoints that weight the a and b entries (abar_b, va1_b, vb1_b of the pass),
+// kept here rather than in registers through the Jacobians' reverse (2D: in registers)
+template <int NDIM>
+struct WarpVjpEntryAdj {
+  double xb[5], va[5], vb[5];
+};
+template <>
+struct WarpVjpEntryAdj<2> {};
+
 // one lane's Gauss point
 template <int NDIM>
-struct WarpVjpPointData : WarpVjpSupg<NDIM> {
+struct WarpVjpPointData : WarpVjpSupg<NDIM>, WarpVjpEntryAdj<NDIM> {
   static constexpr int NNOD = FormTraits<NDIM>::NNOD;
   GpState f;  // state at the point (edited on a face)
   double Phi[NNOD], dPhi[NNOD][3];
@@ -299,7 +308,7 @@ CFDV_HD CFDV_INLINE void pass_node_sums(const WarpVjpElem<NDIM>& El, const WarpV
 // of the Jacobians' reverse in the kernel); a 2D face point has uS = mPsi = 0, which drops
 // the upwind terms.
 template <int NDIM, class Lanes>
-CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpElem<NDIM>& El, const WarpVjpPoint<NDIM>& P,
+CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpElem<NDIM>& El, WarpVjpPoint<NDIM>& P,
                                        const GpState& fr, const double* s, bool face, bool on, bool pass, int q,
                                        int fc, int code, Lanes& L, WarpVjpAcc& acc, PrimAdj& na) {
   using V = WarpVjp<NDIM>;
@@ -432,24 +441,37 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
     }
   }
   // the Jacobians
+  const double *XB = abar_b, *VA = va1_b, *VB = vb1_b;
+  if constexpr (NDIM == 3) {  // the entry weights read them from the lane's slot
+    if (on)
+#pragma unroll
+      for (int r = 0; r < 5; r++) {
+        P.xb[r] = abar_b[r];
+        P.va[r] = va1_b[r];
+        P.vb[r] = vb1_b[r];
+      }
+    XB = P.xb;
+    VA = P.va;
+    VB = P.vb;
+  }
   double gCv = 0.0;
 #pragma unroll 1
   for (int t = 0; t < 1 + 2 * NDIM; t++) {
     if (!face) L.task_sync();
     if (on) {
       switch (t) {
-        case 0: jac_a_adj<NDIM>(gp, P.f, WeightsAB<NDIM, PSI, 0>{P, abar_b, va1_b, vaS_b, Sa_b}, g, gCv); break;
+        case 0: jac_a_adj<NDIM>(gp, P.f, WeightsAB<NDIM, PSI, 0>{P, XB, VA, vaS_b, Sa_b}, g, gCv); break;
         case 1:
-          jac_b_rows_adj<NDIM>(gp, P.f, 0, WeightsAB<NDIM, PSI, 0>{P, abar_b, vb1_b, vbS_b, Sb_b}, g, gCv);
+          jac_b_rows_adj<NDIM>(gp, P.f, 0, WeightsAB<NDIM, PSI, 0>{P, XB, VB, vbS_b, Sb_b}, g, gCv);
           break;
         case 2:
-          jac_b_rows_adj<NDIM>(gp, P.f, 1, WeightsAB<NDIM, PSI, 1>{P, abar_b, vb1_b, vbS_b, Sb_b}, g, gCv);
+          jac_b_rows_adj<NDIM>(gp, P.f, 1, WeightsAB<NDIM, PSI, 1>{P, XB, VB, vbS_b, Sb_b}, g, gCv);
           break;
         case 3: jac_c_rows_adj<NDIM>(gp, P.f, 0, WeightsC<NDIM, 0>{P, Gam_b}, g, gCv); break;
         case 4: jac_c_rows_adj<NDIM>(gp, P.f, 1, WeightsC<NDIM, 1>{P, Gam_b}, g, gCv); break;
         case 5:
           if constexpr (NDIM == 3)
-            jac_b_rows_adj<NDIM>(gp, P.f, 2, WeightsAB<NDIM, PSI, 2>{P, abar_b, vb1_b, vbS_b, Sb_b}, g, gCv);
+            jac_b_rows_adj<NDIM>(gp, P.f, 2, WeightsAB<NDIM, PSI, 2>{P, XB, VB, vbS_b, Sb_b}, g, gCv);
           break;
         default:
           if constexpr (NDIM == 3) jac_c_rows_adj<NDIM>(gp, P.f, 2, WeightsC<NDIM, 2>{P, Gam_b}, g, gCv);
