@@ -153,7 +153,7 @@ int ensure_adjoint_buffers(cfdv_ctx* c) {
   int rc;
   const size_t E = c->n_elements, Ke = c->Ke, n = c->n_dof;
   if (!c->d_adj_e && (rc = dalloc(c, &c->d_adj_e, E * (Ke + 3)))) return rc;
-  if (!c->d_adj_v && (rc = dalloc(c, &c->d_adj_v, 4 * n))) return rc;
+  if (!c->d_adj_v && (rc = dalloc(c, &c->d_adj_v, 5 * n))) return rc;
   return CFDV_OK;
 }
 
@@ -489,7 +489,9 @@ int cfdv_tangent(cfdv_ctx* c, const cfdv_adjoint_opts* o, double dmach, const do
   double* tU = c->d_adj_v;           // tangent of U
   double* dr = c->d_adj_v + n;       // residual tangent
   double* gF = c->d_adj_v + 2 * n;   // dF/dU
-  double* du = c->d_adj_v + 3 * n;   // the step's dU
+  double* du = c->d_adj_v + 3 * n;
+  double* mu_prev = c->d_adj_v + 4 * n;  // the last reverse step's mu: the next solve's start
+  bool have_mu = false;   // the step's dU
   std::vector<double> h0;
   initial_state_tangent(c, dmach, wall, dT_wall, h0);
   if ((rc = reload_initial_state(c))) return rc;
@@ -593,6 +595,8 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
   double* g = c->d_adj_v + n;
   double* gF = c->d_adj_v + 2 * n;
   double* du = c->d_adj_v + 3 * n;
+  double* mu_prev = c->d_adj_v + 4 * n;  // the last reverse step's mu: the next solve's start
+  bool have_mu = false;
   const cfdv_gmres_opts so = solve_opts(o);
   // The last P recomputed steps of a segment form into kept sets of the pool; their reverse
   // steps solve with those matrices instead of forming again.  The context's own buffers
@@ -684,12 +688,16 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
         if ((rc = cfdv_form(c, dt, o->precision))) return rc;
         reverse_forms++;
       }
-      // mu = A^-T lambda; no later step reads these matrices, so their blocks stay transposed
+      // mu = A^-T lambda, started from the previous reverse step's mu (the GMRES stopping test
+      // is relative to ||lambda||, so a close start saves products); no later step reads
+      // these matrices, so their blocks stay transposed
       rep.n_matvec = 0;
-      rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, cfdv::ctxi::kTransposeKeep);
+      rc = cfdv::ctxi::solve_device(c, &so, &rep, lam, cfdv::ctxi::kTransposeKeep, have_mu ? mu_prev : nullptr);
       c->formed = false;  // the context's own buffers hold transposed or older matrices
       own.restore();
       if (rc) return rc;
+      CK(cudaMemcpyAsync(mu_prev, c->d_du, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
+      have_mu = true;
       adj_mv += rep.n_matvec;
       double g_dt, g_m;
       if ((rc = vjp_device(c, dt, c->d_du, du, g, &g_dt, &g_m, nullptr))) return rc;

@@ -522,7 +522,7 @@ int gmres_correct(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep)
 // fills the report, so a caller can enqueue more work (the state update of a step) in
 // between.  The kernel computes ||b|| itself.
 int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double* rhs_vec, int transpose,
-                             SolveLaunch* L) {
+                             SolveLaunch* L, const double* x0) {
   const int m = o->m;
   const int fp32 = (o->precision == CFDV_PREC_MIXED);
   if (fp32 && !c->have32) return fail(c, CFDV_ERR_STATE, "mixed precision needs cfdv_form(..., CFDV_PREC_MIXED)");
@@ -539,7 +539,9 @@ int cfdv::ctxi::solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double
   // stop, cycles, err, barrier count | a neighbour-sync flag per block, 32 apart
   const size_t n_int = 32 + 32 * (size_t)persistent_max_blocks();
   if (!c->d_pers_int && (rc = dalloc(c, &c->d_pers_int, n_int))) return rc;
-  CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
+  if (!x0) CK(cudaMemsetAsync(c->d_du, 0, sizeof(double) * c->n_dof, c->st));
+  else if (x0 != c->d_du)
+    CK(cudaMemcpyAsync(c->d_du, x0, sizeof(double) * c->n_dof, cudaMemcpyDeviceToDevice, c->st));
   // b from the element rhs: assembled by the block-Jacobi launch when there is one
   const bool fuse_b = !rhs_vec && !transpose && o->precond;
   if (rhs_vec) {
@@ -670,9 +672,9 @@ int cfdv::ctxi::solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_repor
 }
 
 int cfdv::ctxi::solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
-                             int transpose) {
+                             int transpose, const double* x0) {
   SolveLaunch L;
-  const int rc = solve_launch(c, o, rhs_vec, transpose, &L);
+  const int rc = solve_launch(c, o, rhs_vec, transpose, &L, x0);
   return rc ? rc : solve_finish(c, L, rep);
 }
 

@@ -131,10 +131,11 @@ inline void dfree(T*& p) {
 // assembled element rhs (rhs_vec == nullptr) or the device vector rhs_vec; transpose = 1
 // solves A^T x = rhs and restores the element blocks afterwards, kTransposeKeep solves
 // A^T x = rhs and leaves them transposed (the caller re-forms before the next use).  The
-// solution is left in c->d_du.
+// iteration starts from the device vector x0 (zero when null): every restart cycle, the first
+// included, starts from r = b - A x.  The solution is left in c->d_du.
 constexpr int kTransposeKeep = 2;
 int solve_device(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep, const double* rhs_vec,
-                 int transpose);
+                 int transpose, const double* x0 = nullptr);
 
 // solve_device in two halves: solve_launch enqueues the persistent launch and the read-back
 // of its results into c->h_pin + kPinSolve without waiting; solve_finish waits for the
@@ -150,7 +151,8 @@ struct SolveLaunch {
   int* err;   // device error flags of the launch (bit 0 barrier timeout, bit 1 non-finite)
   int fp32;
 };
-int solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double* rhs_vec, int transpose, SolveLaunch* L);
+int solve_launch(cfdv_ctx* c, const cfdv_gmres_opts* o, const double* rhs_vec, int transpose, SolveLaunch* L,
+                 const double* x0 = nullptr);
 int solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_report* rep);
 
 }  // namespace ctxi

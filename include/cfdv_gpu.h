@@ -272,8 +272,9 @@ int cfdv_wall_nodes(cfdv_ctx* ctx, int wall_bc, int* ids, int capacity, int* n);
 /* Forward run with checkpoints, then the reverse sweep: lambda_N = (1/N) dF/dU(U_N),
  * mu_n = A_n^-T lambda_{n+1}, lambda_n = lambda_{n+1} + (dr_n/dU)^T mu_n
  * + (mu_n^T dr_n/ddt) d dt_n/dU + [n >= 1] (1/N) dF/dU(U_n); gradients from lambda_0.
- * The context's state is U_N afterwards, with no element matrices formed (the transposed
- * solves leave them transposed): cfdv_form before the next solve. */
+ * Each transposed solve starts from the previous reverse step's mu.  The context's state is
+ * U_N afterwards, with no element matrices formed (the transposed solves leave them
+ * transposed): cfdv_form before the next solve. */
 int cfdv_adjoint(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, cfdv_adjoint_result* res);
 /* FP64 tangent-linear run along (dmach, dT_wall[n_wall_nodes], NULL = 0): J and dJ. */
 int cfdv_tangent(cfdv_ctx* ctx, const cfdv_adjoint_opts* opts, double dmach, const double* dT_wall, double* J,
