@@ -192,9 +192,11 @@ def run_reference_cpu(case, steps, warmup):
     return times
 
 
-def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ranks, sampler=None):
+def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ranks, sampler=None, warm=None):
     """Time FP64 and mixed FDV steps of one workload; returns per-form results and the
-    live EBE element-pass roofline (one extra host-driven step with CUDA events)."""
+    live EBE element-pass roofline (one extra host-driven step with CUDA events).  warm: start
+    each solve from the previous step's dU (default: --warm-start)."""
+    warm = args.warm_start if warm is None else warm
     import numpy as np
     import torch
     from cfdv_b200 import gpu as G, meshgen as mg
@@ -212,7 +214,7 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
         solver.load_node_records()
         for _ in range(warmup):
             solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec,
-                        orth=ORTH[args.orth])
+                        orth=ORTH[args.orth], warm_start=warm)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -231,7 +233,7 @@ def measure_workload(args, name, steps, warmup, flush, ws, barrier, max_over_ran
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(ext)
             rep = solver.step(cfl, mode=G.GMRES_CORRECT, m=m, restarts=200, rtol=rtol, precision=prec,
-                              orth=ORTH[args.orth])
+                              orth=ORTH[args.orth], warm_start=warm)
             with torch.cuda.stream(ext):
                 e1.record(ext)
             e1.synchronize()
@@ -473,6 +475,7 @@ def bench_gpu(args, ws, rank, local):
         "config": {"workload": head["desc"], "elements": case.n_elements, "dof": n,
                    "gmres": f"restarted GMRES({m}), {args.orth.upper()}, right node-block Jacobi, to true relative "
                             f"residual {rtol:g}",
+                   "initial_guess": "the previous step's dU" if args.warm_start else "zero (as the reference)",
                    "l2": "flushed between timed steps (512 MiB write)", "parallelism": f"replicas x{ws}",
                    "deviations": WORKLOADS[args.workload]["deviations"]},
         "fp64": {"value": fp64["steps_per_s"], "ms_per_step": fp64["ms_per_step"],
@@ -514,6 +517,20 @@ def bench_gpu(args, ws, rank, local):
         ex["solver"].close()
         line[name] = summarize(ex, name, k, w, peak, peak_kind, tiles.get(name))
         del ex
+    if not args.warm_start and args.secondary != "none":
+        # the same workloads with each solve started from the previous step's dU (the same
+        # stopping test); the headline above starts from zero, as the reference does
+        warm = {"initial_guess": "the previous step's dU", "note": "same stopping test; headline starts from zero"}
+        for name, k, w in ((args.workload, args.steps, args.warmup), (args.secondary, 3, 3)):
+            if name not in WORKLOADS:
+                continue
+            r = measure_workload(args, name, k, w, flush, ws, barrier, max_over_ranks, warm=True)
+            r["solver"].close()
+            warm[name] = {f: {"value": r[f]["steps_per_s"], "matvecs_per_step": r[f]["matvecs_per_step"],
+                              "true_rel_res_max": r[f]["true_rel_res_max"], "solve_ms": r[f]["solve_ms"]}
+                          for f in ("mixed", "fp64") if f in r}
+            del r
+        line["warm_start"] = warm
     if args.adj_steps > 0:
         line["adjoint"] = measure_adjoint(args, ws, max_over_ranks)
     if rank == 0:
@@ -565,6 +582,9 @@ def main():
     ap.add_argument("--only", choices=["fp64", "mixed", "adjoint"], help="time one form or the adjoint leg only "
                                                                          "(profiling runs)")
     ap.add_argument("--secondary", default="ramp", help="second workload reported beside the headline ('none' to skip)")
+    ap.add_argument("--warm-start", action="store_true",
+                    help="start each step's solve from the previous step's dU instead of zero (the same 1e-8 "
+                         "stopping test)")
     ap.add_argument("--adj-steps", type=int, default=4, help="steps of the adjoint leg on the cylinder (0 to skip)")
     ap.add_argument("--adj-every", type=int, default=2, help="checkpoint spacing of the adjoint leg")
     ap.add_argument("--extra", default="lid,duct", help="further workloads reported beside the headline "

@@ -50,6 +50,7 @@ void free_all(cfdv_ctx* c) {
   c->m_cap = 0;
   c->formed = false;
   c->have32 = false;
+  c->du_valid = false;
 }
 
 // Dirichlet flags per DOF from the faces (LoadBinary.h:264-318) and the per-element
@@ -668,6 +669,7 @@ int cfdv::ctxi::solve_finish(cfdv_ctx* c, const SolveLaunch& L, cfdv_gmres_repor
     const double sr = L.fp32 ? 4.0 : 8.0, E = c->n_elements, K2 = (double)c->Ke * c->Ke, n8 = 8.0 * c->n_dof;
     c->solve_bytes += res[4] * (E * K2 * 8.0 + 2 * n8) + (res[3] - res[4]) * (E * K2 * sr + 2 * n8) + res[5] * n8;
   }
+  c->du_valid = true;  // a finite solution: a start for a warm-started solve
   return CFDV_OK;
 }
 
@@ -924,7 +926,7 @@ int cfdv_gmres(cfdv_ctx* c, const cfdv_gmres_opts* o, cfdv_gmres_report* rep) {
   } else if (o->engine == 1) {
     rc = gmres_correct(c, o, rep);
   } else {
-    rc = cfdv::ctxi::solve_device(c, o, rep, nullptr, 0);
+    rc = cfdv::ctxi::solve_device(c, o, rep, nullptr, 0, (o->warm_start && c->du_valid) ? c->d_du : nullptr);
   }
   if (rc) return rc;
   if (o->true_residual && rep && o->mode == CFDV_GMRES_REFERENCE) rc = true_residual(c, rep);
@@ -1001,7 +1003,8 @@ int cfdv_step_host(cfdv_ctx* c, double cfl, const cfdv_gmres_opts* o, cfdv_gmres
   };
   if ((rc = form_enqueue(c, 0.0, d_dt, o->precision))) return unchanged_out(rc);
   cfdv::ctxi::SolveLaunch L;
-  if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L))) return unchanged_out(rc);
+  if ((rc = cfdv::ctxi::solve_launch(c, o, nullptr, 0, &L, (o->warm_start && c->du_valid) ? c->d_du : nullptr)))
+    return unchanged_out(rc);
   CK(launch_state_update_guarded(c->d_U, c->d_U0, c->d_du, c->n_dof, L.err, c->d_status, d_dt, c->st));
   c->launches++;
   double* hs = c->h_pin + cfdv::ctxi::kPinStep;

@@ -40,6 +40,7 @@ struct cfdv_ctx {
   double* d_Y64 = nullptr;
   float* d_Y32 = nullptr;
   bool formed = false, have32 = false;
+  bool du_valid = false;  // d_du holds a finite solution of an earlier solve
   double dt_formed = 0;
   // krylov
   int m_cap = 0;

@@ -52,7 +52,7 @@ class _Params(C.Structure):
 class _Opts(C.Structure):
     _fields_ = [("mode", C.c_int), ("m", C.c_int), ("restarts", C.c_int), ("rtol", C.c_double),
                 ("precision", C.c_int), ("true_residual", C.c_int), ("engine", C.c_int), ("precond", C.c_int),
-                ("orth", C.c_int)]
+                ("orth", C.c_int), ("warm_start", C.c_int)]
 
 
 class _Report(C.Structure):
@@ -242,9 +242,9 @@ class FDVSolver:
         self._ck(self.L.cfdv_set_element_matrices(self._ctx, _p(R), _p(rhs), int(precision)))
 
     @staticmethod
-    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1, orth=2):
+    def _opts(mode, m, restarts, rtol, precision, true_residual, engine=0, precond=1, orth=2, warm_start=False):
         return _Opts(int(mode), int(m), int(restarts), float(rtol), int(precision), int(bool(true_residual)),
-                     int(engine), int(precond), int(orth))
+                     int(engine), int(precond), int(orth), int(bool(warm_start)))
 
     def _report(self, m, restarts):
         """Report struct and history buffers for (m, restarts), kept between calls (the
@@ -268,8 +268,8 @@ class FDVSolver:
                 "matvecs": rep.n_matvec, "true_rel_res": rep.true_rel_res}
 
     def gmres(self, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64, true_residual=False,
-              engine=0, precond=True, orth=2):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
+              engine=0, precond=True, orth=2, warm_start=False):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth, warm_start)
         rep, est, fin = self._report(m, restarts)
         self._ck(self.L.cfdv_gmres(self._ctx, C.byref(o), C.byref(rep)))
         return self._unpack(rep, est, fin)
@@ -283,8 +283,8 @@ class FDVSolver:
         return r
 
     def step(self, cfl, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-             true_residual=False, engine=0, precond=True, orth=2):
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
+             true_residual=False, engine=0, precond=True, orth=2, warm_start=False):
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth, warm_start)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt)))
@@ -293,13 +293,13 @@ class FDVSolver:
         return out
 
     def step_host(self, cfl, U_in, U_out, mode=GMRES_REFERENCE, m=20, restarts=1, rtol=1e-8, precision=PREC_FP64,
-                  true_residual=False, engine=0, precond=True, orth=2):
+                  true_residual=False, engine=0, precond=True, orth=2, warm_start=False):
         """step() with the state passed in and out as host float64 arrays (None: not copied);
         one host synchronisation for copies and step together."""
         for a in (U_in, U_out):
             if a is not None:
                 assert a.dtype == np.float64 and a.size == self.n_dof and a.flags.c_contiguous
-        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth)
+        o = self._opts(mode, m, restarts, rtol, precision, true_residual, engine, precond, orth, warm_start)
         rep, est, fin = self._report(m, restarts)
         dt = C.c_double()
         self._ck(self.L.cfdv_step_host(self._ctx, float(cfl), C.byref(o), C.byref(rep), C.byref(dt),

@@ -1,7 +1,7 @@
 // cfdv_gpu: the CFDV time loop (src/main.cpp:162-206) with the per-step path on a B200.
 //
 //   cfdv_gpu <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed]
-//            [--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K]
+//            [--rtol R] [--restarts K] [--warm-start] [--physical-3d-flux] [--out DIR] [--save-every K]
 //            [--ensight DIR]
 //
 // Reads the reference case directory (control, aero, binarynodes, binaryelements) and
@@ -25,12 +25,13 @@ int main(int argc, char** argv) {
   if (argc < 2) {
     std::fprintf(stderr,
                  "usage: %s <case_dir> [--steps N] [--mode reference|correct] [--precision fp64|mixed] "
-                 "[--rtol R] [--restarts K] [--physical-3d-flux] [--out DIR] [--save-every K] [--ensight DIR]\n",
+                 "[--rtol R] [--restarts K] [--warm-start] [--physical-3d-flux] [--out DIR] [--save-every K] "
+                 "[--ensight DIR]\n",
                  argv[0]);
     return 2;
   }
   std::string dir = argv[1], out = ".", ensight_dir;
-  int steps = -1, restarts = -1, phys = 0, save_every = 1000;
+  int steps = -1, restarts = -1, phys = 0, save_every = 1000, warm = 0;
   int mode = CFDV_GMRES_REFERENCE, precision = CFDV_PREC_FP64;
   double rtol = 1e-8;
   for (int i = 2; i < argc; i++) {
@@ -41,6 +42,7 @@ int main(int argc, char** argv) {
     else if (a == "--rtol" && i + 1 < argc) rtol = std::atof(argv[++i]);
     else if (a == "--restarts" && i + 1 < argc) restarts = std::atoi(argv[++i]);
     else if (a == "--physical-3d-flux") phys = 1;
+    else if (a == "--warm-start") warm = 1;
     else if (a == "--out" && i + 1 < argc) out = argv[++i];
     else if (a == "--save-every" && i + 1 < argc) save_every = std::atoi(argv[++i]);
     else if (a == "--ensight" && i + 1 < argc) ensight_dir = argv[++i];
@@ -63,6 +65,7 @@ int main(int argc, char** argv) {
     o.engine = 0;
     o.precond = 1;
     o.orth = 2;  // delayed CGS2 (one reduction per Arnoldi step)
+    o.warm_start = warm;  // correct mode: start each solve from the previous step's dU
     std::vector<double> est((size_t)o.m * o.restarts), gfin(o.restarts);
     cfdv_gmres_report rep;
     std::memset(&rep, 0, sizeof(rep));

@@ -100,6 +100,9 @@ typedef struct {
                         synchronisations per step; m <= 62; in 2D the two around the product
                         wait only for the blocks owning neighbouring nodes and elements),
                         3 = delayed CGS2 with grid barriers at all 3 (bitwise equal to 2) */
+  int warm_start;    /* CORRECT mode, engine 0: 1 = start from the context's last solution
+                        (the previous step's dU) instead of zero; the stopping test stays
+                        ||b - A du|| / ||b|| < rtol.  0 = from zero, as the reference does */
 } cfdv_gmres_opts;
 
 typedef struct {

@@ -113,6 +113,38 @@ def test_step_host_equals_set_step_get(gpu, name, engine):
     assert r1["dt"] == r2["dt"] and np.array_equal(r1["est"], r2["est"])
 
 
+@pytest.mark.parametrize("name", ["plate20", "ramp4"])
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_warm_start(gpu, name, prec):
+    """A solve started from the previous solution: solving the same formed system again stops
+    after the one product of its initial residual, with du unchanged; and steps started from
+    the previous step's dU meet the same stopping test as steps started from zero and end at
+    the same state within the solver's tolerance (the first step has no previous dU)."""
+    case = get_case(name)
+    p = gpu.PREC_FP64 if prec == "fp64" else gpu.PREC_MIXED
+    cfl = float(case.control["cfl"])
+    kw = dict(mode=gpu.GMRES_CORRECT, m=30, restarts=200, rtol=1e-10, precision=p, true_residual=True)
+    with gpu.FDVSolver(case) as s:
+        s.load_node_records()
+        s.form(s.cfl(cfl), p)
+        first = s.gmres(**kw)
+        du = s.du().copy()
+        again = s.gmres(warm_start=True, **kw)
+        assert first["matvecs"] > 1 and again["matvecs"] == 1
+        assert again["true_rel_res"] < 1e-10 and np.array_equal(s.du(), du)
+    runs = {}
+    for warm in (False, True):
+        with gpu.FDVSolver(case) as s:
+            s.load_node_records()
+            reps = [s.step(cfl, warm_start=warm, **kw) for _ in range(4)]
+            runs[warm] = (s.get_state(), reps)
+    (Uc, rc), (Uw, rw) = runs[False], runs[True]
+    for r in rc + rw:
+        assert r["true_rel_res"] < 1e-10
+    assert rc[0]["matvecs"] == rw[0]["matvecs"]
+    assert rel_err(Uw, Uc) < 1e-8
+
+
 _PASS_CHILD = r"""
 import sys, numpy as np
 sys.path.insert(0, sys.argv[1]); sys.path.insert(0, sys.argv[1] + "/tests")
