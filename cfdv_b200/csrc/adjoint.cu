@@ -20,26 +20,15 @@ using cfdv::ctxi::fail;
 
 namespace cfdv {
 
+// forward mode (the JVP, a.mode 1): one thread per (element, row), the row's derivative along
+// the tangent (tU, t_dt, t_mach)
 template <int NDIM>
 __global__ void __launch_bounds__(128) functional_kernel(FunctionalArgs a) {
   constexpr int KE = FormTraits<NDIM>::KE;
-  const int ndir = (a.mode == 0) ? KE + 2 : (a.mode == 1) ? KE : 2;
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int e = (int)(t / ndir), k = (int)(t % ndir) + (a.mode == 2 ? KE : 0);
+  const int e = (int)(t / KE), k = (int)(t % KE);
   if (e >= a.n_elements) return;
-  const Dual L = element_functional<NDIM>(a, e, k);
-  if (a.mode == 2) {
-    if (k == KE) a.out_dt[e] = L.d;
-    else a.out_mach[e] = L.d;
-    if (k == KE && a.out_val) a.out_val[e] = L.v;
-  } else if (a.mode == 0) {
-    if (k < KE) a.out[(size_t)e * KE + k] = L.d;
-    else if (k == KE) a.out_dt[e] = L.d;
-    else a.out_mach[e] = L.d;
-    if (k == 0 && a.out_val) a.out_val[e] = L.v;
-  } else {
-    a.out[(size_t)e * KE + k] = L.d;
-  }
+  a.out[(size_t)e * KE + k] = element_functional<NDIM>(a, e, k).d;
 }
 
 // the collectives of warp_vjp: the warp's lanes; task_sync is the block's barrier
@@ -171,8 +160,8 @@ FunctionalArgs functional_args(cfdv_ctx* c, double dt) {
 }
 
 cudaError_t launch_functional(cfdv_ctx* c, const FunctionalArgs& a) {
-  const int ndir = (a.mode == 0) ? c->Ke + 2 : (a.mode == 1) ? c->Ke : 2;
-  const long threads = (long)c->n_elements * ndir;
+  if (a.mode != 1) return cudaErrorInvalidValue;  // the VJP runs through vjp_warp_kernel
+  const long threads = (long)c->n_elements * c->Ke;
   const int grid = (int)((threads + kThreadsFn - 1) / kThreadsFn);
   if (c->ndim == 2) functional_kernel<2><<<grid, kThreadsFn, 0, c->st>>>(a);
   else functional_kernel<3><<<grid, kThreadsFn, 0, c->st>>>(a);

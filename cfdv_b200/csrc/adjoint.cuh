@@ -17,7 +17,8 @@
 // L_e collapses per Gauss point to a few neqn-vectors (m1_i = sum_N dPhi_N,i w_N,
 // u0 = sum_M Phi_M dU_M, u1_j = sum_M dPhi_M,j dU_M, ...) contracted with the flux
 // Jacobians a_i, b_i, c_ij entry by entry.  A thread evaluates L_e for one element and
-// one seed direction:
+// one seed direction (the GPU runs the JVP this way; the VJP runs as the reverse sweep of
+// adjoint_warp.cuh, which the CPU build checks against these VJP seeds):
 //   VJP  (adjoint):  w = mu_e (the adjoint solution), seed = one of the element's Ke
 //                    unknowns, dt, or the Mach number -> one gradient entry per thread;
 //   JVP  (tangent):  w = a unit row, seed = the tangent (dU, ddt, dMach) -> one entry of
@@ -41,7 +42,8 @@ struct FunctionalArgs {
   double dt;
   double gz[2], gw[2];
   int n_elements, physical_3d_flux;
-  int mode;                 // 0: VJP (seeds: Ke unknowns, dt, Mach), 1: JVP, 2: VJP seeds dt and Mach only
+  int mode;                 // 0: VJP seeds (Ke unknowns, dt, Mach; forward mode, the CPU build's check of
+                            // the reverse sweep), 1: JVP (the GPU's functional_kernel)
   const double* U;          // [Nn][neqn]
   const double* x;          // [Nn][ndim]
   const int* conn;          // [E][nnod]

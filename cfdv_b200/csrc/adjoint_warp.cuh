@@ -15,10 +15,9 @@
 //      weights formed where that code reads them) into the state adjoint g, then the stress,
 //      gas law and (2D) upwind test function, or on a face the boundary edits;
 //   4. scatters g to the pass nodes: for each node the element's lanes sum their shares with
-//      shuffles, and the lane whose index is the node's keeps the node's adjoint in
-//      registers.
+//      shuffles, and the lane whose index is the node's adds them to the node's adjoint.
 // A lane's point (state, shape functions, row weights) sits in its own shared-memory slot,
-// the element's nodes in shared memory beside them.  The lanes then reverse the FDV
+// the element's nodes and node adjoints in shared memory beside them.  The lanes then reverse the FDV
 // parameters and the node unpack (lane q for node q).  The same sweep gives d L_e / d dt and
 // d L_e / d Mach: dt enters only the contraction; the Mach number enters through Cv, cgas and
 // cmach (node unpack, node Mach and Reynolds numbers, k(mu) at the points, Cv in the b and c
@@ -231,6 +230,57 @@ CFDV_HD CFDV_INLINE void conv_flux_adj(const NodePrim& n, int i, int r, double f
       np += fb * vi;
     }
   }
+}
+
+// Reverse of the 3D boundary edits that only zero entries and recompute the stress
+// (edit_face_state_3d, formation.cuh): g (of the edited state f) -> graw (of the raw sums),
+// for the fields the edits read (v, dV, dT, dU, mu); E, T, U, k pass through in face_edit_adj
+// and here alike.  Returns false for the codes left to the dual-number face_edit_adj.
+CFDV_HD CFDV_INLINE bool face_edit_adj_3d_direct(int code, const GpState& f, int adiabatic, GpState& g,
+                                                 GpState& graw) {
+  int zero_dV = -1, zero_dT = -1;  // column of dV / entry of dT the edit zeroes (-1: none)
+  bool stress = false;
+  switch (code) {
+    case 2:
+    case 12: zero_dV = 2; zero_dT = 2; break;
+    case -1: break;
+    case 1:
+    case 51: stress = true; zero_dT = adiabatic ? 2 : -1; break;
+    case 21:
+    case 31: stress = true; zero_dT = adiabatic ? 1 : -1; break;
+    case 11: stress = true; zero_dT = adiabatic ? 0 : -1; break;
+    case 8: stress = true; break;
+    case 6:  // dT[0] = 0, stress, tau[i][0] = 0
+      stress = true;
+      zero_dT = 0;
+      for (int i = 0; i < 3; i++) g.tau[i][0] = 0.0;
+      break;
+    case 22:  // dV[:,1] = 0, dT[1] = 0, stress, five entries of tau zeroed
+      stress = true;
+      zero_dV = 1;
+      zero_dT = 1;
+      g.tau[0][1] = g.tau[1][1] = g.tau[2][1] = g.tau[1][0] = g.tau[1][2] = 0.0;
+      break;
+    default: return false;
+  }
+  if (stress) stress_adj<3>(f, g);  // f: the state the stress was formed from (edited dV)
+  if (zero_dV >= 0)
+    for (int i = 0; i < 3; i++) g.dV[i][zero_dV] = 0.0;
+  if (zero_dT >= 0) g.dT[zero_dT] = 0.0;
+  graw.E += g.E;
+  graw.T += g.T;
+  graw.k += g.k;
+  graw.mu += g.mu;
+  for (int q = 0; q < 5; q++) {
+    graw.U[q] += g.U[q];
+    for (int c = 0; c < 3; c++) graw.dU[q][c] += g.dU[q][c];
+  }
+  for (int i = 0; i < 3; i++) {
+    graw.v[i] += g.v[i];
+    graw.dT[i] += g.dT[i];
+    for (int j = 0; j < 3; j++) graw.dV[i][j] += g.dV[i][j];
+  }
+  return true;
 }
 
 // element node of pass node b (face-local numbering on a face)
@@ -499,8 +549,11 @@ CFDV_HD CFDV_INLINE void warp_vjp_pass(const FunctionalArgs& a, const WarpVjpEle
     } else {
       GpState graw;
       gp_zero(graw);
-      face_edit_adj<NDIM>(code, fr, El.nd[face_node(NDIM, fc, 0)].x, El.nd[face_node(NDIM, fc, 1)].x, P.en,
-                          gp.adiabatic, g, graw);
+      bool direct = false;  // the zeroing-and-stress edits of 3D faces, reversed directly
+      if constexpr (NDIM == 3) direct = face_edit_adj_3d_direct(code, P.f, gp.adiabatic, g, graw);
+      if (!direct)
+        face_edit_adj<NDIM>(code, fr, El.nd[face_node(NDIM, fc, 0)].x, El.nd[face_node(NDIM, fc, 1)].x, P.en,
+                            gp.adiabatic, g, graw);
       acc.dmach += graw.k * fr.k * (-2.0 / gp.cmach);
       gas_adj(gp, fr, graw);
       g = graw;

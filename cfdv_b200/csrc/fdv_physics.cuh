@@ -233,6 +233,7 @@ CFDV_HD CFDV_INLINE void viscous_stress(GpStateT<S>& f) {
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_a_2d(const GasT<S>& th, const GpStateT<S>& f, S* m) {
+  #pragma unroll
   for (int i = 0; i < 2 * 25; i++) m[i] = 0.0;
   const S u = f.v[0], v = f.v[1], uu = u * u, uv = u * v, vv = v * v, E = f.E;
   JA(m, 0, 0, 1) = 1.0;
@@ -264,6 +265,7 @@ CFDV_HD CFDV_INLINE void jac_a_2d(const GasT<S>& th, const GpStateT<S>& f, S* m)
 template <class S>
 CFDV_HD CFDV_INLINE void jac_b_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
   S* blk = m;
+  #pragma unroll
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const S reinv = 1.0 / th.creyn, mu = f.mu, E = f.E;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -310,6 +312,7 @@ CFDV_HD CFDV_INLINE void jac_b_rows_2d(const GasT<S>& th, const GpStateT<S>& f, 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_c_rows_2d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
   S* blk = m;
+  #pragma unroll
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const S reinv = 1.0 / th.creyn, mu = f.mu;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -353,6 +356,7 @@ CFDV_HD CFDV_INLINE void jac_c_rows_2d(const GasT<S>& th, const GpStateT<S>& f, 
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_a_3d(const GasT<S>& th, const GpStateT<S>& f, S* m) {
+  #pragma unroll
   for (int i = 0; i < 3 * 25; i++) m[i] = 0.0;
   const S gamma = th.gamma, g1 = th.gamm1, g3 = th.gamm3, gm3d2 = th.gm3d2, gm1d2 = th.gm1d2;
   const S u = f.v[0], v = f.v[1], w = f.v[2];
@@ -389,6 +393,7 @@ CFDV_HD CFDV_INLINE void jac_a_3d(const GasT<S>& th, const GpStateT<S>& f, S* m)
 template <class S>
 CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
   S* blk = m;
+  #pragma unroll
   for (int k = 0; k < 25; k++) blk[k] = 0.0;
   const S mu = f.mu, E = f.E;
   const S lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
@@ -469,12 +474,14 @@ CFDV_HD CFDV_INLINE void jac_b_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
     JA(blk, 0, 4, 4) = TERM1 * drdz;
   }
   const S reinv = 1.0 / th.creyn;
+  #pragma unroll
   for (int k = 0; k < 25; k++) blk[k] *= reinv;
 }
 
 template <class S>
 CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, int i, S* m) {
   S* blk = m;
+  #pragma unroll
   for (int k = 0; k < 75; k++) blk[k] = 0.0;
   const S mu = f.mu, lambda = -2. * mu / 3., mu_R = 2. * mu + lambda;
   const S rho = f.U[0], denom = 1. / (rho * rho);
@@ -565,6 +572,7 @@ CFDV_HD CFDV_INLINE void jac_c_rows_3d(const GasT<S>& th, const GpStateT<S>& f, 
     JC(blk, 0, 1, 4, 3) = (mv * irho) * (-mu * irho);
   }
   const S reinv = 1.0 / th.creyn;
+  #pragma unroll
   for (int k = 0; k < 75; k++) blk[k] *= reinv;
 }
 

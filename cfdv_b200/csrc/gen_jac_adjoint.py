@@ -46,6 +46,7 @@ def function_body(src, name):
 def statements(body):
     """Split a body into a tree: ('stmt', text) | ('if', [(cond, block), ...])."""
     body = re.sub(r"//[^\n]*", "", body)
+    body = re.sub(r"#pragma[^\n]*", "", body)
     s = body.strip()
 
     def parse_block(s, k):
