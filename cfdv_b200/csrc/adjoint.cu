@@ -478,9 +478,7 @@ int cfdv_tangent(cfdv_ctx* c, const cfdv_adjoint_opts* o, double dmach, const do
   double* tU = c->d_adj_v;           // tangent of U
   double* dr = c->d_adj_v + n;       // residual tangent
   double* gF = c->d_adj_v + 2 * n;   // dF/dU
-  double* du = c->d_adj_v + 3 * n;
-  double* mu_prev = c->d_adj_v + 4 * n;  // the last reverse step's mu: the next solve's start
-  bool have_mu = false;   // the step's dU
+  double* du = c->d_adj_v + 3 * n;   // the step's dU
   std::vector<double> h0;
   initial_state_tangent(c, dmach, wall, dT_wall, h0);
   if ((rc = reload_initial_state(c))) return rc;
@@ -523,11 +521,25 @@ int cfdv_tangent(cfdv_ctx* c, const cfdv_adjoint_opts* o, double dmach, const do
   return CFDV_OK;
 }
 
-// Grow the context's pool of element-matrix sets (FP64, and FP32 for the mixed form) toward
-// `want`, while a set fits beside a reserve of free device memory (2 GiB or 5% of the
-// device, the larger).  Returns the number of usable sets.
+// Fit the context's pool of element-matrix sets (FP64, and FP32 for the mixed form) to `want`
+// usable sets, while a set fits beside a reserve of free device memory (2 GiB or 5% of the
+// device, the larger).  A set is usable when it has the parts the form needs.  Parts a run
+// does not use are freed first (sets beyond `want`, FP32 parts in FP64 runs), and in a mixed
+// run trailing sets are freed to complete earlier ones.  Returns the number of usable sets.
 static int grow_matrix_pool(cfdv_ctx* c, int want, bool mixed) {
   const size_t mat = (size_t)c->n_elements * c->Ke * c->Ke;
+  auto drop_last = [&]() {
+    dfree(c->adj_pool64.back());
+    c->adj_pool64.pop_back();
+    if (c->adj_pool32.size() > c->adj_pool64.size()) {
+      dfree(c->adj_pool32.back());
+      c->adj_pool32.pop_back();
+    }
+  };
+  while ((int)c->adj_pool64.size() > want) drop_last();
+  if (!mixed)
+    for (auto& p : c->adj_pool32) dfree(p);
+  if (!mixed) c->adj_pool32.clear();
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
   const size_t reserve = std::max((size_t)2 << 30, total_b / 20);
@@ -537,6 +549,10 @@ static int grow_matrix_pool(cfdv_ctx* c, int want, bool mixed) {
     const bool have32 = !mixed || (i < (int)c->adj_pool32.size() && c->adj_pool32[i]);
     const size_t need = (have64 ? 0 : sizeof(double) * mat) + (have32 ? 0 : sizeof(float) * mat);
     if (need) {
+      while (free_b < need + reserve && (int)c->adj_pool64.size() > i + 1) {  // complete set i first
+        drop_last();
+        cudaMemGetInfo(&free_b, &total_b);
+      }
       if (free_b < need + reserve) break;
       if (!have64) {
         double* p = nullptr;
@@ -546,11 +562,8 @@ static int grow_matrix_pool(cfdv_ctx* c, int want, bool mixed) {
       if (!have32) {
         float* p = nullptr;
         if (cudaMalloc(&p, sizeof(float) * mat) != cudaSuccess) break;
-        if (i < (int)c->adj_pool32.size()) c->adj_pool32[i] = p;
-        else {
-          c->adj_pool32.resize(i + 1, nullptr);
-          c->adj_pool32[i] = p;
-        }
+        if (i >= (int)c->adj_pool32.size()) c->adj_pool32.resize(i + 1, nullptr);
+        c->adj_pool32[i] = p;
       }
       free_b -= need;
     }
@@ -587,12 +600,18 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
   double* mu_prev = c->d_adj_v + 4 * n;  // the last reverse step's mu: the next solve's start
   bool have_mu = false;
   const cfdv_gmres_opts so = solve_opts(o);
-  // The last P recomputed steps of a segment form into kept sets of the pool; their reverse
-  // steps solve with those matrices instead of forming again.  The context's own buffers
-  // are restored on every exit.
+  // Kept sets of the pool: the last P_rec recomputed steps of a segment form into sets
+  // 0 .. P_rec-1 (reused by every segment); the forward run's last step of segment s < P_end
+  // forms into set P_rec + s (the recomputation does not reach that step).  Their reverse
+  // steps solve with those matrices instead of forming again.  Recompute sets come first when
+  // memory is short.  The context's own buffers are restored on every exit.
   const bool mixed = o->precision == CFDV_PREC_MIXED;
   if (mixed && !c->d_R32 && (rc = dalloc(c, &c->d_R32, (size_t)c->n_elements * c->Ke * c->Ke))) return rc;
-  const int P = grow_matrix_pool(c, std::min(k, N) - 1, mixed);
+  int want = std::min(k, N) - 1 + nseg;
+  if (o->max_kept_sets < 0) want = 0;
+  else if (o->max_kept_sets > 0) want = std::min(want, o->max_kept_sets);
+  const int P = grow_matrix_pool(c, want, mixed);
+  const int P_rec = std::min(P, std::min(k, N) - 1), P_end = P - P_rec;
   struct OwnMatrices {
     cfdv_ctx* c;
     double* r64;
@@ -625,7 +644,12 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
     if (step % k == 0)
       CK(cudaMemcpyAsync(ckpt + (size_t)(step / k) * n, c->d_U, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
     rep.n_matvec = 0;
-    if ((rc = cfdv_step(c, o->cfl, &so, &rep, nullptr))) return rc;
+    const int seg = step / k;
+    const bool keep_end = seg < P_end && step == std::min((seg + 1) * k, N) - 1;  // segment's last step
+    if (keep_end) own.use(P_rec + seg, mixed);
+    rc = cfdv_step(c, o->cfl, &so, &rep, nullptr);
+    own.restore();
+    if (rc) return rc;
     fwd_mv += rep.n_matvec;
     double F;
     if ((rc = wall_force_device(c, o->wall_bc, &F, nullptr, nullptr))) return rc;
@@ -648,7 +672,7 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
     // recompute U_{n0} .. U_{n1-1} from the checkpoint; U_{n1} is the next checkpoint or U_N
     CK(cudaMemcpyAsync(c->d_U, ckpt + (size_t)s * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
     CK(cudaMemcpyAsync(seg, c->d_U, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->st));
-    const int first_kept = n1 - 1 - P;  // recomputed steps from here on keep their matrices
+    const int first_kept = n1 - 1 - P_rec;  // recomputed steps from here on keep their matrices
     for (int step = n0; step < n1 - 1; step++) {
       rep.n_matvec = 0;
       if (step >= first_kept) own.use(step - first_kept, mixed);
@@ -668,8 +692,10 @@ int cfdv_adjoint(cfdv_ctx* c, const cfdv_adjoint_opts* o, cfdv_adjoint_result* r
       c->launches++;
       double dt;
       if ((rc = cfdv_cfl(c, o->cfl, &dt))) return rc;
-      if (step < n1 - 1 && step >= first_kept) {  // the recompute formed this step's matrices
-        own.use(step - first_kept, mixed);
+      const bool kept_rec = step < n1 - 1 && step >= first_kept;  // formed by the recompute
+      const bool kept_end = step == n1 - 1 && s < P_end;          // formed by the forward run
+      if (kept_rec || kept_end) {
+        own.use(kept_rec ? step - first_kept : P_rec + s, mixed);
         c->formed = true;
         c->have32 = mixed;
         c->dt_formed = dt;

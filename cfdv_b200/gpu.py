@@ -70,7 +70,8 @@ class _Stats(C.Structure):
 
 class _AdjOpts(C.Structure):
     _fields_ = [("n_steps", C.c_int), ("checkpoint_every", C.c_int), ("cfl", C.c_double), ("m", C.c_int),
-                ("restarts", C.c_int), ("rtol", C.c_double), ("precision", C.c_int), ("wall_bc", C.c_int)]
+                ("restarts", C.c_int), ("rtol", C.c_double), ("precision", C.c_int), ("wall_bc", C.c_int),
+                ("max_kept_sets", C.c_int)]
 
 
 class _AdjResult(C.Structure):
@@ -424,14 +425,15 @@ class FDVSolver:
         return ids[: n.value].copy()
 
     @staticmethod
-    def _adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc):
+    def _adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc, max_kept_sets=0):
         return _AdjOpts(int(n_steps), int(checkpoint_every), float(cfl), int(m), int(restarts), float(rtol),
-                        int(precision), int(wall_bc))
+                        int(precision), int(wall_bc), int(max_kept_sets))
 
     def adjoint(self, n_steps, cfl, checkpoint_every=50, m=30, restarts=200, rtol=1e-10, precision=PREC_FP64,
-                wall_bc=1):
-        """Gradient of J = mean_{n=1..N} F_x(U_n) w.r.t. Mach, wall temperature and each wall-node T0."""
-        o = self._adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc)
+                wall_bc=1, max_kept_sets=0):
+        """Gradient of J = mean_{n=1..N} F_x(U_n) w.r.t. Mach, wall temperature and each wall-node T0.
+        max_kept_sets: element-matrix sets kept for the reverse steps (0: as many as fit, -1: none)."""
+        o = self._adj_opts(n_steps, checkpoint_every, cfl, m, restarts, rtol, precision, wall_bc, max_kept_sets)
         nw = len(self.wall_nodes(wall_bc))
         ids = np.zeros(max(nw, 1), dtype=np.int32)
         gT = np.zeros(max(nw, 1))

@@ -234,14 +234,19 @@ typedef struct {
   int n_steps;          /* N steps from the records of cfdv_load_node_records */
   int checkpoint_every; /* k: the forward run keeps U every k steps; the backward sweep
                            recomputes each segment's states from its checkpoint.  The
-                           element matrices of the recomputed steps stay on the device for
-                           their reverse steps, as many sets as fit beside a reserve of
-                           free memory; the other reverse steps form theirs again */
+                           element matrices of the recomputed steps, and of each segment's
+                           last step from the forward run, stay on the device for their
+                           reverse steps, as many sets as fit beside a reserve of free
+                           memory (recomputed steps first); the other reverse steps form
+                           theirs again */
   double cfl;
   int m, restarts;      /* GMRES(m), at most `restarts` cycles, CORRECT mode, node-block */
   double rtol;          /* Jacobi; forward, tangent and adjoint solves to this rtol */
   int precision;        /* cfdv_precision of every solve (MIXED: FP32 inner products) */
   int wall_bc;          /* boundary code of the wall faces */
+  int max_kept_sets;    /* element-matrix sets kept on the device for the reverse steps (see
+                           checkpoint_every): 0 = as many as fit, n > 0 = at most n, -1 = none
+                           (every reverse step forms its matrices again) */
 } cfdv_adjoint_opts;
 
 typedef struct {
@@ -256,7 +261,7 @@ typedef struct {
   double backward_ms;   /* device time of the backward sweep, recomputation included */
   int forward_matvecs;  /* EBE products of all forward solves (recomputation included) */
   int adjoint_matvecs;  /* EBE products of the transposed solves */
-  int kept_matrix_sets; /* element-matrix sets of recomputed steps kept per segment */
+  int kept_matrix_sets; /* element-matrix sets kept: recomputed steps', then segment ends' */
   int reverse_forms;    /* formations run by reverse steps (the others reused kept sets) */
 } cfdv_adjoint_result;
 

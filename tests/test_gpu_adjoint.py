@@ -226,12 +226,12 @@ def test_checkpoint_spacing_and_mixed_precision(gpu, adj):
         rN = s.adjoint(N_STEPS, CFL, checkpoint_every=N_STEPS, m=M_GMRES, rtol=RTOL)
         s.load_node_records()
         rm = s.adjoint(N_STEPS, CFL, checkpoint_every=3, m=M_GMRES, rtol=1e-10, precision=gpu.PREC_MIXED)
-    # the recomputed steps' element matrices stay on the device for their reverse steps: only
-    # the last step of each segment forms again (k = 1 recomputes nothing)
-    assert (adj["kept_matrix_sets"], adj["reverse_forms"]) == (1, 3)
-    assert (r1["kept_matrix_sets"], r1["reverse_forms"]) == (0, N_STEPS)
-    assert (rN["kept_matrix_sets"], rN["reverse_forms"]) == (N_STEPS - 1, 1)
-    assert (rm["kept_matrix_sets"], rm["reverse_forms"]) == (2, 2)
+    # the recomputed steps' element matrices and each segment's last step's (from the forward
+    # run) stay on the device for their reverse steps: none forms again when they all fit
+    assert (adj["kept_matrix_sets"], adj["reverse_forms"]) == (1 + 3, 0)
+    assert (r1["kept_matrix_sets"], r1["reverse_forms"]) == (N_STEPS, 0)
+    assert (rN["kept_matrix_sets"], rN["reverse_forms"]) == (N_STEPS - 1 + 1, 0)
+    assert (rm["kept_matrix_sets"], rm["reverse_forms"]) == (2 + 2, 0)
     for r in (r1, rN):
         assert r["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-13)
         assert np.abs(r["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-13 * np.abs(adj["dJ_dtnode"]).max()
@@ -241,6 +241,23 @@ def test_checkpoint_spacing_and_mixed_precision(gpu, adj):
     assert rm["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-6)
     assert rm["dJ_dtwall"] == pytest.approx(adj["dJ_dtwall"], rel=1e-6)
     assert np.abs(rm["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-4 * np.abs(adj["dJ_dtnode"]).max()
+
+
+def test_kept_matrix_sets_change_nothing(gpu, adj):
+    """The same gradient whether the reverse steps form their matrices again (no kept sets), keep
+    the recomputed steps' only (one set at k = 2) or keep all (to 1e-13: a kept set was formed
+    inside a step, with dt^2/2 from the device's dt, a re-formed one with the host's)."""
+    case = get_case(ADJ_CASE)
+    with _solver(gpu, case) as s:
+        r0 = s.adjoint(N_STEPS, CFL, checkpoint_every=2, m=M_GMRES, rtol=RTOL, max_kept_sets=-1)
+        s.load_node_records()
+        r1 = s.adjoint(N_STEPS, CFL, checkpoint_every=2, m=M_GMRES, rtol=RTOL, max_kept_sets=1)
+    assert (r0["kept_matrix_sets"], r0["reverse_forms"]) == (0, N_STEPS)
+    assert (r1["kept_matrix_sets"], r1["reverse_forms"]) == (1, 3)
+    for r in (r0, r1):
+        assert r["dJ_dmach"] == pytest.approx(adj["dJ_dmach"], rel=1e-13)
+        assert r["dJ_dtwall"] == pytest.approx(adj["dJ_dtwall"], rel=1e-13)
+        assert np.abs(r["dJ_dtnode"] - adj["dJ_dtnode"]).max() <= 1e-13 * np.abs(adj["dJ_dtnode"]).max()
 
 
 def test_vjp_full_size_cylinder_sampled(gpu, emu, oracle_lib):
